@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark: path samples/s of one raymotion frame on the B200 backend.
+
+Workload (one "step" = one frame): the instanced icosphere field of
+raymotion_b200.scenes.icosphere_field - 200 displaced icospheres + ground +
+4096 small emitters = 1,028,098 triangles - rendered at 1280x720, 64 spp,
+max depth 12, ReSTIR DI on (32 RIS candidates, 5 spatial neighbours within
+30 px, temporal reuse from the previous frame) and the denoiser on; seeded
+synthetic data (no dataset exists for this path).  The scene (181 MB of
+triangles + 49 MB of traversal records) is larger than the 126 MB L2.
+
+Reported on one JSON line (rank 0):
+  value   - path samples/s with the scene resident in HBM, timed with CUDA
+            events on the rendering stream over exactly --steps frames
+            (max over ranks; each rank renders its own frames: replicas);
+  e2e     - the same metric through the reference-facing call
+            rmcuda_render with host buffers: scene upload from pinned host
+            memory, device BVH build, frame, RGB8 read-back, every step;
+  roofline- the dominant kernel (by summed CUDA-event time): algorithmic bytes
+            it fetches (BVH records 64 B x nodes visited + triangle records
+            48 B x tests, counted on the device) / its average launch time,
+            against the measured HBM copy bandwidth;
+  cpu_baseline - the CPU oracle (a restatement of the reference's Metal
+            kernels; the reference itself runs only on Apple GPUs) timed on a
+            band of rows of the same frame with every host core.
+--impl reference times that CPU implementation alone.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "path samples/s"
+UNIT = "path samples/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="icosphere720", choices=["icosphere720", "cornell"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def workload(name: str):
+    from raymotion_b200.scenes import cornell_box, icosphere_field
+    if name == "cornell":
+        sb, cam, cfg = cornell_box(0)
+        desc = dict(workload="cornell box, 36 triangles, 320x180, 16 spp, depth 8, plain NEE+MIS", triangles=36)
+    else:
+        sb, cam, cfg = icosphere_field(seed=1)
+        desc = dict(workload="icosphere field, 1,028,098 triangles, 1280x720, 64 spp, depth 12, ReSTIR DI "
+                             "(32 candidates, 5 spatial neighbours, radius 30 px, temporal) + denoiser")
+    scene = sb.pack()
+    desc.update(triangles=int(scene.n_tris), width=cfg.width, height=cfg.height, spp=cfg.spp,
+                max_depth=cfg.max_bounces, l2="inputs larger than L2 (scene 181 MB + 49 MB BVH leaf records)",
+                bvh="device LBVH (4-triangle leaves)")
+    return scene, cam, cfg, desc
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.rows: list[list[str]] = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[0]) for r in self.rows if len(r) >= 7 and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 7 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 7 for k in range(4) if r[3 + k] == "Active"})
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                    reasons=reasons, samples=len(sm))
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return dict(hbm_gbs=float(d["hbm_gbs"]), source="measured")
+        except Exception:
+            pass
+    return dict(hbm_gbs=6650.0, source="fallback")
+
+
+def ncu_traffic(kernel: str) -> float | None:
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, scaled to this workload."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return float(d[kernel]["dram_bytes_per_launch_full"])
+    except Exception:
+        return None
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def allreduce(values: list[float], op: str, world: int, device=None) -> list[float]:
+    if world <= 1:
+        return values
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return t.tolist()
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- CPU (oracle)
+
+def cpu_band(scene, cam, cfg, seconds: float, rows_hint: int | None = None):
+    """Time the CPU oracle on a band of rows of the same frame; returns (samples/s, desc, threads)."""
+    from oracle import pyoracle
+    if scene.nodes is None:
+        pyoracle.with_reference_bvh(scene)
+    o = pyoracle.Oracle()
+    threads = pyoracle.nthreads()
+    y0 = cfg.height // 2
+    rows = rows_hint or 1
+    # calibrate on one row, then size the band to the time budget
+    if rows_hint is None:
+        t0 = time.perf_counter()
+        o.render(scene, cam, cfg, 777, threads=threads, rows=(y0, y0 + 1))
+        dt = max(time.perf_counter() - t0, 1e-3)
+        rows = int(max(1, min(cfg.height - y0, seconds / dt)))
+        rows = max(rows, min(threads, cfg.height - y0))
+    t0 = time.perf_counter()
+    _, _, st = o.render(scene, cam, cfg, 778, threads=threads, rows=(y0, y0 + rows))
+    dt = time.perf_counter() - t0
+    return st["path_samples"] / dt, f"rows {y0}..{y0 + rows - 1} of the frame ({rows * cfg.width} pixels, " \
+                                     f"{st['path_samples']} path samples, {dt:.1f} s)", threads, rows, dt
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    scene, cam, cfg, desc = workload(args.workload)
+    per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    _, _, threads, rows, _ = cpu_band(scene, cam, cfg, per_step)
+    for _ in range(args.warmup):
+        cpu_band(scene, cam, cfg, per_step, rows_hint=rows)
+    vals, tsum = [], 0.0
+    sample_desc = ""
+    for _ in range(args.steps):
+        v, sample_desc, threads, rows, dt = cpu_band(scene, cam, cfg, per_step, rows_hint=rows)
+        vals.append(v)
+        tsum += dt
+    value = float(np.mean(vals))
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                ms_per_step=1e3 * tsum / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f32", data="synthetic (seeded procedural scene)", impl="reference",
+                config=dict(desc, parallelism="cpu threads"),
+                cpu_baseline=dict(value=value, unit=UNIT, cores=threads, kind="port",
+                                  sample=f"per step: {sample_desc}"),
+                e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU
+
+def run_b200(args, world, rank, local):
+    import torch
+
+    import raymotion_b200 as rb
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    scene, cam, cfg, desc = workload(args.workload)
+    backend = rb.Backend(local)
+    stream = torch.cuda.current_stream(dev)
+    backend.set_stream(stream.cuda_stream)
+    npix = cfg.width * cfg.height
+    seed0 = 12345 + 1000 * rank
+    # ---- device-resident frames (value)
+    backend.upload(scene, use_nodes=False)
+    d_rgb = torch.empty(npix * 3, dtype=torch.uint8, device=dev)
+    for i in range(args.warmup):
+        backend.render_resident_async(cam, cfg, seed0 + i, d_rgb.data_ptr())
+    backend.sync()
+    backend.stats_reset()
+    backend.profile(True)
+    torch.cuda.synchronize()
+    barrier(world)
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        uuid = None
+    clocks = Clocks(uuid)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for k in range(args.steps):
+        backend.render_resident_async(cam, cfg, seed0 + args.warmup + k, d_rgb.data_ptr())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    backend.sync()
+    secs = ev0.elapsed_time(ev1) / 1e3
+    st = backend.stats()
+    stage_t = backend.stage_times()
+    stage_c = backend.stage_counters()
+    secs_max, = allreduce([secs], "max", world, dev)
+    samples_sum, rays_sum = allreduce([float(st["path_samples"]), float(st["rays"])], "sum", world, dev)
+    value = samples_sum / secs_max
+    backend.profile(False)
+    # ---- roofline of the dominant kernel
+    dom = max(stage_t, key=lambda k: stage_t[k][0])
+    ms_total, launches = stage_t[dom]
+    c = stage_c[dom]
+    alg_bytes = (c["nodes_visited"] * 64 + c["tris_tested"] * 48) / max(launches, 1)
+    avg_s = ms_total / 1e3 / max(launches, 1)
+    peak = measured_peaks()
+    achieved = alg_bytes / avg_s / 1e9 if avg_s > 0 else 0.0
+    kernel_names = dict(plain="k_render_paths", shade="k_restir_shade", generate="k_restir_generate",
+                        spatial="k_restir_spatial", temporal="k_denoise_temporal", atrous0="k_denoise_atrous",
+                        atrous1="k_denoise_atrous", hash="k_hash", tonemap="k_tonemap")
+    roofline = dict(bound="hbm", kernel=kernel_names.get(dom, dom), achieved=achieved, peak=peak["hbm_gbs"],
+                    unit="GB/s", frac=achieved / peak["hbm_gbs"], traffic=ncu_traffic(kernel_names.get(dom, dom)),
+                    peak_source=peak["source"],
+                    note="achieved = (64 B x BVH records fetched + 48 B x triangle tests) per launch / average "
+                         "launch time; most of these bytes hit L1/L2")
+    stage_summary = {k: dict(ms_per_launch=(v[0] / v[1]) if v[1] else 0.0, launches=v[1]) for k, v in stage_t.items()
+                     if v[1]}
+    # ---- end to end through rmcuda_render with host buffers
+    e2e = None
+    if not args.no_e2e:
+        pinned = {}
+        for key in ("tris", "light_tri", "light_cdf", "texels"):
+            a = getattr(scene, key)
+            t = torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).reshape(-1)).pin_memory()
+            pinned[key] = t.numpy().view(a.dtype).reshape(a.shape)
+        hscene = rb.PackedScene(tris=pinned["tris"], light_tri=pinned["light_tri"], light_cdf=pinned["light_cdf"],
+                                light_total=scene.light_total, texels=pinned["texels"], verts64=scene.verts64)
+        out_t = torch.empty(npix * 3, dtype=torch.uint8).pin_memory()
+        out = out_t.numpy()
+        backend.render(hscene, cam, cfg, seed0 + 500, use_nodes=False, out=out)  # warm-up
+        backend.stats_reset()
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(args.steps):
+            backend.render(hscene, cam, cfg, seed0 + 501 + k, use_nodes=False, out=out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        esec, = allreduce([e0.elapsed_time(e1) / 1e3], "max", world, dev)
+        es, = allreduce([float(backend.stats()["path_samples"])], "sum", world, dev)
+        h2d = sum(pinned[k].nbytes for k in pinned)
+        e2e = dict(value=es / esec, unit=UNIT, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(npix * 3),
+                   ms_per_step=1e3 * esec / args.steps)
+    # ---- CPU baseline (rank 0, N=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, sample, threads, _, _ = cpu_band(scene, cam, cfg, args.cpu_seconds)
+        cpu = dict(value=v, unit=UNIT, cores=threads, kind="port", sample=sample)
+    if rank == 0:
+        line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=1e3 * secs_max / args.steps, higher_is_better=True, scaling="weak",
+                    vs_baseline=None, dtype="f32", data="synthetic (seeded procedural scene)",
+                    config=dict(desc, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+                    mrays_per_s=rays_sum / secs_max / 1e6, e2e=e2e, roofline=roofline, cpu_baseline=cpu,
+                    gpu_launches=int(st["kernel_launches"]), clocks=clk, stages=stage_summary)
+        print(json.dumps(line), flush=True)
+    backend.close()
+    return 0
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

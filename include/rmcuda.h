@@ -1,0 +1,225 @@
+/*
+ * rmcuda.h - C ABI of the B200 (sm_100a) path-tracing backend for raymotion.
+ *
+ * This library replaces the reference's Metal backend, whose only entry point
+ * is
+ *     bool raymotion::render_image_metal(const Scene&, const Camera&,
+ *                                        const RenderConfig&, uint64_t seed,
+ *                                        std::vector<uint8_t>& rgb,
+ *                                        std::string& error);
+ * (reference include/raymotion/metal.hpp:6-7, implemented in
+ * src/engine/metal.mm:95-414).  The ABI below carries the same information
+ * with plain pointers and sizes: the packed fp32 scene that metal.mm builds
+ * (metal.mm:109-145, layout of src/engine/metal_types.h:5-30), the camera, the
+ * render settings, the seed, and an RGB8 output buffer.  Every function returns
+ * RM_OK (0) or a nonzero status and writes a human-readable message into the
+ * caller's `err` buffer; nothing throws across the boundary.
+ *
+ * Threading: a context serialises its calls with a mutex, like the reference's
+ * process-wide Context (metal.mm:102-104).  Calls are synchronous unless named
+ * *_async.
+ */
+#ifndef RMCUDA_H
+#define RMCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RM_OK 0
+#define RM_ERR_INVALID 1      /* bad dimensions, sizes or pointers */
+#define RM_ERR_UNAVAILABLE 2  /* no CUDA device, or the device is not sm_100 */
+#define RM_ERR_CUDA 3         /* a CUDA call failed; the frame was not completed */
+#define RM_ERR_ALLOC 4        /* device or pinned allocation failed */
+#define RM_ERR_BVH 5          /* the caller's BVH failed validation */
+#define RM_ERR_DEVICE 6       /* a kernel reported an error word (bounded loop ran out) */
+
+typedef struct rm_vec3 { float x, y, z; } rm_vec3;
+
+/* One packed triangle, 176 bytes, field for field the reference's Metal ABI
+ * metal_data::Triangle (src/engine/metal_types.h:5-11): scene-space vertices,
+ * unnormalised geometric normal n = (v1-v0)x(v2-v0), its normalisation nn,
+ * vertex normals, material and texture coordinates.  texture_offset is an index
+ * into rm_scene_view.texels or -1. */
+typedef struct rm_triangle {
+  rm_vec3 v0, v1, v2, n, nn, n0, n1, n2;
+  float ar, ag, ab, er, eg, eb, ior, rough, metallic, alpha;
+  int32_t shader;
+  float tu0, tv0, tu1, tv1, tu2, tv2;
+  int32_t texture_offset, texture_width, texture_height;
+} rm_triangle;
+
+/* A caller-built binary BVH node: Scene::nodes of the reference
+ * (include/raymotion/scene.hpp:57-64, built by src/engine/bvh.cpp:29-248)
+ * rounded to fp32.  Internal nodes have count == 0 and children left/right;
+ * leaves cover bvh_tri[offset, offset+count). */
+typedef struct rm_bvh_node {
+  rm_vec3 mn, mx;
+  int32_t left, right, offset, count;
+} rm_bvh_node;
+
+/* Pinhole camera, the reference's metal_data::Camera (metal_types.h:12-15):
+ * position, focal length in pixels, row-major rotation m0..m8. */
+typedef struct rm_camera {
+  float x, y, z, focal;
+  float m0, m1, m2, m3, m4, m5, m6, m7, m8;
+} rm_camera;
+
+/* The scene of one frame, as metal.mm uploads it (metal.mm:109-186).
+ * nodes == NULL asks the library to build the BVH on the device; nodes != NULL
+ * with n_nodes == 0 is an empty BVH on which every ray misses (the reference's
+ * params.nodes == 0, pathtrace.metal:121); otherwise nodes/bvh_tri are
+ * validated and converted (a caller BVH deeper than 64 levels is rebuilt on
+ * the device instead). */
+typedef struct rm_scene_view {
+  const rm_triangle* tris;
+  int32_t n_tris;
+  int32_t n_nodes;
+  const rm_bvh_node* nodes;
+  const int32_t* bvh_tri;   /* n_tris entries when nodes != NULL */
+  const int32_t* light_tri; /* emissive triangle indices (Scene::light_tri) */
+  const float* light_cdf;   /* running area*luminance sums (Scene::light_cdf) */
+  int32_t n_lights;
+  float light_total;        /* Scene::light_total */
+  const rm_vec3* texels;    /* concatenated linear-RGB textures, top row first */
+  int64_t n_texels;
+} rm_scene_view;
+
+/* Render settings: raymotion::RenderConfig (include/raymotion/pathtrace.hpp:54-81)
+ * in fp32, plus `flags`. */
+typedef struct rm_config {
+  int32_t width, height, spp, max_bounces;
+  float resolution, clamp, adapt_rel, adapt_abs;
+  int32_t adapt_min, adapt_step;
+  int32_t restir_candidates, restir_spatial;
+  float restir_radius;
+  int32_t restir_mcap;
+  uint32_t flags;
+} rm_config;
+
+/* flags.  By default the library reads the reference's environment switches
+ * exactly as metal.mm does: UOW2_NOADAPT (:154), UOW2_NOMIS (:157),
+ * RAYMOTION_RESTIR=0 (:159), RAYMOTION_RESTIR_CANDIDATES / _SPATIAL (:169-170),
+ * RAYMOTION_RESTIR_TEMPORAL=0 (:251-252) and RAYMOTION_DENOISE=0 (:269-271).
+ * RM_FLAG_NO_ENV ignores the environment and takes those switches from the
+ * flag bits instead. */
+#define RM_FLAG_NO_ENV 0x1u
+#define RM_FLAG_NOADAPT 0x2u
+#define RM_FLAG_NOMIS 0x4u
+#define RM_FLAG_RESTIR_OFF 0x8u
+#define RM_FLAG_DENOISE_OFF 0x10u
+#define RM_FLAG_TEMPORAL_OFF 0x20u
+/* Not in the reference (which always applies Russian roulette,
+ * pathtrace.metal:715-724, :1246-1250): turn RR off. */
+#define RM_FLAG_NO_RR 0x40u
+/* Not in the reference: keep temporal ReSTIR / denoise history across frames
+ * whose triangles changed (the reference requires an identical scene hash,
+ * metal.mm:241-253); geometric rejection still applies per pixel. */
+#define RM_FLAG_ANIMATED_HISTORY 0x100u
+
+/* Per-context counters, reset by rmcuda_stats_reset. */
+typedef struct rm_stats {
+  uint64_t path_samples;    /* (pixel, sample) radiance estimates taken */
+  uint64_t rays;            /* traversal queries (closest + any-hit) */
+  uint64_t nodes_visited;   /* BVH child-pair records fetched (64 B each) */
+  uint64_t tris_tested;     /* Moller-Trumbore tests (48 B records) */
+  uint64_t frames;
+  uint64_t kernel_launches; /* this library's kernels launched by frame calls */
+  uint32_t device_error;    /* last nonzero device error word, 0 if none */
+  uint32_t kernel_chain;    /* 1 = render_paths, 8/32 = lane kernels, 2 = ReSTIR chain */
+} rm_stats;
+
+typedef struct rmcuda_ctx rmcuda_ctx;
+
+/* Library version string. */
+const char* rmcuda_version(void);
+
+/* Create a context on CUDA device `device`.  Returns RM_ERR_UNAVAILABLE with
+ * the reference's skip message "Metal backend is not available in this build"
+ * when no usable device exists (reference tests/test_metal.cpp:25 treats that
+ * string as "skip"). */
+int rmcuda_create(rmcuda_ctx** out, int device, char* err, size_t errcap);
+void rmcuda_destroy(rmcuda_ctx* ctx);
+
+/* Use the caller's CUDA stream (a cudaStream_t) for all work of this context;
+ * NULL restores the context's own stream. */
+int rmcuda_set_stream(rmcuda_ctx* ctx, void* cuda_stream, char* err, size_t errcap);
+
+/* One frame, the whole of render_image_metal (metal.mm:95-414): validate, upload
+ * the scene, build or convert the BVH, choose the kernel chain (plain or lane
+ * path tracer, or ReSTIR generate/spatial/shade + denoise), run it, read back
+ * W*H*3 bytes of RGB8 (row-major, top row first) into `rgb` (capacity rgb_cap),
+ * keep temporal history.  `hdr`, when not NULL, receives W*H*3 floats of the
+ * linear radiance that the tonemap consumed.  Synchronous. */
+int rmcuda_render(rmcuda_ctx* ctx, const rm_scene_view* scene, const rm_camera* cam,
+                  const rm_config* cfg, uint64_t seed, uint8_t* rgb, size_t rgb_cap,
+                  float* hdr, char* err, size_t errcap);
+
+/* Upload a scene and make it the context's resident scene (device BVH built or
+ * converted).  Later *_resident calls render it without another upload. */
+int rmcuda_scene_upload(rmcuda_ctx* ctx, const rm_scene_view* scene, char* err, size_t errcap);
+
+/* Replace the resident scene's vertices (same triangle count and topology) and
+ * refit its BVH on the device; `tris` holds n_tris packed triangles.  After
+ * `rebuild_every` refits (0 = never) the BVH is rebuilt instead. */
+int rmcuda_scene_update(rmcuda_ctx* ctx, const rm_triangle* tris, int32_t n_tris,
+                        int32_t rebuild_every, char* err, size_t errcap);
+
+/* Render the resident scene.  d_rgb / d_hdr are DEVICE pointers (either may be
+ * NULL); the work is enqueued on the context stream and not waited for. */
+int rmcuda_render_resident_async(rmcuda_ctx* ctx, const rm_camera* cam, const rm_config* cfg,
+                                 uint64_t seed, uint8_t* d_rgb, float* d_hdr,
+                                 char* err, size_t errcap);
+
+/* Wait for the context stream and check the device error word. */
+int rmcuda_sync(rmcuda_ctx* ctx, char* err, size_t errcap);
+
+/* Trace rays against the resident scene.  rays: n records of 7 floats
+ * (ox, oy, oz, dx, dy, dz, tmax), device pointer.  any_hit = 0: closest hit,
+ * writing tri (original triangle index, -1 for a miss), t, u, v; any_hit = 1:
+ * occlusion only (tri = index of some hit or -1).  Outputs are device
+ * pointers; t/u/v may be NULL.  Synchronous. */
+int rmcuda_trace(rmcuda_ctx* ctx, const float* d_rays, int32_t n, int32_t any_hit,
+                 int32_t* d_tri, float* d_t, float* d_u, float* d_v,
+                 char* err, size_t errcap);
+
+/* Read the last frame's ReSTIR buffers back in the reference record layouts
+ * (metal_types.h:32-56): which = 0 G-buffer (76 B/px), 1 initial reservoir,
+ * 2 merged reservoir (60 B/px), 3 shaded HDR (12 B/px).  Host pointer. */
+int rmcuda_debug_read(rmcuda_ctx* ctx, int32_t which, void* host, size_t cap,
+                      char* err, size_t errcap);
+
+/* Drop temporal history (the reference's CacheGuard, metal.mm:105-108). */
+int rmcuda_reset_history(rmcuda_ctx* ctx);
+
+int rmcuda_stats_get(rmcuda_ctx* ctx, rm_stats* out);
+int rmcuda_stats_reset(rmcuda_ctx* ctx);
+
+/* Per-stage timing with CUDA events recorded on the context stream around
+ * every kernel launch of a frame (off by default).  rmcuda_stage_times
+ * returns, per RM_STAGE_*, the summed milliseconds and the launch count since
+ * the last rmcuda_stats_reset. */
+#define RM_STAGE_PLAIN 0     /* render_paths / lane kernels */
+#define RM_STAGE_HASH 1      /* scene hash guarding temporal reuse */
+#define RM_STAGE_GENERATE 2  /* ReSTIR primary hit + initial reservoir */
+#define RM_STAGE_SPATIAL 3   /* ReSTIR temporal + spatial reuse */
+#define RM_STAGE_SHADE 4     /* ReSTIR shading, spp indirect paths */
+#define RM_STAGE_TEMPORAL 5  /* denoiser temporal pass */
+#define RM_STAGE_ATROUS0 6   /* a-trous stride 1 */
+#define RM_STAGE_ATROUS1 7   /* a-trous stride 2 + tonemap */
+#define RM_STAGE_TONEMAP 8   /* tonemap alone (denoiser off) */
+#define RM_STAGE_COUNT 9
+int rmcuda_profile(rmcuda_ctx* ctx, int enable);
+/* Per-stage device counters since the last reset: n records of
+ * {path samples, rays, BVH nodes visited, triangle tests}. */
+int rmcuda_stage_counters(rmcuda_ctx* ctx, uint64_t* out, int32_t n);
+int rmcuda_stage_times(rmcuda_ctx* ctx, double* ms, uint64_t* launches, int32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RMCUDA_H */

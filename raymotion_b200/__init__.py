@@ -1,0 +1,174 @@
+"""raymotion_b200 - B200 (sm_100a) backend for raymotion's path-tracing hot path.
+
+The native library ``librmcuda.so`` (CUDA kernels + the C ABI of
+include/rmcuda.h) does the work; this module is a thin host-side mirror of the
+reference's backend entry point
+
+    bool render_image_metal(const Scene&, const Camera&, const RenderConfig&,
+                            uint64_t seed, std::vector<uint8_t>& rgb, std::string& error)
+
+(reference include/raymotion/metal.hpp:6-7): ``render_image_metal`` returns
+``(ok, rgb, error)`` with the same error strings, and ``Backend`` exposes the
+context, the device-resident scene and the traversal queries used by the
+benchmark and the parity tests.  There is no CPU fallback: without the
+library or a sm_100 GPU every call fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import GBUF_DTYPE, RESERVOIR_DTYPE, load_library
+from .scene import Camera, PackedScene, RenderConfig, SceneBuilder, Texture
+
+__all__ = ["Backend", "RenderError", "render_image_metal", "Camera", "RenderConfig", "SceneBuilder", "Texture",
+           "PackedScene", "load_library"]
+
+
+class RenderError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+def _err() -> C.Array:
+    return C.create_string_buffer(512)
+
+
+class Backend:
+    """One rmcuda context on a CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        e = _err()
+        rc = self.lib.rmcuda_create(C.byref(h), device, e, 512)
+        if rc != _abi.RM_OK:
+            raise RenderError(rc, e.value.decode())
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.rmcuda_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, e) -> None:
+        if rc != _abi.RM_OK:
+            raise RenderError(rc, e.value.decode())
+
+    # ---- whole frame through the reference-facing call (host buffers)
+    def render(self, scene: PackedScene, cam: Camera, cfg: RenderConfig, seed: int = 12345, hdr: bool = False,
+               use_nodes: bool = True, out: np.ndarray | None = None):
+        """One synchronous frame; ``out`` (uint8, W*H*3) receives the image when given."""
+        npix = cfg.width * cfg.height
+        rgb = out if out is not None else np.empty(max(npix, 0) * 3, np.uint8)
+        out_hdr = np.empty(max(npix, 0) * 3, np.float32) if hdr else None
+        v = scene.view(use_nodes)
+        e = _err()
+        rc = self.lib.rmcuda_render(self.h, C.byref(v), C.byref(cam.packed()), C.byref(cfg.packed()),
+                                    C.c_uint64(seed & 0xFFFFFFFFFFFFFFFF), _abi.ptr(rgb), rgb.nbytes,
+                                    _abi.ptr(out_hdr), e, 512)
+        self._check(rc, e)
+        return (rgb, out_hdr) if hdr else rgb
+
+    # ---- device-resident scene
+    def upload(self, scene: PackedScene, use_nodes: bool = True) -> None:
+        v = scene.view(use_nodes)
+        e = _err()
+        self._check(self.lib.rmcuda_scene_upload(self.h, C.byref(v), e, 512), e)
+
+    def update(self, tris: np.ndarray, rebuild_every: int = 0) -> None:
+        e = _err()
+        self._check(self.lib.rmcuda_scene_update(self.h, _abi.ptr(tris), len(tris), rebuild_every, e, 512), e)
+
+    def render_resident_async(self, cam: Camera, cfg: RenderConfig, seed: int, d_rgb: int | None,
+                              d_hdr: int | None = None) -> None:
+        e = _err()
+        self._check(self.lib.rmcuda_render_resident_async(self.h, C.byref(cam.packed()), C.byref(cfg.packed()),
+                                                          C.c_uint64(seed & 0xFFFFFFFFFFFFFFFF), d_rgb, d_hdr, e,
+                                                          512), e)
+
+    def sync(self) -> None:
+        e = _err()
+        self._check(self.lib.rmcuda_sync(self.h, e, 512), e)
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        e = _err()
+        self._check(self.lib.rmcuda_set_stream(self.h, stream_handle, e, 512), e)
+
+    def trace(self, d_rays: int, n: int, any_hit: bool, d_tri: int, d_t: int | None = None, d_u: int | None = None,
+              d_v: int | None = None) -> None:
+        e = _err()
+        self._check(self.lib.rmcuda_trace(self.h, d_rays, n, int(any_hit), d_tri, d_t, d_u, d_v, e, 512), e)
+
+    def debug_read(self, which: int, npix: int) -> np.ndarray:
+        dt = {0: GBUF_DTYPE, 1: RESERVOIR_DTYPE, 2: RESERVOIR_DTYPE, 3: np.float32, 4: np.uint32}[which]
+        count = npix * (3 if which == 3 else 2 if which == 4 else 1)
+        out = np.empty(count, dt)
+        e = _err()
+        self._check(self.lib.rmcuda_debug_read(self.h, which, _abi.ptr(out), out.nbytes, e, 512), e)
+        return out
+
+    def reset_history(self) -> None:
+        self.lib.rmcuda_reset_history(self.h)
+
+    def stats(self) -> dict:
+        s = _abi.RmStats()
+        rc = self.lib.rmcuda_stats_get(self.h, C.byref(s))
+        if rc != _abi.RM_OK:
+            raise RenderError(rc, "stats read failed")
+        return dict(path_samples=s.path_samples, rays=s.rays, nodes_visited=s.nodes_visited,
+                    tris_tested=s.tris_tested, frames=s.frames, kernel_launches=s.kernel_launches,
+                    device_error=s.device_error, kernel_chain=s.kernel_chain)
+
+    def stats_reset(self) -> None:
+        self.lib.rmcuda_stats_reset(self.h)
+
+    def profile(self, enable: bool = True) -> None:
+        self.lib.rmcuda_profile(self.h, int(enable))
+
+    def stage_times(self) -> dict:
+        n = len(_abi.STAGES)
+        ms = (C.c_double * n)()
+        cnt = (C.c_uint64 * n)()
+        self.lib.rmcuda_stage_times(self.h, ms, cnt, n)
+        return {name: (ms[i], int(cnt[i])) for i, name in enumerate(_abi.STAGES)}
+
+    def stage_counters(self) -> dict:
+        n = len(_abi.STAGES)
+        out = (C.c_uint64 * (4 * n))()
+        rc = self.lib.rmcuda_stage_counters(self.h, out, n)
+        if rc != _abi.RM_OK:
+            raise RenderError(rc, "counter read failed")
+        return {name: dict(path_samples=int(out[4 * i]), rays=int(out[4 * i + 1]), nodes_visited=int(out[4 * i + 2]),
+                           tris_tested=int(out[4 * i + 3])) for i, name in enumerate(_abi.STAGES)}
+
+
+_default: Backend | None = None
+_default_error: RenderError | None = None
+
+
+def render_image_metal(scene: PackedScene, cam: Camera, cfg: RenderConfig, seed: int = 12345):
+    """Python mirror of render_image_metal: returns (ok, rgb, error)."""
+    global _default, _default_error
+    if cfg.width <= 0 or cfg.height <= 0 or cfg.spp <= 0 or cfg.max_bounces < 0 or cfg.width * cfg.height > 100000000:
+        return False, np.zeros(0, np.uint8), "Invalid Metal render dimensions or sample count"
+    if _default is None and _default_error is None:
+        try:
+            _default = Backend(0)
+        except (RenderError, OSError) as ex:
+            _default_error = ex if isinstance(ex, RenderError) else RenderError(_abi.RM_ERR_UNAVAILABLE, str(ex))
+    if _default is None:
+        return False, np.zeros(0, np.uint8), str(_default_error)
+    try:
+        return True, _default.render(scene, cam, cfg, seed), ""
+    except RenderError as ex:
+        return False, np.zeros(0, np.uint8), str(ex)

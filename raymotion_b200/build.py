@@ -1,0 +1,83 @@
+"""Build recipe of the native library, ``raymotion_b200/librmcuda.so``.
+
+Every CUDA translation unit is compiled ahead of time for sm_100a with nvcc
+(no JIT, no torch extension cache): the library is built in the source tree
+so that it travels with it.  ``-fmad=false`` keeps every a*b+c unfused and the
+default ``-prec-div=true -prec-sqrt=true -ftz=false`` keep division, square
+root and denormals IEEE-exact: on identical RNG streams the kernels then
+reproduce the CPU oracle's fp32 radiance bit for bit.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "librmcuda.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ARCH + [
+    "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-fmad=false",
+    "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
+    f"-I{ROOT / 'include'}", f"-I{CSRC}",
+]
+CU_SOURCES = ["rm_kernels.cu", "rm_denoise.cu", "rm_bvh.cu", "rmcuda_api.cu"]
+CXX_SOURCES: list[str] = []
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _run(cmd: list[str]) -> None:
+    proc = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"command failed ({proc.returncode}): {' '.join(cmd)}\n{proc.stdout}")
+
+
+def _stale(obj: Path, deps: list[Path]) -> bool:
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps if d.exists())
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
+    """Compile every source and link ``librmcuda.so``; returns its path."""
+    nvcc = _nvcc()
+    BUILD.mkdir(exist_ok=True)
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((ROOT / "include").rglob("*.h*"))
+    jobs = []
+    objs = []
+    for src in CU_SOURCES + CXX_SOURCES:
+        s = CSRC / src
+        o = BUILD / (src + ".o")
+        objs.append(o)
+        if _stale(o, [s] + headers) or ptxas_info:
+            extra = ["-Xptxas", "-v"] if (ptxas_info and src.endswith(".cu")) else []
+            lang = [] if src.endswith(".cu") else ["-x", "c++"]
+            jobs.append([nvcc, *NVFLAGS, *extra, *lang, "-c", str(s), "-o", str(o)])
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
+        for cmd, fut in [(c, ex.submit(_run, c)) for c in jobs]:
+            fut.result()
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+    if jobs or not LIB.exists():
+        tmp = LIB.with_suffix(".so.tmp")
+        _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"])
+        os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose=True, ptxas_info="--ptxas" in sys.argv))

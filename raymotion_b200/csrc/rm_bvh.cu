@@ -1,0 +1,517 @@
+// rm_bvh.cu - device BVH: caller-BVH conversion, LBVH build, refit, packing.
+//
+// The reference builds a binned-SAH binary BVH on the CPU in fp64
+// (src/engine/bvh.cpp:29-248), refits it in reverse node order (:250-272),
+// and its Metal backend flattens it to preorder escape-link nodes every frame
+// (src/engine/metal.mm:129-144).  Here:
+//  * a caller BVH in the reference layout is validated, converted to the
+//    child-pair layout of rm_device.cuh on the host in O(nodes), and uploaded;
+//  * without a caller BVH the device builds a linear BVH (Karras, "Maximizing
+//    Parallelism in the Construction of BVHs, Octrees, and k-d Trees", HPG
+//    2012): 30-bit Morton codes of the centroids, a radix sort (CUB), one
+//    thread per internal node to find its range and split, bottom-up boxes
+//    with arrival counters; subtrees of at most `leaf_max` triangles collapse
+//    into leaves;
+//  * refit runs bottom-up on the device over the child-pair records with the
+//    same arrival-counter scheme (one pass, no per-level launches).
+// Triangle boxes come from the caller's fp32 vertices, so every box bounds its
+// float triangle exactly.
+#include <cub/device/device_radix_sort.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "rm_launch.h"
+
+namespace rmd {
+
+cudaError_t DevBuf::reserve(size_t bytes) {
+  if (bytes <= cap && ptr) return cudaSuccess;
+  if (ptr) { cudaFree(ptr); ptr = nullptr; cap = 0; }
+  size_t want = std::max<size_t>(bytes, 256);
+  cudaError_t e = cudaMalloc(&ptr, want);
+  if (e != cudaSuccess) { ptr = nullptr; return e; }
+  cap = want;
+  return cudaSuccess;
+}
+void DevBuf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  cap = 0;
+}
+
+namespace {
+
+struct Box { float mn[3], mx[3]; };
+
+__device__ __forceinline__ Box tri_box(const rm_triangle& t) {
+  Box b;
+  b.mn[0] = fminf(t.v0.x, fminf(t.v1.x, t.v2.x)); b.mx[0] = fmaxf(t.v0.x, fmaxf(t.v1.x, t.v2.x));
+  b.mn[1] = fminf(t.v0.y, fminf(t.v1.y, t.v2.y)); b.mx[1] = fmaxf(t.v0.y, fmaxf(t.v1.y, t.v2.y));
+  b.mn[2] = fminf(t.v0.z, fminf(t.v1.z, t.v2.z)); b.mx[2] = fmaxf(t.v0.z, fmaxf(t.v1.z, t.v2.z));
+  return b;
+}
+__device__ __forceinline__ void grow(Box& a, const Box& b) {
+  for (int k = 0; k < 3; ++k) { a.mn[k] = fminf(a.mn[k], b.mn[k]); a.mx[k] = fmaxf(a.mx[k], b.mx[k]); }
+}
+__device__ __forceinline__ Box empty_box() {
+  Box b;
+  for (int k = 0; k < 3; ++k) { b.mn[k] = __int_as_float(0x7f800000); b.mx[k] = -__int_as_float(0x7f800000); }
+  return b;
+}
+
+// Slot boxes live in the first three float4 of a record (see rm_device.cuh).
+__device__ __forceinline__ void write_slot(float4* rec, int slot, const Box& b) {
+  float* f = reinterpret_cast<float*>(rec);
+  if (slot == 0) { f[0] = b.mn[0]; f[1] = b.mx[0]; f[2] = b.mn[1]; f[3] = b.mx[1]; f[8] = b.mn[2]; f[9] = b.mx[2]; }
+  else { f[4] = b.mn[0]; f[5] = b.mx[0]; f[6] = b.mn[1]; f[7] = b.mx[1]; f[10] = b.mn[2]; f[11] = b.mx[2]; }
+}
+__device__ __forceinline__ Box read_slot_cg(const float4* rec, int slot) {
+  const float4 a = __ldcg(rec + slot), c = __ldcg(rec + 2);
+  Box b;
+  b.mn[0] = a.x; b.mx[0] = a.y; b.mn[1] = a.z; b.mx[1] = a.w;
+  if (slot == 0) { b.mn[2] = c.x; b.mx[2] = c.y; } else { b.mn[2] = c.z; b.mx[2] = c.w; }
+  return b;
+}
+
+__global__ void k_pack_tgeo(const rm_triangle* __restrict__ tris, const int32_t* __restrict__ order, int n,
+                            float4* __restrict__ tgeo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int j = order[i];
+  const rm_triangle& t = tris[j];
+  tgeo[size_t(i) * 3 + 0] = make_float4(t.v0.x, t.v0.y, t.v0.z, __int_as_float(j));
+  tgeo[size_t(i) * 3 + 1] = make_float4(t.v1.x - t.v0.x, t.v1.y - t.v0.y, t.v1.z - t.v0.z, 0.f);
+  tgeo[size_t(i) * 3 + 2] = make_float4(t.v2.x - t.v0.x, t.v2.y - t.v0.y, t.v2.z - t.v0.z, 0.f);
+}
+
+// Refit: one thread per record; leaf slots are boxed from their triangles,
+// then the last child to arrive at a record carries the union upward.
+__global__ void k_refit(const rm_triangle* __restrict__ tris, const int32_t* __restrict__ order, float4* recs,
+                        const int32_t* __restrict__ parents, int* counters, int n_records) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_records) return;
+  float4* rec = recs + size_t(i) * 4;
+  const int4 d = *reinterpret_cast<const int4*>(rec + 3);
+  int ready = 0;
+  for (int slot = 0; slot < 2; ++slot) {
+    const int cnt = slot ? d.w : d.z, link = slot ? d.y : d.x;
+    if (cnt < 0) { ++ready; continue; }
+    if (cnt == 0) continue;
+    Box b = empty_box();
+    for (int k = 0; k < cnt; ++k) grow(b, tri_box(tris[order[link + k]]));
+    write_slot(rec, slot, b);
+    ++ready;
+  }
+  if (ready == 0) return;
+  __threadfence();
+  int node = i;
+  int add = ready;
+  for (;;) {
+    const int old = atomicAdd(counters + node, add);
+    if (old + add < 2) return;  // the other child is still on its way
+    __threadfence();
+    const int pr = parents[node];
+    if (pr < 0) return;
+    float4* nrec = recs + size_t(node) * 4;
+    const int4 nd = __ldcg(reinterpret_cast<const int4*>(nrec + 3));
+    Box b = empty_box();
+    if (nd.z >= 0) grow(b, read_slot_cg(nrec, 0));
+    if (nd.w >= 0) grow(b, read_slot_cg(nrec, 1));
+    write_slot(recs + size_t(pr >> 1) * 4, pr & 1, b);
+    __threadfence();
+    node = pr >> 1;
+    add = 1;
+  }
+}
+
+// ---- LBVH -------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned int ordered(float f) {
+  unsigned int u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float unordered(unsigned int u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__global__ void k_centroid_bounds(const rm_triangle* __restrict__ tris, int n, unsigned int* bounds) {
+  unsigned int mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const rm_triangle& t = tris[i];
+    const float c[3] = {t.v0.x + t.v1.x + t.v2.x, t.v0.y + t.v1.y + t.v2.y, t.v0.z + t.v1.z + t.v2.z};
+    for (int k = 0; k < 3; ++k) { mn[k] = min(mn[k], ordered(c[k])); mx[k] = max(mx[k], ordered(c[k])); }
+  }
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o; o >>= 1) {
+      mn[k] = min(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+      mx[k] = max(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; ++k) { atomicMin(bounds + k, mn[k]); atomicMax(bounds + 3 + k, mx[k]); }
+}
+
+__device__ __forceinline__ unsigned int expand_bits(unsigned int v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+
+__global__ void k_morton(const rm_triangle* __restrict__ tris, int n, const unsigned int* __restrict__ bounds,
+                         unsigned int* __restrict__ keys, int* __restrict__ vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const rm_triangle& t = tris[i];
+  const float c[3] = {t.v0.x + t.v1.x + t.v2.x, t.v0.y + t.v1.y + t.v2.y, t.v0.z + t.v1.z + t.v2.z};
+  unsigned int q[3];
+  for (int k = 0; k < 3; ++k) {
+    const float lo = unordered(bounds[k]), hi = unordered(bounds[3 + k]);
+    const float span = hi - lo;
+    float f = span > 0.0f ? (c[k] - lo) / span : 0.5f;
+    f = fminf(fmaxf(f, 0.0f), 1.0f);
+    q[k] = min(unsigned(f * 1024.0f), 1023u);
+  }
+  keys[i] = (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);
+  vals[i] = i;
+}
+
+// Common-prefix length of keys i and j, with the sorted position breaking
+// ties between equal codes (Karras 2012, section 4).
+__device__ __forceinline__ int delta(const unsigned int* keys, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  const unsigned int a = keys[i], b = keys[j];
+  if (a != b) return __clz(a ^ b);
+  return 32 + __clz(unsigned(i) ^ unsigned(j));
+}
+
+// Internal node i of n-1: children encoded as (index << 1) | is_leaf; ranges.
+__global__ void k_karras(const unsigned int* __restrict__ keys, int n, int2* __restrict__ children,
+                         int2* __restrict__ ranges, int* __restrict__ parent_int, int* __restrict__ parent_leaf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+  const int dmin = delta(keys, n, i, i - d);
+  int lmax = 2;
+  while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  const int dnode = delta(keys, n, i, j);
+  int s = 0;
+  for (int t = (l + 1) >> 1;; t = (t + 1) >> 1) {
+    if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    if (t == 1) break;
+  }
+  const int gamma = i + s * d + min(d, 0);
+  const int first = min(i, j), last = max(i, j);
+  const int left = gamma, right = gamma + 1;
+  const bool left_leaf = (first == gamma), right_leaf = (last == gamma + 1);
+  children[i] = make_int2((left << 1) | int(left_leaf), (right << 1) | int(right_leaf));
+  ranges[i] = make_int2(first, last);
+  if (left_leaf) parent_leaf[left] = i; else parent_int[left] = i;
+  if (right_leaf) parent_leaf[right] = i; else parent_int[right] = i;
+}
+
+// Boxes of the Karras tree, bottom-up from the leaves; the sorted triangle
+// order is vals[].  kbox: (n-1) internal boxes.
+__global__ void k_karras_boxes(const rm_triangle* __restrict__ tris, const int* __restrict__ order, int n,
+                               const int2* __restrict__ children, const int* __restrict__ parent_int,
+                               const int* __restrict__ parent_leaf, Box* kbox, int* kcount) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int node = parent_leaf[i];
+  while (node >= 0) {
+    __threadfence();
+    if (atomicAdd(kcount + node, 1) == 0) return;  // first arrival waits for the sibling
+    __threadfence();
+    const int2 ch = children[node];
+    Box b = empty_box();
+    for (int k = 0; k < 2; ++k) {
+      const int c = k ? ch.y : ch.x;
+      if (c & 1) grow(b, tri_box(tris[order[c >> 1]]));
+      else {
+        const Box* src = kbox + (c >> 1);
+        Box cb;
+        for (int q = 0; q < 3; ++q) { cb.mn[q] = __ldcg(&src->mn[q]); cb.mx[q] = __ldcg(&src->mx[q]); }
+        grow(b, cb);
+      }
+    }
+    kbox[node] = b;
+    node = node == 0 ? -1 : parent_int[node];
+  }
+}
+
+// Child-pair records from the Karras tree: record index = Karras index;
+// children with at most leaf_max triangles become leaves.
+__global__ void k_emit_records(const rm_triangle* __restrict__ tris, const int* __restrict__ order, int n,
+                               int leaf_max, const int2* __restrict__ children, const int2* __restrict__ ranges,
+                               const Box* __restrict__ kbox, float4* recs, int* parents) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  float4* rec = recs + size_t(i) * 4;
+  const int2 ch = children[i];
+  int links[2], counts[2];
+  for (int k = 0; k < 2; ++k) {
+    const int c = k ? ch.y : ch.x;
+    Box b;
+    if (c & 1) {
+      b = tri_box(tris[order[c >> 1]]);
+      links[k] = c >> 1; counts[k] = 1;
+    } else {
+      const int2 r = ranges[c >> 1];
+      b = kbox[c >> 1];
+      const int size = r.y - r.x + 1;
+      if (size <= leaf_max) { links[k] = r.x; counts[k] = size; }
+      else { links[k] = c >> 1; counts[k] = 0; parents[c >> 1] = (i << 1) | k; }
+    }
+    write_slot(rec, k, b);
+  }
+  rec[3] = make_float4(__int_as_float(links[0]), __int_as_float(links[1]), __int_as_float(counts[0]),
+                       __int_as_float(counts[1]));
+  if (i == 0) parents[0] = -1;
+}
+
+// Depth of each leaf slot (for the traversal stack bound).
+__global__ void k_depth(const float4* __restrict__ recs, const int* __restrict__ parents, int n_records, int* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_records) return;
+  const int4 d = *reinterpret_cast<const int4*>(recs + size_t(i) * 4 + 3);
+  if (d.z <= 0 && d.w <= 0) return;
+  int depth = 1, node = i, guard = 0;
+  while (parents[node] >= 0 && guard < 4096) { node = parents[node] >> 1; ++depth; ++guard; }
+  atomicMax(out, depth);
+}
+
+__global__ void k_single_leaf(const rm_triangle* __restrict__ tris, int n, float4* rec, int* parents, int* order) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  Box b = empty_box();
+  for (int i = 0; i < n; ++i) { grow(b, tri_box(tris[i])); order[i] = i; }
+  write_slot(rec, 0, b);
+  write_slot(rec, 1, empty_box());
+  rec[3] = make_float4(__int_as_float(0), __int_as_float(0), __int_as_float(n), __int_as_float(-1));
+  parents[0] = -1;
+}
+
+__global__ void k_hash(const unsigned long long* __restrict__ w, size_t n, unsigned long long* out) {
+  unsigned long long acc = 0;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    unsigned long long z = w[i] ^ (0x9E3779B97F4A7C15ull * (i + 1));
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    acc += z ^ (z >> 31);
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+}  // namespace
+
+cudaError_t pack_tgeo(const rm_triangle* d_tris, DevBvh& bvh, cudaStream_t st) {
+  if (bvh.n_tris <= 0) return cudaSuccess;
+  cudaError_t e = bvh.tgeo.reserve(size_t(bvh.n_tris) * 3 * sizeof(float4));
+  if (e != cudaSuccess) return e;
+  k_pack_tgeo<<<(bvh.n_tris + 255) / 256, 256, 0, st>>>(d_tris, bvh.order.as<int32_t>(), bvh.n_tris,
+                                                       bvh.tgeo.as<float4>());
+  return cudaGetLastError();
+}
+
+cudaError_t refit_bvh(const rm_triangle* d_tris, DevBvh& bvh, cudaStream_t st) {
+  if (bvh.n_records <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(bvh.counters.ptr, 0, size_t(bvh.n_records) * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  k_refit<<<(bvh.n_records + 255) / 256, 256, 0, st>>>(d_tris, bvh.order.as<int32_t>(), bvh.records.as<float4>(),
+                                                       bvh.parents.as<int32_t>(), bvh.counters.as<int>(),
+                                                       bvh.n_records);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return pack_tgeo(d_tris, bvh, st);
+}
+
+cudaError_t device_hash(const void* d_bytes, size_t n_bytes, unsigned long long* d_out, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  size_t words = n_bytes / 8;
+  if (words == 0) return cudaSuccess;
+  k_hash<<<148 * 4, 256, 0, st>>>(static_cast<const unsigned long long*>(d_bytes), words, d_out);
+  return cudaGetLastError();
+}
+
+#define RM_TRY(x)                          \
+  do {                                     \
+    cudaError_t e_ = (x);                  \
+    if (e_ != cudaSuccess) return e_;      \
+  } while (0)
+
+cudaError_t build_lbvh(const rm_triangle* d_tris, int n, int leaf_max, DevBvh& b, cudaStream_t st, std::string& err) {
+  b.n_tris = n;
+  b.max_depth = 0;
+  if (n <= 0) { b.n_records = 0; return cudaSuccess; }
+  leaf_max = std::max(1, std::min(leaf_max, kMaxLeaf));
+  if (n >= kMaxLink) { err = "scene exceeds 16777215 triangles"; return cudaErrorInvalidValue; }
+  RM_TRY(b.order.reserve(size_t(n) * sizeof(int)));
+  if (n <= leaf_max) {
+    b.n_records = 1;
+    RM_TRY(b.records.reserve(4 * sizeof(float4)));
+    RM_TRY(b.parents.reserve(sizeof(int)));
+    RM_TRY(b.counters.reserve(sizeof(int)));
+    k_single_leaf<<<1, 1, 0, st>>>(d_tris, n, b.records.as<float4>(), b.parents.as<int>(), b.order.as<int>());
+    RM_TRY(cudaGetLastError());
+    b.max_depth = 1;
+    return pack_tgeo(d_tris, b, st);
+  }
+  const int ni = n - 1;
+  RM_TRY(b.bounds.reserve(6 * sizeof(unsigned int)));
+  RM_TRY(b.keys.reserve(size_t(n) * 4 * 2));
+  RM_TRY(b.keys_alt.reserve(size_t(n) * 4));
+  RM_TRY(b.vals_alt.reserve(size_t(n) * 4));
+  RM_TRY(b.knodes.reserve(size_t(ni) * sizeof(int2) * 2));  // children + ranges
+  RM_TRY(b.ranges.reserve(size_t(ni) * sizeof(int) + size_t(n) * sizeof(int)));  // parent_int + parent_leaf
+  RM_TRY(b.kbox.reserve(size_t(ni) * sizeof(Box)));
+  RM_TRY(b.kcount.reserve(size_t(ni) * sizeof(int)));
+  RM_TRY(b.records.reserve(size_t(ni) * 4 * sizeof(float4)));
+  RM_TRY(b.parents.reserve(size_t(ni) * sizeof(int)));
+  RM_TRY(b.counters.reserve(size_t(ni) * sizeof(int)));
+  RM_TRY(b.depth.reserve(sizeof(int)));
+  unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  RM_TRY(cudaMemcpyAsync(b.bounds.ptr, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  k_centroid_bounds<<<148 * 4, 256, 0, st>>>(d_tris, n, b.bounds.as<unsigned int>());
+  unsigned int* keys = b.keys.as<unsigned int>();
+  int* vals = reinterpret_cast<int*>(keys + n);
+  k_morton<<<(n + 255) / 256, 256, 0, st>>>(d_tris, n, b.bounds.as<unsigned int>(), keys, vals);
+  RM_TRY(cudaGetLastError());
+  cub::DoubleBuffer<unsigned int> dk(keys, b.keys_alt.as<unsigned int>());
+  cub::DoubleBuffer<int> dv(vals, b.vals_alt.as<int>());
+  size_t temp_bytes = 0;
+  RM_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, dk, dv, n, 0, 30, st));
+  RM_TRY(b.temp.reserve(temp_bytes));
+  RM_TRY(cub::DeviceRadixSort::SortPairs(b.temp.ptr, temp_bytes, dk, dv, n, 0, 30, st));
+  const unsigned int* skeys = dk.Current();
+  const int* sorder = dv.Current();
+  RM_TRY(cudaMemcpyAsync(b.order.ptr, sorder, size_t(n) * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  int2* children = b.knodes.as<int2>();
+  int2* ranges = children + ni;
+  int* parent_int = b.ranges.as<int>();
+  int* parent_leaf = parent_int + ni;
+  RM_TRY(cudaMemsetAsync(parent_int, 0xff, size_t(ni) * sizeof(int), st));
+  k_karras<<<(ni + 255) / 256, 256, 0, st>>>(skeys, n, children, ranges, parent_int, parent_leaf);
+  RM_TRY(cudaMemsetAsync(b.kcount.ptr, 0, size_t(ni) * sizeof(int), st));
+  k_karras_boxes<<<(n + 255) / 256, 256, 0, st>>>(d_tris, b.order.as<int>(), n, children, parent_int, parent_leaf,
+                                                  b.kbox.as<Box>(), b.kcount.as<int>());
+  RM_TRY(cudaMemsetAsync(b.parents.ptr, 0xff, size_t(ni) * sizeof(int), st));
+  k_emit_records<<<(ni + 255) / 256, 256, 0, st>>>(d_tris, b.order.as<int>(), n, leaf_max, children, ranges,
+                                                   b.kbox.as<Box>(), b.records.as<float4>(), b.parents.as<int>());
+  RM_TRY(cudaGetLastError());
+  b.n_records = ni;
+  // Records of subtrees that collapsed into a leaf are never reached from the
+  // root; they keep parent -1, so refit ends at them and depth counts them as 1.
+  RM_TRY(cudaMemsetAsync(b.depth.ptr, 0, sizeof(int), st));
+  k_depth<<<(ni + 255) / 256, 256, 0, st>>>(b.records.as<float4>(), b.parents.as<int>(), ni, b.depth.as<int>());
+  RM_TRY(cudaMemcpyAsync(&b.max_depth, b.depth.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  RM_TRY(cudaStreamSynchronize(st));
+  if (b.max_depth > kStack) { err = "device BVH deeper than the traversal stack"; return cudaErrorInvalidValue; }
+  return pack_tgeo(d_tris, b, st);
+}
+
+bool convert_caller_bvh(const rm_bvh_node* nodes, int M, const int32_t* bvh_tri, int n_tris, DevBvh& out,
+                        cudaStream_t st, std::string& err) {
+  out.n_tris = n_tris;
+  if (M <= 0 || n_tris <= 0) { out.n_records = 0; return true; }
+  if (!nodes || !bvh_tri) { err = "BVH nodes without bvh_tri"; return false; }
+  if (n_tris >= kMaxLink || M >= kMaxLink) { err = "BVH exceeds 16777215 nodes or triangles"; return false; }
+  for (int i = 0; i < n_tris; ++i)
+    if (bvh_tri[i] < 0 || bvh_tri[i] >= n_tris) { err = "bvh_tri index out of range"; return false; }
+  // record index of each internal node, in node order (parents precede children)
+  std::vector<int> rec(size_t(M), -1);
+  int n_rec = 0;
+  for (int i = 0; i < M; ++i) {
+    const rm_bvh_node& s = nodes[i];
+    if (s.count > 0) {
+      if (s.count > kMaxLeaf || s.offset < 0 || int64_t(s.offset) + s.count > n_tris) {
+        err = "BVH leaf range invalid (or more than 255 triangles)";
+        return false;
+      }
+    } else {
+      if (s.left <= i || s.right <= i || s.left >= M || s.right >= M) {
+        err = "BVH child index invalid (children must follow their parent)";
+        return false;
+      }
+      rec[size_t(i)] = n_rec++;
+    }
+  }
+  const bool root_leaf = nodes[0].count > 0;
+  if (root_leaf) n_rec = 1;
+  std::vector<float> recs(size_t(n_rec) * 16, 0.0f);
+  std::vector<int> parents(size_t(n_rec), -1);
+  std::vector<int> depth(size_t(M), 0);
+  auto put = [&](int r, int slot, const rm_bvh_node* c, int link, int count) {
+    float* f = recs.data() + size_t(r) * 16;
+    const float inf = __builtin_inff();
+    float mn[3] = {inf, inf, inf}, mx[3] = {-inf, -inf, -inf};
+    if (c) { mn[0] = c->mn.x; mn[1] = c->mn.y; mn[2] = c->mn.z; mx[0] = c->mx.x; mx[1] = c->mx.y; mx[2] = c->mx.z; }
+    int base = slot ? 4 : 0;
+    f[base] = mn[0]; f[base + 1] = mx[0]; f[base + 2] = mn[1]; f[base + 3] = mx[1];
+    f[8 + slot * 2] = mn[2]; f[9 + slot * 2] = mx[2];
+    int* iv = reinterpret_cast<int*>(f + 12);
+    iv[slot] = link;
+    iv[2 + slot] = count;
+  };
+  int max_depth = 1;
+  if (root_leaf) {
+    put(0, 0, &nodes[0], nodes[0].offset, nodes[0].count);
+    put(0, 1, nullptr, 0, -1);
+  } else {
+    depth[0] = 1;
+    for (int i = 0; i < M; ++i) {
+      if (nodes[i].count > 0 || rec[size_t(i)] < 0) continue;
+      const int r = rec[size_t(i)];
+      if (depth[size_t(i)] == 0) continue;  // unreachable from the root
+      for (int slot = 0; slot < 2; ++slot) {
+        const int c = slot ? nodes[i].right : nodes[i].left;
+        const rm_bvh_node& cn = nodes[c];
+        depth[size_t(c)] = depth[size_t(i)] + 1;
+        max_depth = std::max(max_depth, depth[size_t(c)]);
+        if (cn.count > 0) put(r, slot, &cn, cn.offset, cn.count);
+        else {
+          put(r, slot, &cn, rec[size_t(c)], 0);
+          parents[size_t(rec[size_t(c)])] = (r << 1) | slot;
+        }
+      }
+    }
+    // an unreachable internal node keeps an all-empty record
+    for (int i = 0; i < M; ++i)
+      if (rec[size_t(i)] >= 0 && depth[size_t(i)] == 0) {
+        put(rec[size_t(i)], 0, nullptr, 0, -1);
+        put(rec[size_t(i)], 1, nullptr, 0, -1);
+      }
+  }
+  if (max_depth > kStack) { err = "BVH deeper than 64 levels"; return false; }
+  out.max_depth = max_depth;
+  out.n_records = n_rec;
+  cudaError_t e;
+  if ((e = out.records.reserve(recs.size() * sizeof(float))) != cudaSuccess ||
+      (e = out.parents.reserve(parents.size() * sizeof(int))) != cudaSuccess ||
+      (e = out.counters.reserve(parents.size() * sizeof(int))) != cudaSuccess ||
+      (e = out.order.reserve(size_t(n_tris) * sizeof(int))) != cudaSuccess) {
+    err = std::string("BVH allocation failed: ") + cudaGetErrorString(e);
+    return false;
+  }
+  if ((e = cudaMemcpyAsync(out.records.ptr, recs.data(), recs.size() * sizeof(float), cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(out.parents.ptr, parents.data(), parents.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(out.order.ptr, bvh_tri, size_t(n_tris) * sizeof(int), cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+    err = std::string("BVH upload failed: ") + cudaGetErrorString(e);
+    return false;
+  }
+  return true;
+}
+
+}  // namespace rmd

@@ -1,0 +1,772 @@
+// rm_device.cuh - device-side scene layout, traversal and shading for sm_100a.
+//
+// One path tracer, written for the GPU, that reproduces the reference Metal
+// shader's arithmetic (reference src/engine/pathtrace.metal) operation for
+// operation: this file is compiled with -fmad=false and IEEE div/sqrt so that,
+// on identical RNG streams, radiance matches the CPU oracle bit for bit.
+//
+// Scene layout in HBM (built by rm_bvh.cu):
+//  * tgeo: 3 x float4 per triangle, in BVH leaf order: (v0, original index),
+//    (v1 - v0, 0), (v2 - v0, 0).  One 48-byte, 16-byte-aligned record is all a
+//    Moller-Trumbore test reads (the reference fetches a 176-byte AoS record).
+//  * nodes: binary BVH in the child-pair layout of Aila & Laine ("Understanding
+//    the Efficiency of Ray Traversal on GPUs", HPG 2009): each internal node
+//    holds both children's boxes, 64 bytes = four 128-bit loads; a ray tests
+//    both children at once and descends into the nearer one first with a
+//    per-thread stack.
+//  * tris: the caller's packed 176-byte triangles, read only for the surface
+//    attributes of a confirmed hit and for light sampling.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "rm_detmath.h"
+#include "rmcuda.h"
+
+namespace rmd {
+
+constexpr float kFar = 1e30f;
+constexpr float kPi = 3.141592653589793f;
+constexpr float kBoxSlack = 1.0000152587890625f;  // 1 + 2^-16, see traverse()
+constexpr int kStack = 64;                         // max BVH depth accepted at build time
+constexpr int kMaxLeaf = 255;                      // 8-bit leaf count in a stack entry
+constexpr int kMaxLink = 1 << 24;                  // 24-bit node / triangle link
+constexpr int kMaxAlphaCrossings = 1024;
+constexpr uint64_t kSpatialSeedXor = 0x1B54A35A6F31B458ull;  // low 64 bits of pathtrace.metal:937
+
+// device error word bits
+constexpr uint32_t kErrStack = 1u;
+constexpr uint32_t kErrAlpha = 2u;
+
+struct Scene {
+  const rm_triangle* __restrict__ tris;
+  const float4* __restrict__ tgeo;
+  const float4* __restrict__ nodes;
+  int n_nodes;  // internal child-pair records; 0 = empty scene
+  const int32_t* __restrict__ lights;
+  const float* __restrict__ cdf;
+  int n_lights;
+  float light_total;
+  const rm_vec3* __restrict__ texels;
+};
+
+// metal_types.h:21-30 plus this build's switches.
+struct Params {
+  rm_camera camera;
+  int width, height, spp, bounces, nodes, lights, adapt_min, adapt_step, nomis, opaque;
+  float light_total, resolution, clamp_value, adapt_rel, adapt_abs;
+  int restir_candidates, restir_spatial, restir_mcap;
+  float restir_radius;
+  rm_camera prevCamera;
+  int hasHistory;
+  int rr;
+};
+
+// SoA G-buffer: pos|kind, normal|rough, albedo|metallic, wo|ior, emission.
+struct GBufSoA {
+  float4* pos_kind;
+  float4* nor_rough;
+  float4* alb_met;
+  float4* wo_ior;
+  float4* emi;
+};
+// SoA reservoir: lightPos|alpha, lightNormal|p_hat, emission|sumWs, (sumWu, M, valid, 0).
+struct ResSoA {
+  float4* lp_alpha;
+  float4* ln_phat;
+  float4* le_sumws;
+  float4* sumwu_m_valid;
+};
+
+struct Rng {
+  uint32_t state;
+  __device__ __forceinline__ void seed(uint64_t s) {
+    uint64_t z = s + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    state = uint32_t(z ^ (z >> 31));
+  }
+  __device__ __forceinline__ float uniform01() {
+    state = state * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return float(((word >> 22u) ^ word) >> 8u) * 0x1p-24f;
+  }
+};
+
+__device__ __forceinline__ uint64_t seed_pixel(uint64_t seed, uint32_t x, uint32_t y) {
+  return seed ^ (uint64_t(y + 1) * 0x9E3779B97F4A7C15ull) ^ (uint64_t(x + 1) * 0xBF58476D1CE4E5B9ull);
+}
+
+__device__ __forceinline__ float lum3(float r, float g, float b) {
+  return 0.2126f * r + 0.7152f * g + 0.0722f * b;
+}
+
+struct Hit {
+  float t;
+  int tri;
+  float u, v;
+  float px, py, pz;
+  float nix, niy, niz;
+  float ar, ag, ab, er, eg, eb, ior, rough;
+  int shader;
+  float ngx, ngy, ngz;
+};
+
+struct Bsdf { float r, g, b, pdf; };
+
+// ---------------------------------------------------------------- traversal
+//
+// Closest hit = smallest t, ties to the smaller original triangle index; a
+// candidate is accepted under the reference's Moller-Trumbore rules
+// (pathtrace.metal:150-158).  A box is culled only when its entry exceeds
+// its exit by more than a relative 2^-16, so that no BVH culls a triangle that
+// the Moller-Trumbore test would accept: the hit is independent of the BVH.
+struct TraceResult { float t; int tri; float u, v; };
+
+template <bool kAnyHit>
+__device__ __forceinline__ TraceResult traverse(const Scene& s, float ox, float oy, float oz, float dx, float dy,
+                                                float dz, float tmax, uint32_t* err, uint32_t& n_nodes,
+                                                uint32_t& n_tests) {
+  TraceResult r{tmax, -1, 0.f, 0.f};
+  if (s.n_nodes == 0) return r;
+  const float ix = 1.0f / (dx == 0.0f ? 1e-30f : dx);
+  const float iy = 1.0f / (dy == 0.0f ? 1e-30f : dy);
+  const float iz = 1.0f / (dz == 0.0f ? 1e-30f : dz);
+  int stack[kStack];
+  int sp = 0;
+  int node = 0;       // internal node index, or -1 when a leaf is pending
+  int leaf_first = 0, leaf_count = 0;
+  for (;;) {
+    while (node >= 0 && leaf_count == 0) {
+      ++n_nodes;
+      const float4* n = s.nodes + size_t(node) * 4;
+      const float4 a = __ldg(n + 0);
+      const float4 b = __ldg(n + 1);
+      const float4 c = __ldg(n + 2);
+      const int4 d = __ldg(reinterpret_cast<const int4*>(n + 3));
+      // child 0
+      float l0x = (a.x - ox) * ix, h0x = (a.y - ox) * ix;
+      float l0y = (a.z - oy) * iy, h0y = (a.w - oy) * iy;
+      float l0z = (c.x - oz) * iz, h0z = (c.y - oz) * iz;
+      float n0 = fmaxf(0.0f, fmaxf(fminf(l0x, h0x), fmaxf(fminf(l0y, h0y), fminf(l0z, h0z))));
+      float f0 = fminf(r.t, fminf(fmaxf(l0x, h0x), fminf(fmaxf(l0y, h0y), fmaxf(l0z, h0z))));
+      // child 1
+      float l1x = (b.x - ox) * ix, h1x = (b.y - ox) * ix;
+      float l1y = (b.z - oy) * iy, h1y = (b.w - oy) * iy;
+      float l1z = (c.z - oz) * iz, h1z = (c.w - oz) * iz;
+      float n1 = fmaxf(0.0f, fmaxf(fminf(l1x, h1x), fmaxf(fminf(l1y, h1y), fminf(l1z, h1z))));
+      float f1 = fminf(r.t, fminf(fmaxf(l1x, h1x), fminf(fmaxf(l1y, h1y), fmaxf(l1z, h1z))));
+      bool hit0 = d.z >= 0 && !(n0 > f0 * kBoxSlack);
+      bool hit1 = d.w >= 0 && !(n1 > f1 * kBoxSlack);
+      // a child record: link d.x/d.y, count d.z/d.w (>0 leaf, 0 internal, <0 empty)
+      if (hit0 && hit1) {
+        int first = d.x, firstc = d.z, second = d.y, secondc = d.w;
+        if (n1 < n0) { first = d.y; firstc = d.w; second = d.x; secondc = d.z; }
+        if (sp >= kStack) { atomicOr(err, kErrStack); return r; }
+        stack[sp++] = int((uint32_t(secondc) << 24) | uint32_t(second));  // far child: 8-bit count, 24-bit link
+        if (firstc > 0) { leaf_first = first; leaf_count = firstc; node = -1; }
+        else node = first;
+      } else if (hit0 || hit1) {
+        int link = hit0 ? d.x : d.y, cnt = hit0 ? d.z : d.w;
+        if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
+        else node = link;
+      } else {
+        if (sp == 0) return r;
+        const int e = stack[--sp];
+        const int cnt = int(uint32_t(e) >> 24), link = e & 0xFFFFFF;
+        if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
+        else node = link;
+      }
+    }
+    // leaf: Moller-Trumbore, pathtrace.metal:150-158
+    n_tests += uint32_t(leaf_count);
+    for (int k = 0; k < leaf_count; ++k) {
+      const float4* g = s.tgeo + size_t(leaf_first + k) * 3;
+      const float4 q0 = __ldg(g + 0);
+      const float4 q1 = __ldg(g + 1);
+      const float4 q2 = __ldg(g + 2);
+      const int j = __float_as_int(q0.w);
+      // p = cross(rd, e2)
+      float px = dy * q2.z - dz * q2.y;
+      float py = dz * q2.x - dx * q2.z;
+      float pz = dx * q2.y - dy * q2.x;
+      float det = q1.x * px + q1.y * py + q1.z * pz;
+      if (fabsf(det) < 1e-12f) continue;
+      float tx = ox - q0.x, ty = oy - q0.y, tz = oz - q0.z;
+      float u = (tx * px + ty * py + tz * pz) / det;
+      if (u < 0.0f || u > 1.0f) continue;
+      // q = cross(tv, e1)
+      float qx = ty * q1.z - tz * q1.y;
+      float qy = tz * q1.x - tx * q1.z;
+      float qz = tx * q1.y - ty * q1.x;
+      float v = (dx * qx + dy * qy + dz * qz) / det;
+      if (v < 0.0f || u + v > 1.0f) continue;
+      float dd = (q2.x * qx + q2.y * qy + q2.z * qz) / det;
+      if (dd > 1e-8f && (dd < r.t || (dd == r.t && r.tri >= 0 && j < r.tri))) {
+        r.t = dd; r.tri = j; r.u = u; r.v = v;
+        if (kAnyHit) return r;
+      }
+    }
+    leaf_count = 0;
+    if (sp == 0) return r;
+    const int e = stack[--sp];
+    const int cnt = int(uint32_t(e) >> 24), link = e & 0xFFFFFF;
+    if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
+    else node = link;
+  }
+}
+
+// ---------------------------------------------------------------- tracer
+struct Tracer {
+  const Scene& s;
+  const Params& p;
+  Rng rng;
+  uint32_t rays, nodes, tests;
+  uint32_t* err;
+
+  __device__ __forceinline__ Tracer(const Scene& s_, const Params& p_, uint32_t* e)
+      : s(s_), p(p_), rays(0), nodes(0), tests(0), err(e) {}
+
+  __device__ __forceinline__ float U() { return rng.uniform01(); }
+
+  __device__ __forceinline__ bool shadow(float ox, float oy, float oz, float dx, float dy, float dz, float dist) {
+    ++rays;
+    return traverse<true>(s, ox, oy, oz, dx, dy, dz, dist, err, nodes, tests).tri >= 0;
+  }
+
+  __device__ static void hsv2rgb(float h, float sat, float val, float& r, float& g, float& b) {
+    float c = sat * val;
+    float hm = h / 60.0f;
+    float md = hm - floorf(hm / 2.0f) * 2.0f;
+    float x = c * (1.0f - fabsf(md - 1.0f));
+    float m = val - c;
+    float cr = 0, cg = 0, cb = 0;
+    if (h < 60.0f) { cr = c; cg = x; }
+    else if (h < 120.0f) { cr = x; cg = c; }
+    else if (h < 180.0f) { cg = c; cb = x; }
+    else if (h < 240.0f) { cg = x; cb = c; }
+    else if (h < 300.0f) { cr = x; cb = c; }
+    else if (h < 360.0f) { cr = c; cb = x; }
+    cr += m; cg += m; cb += m;
+    r = cr * 255.0f; g = cg * 255.0f; b = cb * 255.0f;
+  }
+
+  // pathtrace.metal:165-204
+  __device__ __noinline__ Hit cast_ray(float ox, float oy, float oz, float dx, float dy, float dz, float dist) {
+    ++rays;
+    TraceResult tr = traverse<false>(s, ox, oy, oz, dx, dy, dz, dist, err, nodes, tests);
+    Hit h;
+    h.t = tr.t; h.tri = tr.tri; h.u = tr.u; h.v = tr.v;
+    h.px = ox + dx * h.t; h.py = oy + dy * h.t; h.pz = oz + dz * h.t;
+    h.shader = 0;
+    if (h.tri >= 0) {
+      const rm_triangle& t = s.tris[h.tri];
+      float w = 1.0f - (h.u + h.v);
+      float nx = w * t.n0.x + (h.u * t.n1.x + h.v * t.n2.x);
+      float ny = w * t.n0.y + (h.u * t.n1.y + h.v * t.n2.y);
+      float nz = w * t.n0.z + (h.u * t.n1.z + h.v * t.n2.z);
+      float d = 1.0f / sqrtf(nx * nx + (ny * ny + nz * nz));
+      h.nix = nx * d; h.niy = ny * d; h.niz = nz * d;
+      h.ar = t.ar; h.ag = t.ag; h.ab = t.ab;
+      if (t.texture_offset >= 0) {
+        float tu = w * t.tu0 + h.u * t.tu1 + h.v * t.tu2;
+        float tv = w * t.tv0 + h.u * t.tv1 + h.v * t.tv2;
+        tu = fminf(tu - floorf(tu), 0.99999994f);
+        tv = fminf(tv - floorf(tv), 0.99999994f);
+        int x = min(int(tu * float(t.texture_width)), t.texture_width - 1);
+        int y = t.texture_height - 1 - min(int(tv * float(t.texture_height)), t.texture_height - 1);
+        const rm_vec3 c = s.texels[size_t(t.texture_offset) + size_t(y) * size_t(t.texture_width) + size_t(x)];
+        h.ar *= c.x; h.ag *= c.y; h.ab *= c.z;
+      }
+      h.er = t.er; h.eg = t.eg; h.eb = t.eb;
+      h.ior = t.ior; h.rough = t.rough; h.shader = t.shader;
+      h.ngx = t.n.x; h.ngy = t.n.y; h.ngz = t.n.z;
+      if (h.shader == 1) {
+        float az = rm_atanf(h.px / h.pz) * 180.0f / kPi + ((h.pz > 0.0f) ? 0.0f : 180.0f);
+        float hh = (az - floorf(az / 360.0f) * 360.0f) / 360.0f;
+        hsv2rgb(hh, 0.8f, 1.0f, h.ar, h.ag, h.ab);
+      }
+    }
+    return h;
+  }
+
+  // pathtrace.metal:536-550, crossings capped at kMaxAlphaCrossings.
+  __device__ __forceinline__ Hit cast_alpha_ray(float ox, float oy, float oz, float dx, float dy, float dz, float dist) {
+    if (p.opaque) return cast_ray(ox, oy, oz, dx, dy, dz, dist);
+    float traveled = 0.0f;
+    for (int it = 0; it < kMaxAlphaCrossings && traveled < dist; ++it) {
+      Hit h = cast_ray(ox + dx * traveled, oy + dy * traveled, oz + dz * traveled, dx, dy, dz, dist - traveled);
+      if (h.tri < 0) return h;
+      float opacity = s.tris[h.tri].alpha;
+      if (opacity >= 1.0f || (opacity > 0.0f && U() < opacity)) {
+        h.t += traveled;
+        return h;
+      }
+      traveled += h.t + 0.0001f;
+    }
+    Hit miss;
+    miss.t = kFar; miss.tri = -1;
+    return miss;
+  }
+
+  __device__ __forceinline__ bool occluded(float ox, float oy, float oz, float dx, float dy, float dz, float dist) {
+    return p.opaque ? shadow(ox, oy, oz, dx, dy, dz, dist) : cast_alpha_ray(ox, oy, oz, dx, dy, dz, dist).tri >= 0;
+  }
+
+  __device__ static __forceinline__ void tangent(float nx, float ny, float nz, float& tx, float& ty, float& tz,
+                                                 float& bx, float& by, float& bz) {
+    if (fabsf(nx) > 0.1f) { tx = nz; ty = 0.0f; tz = -nx; }
+    else { tx = 0.0f; ty = -nz; tz = ny; }
+    float l = 1.0f / sqrtf(tx * tx + ty * ty + tz * tz);
+    tx *= l; ty *= l; tz *= l;
+    bx = ny * tz - nz * ty;
+    by = nz * tx - nx * tz;
+    bz = nx * ty - ny * tx;
+  }
+
+  __device__ __forceinline__ void sample_cosine(float nx, float ny, float nz, float& ox, float& oy, float& oz) {
+    float ru = U();
+    float phi = U() * (2.0f * kPi);
+    float sp, c;
+    rm_sincosf(phi, &sp, &c);
+    float rr = sqrtf(ru);
+    float lx = rr * c, ly = rr * sp, lz = sqrtf(fmaxf(0.0f, 1.0f - ru));
+    float tx, ty, tz, bx, by, bz;
+    tangent(nx, ny, nz, tx, ty, tz, bx, by, bz);
+    ox = tx * lx + (bx * ly + nx * lz);
+    oy = ty * lx + (by * ly + ny * lz);
+    oz = tz * lx + (bz * ly + nz * lz);
+  }
+
+  __device__ __forceinline__ void sample_ggx_half(float alpha2, float nx, float ny, float nz, float& hx, float& hy,
+                                                  float& hz) {
+    (void)U();
+    float rv = U();
+    float phi = U() * (2.0f * kPi);
+    float sp, c;
+    rm_sincosf(phi, &sp, &c);
+    float cs = sqrtf((1.0f - rv) / (1.0f + (alpha2 - 1.0f) * rv));
+    float sn = sqrtf(fmaxf(0.0f, 1.0f - cs * cs));
+    float lx = sn * c, ly = sn * sp, lz = cs;
+    float tx, ty, tz, bx, by, bz;
+    tangent(nx, ny, nz, tx, ty, tz, bx, by, bz);
+    hx = tx * lx + (bx * ly + nx * lz);
+    hy = ty * lx + (by * ly + ny * lz);
+    hz = tz * lx + (bz * ly + nz * lz);
+    float d = 1.0f / sqrtf(hx * hx + hy * hy + hz * hz);
+    hx *= d; hy *= d; hz *= d;
+  }
+
+  // pathtrace.metal:243-295
+  __device__ static __forceinline__ Bsdf eval_bsdf(float wix, float wiy, float wiz, float wox, float woy, float woz,
+                                                   float nx, float ny, float nz, float alpha2, float metallic,
+                                                   float spec_prob, float ar, float ag, float ab) {
+    Bsdf out{0.f, 0.f, 0.f, 0.f};
+    float cos_i = wix * nx + (wiy * ny + wiz * nz);
+    float cos_o = wox * nx + (woy * ny + woz * nz);
+    if (!(cos_i > 1e-8f && cos_o > 1e-8f)) return out;
+    float hx = wix + wox, hy = wiy + woy, hz = wiz + woz;
+    float hl = sqrtf(hx * hx + hy * hy + hz * hz);
+    if (!(hl > 1e-8f)) return out;
+    float inv = 1.0f / hl;
+    hx *= inv; hy *= inv; hz *= inv;
+    float cos_h = hx * nx + (hy * ny + hz * nz);
+    float vo_h = wox * hx + (woy * hy + woz * hz);
+    if (cos_h < 0.0f) { hx = -hx; hy = -hy; hz = -hz; cos_h = -cos_h; vo_h = -vo_h; }
+    if (!(vo_h > 1e-8f)) return out;
+    float dd = cos_h * cos_h * (alpha2 - 1.0f) + 1.0f;
+    float D = alpha2 / (kPi * dd * dd);
+    float g1 = 2.0f * cos_o / (cos_o + sqrtf(cos_o * cos_o + alpha2 * (1.0f - cos_o * cos_o)));
+    float g2 = 2.0f * cos_i / (cos_i + sqrtf(cos_i * cos_i + alpha2 * (1.0f - cos_i * cos_i)));
+    float G = g1 * g2;
+    float om = 1.0f - vo_h;
+    om *= om; om *= om; om *= 1.0f - vo_h;
+    float di = 1.0f - metallic;
+    float f0r = 0.04f * di + ar * metallic, f0g = 0.04f * di + ag * metallic, f0b = 0.04f * di + ab * metallic;
+    float fr = f0r + (1.0f - f0r) * om, fg = f0g + (1.0f - f0g) * om, fb = f0b + (1.0f - f0b) * om;
+    float kdr = ar * di * (1.0f - fr), kdg = ag * di * (1.0f - fg), kdb = ab * di * (1.0f - fb);
+    float base = D * G / (4.0f * cos_i * cos_o);
+    out.r = kdr / kPi + base * fr;
+    out.g = kdg / kPi + base * fg;
+    out.b = kdb / kPi + base * fb;
+    float pdf_d = cos_i / kPi;
+    float pdf_s = D * cos_h / (4.0f * vo_h);
+    out.pdf = (1.0f - spec_prob) * pdf_d + spec_prob * pdf_s;
+    return out;
+  }
+
+  __device__ __forceinline__ int pick_light(float pick) {
+    int lo = 0, hi = p.lights - 1;
+    while (lo < hi) {
+      int mid = (lo + hi) / 2;
+      if (__ldg(s.cdf + mid) >= pick) hi = mid; else lo = mid + 1;
+    }
+    return __ldg(s.lights + lo);
+  }
+
+  // pathtrace.metal:299-469
+  __device__ __noinline__ void direct_lighting(float px, float py, float pz, float nx, float ny, float nz, float wox,
+                                               float woy, float woz, float rough, float metallic, float spec_prob,
+                                               float ar, float ag, float ab, float& o_r, float& o_g, float& o_b,
+                                               float& out_sumW, uint32_t& out_M) {
+    o_r = o_g = o_b = 0.0f;
+    out_sumW = 0.0f;
+    out_M = 0;
+    if (p.lights == 0 || !(p.light_total > 1e-12f)) return;
+    int Mc = p.restir_candidates;
+    if (Mc < 1) Mc = 1;
+    if (Mc > 32) Mc = 32;
+    float r2 = rough;
+    if (r2 < 0.0f) r2 = 0.0f;
+    if (r2 > 1.0f) r2 = 1.0f;
+    if (r2 < 0.02f) r2 = 0.02f;
+    float alpha2 = (r2 * r2) * (r2 * r2);
+    const float LT = p.light_total;
+    if (Mc <= 1) {
+      float pick = U() * LT;
+      const rm_triangle& t = s.tris[pick_light(pick)];
+      float lu = U(), lv = U();
+      if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
+      float lw = 1.0f - lu - lv;
+      float ldx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x) - px;
+      float ldy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y) - py;
+      float ldz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z) - pz;
+      float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
+      if (!(dist > 0.003f)) { out_M = 1; return; }
+      float inv = 1.0f / dist;
+      ldx *= inv; ldy *= inv; ldz *= inv;
+      float lcos = -(t.nn.x * ldx + (t.nn.y * ldy + t.nn.z * ldz));
+      float scos = nx * ldx + (ny * ldy + nz * ldz);
+      if (!(lcos > 1e-8f && scos > 1e-8f)) { out_M = 1; return; }
+      float lt_lum = lum3(t.er, t.eg, t.eb);
+      if (lt_lum < 1e-6f) lt_lum = 1e-6f;
+      float pdf = dist * dist * lt_lum / (lcos * LT);
+      float sox = px + nx * 0.002f, soy = py + ny * 0.002f, soz = pz + nz * 0.002f;
+      if (occluded(sox, soy, soz, ldx, ldy, ldz, dist - 0.003f)) {
+        Bsdf eo = eval_bsdf(ldx, ldy, ldz, wox, woy, woz, nx, ny, nz, alpha2, metallic, spec_prob, ar, ag, ab);
+        float Fr0 = t.er * eo.r * scos * t.alpha;
+        float Fg0 = t.eg * eo.g * scos * t.alpha;
+        float Fb0 = t.eb * eo.b * scos * t.alpha;
+        float ph0 = lum3(Fr0, Fg0, Fb0);
+        out_sumW = (ph0 > 0.0f && pdf > 1e-12f) ? ph0 / pdf : 0.0f;
+        out_M = 1;
+        return;
+      }
+      Bsdf e = eval_bsdf(ldx, ldy, ldz, wox, woy, woz, nx, ny, nz, alpha2, metallic, spec_prob, ar, ag, ab);
+      if (!(pdf > 1e-12f)) { out_M = 1; return; }
+      float Fr = t.er * e.r * scos * t.alpha;
+      float Fg = t.eg * e.g * scos * t.alpha;
+      float Fb = t.eb * e.b * scos * t.alpha;
+      float ph = lum3(Fr, Fg, Fb);
+      out_sumW = (ph > 0.0f) ? ph / pdf : 0.0f;
+      out_M = 1;
+      float wnee = 1.0f;
+      if (!p.nomis && e.pdf > 1e-20f) wnee = pdf / (pdf + e.pdf);
+      float k = scos * wnee * t.alpha / pdf;
+      o_r = t.er * e.r * k;
+      o_g = t.eg * e.g * k;
+      o_b = t.eb * e.b * k;
+      return;
+    }
+    float sumW = 0.0f;
+    float sel_lx = 0, sel_ly = 0, sel_lz = 0, sel_Fr = 0, sel_Fg = 0, sel_Fb = 0, sel_phat = 0, sel_epdf = 0;
+    bool have = false;
+    for (int j = 0; j < Mc; ++j) {
+      float pick = U() * LT;
+      const rm_triangle& t = s.tris[pick_light(pick)];
+      float lu = U(), lv = U();
+      if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
+      float lw = 1.0f - lu - lv;
+      float qx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x);
+      float qy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y);
+      float qz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z);
+      float ldx = qx - px, ldy = qy - py, ldz = qz - pz;
+      float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
+      float w = 0, ph = 0, epdf = 0, Fr = 0, Fg = 0, Fb = 0;
+      if (dist > 0.003f) {
+        float inv = 1.0f / dist;
+        float dxn = ldx * inv, dyn = ldy * inv, dzn = ldz * inv;
+        float lcos = -(t.nn.x * dxn + (t.nn.y * dyn + t.nn.z * dzn));
+        float scos = nx * dxn + (ny * dyn + nz * dzn);
+        if (lcos > 1e-8f && scos > 1e-8f) {
+          float lt_lum = lum3(t.er, t.eg, t.eb);
+          if (lt_lum < 1e-6f) lt_lum = 1e-6f;
+          float q = dist * dist * lt_lum / (lcos * LT);
+          if (q > 1e-12f) {
+            Bsdf e = eval_bsdf(dxn, dyn, dzn, wox, woy, woz, nx, ny, nz, alpha2, metallic, spec_prob, ar, ag, ab);
+            epdf = e.pdf;
+            Fr = t.er * e.r * scos * t.alpha;
+            Fg = t.eg * e.g * scos * t.alpha;
+            Fb = t.eb * e.b * scos * t.alpha;
+            ph = lum3(Fr, Fg, Fb);
+            if (ph > 0.0f) w = ph / q;
+          }
+        }
+      }
+      sumW += w;
+      float r = U();
+      if (w > 0.0f && r * sumW < w) {
+        have = true;
+        sel_lx = qx; sel_ly = qy; sel_lz = qz;
+        sel_Fr = Fr; sel_Fg = Fg; sel_Fb = Fb;
+        sel_phat = ph; sel_epdf = epdf;
+      }
+    }
+    out_sumW = sumW;
+    out_M = uint32_t(Mc);
+    if (!have || !(sumW > 0.0f) || !(sel_phat > 0.0f)) return;
+    float pdf_ris = float(Mc) * sel_phat / sumW;
+    float wnee = 1.0f;
+    if (!p.nomis && sel_epdf > 1e-20f) wnee = pdf_ris / (pdf_ris + sel_epdf);
+    float vdx = sel_lx - px, vdy = sel_ly - py, vdz = sel_lz - pz;
+    float vdist = sqrtf(vdx * vdx + vdy * vdy + vdz * vdz);
+    if (!(vdist > 0.003f)) return;
+    float vinv = 1.0f / vdist;
+    vdx *= vinv; vdy *= vinv; vdz *= vinv;
+    float sox = px + nx * 0.002f, soy = py + ny * 0.002f, soz = pz + nz * 0.002f;
+    if (occluded(sox, soy, soz, vdx, vdy, vdz, vdist - 0.003f)) return;
+    float W = sumW / (float(Mc) * sel_phat);
+    o_r = sel_Fr * W * wnee;
+    o_g = sel_Fg * W * wnee;
+    o_b = sel_Fb * W * wnee;
+  }
+
+  __device__ static __forceinline__ float fresnel(float ci_in, float eta_in, float eta_out) {
+    float ci = ci_in;
+    if (ci < 0.0f) ci = 0.0f;
+    if (ci > 1.0f) ci = 1.0f;
+    float eta = eta_in / eta_out;
+    float s2 = eta * eta * (1.0f - ci * ci);
+    if (s2 >= 1.0f) return 1.0f;
+    float ct = sqrtf(1.0f - s2);
+    float rp = (eta_out * ci - eta_in * ct) / (eta_out * ci + eta_in * ct);
+    float rs = (eta_in * ci - eta_out * ct) / (eta_in * ci + eta_out * ct);
+    return 0.5f * (rp * rp + rs * rs);
+  }
+
+  // pathtrace.metal:470-534; returns valid, writes direction and eta scale.
+  __device__ __noinline__ bool sample_dielectric(float wox, float woy, float woz, float nx, float ny, float nz,
+                                                 float cdx, float cdy, float cdz, float ior, bool front, float rough,
+                                                 float alpha2, float& o_x, float& o_y, float& o_z, float& eta_scale) {
+    bool valid = true;
+    float eta_i = 1.0f, eta_t = ior;
+    if (!front) { eta_i = ior; eta_t = 1.0f; }
+    float hx, hy, hz;
+    if (rough <= 0.0201f) { hx = nx; hy = ny; hz = nz; }
+    else {
+      sample_ggx_half(alpha2, nx, ny, nz, hx, hy, hz);
+      float md = wox * hx + (woy * hy + woz * hz);
+      if (!(md > 1e-8f)) valid = false;
+    }
+    float cos_m = wox * hx + (woy * hy + woz * hz);
+    if (cos_m < 0.0f) { hx = -hx; hy = -hy; hz = -hz; cos_m = -cos_m; }
+    if (cos_m > 1.0f) cos_m = 1.0f;
+    float fres = fresnel(cos_m, eta_i, eta_t);
+    float eta = eta_i / eta_t;
+    float s2 = eta * eta * (1.0f - cos_m * cos_m);
+    if (s2 >= 1.0f || U() < fres) {
+      o_x = 2.0f * cos_m * hx - wox;
+      o_y = 2.0f * cos_m * hy - woy;
+      o_z = 2.0f * cos_m * hz - woz;
+      eta_scale = 1.0f;
+    } else {
+      float cos_t = sqrtf(1.0f - s2);
+      o_x = eta * cdx + hx * (eta * cos_m - cos_t);
+      o_y = eta * cdy + hy * (eta * cos_m - cos_t);
+      o_z = eta * cdz + hz * (eta * cos_m - cos_t);
+      eta_scale = eta * eta;
+    }
+    {
+      float d = 1.0f / sqrtf(o_x * o_x + o_y * o_y + o_z * o_z);
+      o_x *= d; o_y *= d; o_z *= d;
+    }
+    if (rough > 0.0201f) {
+      float cos_i = fabsf(o_x * nx + (o_y * ny + o_z * nz));
+      float cos_o = fabsf(wox * nx + (woy * ny + woz * nz));
+      float cos_h = fabsf(hx * nx + (hy * ny + hz * nz));
+      float vo_h = fabsf(wox * hx + (woy * hy + woz * hz));
+      if (cos_i > 1e-8f && cos_o > 1e-8f && cos_h > 1e-8f && vo_h > 1e-8f) {
+        float g1 = 2.0f * cos_o / (cos_o + sqrtf(cos_o * cos_o + alpha2 * (1.0f - cos_o * cos_o)));
+        float g2 = 2.0f * cos_i / (cos_i + sqrtf(cos_i * cos_i + alpha2 * (1.0f - cos_i * cos_i)));
+        float w = g1 * g2 * vo_h / (cos_o * cos_h);
+        if (w > 10.0f) w = 10.0f;
+        eta_scale *= w;
+      } else {
+        valid = false;
+      }
+    }
+    return valid;
+  }
+
+  // pathtrace.metal:552-728
+  __device__ __noinline__ void pathtrace(float ox, float oy, float oz, float dx, float dy, float dz, int max_bounces,
+                                         float& out_r, float& out_g, float& out_b) {
+    float accr = 0, accg = 0, accb = 0, thr_r = 1, thr_g = 1, thr_b = 1;
+    int bounce = 0, prev_delta = 1;
+    float last_pdf = 0, prev_sumW = 0;
+    uint32_t prev_M = 0;
+    float prev_br = 0, prev_bg = 0, prev_bb = 0, prev_cos = 0;
+    const float LT = p.light_total;
+    for (int b = 0; b < max_bounces; ++b) {
+      Hit hit = cast_alpha_ray(ox, oy, oz, dx, dy, dz, kFar);
+      if (hit.tri < 0) break;
+      float pnx = hit.nix, pny = hit.niy, pnz = hit.niz;
+      float geom = hit.ngx * pnx + (hit.ngy * pny + hit.ngz * pnz);
+      if (geom < 0.0f) { pnx = -pnx; pny = -pny; pnz = -pnz; }
+      float ndot = dx * pnx + (dy * pny + dz * pnz);
+      bool front = true;
+      if (ndot > 0.0f) { pnx = -pnx; pny = -pny; pnz = -pnz; front = false; }
+      float wox = -dx, woy = -dy, woz = -dz;
+      float rough = hit.rough;
+      if (rough < 0.0f) rough = 0.0f;
+      if (rough > 1.0f) rough = 1.0f;
+      if (rough < 0.02f) rough = 0.02f;
+      float alpha = rough * rough;
+      float alpha2 = alpha * alpha;
+      const rm_triangle& lt = s.tris[hit.tri];
+      float metallic = lt.metallic;
+      if (metallic < 0.0f) metallic = 0.0f;
+      if (metallic > 1.0f) metallic = 1.0f;
+      if (bounce == 0 || prev_delta == 1) {
+        accr += hit.er * thr_r; accg += hit.eg * thr_g; accb += hit.eb * thr_b;
+      } else {
+        float lx = hit.px - ox, ly = hit.py - oy, lz = hit.pz - oz;
+        float dist2 = lx * lx + ly * ly + lz * lz;
+        float dist = sqrtf(dist2);
+        float pl = 1e30f;
+        float lta = lt.alpha;
+        if (dist > 1e-20f && last_pdf > 1e-20f && prev_M > 0 && prev_sumW > 1e-20f) {
+          float ph = lum3(hit.er * prev_br * prev_cos * lta, hit.eg * prev_bg * prev_cos * lta,
+                          hit.eb * prev_bb * prev_cos * lta);
+          if (ph > 1e-20f) pl = float(prev_M) * ph / prev_sumW;
+          else {
+            float inv = 1.0f / dist;
+            float lxn = lx * inv, lyn = ly * inv, lzn = lz * inv;
+            float cos_l = -(lt.nn.x * lxn + (lt.nn.y * lyn + lt.nn.z * lzn));
+            if (cos_l > 1e-8f) {
+              float lum = lum3(lt.er, lt.eg, lt.eb);
+              if (lum < 1e-6f) lum = 1e-6f;
+              pl = dist2 * lum / (cos_l * LT);
+            }
+          }
+        } else if (dist > 1e-20f && last_pdf > 1e-20f) {
+          float inv = 1.0f / dist;
+          lx *= inv; ly *= inv; lz *= inv;
+          float cos_l = -(lt.nn.x * lx + (lt.nn.y * ly + lt.nn.z * lz));
+          if (cos_l > 1e-8f) {
+            float lum = lum3(lt.er, lt.eg, lt.eb);
+            if (lum < 1e-6f) lum = 1e-6f;
+            pl = dist2 * lum / (cos_l * LT);
+          }
+        }
+        float w = p.nomis ? 0.0f : ((last_pdf + pl > 1e-20f) ? last_pdf / (last_pdf + pl) : 0.0f);
+        accr += hit.er * thr_r * w; accg += hit.eg * thr_g * w; accb += hit.eb * thr_b * w;
+      }
+      if (hit.ior > 1.0001f) {
+        float nx2, ny2, nz2, eta_scale;
+        bool valid = sample_dielectric(wox, woy, woz, pnx, pny, pnz, dx, dy, dz, hit.ior, front, rough, alpha2, nx2,
+                                       ny2, nz2, eta_scale);
+        if (!valid) break;
+        thr_r *= eta_scale; thr_g *= eta_scale; thr_b *= eta_scale;
+        float sg = 1.0f;
+        if (nx2 * pnx + (ny2 * pny + nz2 * pnz) < 0.0f) sg = -1.0f;
+        ox = hit.px + pnx * 0.001f * sg;
+        oy = hit.py + pny * 0.001f * sg;
+        oz = hit.pz + pnz * 0.001f * sg;
+        dx = nx2; dy = ny2; dz = nz2;
+        prev_delta = 1;
+        prev_sumW = 0; prev_M = 0;
+      } else {
+        float spec_prob = 0.05f + 0.95f * metallic;
+        if (spec_prob > 0.98f) spec_prob = 0.98f;
+        if (metallic >= 0.999f) spec_prob = 1.0f;
+        float cur_sumW = 0;
+        uint32_t cur_M = 0;
+        {
+          float dlr, dlg, dlb;
+          direct_lighting(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob, hit.ar,
+                          hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M);
+          accr += dlr * thr_r; accg += dlg * thr_g; accb += dlb * thr_b;
+        }
+        float nx2, ny2, nz2;
+        if (U() < spec_prob) {
+          float hx, hy, hz;
+          sample_ggx_half(alpha2, pnx, pny, pnz, hx, hy, hz);
+          float md = wox * hx + (woy * hy + woz * hz);
+          if (!(md > 1e-8f)) break;
+          nx2 = 2.0f * md * hx - wox;
+          ny2 = 2.0f * md * hy - woy;
+          nz2 = 2.0f * md * hz - woz;
+          prev_delta = (rough <= 0.0201f) ? 1 : 0;
+        } else {
+          sample_cosine(pnx, pny, pnz, nx2, ny2, nz2);
+          prev_delta = 0;
+        }
+        float ncos = nx2 * pnx + (ny2 * pny + nz2 * pnz);
+        if (!(ncos > 1e-8f)) break;
+        {
+          float d = 1.0f / sqrtf(nx2 * nx2 + ny2 * ny2 + nz2 * nz2);
+          nx2 *= d; ny2 *= d; nz2 *= d;
+        }
+        Bsdf e = eval_bsdf(nx2, ny2, nz2, wox, woy, woz, pnx, pny, pnz, alpha2, metallic, spec_prob, hit.ar, hit.ag,
+                           hit.ab);
+        if (!(e.pdf > 1e-12f)) break;
+        last_pdf = e.pdf;
+        float cos_i = nx2 * pnx + (ny2 * pny + nz2 * pnz);
+        thr_r *= e.r * cos_i / e.pdf;
+        thr_g *= e.g * cos_i / e.pdf;
+        thr_b *= e.b * cos_i / e.pdf;
+        prev_sumW = cur_sumW; prev_M = cur_M;
+        prev_br = e.r; prev_bg = e.g; prev_bb = e.b; prev_cos = cos_i;
+        ox = hit.px + pnx * 0.001f;
+        oy = hit.py + pny * 0.001f;
+        oz = hit.pz + pnz * 0.001f;
+        dx = nx2; dy = ny2; dz = nz2;
+      }
+      if (thr_r < 0.0f) thr_r = 0.0f;
+      if (thr_g < 0.0f) thr_g = 0.0f;
+      if (thr_b < 0.0f) thr_b = 0.0f;
+      float mx = fmaxf(thr_r, thr_g);
+      mx = fmaxf(mx, thr_b);
+      if (!(mx >= 1e-12f)) break;
+      if (p.rr && bounce >= 1) {
+        float rr = mx;
+        if (rr < 0.05f) rr = 0.05f;
+        if (rr > 0.9f) rr = 0.9f;
+        if (!(U() <= rr)) break;
+        float ir = 1.0f / rr;
+        thr_r *= ir; thr_g *= ir; thr_b *= ir;
+      }
+      bounce++;
+    }
+    out_r = accr; out_g = accg; out_b = accb;
+  }
+
+  // pathtrace.metal:729-737
+  __device__ __forceinline__ void sample_sensor(float sx, float sy, int max_bounces, float& r, float& g, float& b) {
+    const rm_camera& cam = p.camera;
+    float focal2 = cam.focal * cam.focal;
+    float dist = 1.0f / sqrtf(sx * sx + (sy * sy + focal2));
+    float tx = sx * dist, ty = sy * dist, tz = cam.focal * dist;
+    float dx = tx * cam.m0 + (ty * cam.m1 + tz * cam.m2);
+    float dy = tx * cam.m3 + (ty * cam.m4 + tz * cam.m5);
+    float dz = tx * cam.m6 + (ty * cam.m7 + tz * cam.m8);
+    pathtrace(cam.x, cam.y, cam.z, dx, dy, dz, max_bounces, r, g, b);
+  }
+
+  // pathtrace.metal:754-755
+  __device__ __forceinline__ void jitter(uint32_t x, uint32_t y, float& sx, float& sy) {
+    const float res = p.resolution;
+    sx = float(x) + 1e-12f + (res - 2e-12f) * U() - float(p.width) * 0.5f;
+    sy = float(p.height) * 0.5f - (float(y) + 1e-12f + (res - 2e-12f) * U());
+  }
+};
+
+__device__ __forceinline__ uint8_t tonemap8(float c) {
+  float v = floorf(c / (c + 1.0f) * 255.0f);
+  v = fminf(fmaxf(v, 0.0f), 255.0f);
+  return uint8_t(v);
+}
+
+}  // namespace rmd

@@ -1,0 +1,69 @@
+// rm_launch.h - host-side launch wrappers shared by the .cu translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rm_device.cuh"
+
+namespace rmd {
+
+// rm_kernels.cu
+cudaError_t launch_render_paths(int lanes, const Scene& s, const Params& p, uint64_t seed, float* hdr, uint8_t* rgb,
+                                uint32_t* dbg, unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+// stage 0 generate, 1 spatial (temporal + spatial reuse), 2 shade
+cudaError_t launch_restir_stage(int stage, const Scene& s, const Params& p, uint64_t seed, const GBufSoA& gb,
+                                const ResSoA& ri, const ResSoA& rm, const GBufSoA& hg, const ResSoA& hr, float* hdr,
+                                uint32_t* dbg, unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+cudaError_t launch_trace(const Scene& s, const float* rays, int n, int any_hit, int32_t* tri, float* t, float* u,
+                         float* v, uint32_t* err, cudaStream_t st);
+
+// rm_denoise.cu
+// stage 0 temporal (in + hist_in -> out), 1 / 2 a-trous step 0 / 1 (in -> out, + RGB8 when rgb != nullptr)
+cudaError_t launch_denoise_stage(int stage, const Params& p, const GBufSoA& gb, const GBufSoA& hg, const float* in,
+                                 const float* hist_in, float* out, uint8_t* rgb, cudaStream_t st);
+cudaError_t launch_tonemap(const float* hdr, uint8_t* rgb, uint32_t npix, cudaStream_t st);
+
+// rm_bvh.cu ------------------------------------------------------------------
+
+// Growable device allocation.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t cap = 0;
+  cudaError_t reserve(size_t bytes);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Device-resident BVH + triangle geometry of one scene.
+struct DevBvh {
+  DevBuf records;   // float4 x 4 per internal record
+  DevBuf parents;   // int per record: (parent << 1) | slot, -1 for the root
+  DevBuf counters;  // int per record, refit arrival counts
+  DevBuf order;     // int per leaf slot: original triangle index (leaf order)
+  DevBuf tgeo;      // float4 x 3 per triangle in leaf order
+  // LBVH temporaries
+  DevBuf keys, keys_alt, vals_alt, knodes, kbox, kcount, ranges, temp, bounds, depth;
+  int n_records = 0;
+  int n_tris = 0;
+  int max_depth = 0;
+};
+
+// Convert and validate a caller BVH (reference Scene::nodes layout) on the
+// host, then upload it.  Returns false with a message on invalid input.
+bool convert_caller_bvh(const rm_bvh_node* nodes, int n_nodes, const int32_t* bvh_tri, int n_tris, DevBvh& out,
+                        cudaStream_t st, std::string& err);
+// Build an LBVH on the device from the device triangle array.
+cudaError_t build_lbvh(const rm_triangle* d_tris, int n_tris, int leaf_max, DevBvh& out, cudaStream_t st,
+                       std::string& err);
+// Write the leaf-ordered Moller-Trumbore records from the triangles.
+cudaError_t pack_tgeo(const rm_triangle* d_tris, DevBvh& bvh, cudaStream_t st);
+// Refit all boxes bottom-up from the current triangle positions.
+cudaError_t refit_bvh(const rm_triangle* d_tris, DevBvh& bvh, cudaStream_t st);
+// 64-bit content hash of a device byte range (order-sensitive per 8-byte word).
+cudaError_t device_hash(const void* d_bytes, size_t n_bytes, unsigned long long* d_out, cudaStream_t st);
+
+}  // namespace rmd

@@ -1,0 +1,740 @@
+// rmcuda_api.cu - the C ABI of include/rmcuda.h: context, scene upload, and
+// the per-frame policy of the reference's render_image_metal
+// (src/engine/metal.mm:95-414), re-expressed for CUDA streams.
+//
+// Differences in mechanism, not in results:
+//  * the scene is uploaded once per call into grow-only device buffers (the
+//    reference re-packs into Metal shared buffers, metal.mm:171-186); the
+//    BVH is either the caller's (validated and converted, rm_bvh.cu) or built
+//    on the device;
+//  * the scene hash that guards temporal reuse (metal.mm:241-248) is computed
+//    on the device over the uploaded bytes;
+//  * the plain path runs the lane kernels (metal.mm:390-394) and the ReSTIR
+//    path runs generate / spatial / shade / denoise (metal.mm:287-366) as
+//    kernels on one stream, then one device-to-host copy of the RGB8 image.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "rm_launch.h"
+#include "rmcuda.h"
+
+using namespace rmd;
+
+namespace {
+
+constexpr const char* kUnavailable = "Metal backend is not available in this build";
+constexpr const char* kInvalidDims = "Invalid Metal render dimensions or sample count";
+constexpr int kLbvhLeaf = 4;
+
+void set_err(char* err, size_t cap, const std::string& m) {
+  if (err && cap) std::snprintf(err, cap, "%s", m.c_str());
+}
+
+struct GBufSet {
+  DevBuf pos_kind, nor_rough, alb_met, wo_ior, emi;
+  cudaError_t reserve(size_t npix) {
+    cudaError_t e;
+    for (DevBuf* b : {&pos_kind, &nor_rough, &alb_met, &wo_ior, &emi})
+      if ((e = b->reserve(npix * sizeof(float4))) != cudaSuccess) return e;
+    return cudaSuccess;
+  }
+  GBufSoA view() const {
+    return GBufSoA{pos_kind.as<float4>(), nor_rough.as<float4>(), alb_met.as<float4>(), wo_ior.as<float4>(),
+                   emi.as<float4>()};
+  }
+  void release() { for (DevBuf* b : {&pos_kind, &nor_rough, &alb_met, &wo_ior, &emi}) b->release(); }
+};
+struct ResSet {
+  DevBuf lp, ln, le, wm;
+  cudaError_t reserve(size_t npix) {
+    cudaError_t e;
+    for (DevBuf* b : {&lp, &ln, &le, &wm})
+      if ((e = b->reserve(npix * sizeof(float4))) != cudaSuccess) return e;
+    return cudaSuccess;
+  }
+  ResSoA view() const { return ResSoA{lp.as<float4>(), ln.as<float4>(), le.as<float4>(), wm.as<float4>()}; }
+  void release() { for (DevBuf* b : {&lp, &ln, &le, &wm}) b->release(); }
+};
+
+struct Env {
+  bool noadapt = false, nomis = false, restir_off = false, denoise_off = false, temporal_off = false;
+  bool have_cand = false, have_spatial = false;
+  int cand = 0, spatial = 0;
+};
+
+Env read_env(uint32_t flags) {
+  Env e;
+  if (flags & RM_FLAG_NO_ENV) {
+    e.noadapt = flags & RM_FLAG_NOADAPT;
+    e.nomis = flags & RM_FLAG_NOMIS;
+    e.restir_off = flags & RM_FLAG_RESTIR_OFF;
+    e.denoise_off = flags & RM_FLAG_DENOISE_OFF;
+    e.temporal_off = flags & RM_FLAG_TEMPORAL_OFF;
+    return e;
+  }
+  auto eq0 = [](const char* v) { return v && std::string(v) == "0"; };
+  e.noadapt = std::getenv("UOW2_NOADAPT") != nullptr;
+  e.nomis = std::getenv("UOW2_NOMIS") != nullptr;
+  e.restir_off = eq0(std::getenv("RAYMOTION_RESTIR"));
+  e.denoise_off = eq0(std::getenv("RAYMOTION_DENOISE"));
+  e.temporal_off = eq0(std::getenv("RAYMOTION_RESTIR_TEMPORAL"));
+  if (const char* v = std::getenv("RAYMOTION_RESTIR_CANDIDATES")) { e.have_cand = true; e.cand = std::atoi(v); }
+  if (const char* v = std::getenv("RAYMOTION_RESTIR_SPATIAL")) { e.have_spatial = true; e.spatial = std::atoi(v); }
+  return e;
+}
+
+}  // namespace
+
+struct rmcuda_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  std::mutex mu;
+  // resident scene
+  DevBuf tris, lights, cdf, texels;
+  DevBvh bvh;
+  int n_tris = 0, n_lights = 0;
+  float light_total = 0;
+  bool opaque = true;
+  bool have_scene = false;
+  int refits = 0;
+  bool device_built = false;
+  unsigned long long scene_hash = 0;
+  // frame buffers
+  GBufSet gb, hg;
+  ResSet rinit, rmerged, hres;
+  DevBuf hdr, tmp_a, tmp_b, hist_col, rgb, dbg, hash_out;
+  DevBuf ctr, err;
+  size_t npix_cap = 0;
+  // temporal history (metal.mm:35-40)
+  rm_camera hist_cam{};
+  int hist_w = 0, hist_h = 0;
+  uint64_t hist_seed = 0;
+  unsigned long long hist_hash = 0;
+  bool hist_valid = false, have_hist_bufs = false;
+  // last frame
+  int last_chain = 0;
+  uint64_t frames = 0;
+  uint64_t launches = 0;
+  float* last_final = nullptr;  // device pointer of the last frame's tonemap input
+  int last_w = 0, last_h = 0;
+  // per-stage CUDA-event timing (rmcuda_profile)
+  bool profiling = false;
+  struct Pending { int stage; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  double stage_ms[RM_STAGE_COUNT] = {};
+  uint64_t stage_n[RM_STAGE_COUNT] = {};
+};
+
+namespace {
+
+std::string cuda_msg(const char* what, cudaError_t e) { return std::string(what) + ": " + cudaGetErrorString(e); }
+
+// Launch through `fn`, bracketed by events on the context stream when profiling.
+template <class Fn> cudaError_t staged(rmcuda_ctx* c, int stage, Fn&& fn) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (c->profiling && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess)
+    cudaEventRecord(a, c->stream);
+  cudaError_t e = fn();
+  if (a && b) {
+    cudaEventRecord(b, c->stream);
+    c->pending.push_back({stage, a, b});
+  }
+  c->launches += 1;
+  return e;
+}
+
+void resolve_pending(rmcuda_ctx* c) {
+  for (auto& pe : c->pending) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(pe.b) == cudaSuccess && cudaEventElapsedTime(&ms, pe.a, pe.b) == cudaSuccess) {
+      c->stage_ms[pe.stage] += ms;
+      c->stage_n[pe.stage] += 1;
+    }
+    cudaEventDestroy(pe.a);
+    cudaEventDestroy(pe.b);
+  }
+  c->pending.clear();
+}
+
+Scene scene_view(const rmcuda_ctx* c) {
+  Scene s;
+  s.tris = c->tris.as<rm_triangle>();
+  s.tgeo = c->bvh.tgeo.as<float4>();
+  s.nodes = c->bvh.records.as<float4>();
+  s.n_nodes = c->n_tris > 0 ? c->bvh.n_records : 0;
+  s.lights = c->lights.as<int32_t>();
+  s.cdf = c->cdf.as<float>();
+  s.n_lights = c->n_lights;
+  s.light_total = c->light_total;
+  s.texels = c->texels.as<rm_vec3>();
+  return s;
+}
+
+// Validate and upload one scene; build or convert its BVH.
+int upload_scene(rmcuda_ctx* c, const rm_scene_view* sv, std::string& msg) {
+  if (!sv || sv->n_tris < 0 || sv->n_lights < 0 || sv->n_texels < 0 || (sv->n_tris > 0 && !sv->tris) ||
+      (sv->n_lights > 0 && (!sv->light_tri || !sv->light_cdf)) || (sv->n_texels > 0 && !sv->texels)) {
+    msg = "invalid scene view";
+    return RM_ERR_INVALID;
+  }
+  bool opaque = true;
+  for (int i = 0; i < sv->n_tris; ++i) {
+    const rm_triangle& t = sv->tris[i];
+    if (!(t.alpha >= 1.0f)) opaque = false;
+    if (t.texture_offset >= 0) {
+      if (t.texture_width <= 0 || t.texture_height <= 0 ||
+          int64_t(t.texture_offset) + int64_t(t.texture_width) * t.texture_height > sv->n_texels) {
+        msg = "triangle texture outside the texel array";
+        return RM_ERR_INVALID;
+      }
+    }
+  }
+  for (int i = 0; i < sv->n_lights; ++i)
+    if (sv->light_tri[i] < 0 || sv->light_tri[i] >= sv->n_tris) { msg = "light index out of range"; return RM_ERR_INVALID; }
+  cudaStream_t st = c->stream;
+  cudaError_t e;
+  const size_t tb = size_t(sv->n_tris) * sizeof(rm_triangle);
+  if ((e = c->tris.reserve(tb)) != cudaSuccess || (e = c->lights.reserve(size_t(sv->n_lights) * 4)) != cudaSuccess ||
+      (e = c->cdf.reserve(size_t(sv->n_lights) * 4)) != cudaSuccess ||
+      (e = c->texels.reserve(size_t(sv->n_texels) * sizeof(rm_vec3))) != cudaSuccess) {
+    msg = cuda_msg("Metal scene buffer allocation failed", e);
+    return RM_ERR_ALLOC;
+  }
+  if ((tb && (e = cudaMemcpyAsync(c->tris.ptr, sv->tris, tb, cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+      (sv->n_lights &&
+       (e = cudaMemcpyAsync(c->lights.ptr, sv->light_tri, size_t(sv->n_lights) * 4, cudaMemcpyHostToDevice, st)) !=
+           cudaSuccess) ||
+      (sv->n_lights &&
+       (e = cudaMemcpyAsync(c->cdf.ptr, sv->light_cdf, size_t(sv->n_lights) * 4, cudaMemcpyHostToDevice, st)) !=
+           cudaSuccess) ||
+      (sv->n_texels && (e = cudaMemcpyAsync(c->texels.ptr, sv->texels, size_t(sv->n_texels) * sizeof(rm_vec3),
+                                            cudaMemcpyHostToDevice, st)) != cudaSuccess)) {
+    msg = cuda_msg("scene upload failed", e);
+    return RM_ERR_CUDA;
+  }
+  c->n_tris = sv->n_tris;
+  c->n_lights = sv->n_lights;
+  c->light_total = sv->light_total;
+  c->opaque = opaque;
+  c->refits = 0;
+  c->have_scene = false;
+  if (sv->n_tris > 0 && sv->nodes && sv->n_nodes == 0) {
+    // caller passed an empty BVH: every ray misses, as with params.nodes == 0
+    // in the reference (pathtrace.metal:121)
+    c->bvh.n_records = 0;
+    c->bvh.n_tris = 0;
+    c->device_built = false;
+  } else if (sv->n_tris > 0) {
+    bool converted = false;
+    if (sv->nodes && sv->n_nodes > 0) {
+      std::string berr;
+      if (convert_caller_bvh(sv->nodes, sv->n_nodes, sv->bvh_tri, sv->n_tris, c->bvh, st, berr)) {
+        converted = true;
+      } else if (berr.find("deeper") == std::string::npos) {
+        msg = berr;
+        return RM_ERR_BVH;
+      }
+      if (converted && (e = pack_tgeo(c->tris.as<rm_triangle>(), c->bvh, st)) != cudaSuccess) {
+        msg = cuda_msg("BVH packing failed", e);
+        return RM_ERR_CUDA;
+      }
+    }
+    c->device_built = !converted;
+    if (!converted) {
+      std::string berr;
+      if ((e = build_lbvh(c->tris.as<rm_triangle>(), sv->n_tris, kLbvhLeaf, c->bvh, st, berr)) != cudaSuccess) {
+        msg = berr.empty() ? cuda_msg("device BVH build failed", e) : berr;
+        return RM_ERR_CUDA;
+      }
+    }
+  } else {
+    c->bvh.n_records = 0;
+    c->bvh.n_tris = 0;
+  }
+  c->have_scene = true;
+  return RM_OK;
+}
+
+struct Plan {
+  Params p;
+  int lanes = 1;
+  bool use_spatial = false;
+  bool denoise = true;
+  bool temporal_off = false;
+};
+
+// metal.mm:146-170, :236-237, :390-394
+Plan make_plan(const rmcuda_ctx* c, const rm_camera& cam, const rm_config& cfg) {
+  Env env = read_env(cfg.flags);
+  Plan pl;
+  Params& p = pl.p;
+  std::memset(&p, 0, sizeof(p));
+  p.camera = cam;
+  p.width = cfg.width; p.height = cfg.height; p.spp = cfg.spp; p.bounces = cfg.max_bounces;
+  p.nodes = c->n_tris > 0 ? c->bvh.n_records : 0;
+  p.lights = c->n_lights; p.light_total = c->light_total;
+  p.resolution = cfg.resolution; p.clamp_value = cfg.clamp; p.adapt_rel = cfg.adapt_rel; p.adapt_abs = cfg.adapt_abs;
+  p.adapt_min = env.noadapt ? 0 : cfg.adapt_min;
+  p.adapt_step = cfg.adapt_step > 0 ? cfg.adapt_step : 8;
+  p.opaque = c->opaque ? 1 : 0;
+  p.nomis = env.nomis ? 1 : 0;
+  p.restir_candidates = env.restir_off ? 1 : (cfg.restir_candidates > 0 ? cfg.restir_candidates : 1);
+  p.restir_candidates = std::min(32, std::max(1, p.restir_candidates));
+  p.restir_spatial = env.restir_off ? 0 : (cfg.restir_spatial > 0 ? cfg.restir_spatial : 0);
+  p.restir_spatial = std::min(8, std::max(0, p.restir_spatial));
+  p.restir_mcap = cfg.restir_mcap > 0 ? cfg.restir_mcap : 128;
+  p.restir_radius = cfg.restir_radius > 0 ? cfg.restir_radius : 16.0f;
+  if (env.have_cand) p.restir_candidates = std::max(1, env.cand);
+  if (env.have_spatial) p.restir_spatial = std::max(0, env.spatial);
+  p.rr = (cfg.flags & RM_FLAG_NO_RR) ? 0 : 1;
+  const size_t pixels = size_t(cfg.width) * size_t(cfg.height);
+  const size_t restir_bytes = pixels * (76 + 2 * 60);  // reference record sizes, metal.mm:236
+  pl.use_spatial = p.restir_spatial > 0 && p.lights > 0 && p.bounces > 0 && p.opaque &&
+                   restir_bytes <= size_t(512) * 1024 * 1024;
+  pl.denoise = !env.denoise_off;
+  pl.temporal_off = env.temporal_off;
+  if (cfg.spp >= 8 && (p.adapt_min <= 0 || p.adapt_step % 8 == 0)) pl.lanes = 8;
+  if (cfg.spp >= 32 && (p.adapt_min <= 0 || p.adapt_step % 32 == 0)) pl.lanes = 32;
+  return pl;
+}
+
+cudaError_t ensure_frame(rmcuda_ctx* c, size_t npix, bool restir) {
+  cudaError_t e;
+  if ((e = c->hdr.reserve(npix * 12)) != cudaSuccess || (e = c->rgb.reserve(npix * 3)) != cudaSuccess ||
+      (e = c->dbg.reserve(npix * 8)) != cudaSuccess)
+    return e;
+  if (restir) {
+    if ((e = c->gb.reserve(npix)) != cudaSuccess || (e = c->rinit.reserve(npix)) != cudaSuccess ||
+        (e = c->rmerged.reserve(npix)) != cudaSuccess || (e = c->tmp_a.reserve(npix * 12)) != cudaSuccess ||
+        (e = c->tmp_b.reserve(npix * 12)) != cudaSuccess ||
+        (e = c->hist_col.reserve(npix * 12)) != cudaSuccess || (e = c->hg.reserve(npix)) != cudaSuccess ||
+        (e = c->hres.reserve(npix)) != cudaSuccess)
+      return e;
+  }
+  return cudaSuccess;
+}
+
+// Enqueue one frame of the resident scene.  d_rgb (device) receives the
+// image; the final linear radiance stays in c->last_final.
+int enqueue_frame(rmcuda_ctx* c, const rm_camera& cam, const rm_config& cfg, uint64_t seed, uint8_t* d_rgb,
+                  std::string& msg) {
+  if (cfg.width <= 0 || cfg.height <= 0 || cfg.spp <= 0 || cfg.max_bounces < 0 ||
+      size_t(cfg.width) * size_t(cfg.height) > 100000000) {
+    msg = kInvalidDims;
+    return RM_ERR_INVALID;
+  }
+  if (!c->have_scene) { msg = "no resident scene"; return RM_ERR_INVALID; }
+  Plan pl = make_plan(c, cam, cfg);
+  Params& p = pl.p;
+  const size_t npix = size_t(cfg.width) * size_t(cfg.height);
+  cudaStream_t st = c->stream;
+  cudaError_t e = ensure_frame(c, npix, pl.use_spatial);
+  if (e != cudaSuccess) {
+    msg = cuda_msg(pl.use_spatial ? "Metal ReSTIR buffer allocation failed" : "Metal image buffer allocation failed", e);
+    return RM_ERR_ALLOC;
+  }
+  Scene s = scene_view(c);
+  unsigned long long* ctr = c->ctr.as<unsigned long long>();
+  uint32_t* err = c->err.as<uint32_t>();
+  if (!pl.use_spatial) {
+    c->last_chain = pl.lanes;
+    e = staged(c, RM_STAGE_PLAIN, [&] {
+      return launch_render_paths(pl.lanes, s, p, seed, c->hdr.as<float>(), d_rgb, c->dbg.as<uint32_t>(),
+                                 ctr + 4 * RM_STAGE_PLAIN, err, st);
+    });
+    if (e != cudaSuccess) { msg = cuda_msg("render_paths launch failed", e); return RM_ERR_CUDA; }
+    c->last_final = c->hdr.as<float>();
+  } else {
+    c->last_chain = 2;
+    // scene hash over the uploaded triangle bytes (metal.mm:241-248)
+    if ((e = c->hash_out.reserve(8)) != cudaSuccess) { msg = cuda_msg("hash buffer", e); return RM_ERR_ALLOC; }
+    e = staged(c, RM_STAGE_HASH, [&] {
+      return device_hash(c->tris.ptr, size_t(c->n_tris) * sizeof(rm_triangle), c->hash_out.as<unsigned long long>(), st);
+    });
+    unsigned long long h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, c->hash_out.ptr, 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { msg = cuda_msg("scene hash failed", e); return RM_ERR_CUDA; }
+    uint32_t lt_bits;
+    std::memcpy(&lt_bits, &c->light_total, 4);
+    h ^= uint64_t(c->n_tris) * 0x9E3779B97F4A7C15ull ^ uint64_t(c->n_lights) * 0xBF58476D1CE4E5B9ull ^
+         uint64_t(lt_bits) * 0x94D049BB133111EBull;
+    const bool animated = (cfg.flags & RM_FLAG_ANIMATED_HISTORY) != 0;
+    bool have_hist = c->hist_valid && c->hist_w == cfg.width && c->hist_h == cfg.height && c->have_hist_bufs &&
+                     seed != c->hist_seed && (animated || h == c->hist_hash);
+    if (pl.temporal_off) have_hist = false;
+    p.hasHistory = have_hist ? 1 : 0;
+    p.prevCamera = c->hist_cam;
+    for (int stage = 0; stage < 3 && e == cudaSuccess; ++stage)
+      e = staged(c, RM_STAGE_GENERATE + stage, [&] {
+        return launch_restir_stage(stage, s, p, seed, c->gb.view(), c->rinit.view(), c->rmerged.view(), c->hg.view(),
+                                   c->hres.view(), c->hdr.as<float>(), c->dbg.as<uint32_t>(),
+                                   ctr + 4 * (RM_STAGE_GENERATE + stage), err, st);
+      });
+    if (e != cudaSuccess) { msg = cuda_msg("ReSTIR launch failed", e); return RM_ERR_CUDA; }
+    if (pl.denoise) {
+      // temporal(hdr, hist_col) -> tmp_a -> a-trous -> tmp_b -> a-trous + tonemap -> tmp_a
+      float* ins[3] = {c->hdr.as<float>(), c->tmp_a.as<float>(), c->tmp_b.as<float>()};
+      float* outs[3] = {c->tmp_a.as<float>(), c->tmp_b.as<float>(), c->tmp_a.as<float>()};
+      for (int stage = 0; stage < 3 && e == cudaSuccess; ++stage)
+        e = staged(c, RM_STAGE_TEMPORAL + stage, [&] {
+          return launch_denoise_stage(stage, p, c->gb.view(), c->hg.view(), ins[stage], c->hist_col.as<float>(),
+                                      outs[stage], stage == 2 ? d_rgb : nullptr, st);
+        });
+      if (e != cudaSuccess) { msg = cuda_msg("denoise launch failed", e); return RM_ERR_CUDA; }
+      c->last_final = c->tmp_a.as<float>();
+    } else {
+      if (d_rgb) {
+        e = staged(c, RM_STAGE_TONEMAP, [&] { return launch_tonemap(c->hdr.as<float>(), d_rgb, uint32_t(npix), st); });
+        if (e != cudaSuccess) { msg = cuda_msg("tonemap launch failed", e); return RM_ERR_CUDA; }
+      }
+      c->last_final = c->hdr.as<float>();
+    }
+    // publish history (metal.mm:374-385); buffers swap by ownership
+    std::swap(c->gb, c->hg);
+    std::swap(c->rmerged, c->hres);
+    if (pl.denoise) { std::swap(c->tmp_a, c->hist_col); c->last_final = c->hist_col.as<float>(); }
+    c->have_hist_bufs = true;
+    c->hist_cam = cam;
+    c->hist_w = cfg.width; c->hist_h = cfg.height;
+    c->hist_seed = seed; c->hist_hash = h;
+    c->hist_valid = true;
+  }
+  c->last_w = cfg.width;
+  c->last_h = cfg.height;
+  c->frames++;
+  return RM_OK;
+}
+
+int check_device_error(rmcuda_ctx* c, std::string& msg) {
+  uint32_t dev_err = 0;
+  cudaError_t e = cudaMemcpyAsync(&dev_err, c->err.ptr, 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) { msg = cuda_msg("Metal command buffer failed", e); return RM_ERR_CUDA; }
+  if (dev_err) {
+    cudaMemsetAsync(c->err.ptr, 0, 4, c->stream);
+    msg = "device error word " + std::to_string(dev_err) + " (traversal stack or loop bound exceeded)";
+    return RM_ERR_DEVICE;
+  }
+  return RM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rmcuda_version(void) { return "rmcuda 0.1 (sm_100a)"; }
+
+int rmcuda_create(rmcuda_ctx** out, int device, char* err, size_t errcap) {
+  if (!out) { set_err(err, errcap, "null output pointer"); return RM_ERR_INVALID; }
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) {
+    cudaGetLastError();
+    set_err(err, errcap, kUnavailable);
+    return RM_ERR_UNAVAILABLE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+    set_err(err, errcap, kUnavailable);
+    return RM_ERR_UNAVAILABLE;
+  }
+  auto* c = new rmcuda_ctx();
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = c->ctr.reserve(RM_STAGE_COUNT * 32);
+  if (e == cudaSuccess) e = c->err.reserve(4);
+  if (e == cudaSuccess) e = cudaMemset(c->ctr.ptr, 0, RM_STAGE_COUNT * 32);
+  if (e == cudaSuccess) e = cudaMemset(c->err.ptr, 0, 4);
+  if (e != cudaSuccess) {
+    set_err(err, errcap, cuda_msg("context creation failed", e));
+    delete c;
+    return RM_ERR_CUDA;
+  }
+  c->stream = c->own;
+  *out = c;
+  return RM_OK;
+}
+
+void rmcuda_destroy(rmcuda_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (DevBuf* b : {&c->tris, &c->lights, &c->cdf, &c->texels, &c->hdr, &c->tmp_a, &c->tmp_b, &c->hist_col, &c->rgb, &c->dbg,
+                    &c->hash_out, &c->ctr, &c->err, &c->bvh.records, &c->bvh.parents, &c->bvh.counters,
+                    &c->bvh.order, &c->bvh.tgeo, &c->bvh.keys, &c->bvh.keys_alt, &c->bvh.vals_alt, &c->bvh.knodes,
+                    &c->bvh.kbox, &c->bvh.kcount, &c->bvh.ranges, &c->bvh.temp, &c->bvh.bounds, &c->bvh.depth})
+    b->release();
+  c->gb.release(); c->hg.release();
+  c->rinit.release(); c->rmerged.release(); c->hres.release();
+  resolve_pending(c);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+}
+
+int rmcuda_set_stream(rmcuda_ctx* c, void* s, char* err, size_t errcap) {
+  if (!c) { set_err(err, errcap, "null context"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaStreamSynchronize(c->stream);
+  c->stream = s ? static_cast<cudaStream_t>(s) : c->own;
+  return RM_OK;
+}
+
+int rmcuda_scene_upload(rmcuda_ctx* c, const rm_scene_view* sv, char* err, size_t errcap) {
+  if (!c) { set_err(err, errcap, "null context"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  std::string msg;
+  int rc = upload_scene(c, sv, msg);
+  if (rc == RM_OK) {
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { msg = cuda_msg("scene upload failed", e); rc = RM_ERR_CUDA; }
+  }
+  if (rc != RM_OK) { c->hist_valid = false; set_err(err, errcap, msg); }
+  return rc;
+}
+
+int rmcuda_scene_update(rmcuda_ctx* c, const rm_triangle* tris, int32_t n, int32_t rebuild_every, char* err,
+                        size_t errcap) {
+  if (!c) { set_err(err, errcap, "null context"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (!c->have_scene || n != c->n_tris || (n > 0 && !tris)) {
+    set_err(err, errcap, "scene update needs a resident scene with the same triangle count");
+    return RM_ERR_INVALID;
+  }
+  cudaError_t e = cudaMemcpyAsync(c->tris.ptr, tris, size_t(n) * sizeof(rm_triangle), cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("scene update upload failed", e)); return RM_ERR_CUDA; }
+  bool opaque = true;
+  for (int i = 0; i < n; ++i)
+    if (!(tris[i].alpha >= 1.0f)) { opaque = false; break; }
+  c->opaque = opaque;
+  if (n == 0) return RM_OK;
+  if (rebuild_every > 0 && c->refits + 1 >= rebuild_every) {
+    std::string berr;
+    e = build_lbvh(c->tris.as<rm_triangle>(), n, kLbvhLeaf, c->bvh, c->stream, berr);
+    c->refits = 0;
+    c->device_built = true;
+    if (e != cudaSuccess) { set_err(err, errcap, berr.empty() ? cuda_msg("rebuild failed", e) : berr); return RM_ERR_CUDA; }
+  } else {
+    e = refit_bvh(c->tris.as<rm_triangle>(), c->bvh, c->stream);
+    c->refits++;
+    if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("refit failed", e)); return RM_ERR_CUDA; }
+  }
+  return RM_OK;
+}
+
+int rmcuda_render_resident_async(rmcuda_ctx* c, const rm_camera* cam, const rm_config* cfg, uint64_t seed,
+                                 uint8_t* d_rgb, float* d_hdr, char* err, size_t errcap) {
+  if (!c || !cam || !cfg) { set_err(err, errcap, "null argument"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  std::string msg;
+  int rc = enqueue_frame(c, *cam, *cfg, seed, d_rgb, msg);
+  if (rc == RM_OK && d_hdr) {
+    const size_t bytes = size_t(cfg->width) * size_t(cfg->height) * 12;
+    cudaError_t e = cudaMemcpyAsync(d_hdr, c->last_final, bytes, cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) { msg = cuda_msg("hdr copy failed", e); rc = RM_ERR_CUDA; }
+  }
+  if (rc != RM_OK) { c->hist_valid = false; set_err(err, errcap, msg); }
+  return rc;
+}
+
+int rmcuda_sync(rmcuda_ctx* c, char* err, size_t errcap) {
+  if (!c) { set_err(err, errcap, "null context"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  std::string msg;
+  int rc = check_device_error(c, msg);
+  if (rc != RM_OK) { c->hist_valid = false; set_err(err, errcap, msg); }
+  return rc;
+}
+
+int rmcuda_render(rmcuda_ctx* c, const rm_scene_view* sv, const rm_camera* cam, const rm_config* cfg, uint64_t seed,
+                  uint8_t* rgb, size_t rgb_cap, float* hdr, char* err, size_t errcap) {
+  if (!cfg || cfg->width <= 0 || cfg->height <= 0 || cfg->spp <= 0 || cfg->max_bounces < 0 ||
+      size_t(cfg->width) * size_t(cfg->height) > 100000000) {
+    set_err(err, errcap, kInvalidDims);
+    return RM_ERR_INVALID;
+  }
+  if (!c || !sv || !cam) { set_err(err, errcap, "null argument"); return RM_ERR_INVALID; }
+  const size_t npix = size_t(cfg->width) * size_t(cfg->height);
+  if (rgb && rgb_cap < npix * 3) { set_err(err, errcap, "rgb buffer too small"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  std::string msg;
+  int rc = upload_scene(c, sv, msg);
+  if (rc == RM_OK) {
+    cudaError_t e = c->rgb.reserve(npix * 3);
+    if (e != cudaSuccess) { msg = cuda_msg("Metal image buffer allocation failed", e); rc = RM_ERR_ALLOC; }
+  }
+  if (rc == RM_OK) rc = enqueue_frame(c, *cam, *cfg, seed, c->rgb.as<uint8_t>(), msg);
+  if (rc == RM_OK) {
+    cudaError_t e = cudaSuccess;
+    if (rgb) e = cudaMemcpyAsync(rgb, c->rgb.ptr, npix * 3, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && hdr) e = cudaMemcpyAsync(hdr, c->last_final, npix * 12, cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) { msg = cuda_msg("image readback failed", e); rc = RM_ERR_CUDA; }
+  }
+  if (rc == RM_OK) rc = check_device_error(c, msg);
+  if (rc != RM_OK) {
+    c->hist_valid = false;  // CacheGuard, metal.mm:105-108
+    cudaGetLastError();
+    set_err(err, errcap, msg);
+  }
+  return rc;
+}
+
+int rmcuda_trace(rmcuda_ctx* c, const float* d_rays, int32_t n, int32_t any_hit, int32_t* d_tri, float* d_t,
+                 float* d_u, float* d_v, char* err, size_t errcap) {
+  if (!c || (n > 0 && (!d_rays || !d_tri)) || n < 0) { set_err(err, errcap, "invalid trace arguments"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (!c->have_scene) { set_err(err, errcap, "no resident scene"); return RM_ERR_INVALID; }
+  cudaError_t e = launch_trace(scene_view(c), d_rays, n, any_hit, d_tri, d_t, d_u, d_v, c->err.as<uint32_t>(), c->stream);
+  if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("trace launch failed", e)); return RM_ERR_CUDA; }
+  std::string msg;
+  int rc = check_device_error(c, msg);
+  if (rc != RM_OK) set_err(err, errcap, msg);
+  return rc;
+}
+
+int rmcuda_debug_read(rmcuda_ctx* c, int32_t which, void* host, size_t cap, char* err, size_t errcap) {
+  if (!c || !host) { set_err(err, errcap, "null argument"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  const size_t npix = size_t(c->last_w) * size_t(c->last_h);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("sync failed", e)); return RM_ERR_CUDA; }
+  auto fetch = [&](const DevBuf& b, std::vector<float4>& v) {
+    v.resize(npix);
+    return cudaMemcpy(v.data(), b.ptr, npix * sizeof(float4), cudaMemcpyDeviceToHost);
+  };
+  if (which == 0 || which == 1 || which == 2) {
+    // after a ReSTIR frame the just-written buffers were swapped into the history slots
+    const size_t rec = which == 0 ? 76 : 60;
+    if (cap < npix * rec) { set_err(err, errcap, "buffer too small"); return RM_ERR_INVALID; }
+    unsigned char* out = static_cast<unsigned char*>(host);
+    std::vector<float4> a, b, cc, d, f;
+    if (which == 0) {
+      const GBufSet& g = c->hg;
+      if ((e = fetch(g.pos_kind, a)) != cudaSuccess || (e = fetch(g.nor_rough, b)) != cudaSuccess ||
+          (e = fetch(g.alb_met, cc)) != cudaSuccess || (e = fetch(g.wo_ior, d)) != cudaSuccess ||
+          (e = fetch(g.emi, f)) != cudaSuccess) {
+        set_err(err, errcap, cuda_msg("read failed", e));
+        return RM_ERR_CUDA;
+      }
+      for (size_t i = 0; i < npix; ++i) {
+        float r[19] = {a[i].x, a[i].y, a[i].z, b[i].x, b[i].y, b[i].z, cc[i].x, cc[i].y, cc[i].z, d[i].x,
+                       d[i].y, d[i].z, f[i].x, f[i].y, f[i].z, b[i].w, cc[i].w, d[i].w, a[i].w};
+        std::memcpy(out + i * 76, r, 76);
+      }
+    } else {
+      const ResSet& r = which == 1 ? c->rinit : c->hres;
+      if ((e = fetch(r.lp, a)) != cudaSuccess || (e = fetch(r.ln, b)) != cudaSuccess ||
+          (e = fetch(r.le, cc)) != cudaSuccess || (e = fetch(r.wm, d)) != cudaSuccess) {
+        set_err(err, errcap, cuda_msg("read failed", e));
+        return RM_ERR_CUDA;
+      }
+      for (size_t i = 0; i < npix; ++i) {
+        float rr[15] = {a[i].x, a[i].y, a[i].z, b[i].x, b[i].y, b[i].z, cc[i].x, cc[i].y, cc[i].z,
+                        a[i].w, b[i].w, cc[i].w, d[i].x, d[i].y, d[i].z};
+        std::memcpy(out + i * 60, rr, 60);
+      }
+    }
+    return RM_OK;
+  }
+  if (which == 3 || which == 4) {
+    const size_t bytes = npix * (which == 3 ? 12 : 8);
+    if (cap < bytes) { set_err(err, errcap, "buffer too small"); return RM_ERR_INVALID; }
+    const void* src = which == 3 ? static_cast<const void*>(c->last_final) : c->dbg.ptr;
+    if (!src) { set_err(err, errcap, "no frame rendered"); return RM_ERR_INVALID; }
+    e = cudaMemcpy(host, src, bytes, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("read failed", e)); return RM_ERR_CUDA; }
+    return RM_OK;
+  }
+  set_err(err, errcap, "unknown buffer");
+  return RM_ERR_INVALID;
+}
+
+int rmcuda_reset_history(rmcuda_ctx* c) {
+  if (!c) return RM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->hist_valid = false;
+  return RM_OK;
+}
+
+int rmcuda_stats_get(rmcuda_ctx* c, rm_stats* out) {
+  if (!c || !out) return RM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  unsigned long long all[RM_STAGE_COUNT * 4] = {};
+  uint32_t e32 = 0;
+  if (cudaMemcpyAsync(all, c->ctr.ptr, sizeof(all), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaMemcpyAsync(&e32, c->err.ptr, 4, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return RM_ERR_CUDA;
+  unsigned long long v[4] = {0, 0, 0, 0};
+  for (int i = 0; i < RM_STAGE_COUNT * 4; ++i) v[i % 4] += all[i];
+  out->path_samples = v[0];
+  out->rays = v[1];
+  out->nodes_visited = v[2];
+  out->tris_tested = v[3];
+  out->frames = c->frames;
+  out->kernel_launches = c->launches;
+  out->device_error = e32;
+  out->kernel_chain = uint32_t(c->last_chain);
+  return RM_OK;
+}
+
+int rmcuda_profile(rmcuda_ctx* c, int enable) {
+  if (!c) return RM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->profiling = enable != 0;
+  return RM_OK;
+}
+
+int rmcuda_stage_counters(rmcuda_ctx* c, uint64_t* out, int32_t n) {
+  if (!c || !out || n < 0) return RM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  unsigned long long all[RM_STAGE_COUNT * 4] = {};
+  if (cudaMemcpyAsync(all, c->ctr.ptr, sizeof(all), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return RM_ERR_CUDA;
+  for (int i = 0; i < n * 4 && i < RM_STAGE_COUNT * 4; ++i) out[i] = all[i];
+  return RM_OK;
+}
+
+int rmcuda_stage_times(rmcuda_ctx* c, double* ms, uint64_t* launches, int32_t n) {
+  if (!c || n < 0) return RM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  resolve_pending(c);
+  for (int i = 0; i < n && i < RM_STAGE_COUNT; ++i) {
+    if (ms) ms[i] = c->stage_ms[i];
+    if (launches) launches[i] = c->stage_n[i];
+  }
+  return RM_OK;
+}
+
+int rmcuda_stats_reset(rmcuda_ctx* c) {
+  if (!c) return RM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  resolve_pending(c);
+  for (int i = 0; i < RM_STAGE_COUNT; ++i) { c->stage_ms[i] = 0; c->stage_n[i] = 0; }
+  c->frames = 0;
+  c->launches = 0;
+  return cudaMemsetAsync(c->ctr.ptr, 0, RM_STAGE_COUNT * 32, c->stream) == cudaSuccess ? RM_OK : RM_ERR_CUDA;
+}
+
+}  // extern "C"

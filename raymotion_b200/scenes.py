@@ -1,0 +1,169 @@
+"""Seeded synthetic scenes of the benchmark workloads (no external assets).
+
+* ``cornell_box(seed)``: 36 triangles - five walls (albedo 0.75 grey, left
+  wall red 0.63/0.065/0.05, right wall green 0.14/0.45/0.09), a tall diffuse
+  box, a short GGX-metal box of roughness 0.3 and one emissive quad light of
+  radiance (17, 12, 4); box placement and the camera are drawn from ``seed``.
+* ``icosphere_field(...)``: instanced icospheres (subdivision 4, 5120
+  triangles each) displaced by seeded 3-D value noise of amplitude 0.05 r,
+  radii uniform in [0.2, 1.5], centres uniform in a 40 x 10 x 40 box, a ground
+  plane, materials 50 % diffuse (albedo U[0.1, 0.9]^3) / 30 % GGX metal
+  (roughness U[0.05, 1]) / 20 % dielectric (IOR 1.5, roughness 0 or 0.2), and
+  small emissive triangles with log-uniform radiance in [1, 100].  The default
+  arguments give 200 spheres + 2 + 4096 = 1,028,098 triangles.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .scene import Camera, RenderConfig, SceneBuilder
+
+
+def _quad(sb: SceneBuilder, a, b, c, d, normal=None, **mat) -> None:
+    a, b, c, d = (np.asarray(x, np.float64) for x in (a, b, c, d))
+    n = None if normal is None else [normal]
+    sb.add_triangles([a], [b], [c], n, n, n, **mat)
+    sb.add_triangles([a], [c], [d], n, n, n, **mat)
+
+
+def _box(sb: SceneBuilder, center, half, angle_deg, **mat) -> None:
+    cx, cy, cz = center
+    hx, hy, hz = half
+    ca, sa = math.cos(math.radians(angle_deg)), math.sin(math.radians(angle_deg))
+
+    def p(x, y, z):
+        return (cx + ca * x - sa * z, cy + y, cz + sa * x + ca * z)
+
+    corners = {(i, j, k): p(i * hx, j * hy, k * hz) for i in (-1, 1) for j in (-1, 1) for k in (-1, 1)}
+    faces = [  # (corner keys counter-clockwise seen from outside), outward normal in box space
+        ([(-1, 1, -1), (-1, 1, 1), (1, 1, 1), (1, 1, -1)], (0, 1, 0)),
+        ([(-1, -1, -1), (1, -1, -1), (1, -1, 1), (-1, -1, 1)], (0, -1, 0)),
+        ([(-1, -1, -1), (-1, 1, -1), (1, 1, -1), (1, -1, -1)], (0, 0, -1)),
+        ([(-1, -1, 1), (1, -1, 1), (1, 1, 1), (-1, 1, 1)], (0, 0, 1)),
+        ([(-1, -1, -1), (-1, -1, 1), (-1, 1, 1), (-1, 1, -1)], (-1, 0, 0)),
+        ([(1, -1, -1), (1, 1, -1), (1, 1, 1), (1, -1, 1)], (1, 0, 0)),
+    ]
+    for keys, (nx, ny, nz) in faces:
+        n = (ca * nx - sa * nz, ny, sa * nx + ca * nz)
+        _quad(sb, *(corners[k] for k in keys), normal=n, **mat)
+
+
+def cornell_box(seed: int = 0):
+    """Returns (SceneBuilder, Camera, RenderConfig) of the 320x180 / 16 spp / depth 8 workload."""
+    rng = np.random.default_rng(seed)
+    sb = SceneBuilder()
+    grey, red, green = (0.75, 0.75, 0.75), (0.63, 0.065, 0.05), (0.14, 0.45, 0.09)
+    _quad(sb, (-1, 0, 0), (1, 0, 0), (1, 0, 2), (-1, 0, 2), normal=(0, 1, 0), albedo=grey)     # floor
+    _quad(sb, (-1, 2, 0), (-1, 2, 2), (1, 2, 2), (1, 2, 0), normal=(0, -1, 0), albedo=grey)    # ceiling
+    _quad(sb, (-1, 0, 2), (1, 0, 2), (1, 2, 2), (-1, 2, 2), normal=(0, 0, -1), albedo=grey)    # back
+    _quad(sb, (-1, 0, 0), (-1, 0, 2), (-1, 2, 2), (-1, 2, 0), normal=(1, 0, 0), albedo=red)    # left
+    _quad(sb, (1, 0, 0), (1, 2, 0), (1, 2, 2), (1, 0, 2), normal=(-1, 0, 0), albedo=green)     # right
+    j = rng.uniform(-0.08, 0.08, size=4)
+    _box(sb, (-0.35 + j[0], 0.6, 1.3 + j[1]), (0.28, 0.6, 0.28), 17 + 10 * j[2], albedo=grey)
+    _box(sb, (0.38 + j[3], 0.3, 0.7), (0.27, 0.3, 0.27), -18, albedo=(0.8, 0.8, 0.8), metallic=1.0, rough=0.3)
+    # emitters are one-sided along their geometric normal (v1-v0)x(v2-v0): wind it downwards
+    _quad(sb, (-0.25, 1.98, 0.75), (0.25, 1.98, 0.75), (0.25, 1.98, 1.25), (-0.25, 1.98, 1.25),
+          normal=(0, -1, 0), albedo=(0.78, 0.78, 0.78), emission=(17, 12, 4))
+    cj = rng.uniform(-0.05, 0.05, size=3)
+    cam = Camera().set((cj[0], 1.0 + cj[1], -2.2 + cj[2]), (0, 0, 0), 106)
+    cfg = RenderConfig(width=320, height=180, spp=16, max_bounces=8, restir_candidates=1, restir_spatial=0)
+    return sb, cam, cfg
+
+
+def _icosphere(subdiv: int):
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    v = [np.asarray(p, np.float64) / np.linalg.norm(p) for p in verts]
+    for _ in range(subdiv):
+        cache = {}
+        nf = []
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = v[a] + v[b]
+                v.append(m / np.linalg.norm(m))
+                cache[key] = len(v) - 1
+            return cache[key]
+
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return np.asarray(v), np.asarray(faces, np.int64)
+
+
+def _value_noise(p: np.ndarray, seed: int) -> np.ndarray:
+    """Trilinear value noise in [-1, 1] on the integer lattice, hashed from ``seed``."""
+    base = np.floor(p).astype(np.int64)
+    f = p - base
+    w = f * f * (3 - 2 * f)
+
+    def h(ix, iy, iz):
+        z = (ix * 73856093) ^ (iy * 19349663) ^ (iz * 83492791) ^ (seed * 2654435761)
+        z = (z ^ (z >> 13)) * 1274126177
+        z = z ^ (z >> 16)
+        return ((z & 0xFFFF) / 32767.5) - 1.0
+
+    out = 0.0
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                wx = w[:, 0] if dx else 1 - w[:, 0]
+                wy = w[:, 1] if dy else 1 - w[:, 1]
+                wz = w[:, 2] if dz else 1 - w[:, 2]
+                out = out + wx * wy * wz * h(base[:, 0] + dx, base[:, 1] + dy, base[:, 2] + dz)
+    return out
+
+
+def icosphere_field(seed: int = 1, n_spheres: int = 200, subdiv: int = 4, n_emitters: int = 4096,
+                    width: int = 1280, height: int = 720, spp: int = 64, depth: int = 12):
+    """Returns (SceneBuilder, Camera, RenderConfig) of the instanced icosphere workload."""
+    rng = np.random.default_rng(seed)
+    sb = SceneBuilder()
+    unit_v, faces = _icosphere(subdiv)
+    radii = rng.uniform(0.2, 1.5, n_spheres)
+    centers = np.stack([rng.uniform(-20, 20, n_spheres), rng.uniform(0, 10, n_spheres),
+                        rng.uniform(-20, 20, n_spheres)], axis=1)
+    kind = rng.choice(3, size=n_spheres, p=[0.5, 0.3, 0.2])
+    for i in range(n_spheres):
+        r = radii[i]
+        world = centers[i] + unit_v * r
+        disp = 0.05 * r * _value_noise(world * (2.0 / r), seed * 1000 + i)
+        pos = centers[i] + unit_v * (r + disp)[:, None]
+        fa, fb, fc = pos[faces[:, 0]], pos[faces[:, 1]], pos[faces[:, 2]]
+        fn = np.cross(fb - fa, fc - fa)
+        vn = np.zeros_like(pos)
+        for k in range(3):
+            np.add.at(vn, faces[:, k], fn)
+        vn /= np.linalg.norm(vn, axis=1, keepdims=True)
+        if kind[i] == 0:
+            mat = dict(albedo=tuple(rng.uniform(0.1, 0.9, 3)), rough=0.5)
+        elif kind[i] == 1:
+            mat = dict(albedo=tuple(rng.uniform(0.5, 0.95, 3)), metallic=1.0, rough=float(rng.uniform(0.05, 1.0)))
+        else:
+            mat = dict(albedo=(1.0, 1.0, 1.0), ior=1.5, rough=float(rng.choice([0.0, 0.2])))
+        sb.add_triangles(fa, fb, fc, vn[faces[:, 0]], vn[faces[:, 1]], vn[faces[:, 2]], **mat)
+    g = 100.0
+    _quad(sb, (-g, 0, -g), (-g, 0, g), (g, 0, g), (g, 0, -g), normal=(0, 1, 0), albedo=(0.5, 0.5, 0.5), rough=0.8)
+    # small emitters facing down, scattered above the spheres
+    c = np.stack([rng.uniform(-24, 24, n_emitters), rng.uniform(11, 14, n_emitters),
+                  rng.uniform(-24, 24, n_emitters)], axis=1)
+    s = rng.uniform(0.15, 0.35, n_emitters)[:, None]
+    a0 = c + np.concatenate([-s, 0 * s, -s], axis=1)
+    a1 = c + np.concatenate([s, 0 * s, -s * 0.2], axis=1)
+    a2 = c + np.concatenate([-s * 0.3, 0 * s, s], axis=1)
+    radiance = np.exp(rng.uniform(math.log(1.0), math.log(100.0), n_emitters))
+    tint = rng.uniform(0.6, 1.0, (n_emitters, 3))
+    down = np.broadcast_to(np.asarray([0.0, -1.0, 0.0]), (n_emitters, 3))
+    sb.add_triangles(a0, a1, a2, down, down, down, albedo=(0.8, 0.8, 0.8), emission=tint * radiance[:, None])
+    cam = Camera().set((0.0, 9.0, -34.0), (14.0, 0.0, 0.0), 60)
+    cfg = RenderConfig(width=width, height=height, spp=spp, max_bounces=depth, restir_candidates=32,
+                       restir_spatial=5, restir_radius=30.0)
+    return sb, cam, cfg

@@ -1,0 +1,59 @@
+"""librmcuda.so loads without a GPU and exports every function include/rmcuda.h declares."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+import raymotion_b200 as rb
+from raymotion_b200 import _abi, build
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared():
+    text = (ROOT / "include" / "rmcuda.h").read_text()
+    return sorted(set(re.findall(r"\b(rmcuda_[a-z_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not build.LIB.exists():
+        build.build()
+    return _abi.load_library()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = _declared()
+    assert len(names) >= 14
+    bound = {n for n, _, _ in _abi.EXPORTS}
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in bound, f"{n} lacks a ctypes binding"
+
+
+def test_record_sizes_match_reference_abi():
+    # metal_types.h sizes, asserted in metal.mm:13-17
+    assert _abi.TRIANGLE_DTYPE.itemsize == 176
+    assert _abi.GBUF_DTYPE.itemsize == 76
+    assert _abi.RESERVOIR_DTYPE.itemsize == 60
+    assert C.sizeof(_abi.RmCamera) == 52
+
+
+def test_version_and_unavailable_without_gpu(lib):
+    assert lib.rmcuda_version().startswith(b"rmcuda")
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    err = C.create_string_buffer(256)
+    rc = lib.rmcuda_create(C.byref(h), 0, err, 256)
+    assert rc == _abi.RM_ERR_UNAVAILABLE
+    # the reference test suite treats this exact string as "skip" (tests/test_metal.cpp:25)
+    assert err.value == b"Metal backend is not available in this build"
+
+
+def test_render_image_metal_validates_first():
+    from raymotion_b200.scene import Camera, RenderConfig, SceneBuilder
+    ok, rgb, err = rb.render_image_metal(SceneBuilder().pack(), Camera(), RenderConfig(width=0), 1)
+    assert not ok and err == "Invalid Metal render dimensions or sample count"

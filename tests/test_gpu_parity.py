@@ -1,0 +1,147 @@
+"""CUDA path vs the CPU oracle on identical inputs and RNG streams (GPU)."""
+import numpy as np
+import pytest
+
+from raymotion_b200 import _abi
+from raymotion_b200.scene import Camera, RenderConfig
+from raymotion_b200.scenes import cornell_box, icosphere_field
+
+from .gpu_util import camera_rays, exact_fraction, random_rays, rel_close_fraction
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _trace_gpu(backend, rays, any_hit=False):
+    torch = _torch()
+    r = torch.from_numpy(rays).cuda()
+    n = len(rays)
+    tri = torch.empty(n, dtype=torch.int32, device="cuda")
+    t = torch.empty(n, dtype=torch.float32, device="cuda")
+    u = torch.empty_like(t)
+    v = torch.empty_like(t)
+    backend.trace(r.data_ptr(), n, any_hit, tri.data_ptr(), t.data_ptr(), u.data_ptr(), v.data_ptr())
+    return tri.cpu().numpy(), t.cpu().numpy(), u.cpu().numpy(), v.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def small_field(oracle):
+    sb, cam, cfg = icosphere_field(seed=3, n_spheres=16, subdiv=3, n_emitters=96, width=160, height=90, spp=4,
+                                   depth=6)
+    sc = oracle.with_reference_bvh(sb.pack())
+    return sc, cam, cfg
+
+
+@pytest.mark.parametrize("use_nodes", [False, True], ids=["device_lbvh", "caller_bvh"])
+def test_closest_hit_ids_bit_exact(backend, oracle, small_field, use_nodes):
+    sc, cam, cfg = small_field
+    backend.upload(sc, use_nodes=use_nodes)
+    rays = np.concatenate([camera_rays(cam, RenderConfig(width=320, height=180), 1),
+                           random_rays(40000, [-22, -1, -22], [22, 12, 22], 2)])
+    g_tri, g_t, g_u, g_v = _trace_gpu(backend, rays)
+    o_tri, o_t, o_u, o_v = oracle.trace(sc, rays)
+    assert (o_tri >= 0).mean() > 0.2
+    assert np.array_equal(g_tri, o_tri)
+    hit = o_tri >= 0
+    assert np.array_equal(g_t[hit].view(np.uint32), o_t[hit].view(np.uint32))
+    assert np.array_equal(g_u[hit].view(np.uint32), o_u[hit].view(np.uint32))
+    assert np.array_equal(g_v[hit].view(np.uint32), o_v[hit].view(np.uint32))
+    g_any, _, _, _ = _trace_gpu(backend, rays, any_hit=True)
+    o_any, _, _, _ = oracle.trace(sc, rays, any_hit=True)
+    assert np.array_equal(g_any >= 0, o_any >= 0)
+
+
+def _compare_render(backend, oracle, sc, cam, cfg, seed, use_nodes=False):
+    o = oracle.Oracle()
+    o_rgb, o_hdr, o_st = o.render(sc, cam, cfg, seed)
+    backend.stats_reset()
+    g_rgb, g_hdr = backend.render(sc, cam, cfg, seed, hdr=True, use_nodes=use_nodes)
+    npix = cfg.width * cfg.height
+    g_dbg = backend.debug_read(4, npix).reshape(-1, 2)
+    o_dbg = o.debug_read(4, npix).reshape(-1, 2)
+    st = backend.stats()
+    return dict(o_rgb=o_rgb, o_hdr=o_hdr, o_st=o_st, g_rgb=g_rgb, g_hdr=g_hdr, g_dbg=g_dbg, o_dbg=o_dbg, st=st)
+
+
+@pytest.mark.parametrize("spp,adapt,lanes", [(16, 16, 8), (4, 16, 1), (64, 0, 32)])
+def test_cornell_plain_path_bit_exact(backend, oracle, spp, adapt, lanes):
+    sb, cam, cfg = cornell_box(0)
+    sc = oracle.with_reference_bvh(sb.pack())
+    cfg.spp, cfg.adapt_min = spp, adapt
+    r = _compare_render(backend, oracle, sc, cam, cfg, 12345)
+    assert r["st"]["kernel_chain"] == lanes == r["o_st"]["chain"]
+    assert np.array_equal(r["g_dbg"], r["o_dbg"]), "RNG state / sample count per pixel differ"
+    assert exact_fraction(r["g_hdr"], r["o_hdr"]) == 1.0
+    assert np.array_equal(r["g_rgb"], r["o_rgb"])
+    assert r["st"]["path_samples"] == r["o_st"]["path_samples"]
+    assert r["st"]["rays"] == r["o_st"]["rays"]
+
+
+def test_field_plain_path_with_caller_bvh(backend, oracle, small_field):
+    sc, cam, cfg = small_field
+    cfg = RenderConfig(width=160, height=90, spp=8, max_bounces=6, adapt_min=0, restir_candidates=4,
+                       restir_spatial=0)
+    r = _compare_render(backend, oracle, sc, cam, cfg, 777, use_nodes=True)
+    assert np.array_equal(r["g_dbg"], r["o_dbg"])
+    assert exact_fraction(r["g_hdr"], r["o_hdr"]) == 1.0
+
+
+def test_non_opaque_textured_nomis_norr(backend, oracle):
+    from . import kat_scenes as K
+    cam, cfg = K.metal_config()
+    cfg.spp = 24
+    cfg.flags = _abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_NOMIS | _abi.RM_FLAG_NO_RR
+    sc = K.metal_scene().pack()
+    sc.tris["alpha"][::3] = np.float32(0.6)
+    oracle.with_reference_bvh(sc, 2)
+    r = _compare_render(backend, oracle, sc, cam, cfg, 4242)
+    assert np.array_equal(r["g_dbg"], r["o_dbg"])
+    assert exact_fraction(r["g_hdr"], r["o_hdr"]) == 1.0
+
+
+def _restir_cfg(flags=0):
+    return RenderConfig(width=160, height=90, spp=4, max_bounces=6, adapt_min=0, restir_candidates=8,
+                        restir_spatial=4, restir_radius=12.0, flags=flags)
+
+
+def test_restir_chain_matches_oracle(backend, oracle, small_field):
+    sc, cam, _ = small_field
+    cfg = _restir_cfg(_abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_DENOISE_OFF)
+    o = oracle.Oracle()
+    backend.reset_history()
+    npix = cfg.width * cfg.height
+    for frame, seed in enumerate((11, 12)):  # the second frame reuses the first as temporal history
+        o_rgb, o_hdr, o_st = o.render(sc, cam, cfg, seed)
+        g_rgb, g_hdr = backend.render(sc, cam, cfg, seed, hdr=True)
+        assert o_st["chain"] == 2 and backend.stats()["kernel_chain"] == 2
+        og, gg = o.debug_read(0, npix), backend.debug_read(0, npix)
+        assert np.array_equal(og["kind"], gg["kind"])
+        live = og["kind"] != 0
+        assert live.mean() > 0.3
+        for f in ("pos", "normal", "albedo", "wo", "emission", "rough", "metallic", "ior"):
+            assert np.array_equal(og[f][live], gg[f][live]), f
+        for which in (1, 2):
+            orr, grr = o.debug_read(which, npix), backend.debug_read(which, npix)
+            assert np.array_equal(orr["valid"], grr["valid"])
+            v = orr["valid"] != 0
+            for f in ("lightPos", "lightNormal", "emission", "alpha", "p_hat", "sumWs", "sumWu", "M"):
+                assert np.array_equal(orr[f][v], grr[f][v]), (which, f, frame)
+        assert np.array_equal(backend.debug_read(4, npix), o.debug_read(4, npix))
+        assert exact_fraction(g_hdr, o_hdr) == 1.0
+        assert np.array_equal(g_rgb, o_rgb)
+
+
+def test_denoiser_within_tolerance(backend, oracle, small_field):
+    sc, cam, _ = small_field
+    cfg = _restir_cfg(_abi.RM_FLAG_NO_ENV)
+    o = oracle.Oracle()
+    backend.reset_history()
+    for seed in (21, 22, 23):  # frames 2 and 3 blend temporal history
+        _, o_hdr, _ = o.render(sc, cam, cfg, seed)
+        g_rgb, g_hdr = backend.render(sc, cam, cfg, seed, hdr=True)
+        assert rel_close_fraction(g_hdr, o_hdr, 1e-4) >= 0.999
