@@ -29,7 +29,7 @@ NVFLAGS = ARCH + [
     f"-I{ROOT / 'include'}", f"-I{CSRC}",
 ]
 CU_SOURCES = ["rm_kernels.cu", "rm_denoise.cu", "rm_bvh.cu", "rmcuda_api.cu"]
-CXX_SOURCES: list[str] = []
+CXX_SOURCES = ["shim_metal.cpp"]
 
 
 def _nvcc() -> str:
