@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="icosphere720", choices=["icosphere720", "cornell"])
+    ap.add_argument("--workload", default="icosphere720", choices=["icosphere720", "icosphere180", "cornell"],
+                    help="icosphere180: the same scene at 320x180, 16 spp (profiling size)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -65,6 +66,10 @@ def workload(name: str):
     if name == "cornell":
         sb, cam, cfg = cornell_box(0)
         desc = dict(workload="cornell box, 36 triangles, 320x180, 16 spp, depth 8, plain NEE+MIS", triangles=36)
+    elif name == "icosphere180":
+        sb, cam, cfg = icosphere_field(seed=1, width=320, height=180, spp=16)
+        desc = dict(workload="icosphere field, 1,028,098 triangles, 320x180, 16 spp, depth 12, ReSTIR DI "
+                             "(32 candidates, 5 spatial neighbours, radius 30 px, temporal) + denoiser")
     else:
         sb, cam, cfg = icosphere_field(seed=1)
         desc = dict(workload="icosphere field, 1,028,098 triangles, 1280x720, 64 spp, depth 12, ReSTIR DI "
