@@ -186,6 +186,25 @@ int rmcuda_trace(rmcuda_ctx* ctx, const float* d_rays, int32_t n, int32_t any_hi
                  int32_t* d_tri, float* d_t, float* d_u, float* d_v,
                  char* err, size_t errcap);
 
+/* Ray queries that allocate nothing.  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory while they run (an engine
+ * whose allocator owns the whole GPU, a fixed-budget real-time loop, a stack
+ * that forbids runtime allocation).  Builds a BVH over n_tris caller-owned
+ * device triangles and answers n_rays device rays exactly like rmcuda_trace,
+ * using only the caller's buffers and one fixed device array inside the
+ * library (24 MiB, held by every GPU that loads the library until exit), so
+ * n_tris is limited to RMCUDA_NOALLOC_MAX_TRIS; larger scenes are rejected
+ * with RM_ERR_INVALID.  The array keeps the last call's contents and is
+ * shared by all calls: calls that overlap on the GPU race and must be
+ * serialised by the caller.  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress), so make it before any stream capture.
+ * Works on the current device and `cuda_stream` (NULL: the default stream);
+ * returns after the queries finish. */
+#define RMCUDA_NOALLOC_MAX_TRIS 65536
+int rmcuda_trace_noalloc(const rm_triangle* d_tris, int32_t n_tris, const float* d_rays, int32_t n_rays,
+                         int32_t any_hit, int32_t* d_tri, float* d_t, float* d_u, float* d_v,
+                         void* cuda_stream, char* err, size_t errcap);
+
 /* Read the last frame's ReSTIR buffers back in the reference record layouts
  * (metal_types.h:32-56): which = 0 G-buffer (76 B/px), 1 initial reservoir,
  * 2 merged reservoir (60 B/px), 3 shaded HDR (12 B/px).  Host pointer. */

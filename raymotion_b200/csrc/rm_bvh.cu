@@ -418,6 +418,51 @@ cudaError_t build_lbvh(const rm_triangle* d_tris, int n, int leaf_max, DevBvh& b
   return pack_tgeo(d_tris, b, st);
 }
 
+cudaError_t build_lbvh_into(const rm_triangle* d_tris, int n, int leaf_max, const LbvhScratch& w, DevBvhView& out,
+                            cudaStream_t st, std::string& err) {
+  out.n_records = 0;
+  if (n <= 0) return cudaSuccess;
+  leaf_max = std::max(1, std::min(leaf_max, kMaxLeaf));
+  RM_TRY(cudaMemsetAsync(w.err_word, 0, sizeof(uint32_t), st));
+  if (n <= leaf_max) {
+    k_single_leaf<<<1, 1, 0, st>>>(d_tris, n, w.records, w.parents, w.order);
+    RM_TRY(cudaGetLastError());
+    out.n_records = 1;
+  } else {
+    const int ni = n - 1;
+    // centroid bounds start at (+max ordered, 0): min slots all ones, max slots zero
+    RM_TRY(cudaMemsetAsync(w.bounds, 0xff, 3 * sizeof(unsigned int), st));
+    RM_TRY(cudaMemsetAsync(w.bounds + 3, 0, 3 * sizeof(unsigned int), st));
+    k_centroid_bounds<<<148 * 4, 256, 0, st>>>(d_tris, n, w.bounds);
+    k_morton<<<(n + 255) / 256, 256, 0, st>>>(d_tris, n, w.bounds, w.keys, w.vals);
+    RM_TRY(cudaGetLastError());
+    cub::DoubleBuffer<unsigned int> dk(w.keys, w.keys_alt);
+    cub::DoubleBuffer<int> dv(w.vals, w.vals_alt);
+    size_t temp_bytes = 0;
+    RM_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, dk, dv, n, 0, 30, st));
+    if (temp_bytes > w.sort_temp_bytes) { err = "sort scratch too small"; return cudaErrorInvalidValue; }
+    RM_TRY(cub::DeviceRadixSort::SortPairs(w.sort_temp, temp_bytes, dk, dv, n, 0, 30, st));
+    RM_TRY(cudaMemcpyAsync(w.order, dv.Current(), size_t(n) * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    RM_TRY(cudaMemsetAsync(w.parent_int, 0xff, size_t(ni) * sizeof(int), st));
+    k_karras<<<(ni + 255) / 256, 256, 0, st>>>(dk.Current(), n, w.children, w.ranges, w.parent_int, w.parent_leaf);
+    RM_TRY(cudaMemsetAsync(w.kcount, 0, size_t(ni) * sizeof(int), st));
+    k_karras_boxes<<<(n + 255) / 256, 256, 0, st>>>(d_tris, w.order, n, w.children, w.parent_int, w.parent_leaf,
+                                                    reinterpret_cast<Box*>(w.kbox), w.kcount);
+    RM_TRY(cudaMemsetAsync(w.parents, 0xff, size_t(ni) * sizeof(int), st));
+    k_emit_records<<<(ni + 255) / 256, 256, 0, st>>>(d_tris, w.order, n, leaf_max, w.children, w.ranges,
+                                                     reinterpret_cast<const Box*>(w.kbox), w.records, w.parents);
+    RM_TRY(cudaGetLastError());
+    out.n_records = ni;
+  }
+  k_pack_tgeo<<<(n + 255) / 256, 256, 0, st>>>(d_tris, w.order, n, w.tgeo);
+  RM_TRY(cudaGetLastError());
+  out.records = w.records;
+  out.tgeo = w.tgeo;
+  return cudaSuccess;
+}
+
+size_t lbvh_box_bytes() { return sizeof(Box); }
+
 bool convert_caller_bvh(const rm_bvh_node* nodes, int M, const int32_t* bvh_tri, int n_tris, DevBvh& out,
                         cudaStream_t st, std::string& err) {
   out.n_tris = n_tris;

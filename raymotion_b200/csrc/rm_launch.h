@@ -63,6 +63,37 @@ cudaError_t build_lbvh(const rm_triangle* d_tris, int n_tris, int leaf_max, DevB
 cudaError_t pack_tgeo(const rm_triangle* d_tris, DevBvh& bvh, cudaStream_t st);
 // Refit all boxes bottom-up from the current triangle positions.
 cudaError_t refit_bvh(const rm_triangle* d_tris, DevBvh& bvh, cudaStream_t st);
+// Caller-provided scratch of an LBVH build (device pointers; see rm_noalloc.cu).
+struct LbvhScratch {
+  float4* records;        // (n-1) x 4 float4
+  int* parents;           // n ints
+  int* order;             // n ints
+  float4* tgeo;           // n x 3 float4
+  unsigned int* keys;     // n
+  int* vals;              // n
+  unsigned int* keys_alt; // n
+  int* vals_alt;          // n
+  int2* children;         // n - 1
+  int2* ranges;           // n - 1
+  int* parent_int;        // n - 1
+  int* parent_leaf;       // n
+  void* kbox;             // (n - 1) x lbvh_box_bytes()
+  int* kcount;            // n - 1
+  unsigned int* bounds;   // 6
+  uint32_t* err_word;     // 1
+  void* sort_temp;
+  size_t sort_temp_bytes;
+};
+struct DevBvhView {
+  const float4* records = nullptr;
+  const float4* tgeo = nullptr;
+  int n_records = 0;
+};
+// Build an LBVH into caller scratch without allocating (no depth check: the
+// traversal's stack guard reports overflow through err_word).
+cudaError_t build_lbvh_into(const rm_triangle* d_tris, int n, int leaf_max, const LbvhScratch& w, DevBvhView& out,
+                            cudaStream_t st, std::string& err);
+size_t lbvh_box_bytes();
 // 64-bit content hash of a device byte range (order-sensitive per 8-byte word).
 cudaError_t device_hash(const void* d_bytes, size_t n_bytes, unsigned long long* d_out, cudaStream_t st);
 
