@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-breakdown", action="store_true", help="skip the per-kernel timing frame")
     return ap.parse_args()
 
 
@@ -240,7 +241,10 @@ def run_b200(args, world, rank, local):
     dev = torch.device("cuda", local)
     scene, cam, cfg, desc = workload(args.workload)
     backend = rb.Backend(local)
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated stream: the rendering and the CUDA events that time it share it
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    assert stream.cuda_stream != 0
     backend.set_stream(stream.cuda_stream)
     npix = cfg.width * cfg.height
     seed0 = 12345 + 1000 * rank
@@ -251,7 +255,7 @@ def run_b200(args, world, rank, local):
         backend.render_resident_async(cam, cfg, seed0 + i, d_rgb.data_ptr())
     backend.sync()
     backend.stats_reset()
-    backend.profile(True)
+    backend.profile(1)
     torch.cuda.synchronize()
     barrier(world)
     try:
@@ -276,25 +280,55 @@ def run_b200(args, world, rank, local):
     secs_max, = allreduce([secs], "max", world, dev)
     samples_sum, rays_sum = allreduce([float(st["path_samples"]), float(st["rays"])], "sum", world, dev)
     value = samples_sum / secs_max
-    backend.profile(False)
-    # ---- roofline of the dominant kernel
-    dom = max(stage_t, key=lambda k: stage_t[k][0])
-    ms_total, launches = stage_t[dom]
-    c = stage_c[dom]
+    # ---- per-kernel breakdown on one more (untimed) frame: every launch event-timed
+    backend.stats_reset()
+    backend.profile(2)
+    if not args.no_breakdown:
+        backend.render_resident_async(cam, cfg, seed0 + args.warmup + args.steps, d_rgb.data_ptr())
+    backend.sync()
+    kern_t = backend.stage_times()
+    kern_c = backend.stage_counters()
+    kern_st = backend.stats()
+    backend.profile(0)
+    wlog = backend.wave_log()
+    wave_summary = None
+    if len(wlog):
+        act = wlog[:, 0]
+        first = int(act[0])
+        marks = {f"batches_until_{int(f * 100)}pct": int(np.argmax(act < f * first)) for f in (0.5, 0.1, 0.01)}
+        wave_summary = dict(batches=int(len(act)), waves_per_batch=4, first_act=first, **marks)
+    # ---- roofline of the dominant kernel (the wavefront loop counts as its kernels)
+    if args.no_breakdown:
+        kern_t, kern_c = stage_t, stage_c
+    kernel_stages = {k: v for k, v in kern_t.items() if k != "shade" or kern_t["wf_extend"][1] == 0}
+    dom = max(kernel_stages, key=lambda k: kernel_stages[k][0])
+    ms_total, launches = kern_t[dom]
+    c = kern_c[dom]
     alg_bytes = (c["nodes_visited"] * 64 + c["tris_tested"] * 48) / max(launches, 1)
     avg_s = ms_total / 1e3 / max(launches, 1)
     peak = measured_peaks()
     achieved = alg_bytes / avg_s / 1e9 if avg_s > 0 else 0.0
     kernel_names = dict(plain="k_render_paths", shade="k_restir_shade", generate="k_restir_generate",
                         spatial="k_restir_spatial", temporal="k_denoise_temporal", atrous0="k_denoise_atrous",
-                        atrous1="k_denoise_atrous", hash="k_hash", tonemap="k_tonemap")
+                        atrous1="k_denoise_atrous", hash="k_hash", tonemap="k_tonemap", wf_extend="k_wf_extend",
+                        wf_shadow="k_wf_shadow", wf_shade="k_wf_shade")
     roofline = dict(bound="hbm", kernel=kernel_names.get(dom, dom), achieved=achieved, peak=peak["hbm_gbs"],
                     unit="GB/s", frac=achieved / peak["hbm_gbs"], traffic=ncu_traffic(kernel_names.get(dom, dom)),
                     peak_source=peak["source"],
                     note="achieved = (64 B x BVH records fetched + 48 B x triangle tests) per launch / average "
                          "launch time; most of these bytes hit L1/L2")
-    stage_summary = {k: dict(ms_per_launch=(v[0] / v[1]) if v[1] else 0.0, launches=v[1]) for k, v in stage_t.items()
-                     if v[1]}
+    stage_summary = {k: dict(ms_per_frame=v[0] / args.steps, launches_per_frame=v[1] / args.steps)
+                     for k, v in stage_t.items() if v[1]}
+    kernel_summary = {}
+    for k, v in kern_t.items():
+        if not v[1]:
+            continue
+        e = dict(ms=v[0], launches=v[1])
+        rc = kern_c.get(k, {})
+        if rc.get("rays"):
+            e.update(rays=rc["rays"], nodes_per_ray=rc["nodes_visited"] / rc["rays"],
+                     tests_per_ray=rc["tris_tested"] / rc["rays"], mrays_per_s=rc["rays"] / (v[0] * 1e3))
+        kernel_summary[k] = e
     # ---- end to end through rmcuda_render with host buffers
     e2e = None
     if not args.no_e2e:
@@ -333,7 +367,8 @@ def run_b200(args, world, rank, local):
                     vs_baseline=None, dtype="f32", data="synthetic (seeded procedural scene)",
                     config=dict(desc, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
                     mrays_per_s=rays_sum / secs_max / 1e6, e2e=e2e, roofline=roofline, cpu_baseline=cpu,
-                    gpu_launches=int(st["kernel_launches"]), clocks=clk, stages=stage_summary)
+                    gpu_launches=int(st["kernel_launches"]), clocks=clk, stages=stage_summary,
+                    kernels_one_frame=kernel_summary, wavefront=wave_summary)
         print(json.dumps(line), flush=True)
     backend.close()
     return 0

@@ -230,11 +230,20 @@ int rmcuda_stats_reset(rmcuda_ctx* ctx);
 #define RM_STAGE_ATROUS0 6   /* a-trous stride 1 */
 #define RM_STAGE_ATROUS1 7   /* a-trous stride 2 + tonemap */
 #define RM_STAGE_TONEMAP 8   /* tonemap alone (denoiser off) */
-#define RM_STAGE_COUNT 9
-int rmcuda_profile(rmcuda_ctx* ctx, int enable);
+#define RM_STAGE_WF_EXTEND 9 /* wavefront shading: closest-hit traversal waves */
+#define RM_STAGE_WF_SHADOW 10 /* wavefront shading: shadow-ray traversal waves */
+#define RM_STAGE_WF_SHADE 11 /* wavefront shading: shading waves (incl. the first) */
+#define RM_STAGE_COUNT 12
+/* level 0: off; 1: one event pair per stage (the wavefront shading loop counts
+ * as RM_STAGE_SHADE); 2: also every wavefront launch in its own stage. */
+int rmcuda_profile(rmcuda_ctx* ctx, int level);
 /* Per-stage device counters since the last reset: n records of
  * {path samples, rays, BVH nodes visited, triangle tests}. */
 int rmcuda_stage_counters(rmcuda_ctx* ctx, uint64_t* out, int32_t n);
+/* Queue lengths of the last frame's wavefront shading: for each wave
+ * (paths shaded, extension rays, shadow rays), at most `cap` waves written
+ * to `out` (3 ints each).  Returns the number of waves of that frame. */
+int rmcuda_wave_log(rmcuda_ctx* ctx, int32_t* out, int32_t cap);
 int rmcuda_stage_times(rmcuda_ctx* ctx, double* ms, uint64_t* launches, int32_t n);
 
 #ifdef __cplusplus

@@ -132,8 +132,8 @@ class Backend:
     def stats_reset(self) -> None:
         self.lib.rmcuda_stats_reset(self.h)
 
-    def profile(self, enable: bool = True) -> None:
-        self.lib.rmcuda_profile(self.h, int(enable))
+    def profile(self, level: int = 1) -> None:
+        self.lib.rmcuda_profile(self.h, int(level))
 
     def stage_times(self) -> dict:
         n = len(_abi.STAGES)
@@ -141,6 +141,14 @@ class Backend:
         cnt = (C.c_uint64 * n)()
         self.lib.rmcuda_stage_times(self.h, ms, cnt, n)
         return {name: (ms[i], int(cnt[i])) for i, name in enumerate(_abi.STAGES)}
+
+    def wave_log(self) -> np.ndarray:
+        """(act, ext, shd) queue lengths per wave of the last wavefront frame."""
+        n = self.lib.rmcuda_wave_log(self.h, None, 0)
+        out = np.zeros((max(n, 0), 3), np.int32)
+        if n > 0:
+            self.lib.rmcuda_wave_log(self.h, out.ctypes.data_as(C.POINTER(C.c_int32)), n)
+        return out
 
     def stage_counters(self) -> dict:
         n = len(_abi.STAGES)

@@ -106,11 +106,13 @@ EXPORTS = [
     ("rmcuda_stats_reset", C.c_int, [_P]),
     ("rmcuda_profile", C.c_int, [_P, C.c_int]),
     ("rmcuda_stage_counters", C.c_int, [_P, C.POINTER(C.c_uint64), C.c_int32]),
+    ("rmcuda_wave_log", C.c_int, [_P, C.POINTER(C.c_int32), C.c_int32]),
     ("rmcuda_trace_noalloc", C.c_int, [_P, C.c_int32, _P, C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _S, _Z]),
     ("rmcuda_stage_times", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int32]),
 ]
 
-STAGES = ["plain", "hash", "generate", "spatial", "shade", "temporal", "atrous0", "atrous1", "tonemap"]
+STAGES = ["plain", "hash", "generate", "spatial", "shade", "temporal", "atrous0", "atrous1", "tonemap", "wf_extend",
+          "wf_shadow", "wf_shade"]
 
 _lib = None
 

@@ -28,7 +28,7 @@ NVFLAGS = ARCH + [
     "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
     f"-I{ROOT / 'include'}", f"-I{CSRC}",
 ]
-CU_SOURCES = ["rm_kernels.cu", "rm_denoise.cu", "rm_bvh.cu", "rmcuda_api.cu", "rm_noalloc.cu"]
+CU_SOURCES = ["rm_kernels.cu", "rm_denoise.cu", "rm_bvh.cu", "rmcuda_api.cu", "rm_noalloc.cu", "rm_wavefront.cu"]
 CXX_SOURCES = ["shim_metal.cpp"]
 
 

@@ -27,6 +27,13 @@
 
 namespace rmd {
 
+#define RM_TRY_(x)                         \
+  do {                                     \
+    cudaError_t e_ = (x);                  \
+    if (e_ != cudaSuccess) return e_;      \
+  } while (0)
+
+
 cudaError_t DevBuf::reserve(size_t bytes) {
   if (bytes <= cap && ptr) return cudaSuccess;
   if (ptr) { cudaFree(ptr); ptr = nullptr; cap = 0; }
@@ -309,6 +316,54 @@ __global__ void k_hash(const unsigned long long* __restrict__ w, size_t n, unsig
   for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
 }
+
+__global__ void k_light_records(const rm_triangle* __restrict__ tris, const int32_t* __restrict__ lights, int n,
+                                float4* __restrict__ rec) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const rm_triangle& t = tris[lights[i]];
+  rec[size_t(i) * 4 + 0] = make_float4(t.v0.x, t.v0.y, t.v0.z, t.er);
+  rec[size_t(i) * 4 + 1] = make_float4(t.v1.x, t.v1.y, t.v1.z, t.eg);
+  rec[size_t(i) * 4 + 2] = make_float4(t.v2.x, t.v2.y, t.v2.z, t.eb);
+  rec[size_t(i) * 4 + 3] = make_float4(t.nn.x, t.nn.y, t.nn.z, t.alpha);
+}
+
+// guide[g] = first index with cdf >= g * step (the last index if none);
+// guide[G] = L - 1.
+__global__ void k_light_guide(const float* __restrict__ cdf, int L, int G, float step, int32_t* __restrict__ guide) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > G) return;
+  if (g == G) { guide[g] = L - 1; return; }
+  const float th = float(g) * step;
+  int lo = 0, hi = L - 1;
+  while (lo < hi) {
+    int mid = (lo + hi) / 2;
+    if (cdf[mid] >= th) hi = mid; else lo = mid + 1;
+  }
+  guide[g] = lo;
+}
+
+}  // namespace
+
+cudaError_t prepare_lights(const rm_triangle* d_tris, const int32_t* d_lights, const float* d_cdf, int n_lights,
+                           float light_total, DevBuf& rec, DevBuf& guide, int& guide_n, float& guide_inv,
+                           cudaStream_t st) {
+  guide_n = 0;
+  guide_inv = 0.0f;
+  if (n_lights <= 0 || !(light_total > 1e-12f)) return cudaSuccess;
+  RM_TRY_(rec.reserve(size_t(n_lights) * 4 * sizeof(float4)));
+  k_light_records<<<(n_lights + 255) / 256, 256, 0, st>>>(d_tris, d_lights, n_lights, rec.as<float4>());
+  int G = 1;
+  while (G < n_lights && G < 65536) G <<= 1;
+  RM_TRY_(guide.reserve(size_t(G + 1) * sizeof(int32_t)));
+  const float step = light_total / float(G);
+  k_light_guide<<<(G + 1 + 255) / 256, 256, 0, st>>>(d_cdf, n_lights, G, step, guide.as<int32_t>());
+  guide_n = G;
+  guide_inv = float(G) / light_total;
+  return cudaGetLastError();
+}
+
+namespace {
 
 }  // namespace
 

@@ -49,7 +49,33 @@ struct Scene {
   int n_lights;
   float light_total;
   const rm_vec3* __restrict__ texels;
+  // Light sampling accelerators (built at upload, rm_bvh.cu k_light_prep):
+  // lrec: 4 x float4 per light, in light-list order: (v0, er), (v1, eg),
+  // (v2, eb), (nn, alpha) of triangle lights[i];  guide: guide_n + 1 entries,
+  // guide[g] = first light index whose CDF value is >= g * guide_step.
+  const float4* __restrict__ lrec;
+  const int32_t* __restrict__ guide;
+  int guide_n;
+  float guide_inv;  // guide_n / light_total
 };
+
+// One emissive triangle as light sampling reads it (the fields of
+// rm_triangle that NEE uses, with the same names).
+struct LightRec {
+  rm_vec3 v0, v1, v2, nn;
+  float er, eg, eb, alpha;
+};
+
+__device__ __forceinline__ LightRec load_light(const Scene& s, int i) {
+  const float4* r = s.lrec + size_t(i) * 4;
+  const float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
+  LightRec t;
+  t.v0 = rm_vec3{a.x, a.y, a.z}; t.er = a.w;
+  t.v1 = rm_vec3{b.x, b.y, b.z}; t.eg = b.w;
+  t.v2 = rm_vec3{c.x, c.y, c.z}; t.eb = c.w;
+  t.nn = rm_vec3{d.x, d.y, d.z}; t.alpha = d.w;
+  return t;
+}
 
 // metal_types.h:21-30 plus this build's switches.
 struct Params {
@@ -124,20 +150,36 @@ struct Bsdf { float r, g, b, pdf; };
 // the Moller-Trumbore test would accept: the hit is independent of the BVH.
 struct TraceResult { float t; int tri; float u, v; };
 
-template <bool kAnyHit>
-__device__ __forceinline__ TraceResult traverse(const Scene& s, float ox, float oy, float oz, float dx, float dy,
-                                                float dz, float tmax, uint32_t* err, uint32_t& n_nodes,
-                                                uint32_t& n_tests) {
-  TraceResult r{tmax, -1, 0.f, 0.f};
-  if (s.n_nodes == 0) return r;
-  const float ix = 1.0f / (dx == 0.0f ? 1e-30f : dx);
-  const float iy = 1.0f / (dy == 0.0f ? 1e-30f : dy);
-  const float iz = 1.0f / (dz == 0.0f ? 1e-30f : dz);
-  int stack[kStack];
-  int sp = 0;
-  int node = 0;       // internal node index, or -1 when a leaf is pending
-  int leaf_first = 0, leaf_count = 0;
-  for (;;) {
+// Resumable traversal of one ray: init() then step() until it returns true.
+// A step visits child-pair records until a leaf is pending (descending into
+// the nearer child, pushing the farther one as an 8-bit count / 24-bit link
+// word), tests that leaf, and pops the next subtree.  The persistent kernels
+// interleave steps of different rays on one thread; traverse() below runs
+// one ray to the end.
+struct Trav {
+  float ox, oy, oz, dx, dy, dz, ix, iy, iz;
+  TraceResult r;
+  int sp, node, leaf_first, leaf_count;
+
+  __device__ __forceinline__ void init(float ox_, float oy_, float oz_, float dx_, float dy_, float dz_, float tmax) {
+    ox = ox_; oy = oy_; oz = oz_; dx = dx_; dy = dy_; dz = dz_;
+    ix = 1.0f / (dx == 0.0f ? 1e-30f : dx);
+    iy = 1.0f / (dy == 0.0f ? 1e-30f : dy);
+    iz = 1.0f / (dz == 0.0f ? 1e-30f : dz);
+    r = TraceResult{tmax, -1, 0.f, 0.f};
+    sp = 0;
+    node = 0;
+    leaf_first = 0;
+    leaf_count = 0;
+  }
+
+  // Returns true when the ray is finished (r holds the result).  `stack` is
+  // the caller's kStack-entry array (kept out of the struct so that the scalar
+  // state stays in registers).
+  template <bool kAnyHit>
+  __device__ __forceinline__ bool step(const Scene& s, int* stack, uint32_t* err, uint32_t& n_nodes,
+                                       uint32_t& n_tests) {
+    if (s.n_nodes == 0) return true;
     while (node >= 0 && leaf_count == 0) {
       ++n_nodes;
       const float4* n = s.nodes + size_t(node) * 4;
@@ -163,7 +205,7 @@ __device__ __forceinline__ TraceResult traverse(const Scene& s, float ox, float 
       if (hit0 && hit1) {
         int first = d.x, firstc = d.z, second = d.y, secondc = d.w;
         if (n1 < n0) { first = d.y; firstc = d.w; second = d.x; secondc = d.z; }
-        if (sp >= kStack) { atomicOr(err, kErrStack); return r; }
+        if (sp >= kStack) { atomicOr(err, kErrStack); return true; }
         stack[sp++] = int((uint32_t(secondc) << 24) | uint32_t(second));  // far child: 8-bit count, 24-bit link
         if (firstc > 0) { leaf_first = first; leaf_count = firstc; node = -1; }
         else node = first;
@@ -172,7 +214,7 @@ __device__ __forceinline__ TraceResult traverse(const Scene& s, float ox, float 
         if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
         else node = link;
       } else {
-        if (sp == 0) return r;
+        if (sp == 0) return true;
         const int e = stack[--sp];
         const int cnt = int(uint32_t(e) >> 24), link = e & 0xFFFFFF;
         if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
@@ -205,16 +247,29 @@ __device__ __forceinline__ TraceResult traverse(const Scene& s, float ox, float 
       float dd = (q2.x * qx + q2.y * qy + q2.z * qz) / det;
       if (dd > 1e-8f && (dd < r.t || (dd == r.t && r.tri >= 0 && j < r.tri))) {
         r.t = dd; r.tri = j; r.u = u; r.v = v;
-        if (kAnyHit) return r;
+        if (kAnyHit) return true;
       }
     }
     leaf_count = 0;
-    if (sp == 0) return r;
+    if (sp == 0) return true;
     const int e = stack[--sp];
     const int cnt = int(uint32_t(e) >> 24), link = e & 0xFFFFFF;
     if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
     else node = link;
+    return false;
   }
+};
+
+template <bool kAnyHit>
+__device__ __forceinline__ TraceResult traverse(const Scene& s, float ox, float oy, float oz, float dx, float dy,
+                                                float dz, float tmax, uint32_t* err, uint32_t& n_nodes,
+                                                uint32_t& n_tests) {
+  Trav t;
+  int stack[kStack];
+  t.init(ox, oy, oz, dx, dy, dz, tmax);
+  while (!t.step<kAnyHit>(s, stack, err, n_nodes, n_tests)) {
+  }
+  return t.r;
 }
 
 // ---------------------------------------------------------------- tracer
@@ -256,6 +311,12 @@ struct Tracer {
   __device__ __noinline__ Hit cast_ray(float ox, float oy, float oz, float dx, float dy, float dz, float dist) {
     ++rays;
     TraceResult tr = traverse<false>(s, ox, oy, oz, dx, dy, dz, dist, err, nodes, tests);
+    return attributes(tr, ox, oy, oz, dx, dy, dz);
+  }
+
+  // Surface attributes of a traversal result (the second half of cast_ray).
+  __device__ __forceinline__ Hit attributes(const TraceResult& tr, float ox, float oy, float oz, float dx, float dy,
+                                            float dz) const {
     Hit h;
     h.t = tr.t; h.tri = tr.tri; h.u = tr.u; h.v = tr.v;
     h.px = ox + dx * h.t; h.py = oy + dy * h.t; h.pz = oz + dz * h.t;
@@ -396,13 +457,24 @@ struct Tracer {
     return out;
   }
 
-  __device__ __forceinline__ int pick_light(float pick) {
+  // Index into the light list of the first CDF entry >= pick, or the last
+  // entry (pathtrace.metal:323-331).  The guide table narrows the binary
+  // search to the entries between guide[g-1] and guide[g+2] around the
+  // pick's bucket g; the one-bucket margins absorb the rounding of the bucket
+  // index, so the result is the same index the full search returns.
+  __device__ __forceinline__ int pick_light(float pick) const {
     int lo = 0, hi = p.lights - 1;
+    if (s.guide_n > 0) {
+      int g = int(pick * s.guide_inv);
+      g = g < 0 ? 0 : (g >= s.guide_n ? s.guide_n - 1 : g);
+      lo = __ldg(s.guide + (g > 0 ? g - 1 : 0));
+      hi = __ldg(s.guide + (g + 2 < s.guide_n ? g + 2 : s.guide_n));
+    }
     while (lo < hi) {
       int mid = (lo + hi) / 2;
       if (__ldg(s.cdf + mid) >= pick) hi = mid; else lo = mid + 1;
     }
-    return __ldg(s.lights + lo);
+    return lo;
   }
 
   // pathtrace.metal:299-469
@@ -425,7 +497,7 @@ struct Tracer {
     const float LT = p.light_total;
     if (Mc <= 1) {
       float pick = U() * LT;
-      const rm_triangle& t = s.tris[pick_light(pick)];
+      const LightRec t = load_light(s, pick_light(pick));
       float lu = U(), lv = U();
       if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
       float lw = 1.0f - lu - lv;
@@ -474,7 +546,7 @@ struct Tracer {
     bool have = false;
     for (int j = 0; j < Mc; ++j) {
       float pick = U() * LT;
-      const rm_triangle& t = s.tris[pick_light(pick)];
+      const LightRec t = load_light(s, pick_light(pick));
       float lu = U(), lv = U();
       if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
       float lw = 1.0f - lu - lv;
@@ -526,6 +598,134 @@ struct Tracer {
     vdx *= vinv; vdy *= vinv; vdz *= vinv;
     float sox = px + nx * 0.002f, soy = py + ny * 0.002f, soz = pz + nz * 0.002f;
     if (occluded(sox, soy, soz, vdx, vdy, vdz, vdist - 0.003f)) return;
+    float W = sumW / (float(Mc) * sel_phat);
+    o_r = sel_Fr * W * wnee;
+    o_g = sel_Fg * W * wnee;
+    o_b = sel_Fb * W * wnee;
+  }
+
+  // direct_lighting for opaque scenes with the visibility test left to the
+  // caller: the same draws and arithmetic, returning the contribution a
+  // visible light would add (o_*) and the shadow ray to test (has_ray).  In an
+  // opaque scene the visibility test consumes no random numbers and changes
+  // nothing but the contribution (out_sumW is the same either way), so testing
+  // the ray later in a separate pass gives the same result.
+  __device__ __noinline__ void direct_lighting_deferred(float px, float py, float pz, float nx, float ny, float nz,
+                                                        float wox, float woy, float woz, float rough, float metallic,
+                                                        float spec_prob, float ar, float ag, float ab, float& o_r,
+                                                        float& o_g, float& o_b, float& out_sumW, uint32_t& out_M,
+                                                        bool& has_ray, float& sox, float& soy, float& soz,
+                                                        float& sdx, float& sdy, float& sdz, float& sdist) {
+    o_r = o_g = o_b = 0.0f;
+    out_sumW = 0.0f;
+    out_M = 0;
+    has_ray = false;
+    if (p.lights == 0 || !(p.light_total > 1e-12f)) return;
+    int Mc = p.restir_candidates;
+    if (Mc < 1) Mc = 1;
+    if (Mc > 32) Mc = 32;
+    float r2 = rough;
+    if (r2 < 0.0f) r2 = 0.0f;
+    if (r2 > 1.0f) r2 = 1.0f;
+    if (r2 < 0.02f) r2 = 0.02f;
+    float alpha2 = (r2 * r2) * (r2 * r2);
+    const float LT = p.light_total;
+    if (Mc <= 1) {
+      float pick = U() * LT;
+      const LightRec t = load_light(s, pick_light(pick));
+      float lu = U(), lv = U();
+      if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
+      float lw = 1.0f - lu - lv;
+      float ldx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x) - px;
+      float ldy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y) - py;
+      float ldz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z) - pz;
+      float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
+      if (!(dist > 0.003f)) { out_M = 1; return; }
+      float inv = 1.0f / dist;
+      ldx *= inv; ldy *= inv; ldz *= inv;
+      float lcos = -(t.nn.x * ldx + (t.nn.y * ldy + t.nn.z * ldz));
+      float scos = nx * ldx + (ny * ldy + nz * ldz);
+      if (!(lcos > 1e-8f && scos > 1e-8f)) { out_M = 1; return; }
+      float lt_lum = lum3(t.er, t.eg, t.eb);
+      if (lt_lum < 1e-6f) lt_lum = 1e-6f;
+      float pdf = dist * dist * lt_lum / (lcos * LT);
+      has_ray = true;
+      sox = px + nx * 0.002f; soy = py + ny * 0.002f; soz = pz + nz * 0.002f;
+      sdx = ldx; sdy = ldy; sdz = ldz; sdist = dist - 0.003f;
+      Bsdf e = eval_bsdf(ldx, ldy, ldz, wox, woy, woz, nx, ny, nz, alpha2, metallic, spec_prob, ar, ag, ab);
+      out_M = 1;
+      if (!(pdf > 1e-12f)) return;
+      float Fr = t.er * e.r * scos * t.alpha;
+      float Fg = t.eg * e.g * scos * t.alpha;
+      float Fb = t.eb * e.b * scos * t.alpha;
+      float ph = lum3(Fr, Fg, Fb);
+      out_sumW = (ph > 0.0f) ? ph / pdf : 0.0f;
+      float wnee = 1.0f;
+      if (!p.nomis && e.pdf > 1e-20f) wnee = pdf / (pdf + e.pdf);
+      float k = scos * wnee * t.alpha / pdf;
+      o_r = t.er * e.r * k;
+      o_g = t.eg * e.g * k;
+      o_b = t.eb * e.b * k;
+      return;
+    }
+    float sumW = 0.0f;
+    float sel_lx = 0, sel_ly = 0, sel_lz = 0, sel_Fr = 0, sel_Fg = 0, sel_Fb = 0, sel_phat = 0, sel_epdf = 0;
+    bool have = false;
+    for (int j = 0; j < Mc; ++j) {
+      float pick = U() * LT;
+      const LightRec t = load_light(s, pick_light(pick));
+      float lu = U(), lv = U();
+      if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
+      float lw = 1.0f - lu - lv;
+      float qx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x);
+      float qy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y);
+      float qz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z);
+      float ldx = qx - px, ldy = qy - py, ldz = qz - pz;
+      float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
+      float w = 0, ph = 0, epdf = 0, Fr = 0, Fg = 0, Fb = 0;
+      if (dist > 0.003f) {
+        float inv = 1.0f / dist;
+        float dxn = ldx * inv, dyn = ldy * inv, dzn = ldz * inv;
+        float lcos = -(t.nn.x * dxn + (t.nn.y * dyn + t.nn.z * dzn));
+        float scos = nx * dxn + (ny * dyn + nz * dzn);
+        if (lcos > 1e-8f && scos > 1e-8f) {
+          float lt_lum = lum3(t.er, t.eg, t.eb);
+          if (lt_lum < 1e-6f) lt_lum = 1e-6f;
+          float q = dist * dist * lt_lum / (lcos * LT);
+          if (q > 1e-12f) {
+            Bsdf e = eval_bsdf(dxn, dyn, dzn, wox, woy, woz, nx, ny, nz, alpha2, metallic, spec_prob, ar, ag, ab);
+            epdf = e.pdf;
+            Fr = t.er * e.r * scos * t.alpha;
+            Fg = t.eg * e.g * scos * t.alpha;
+            Fb = t.eb * e.b * scos * t.alpha;
+            ph = lum3(Fr, Fg, Fb);
+            if (ph > 0.0f) w = ph / q;
+          }
+        }
+      }
+      sumW += w;
+      float r = U();
+      if (w > 0.0f && r * sumW < w) {
+        have = true;
+        sel_lx = qx; sel_ly = qy; sel_lz = qz;
+        sel_Fr = Fr; sel_Fg = Fg; sel_Fb = Fb;
+        sel_phat = ph; sel_epdf = epdf;
+      }
+    }
+    out_sumW = sumW;
+    out_M = uint32_t(Mc);
+    if (!have || !(sumW > 0.0f) || !(sel_phat > 0.0f)) return;
+    float pdf_ris = float(Mc) * sel_phat / sumW;
+    float wnee = 1.0f;
+    if (!p.nomis && sel_epdf > 1e-20f) wnee = pdf_ris / (pdf_ris + sel_epdf);
+    float vdx = sel_lx - px, vdy = sel_ly - py, vdz = sel_lz - pz;
+    float vdist = sqrtf(vdx * vdx + vdy * vdy + vdz * vdz);
+    if (!(vdist > 0.003f)) return;
+    float vinv = 1.0f / vdist;
+    vdx *= vinv; vdy *= vinv; vdz *= vinv;
+    has_ray = true;
+    sox = px + nx * 0.002f; soy = py + ny * 0.002f; soz = pz + nz * 0.002f;
+    sdx = vdx; sdy = vdy; sdz = vdz; sdist = vdist - 0.003f;
     float W = sumW / (float(Mc) * sel_phat);
     o_r = sel_Fr * W * wnee;
     o_g = sel_Fg * W * wnee;

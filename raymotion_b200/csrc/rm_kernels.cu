@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256) k_restir_generate(Scene s, Params p, uint
         const float sox = px + pnx * 0.002f, soy = py + pny * 0.002f, soz = pz + pnz * 0.002f;
         for (int j = 0; j < Mc; ++j) {
           float pick = pt.U() * p.light_total;
-          const rm_triangle& t = s.tris[pt.pick_light(pick)];
+          const LightRec t = load_light(s, pt.pick_light(pick));
           float lu = pt.U(), lv = pt.U();
           if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
           float lw = 1.0f - lu - lv;

@@ -21,6 +21,45 @@ cudaError_t launch_restir_stage(int stage, const Scene& s, const Params& p, uint
 cudaError_t launch_trace(const Scene& s, const float* rays, int n, int any_hit, int32_t* tri, float* t, float* u,
                          float* v, uint32_t* err, cudaStream_t st);
 
+// rm_wavefront.cu: ReSTIR shading as wavefront stages.  Path slots are SoA
+// arrays indexed by pixel id.
+struct WfState {
+  uint4* u;      // rng, meta, samples done, vertex index
+  float4* sum;   // sample sum, last_pdf
+  float4* acc;   // path radiance, psumW
+  float4* thr;   // throughput, previous BSDF cosine
+  float4* pb;    // previous BSDF value, previous reservoir M
+  float4* o;     // extension ray origin
+  float4* d;     // extension ray direction
+  float4* c;     // contribution of the pending shadow ray if visible
+  float4* so;    // shadow ray origin, length
+  float4* sd;    // shadow ray direction
+  float4* hit;   // t, u, v, triangle
+  float4* base;  // kind 1: emission + primary direct light, reservoir sumWu
+  uint32_t* occ;
+  uint32_t* mM;  // kind 1: reservoir M
+};
+// Queue slots of one wave: extension rays, shadow rays, then the paths to
+// shade sorted by vertex type (a: opaque hit, b: dielectric hit, c: no vertex).
+constexpr int kCntExt = 0, kCntShd = 1, kCntA = 2, kCntB = 3, kCntC = 4, kCntFetchExt = 5, kCntFetchShd = 6;
+constexpr int kCntSlots = 8;
+struct WfQueues {
+  int* ext;
+  int* shd;
+  int* qa;
+  int* qb;
+  int* qc;
+  int* counts;  // kCntSlots ints
+};
+cudaError_t launch_wavefront_init(const Scene& s, const Params& p, uint64_t seed, const GBufSoA& gb, const ResSoA& rm,
+                                  const WfState& w, const WfQueues& q, float* hdr, uint32_t* dbg,
+                                  unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+cudaError_t launch_wavefront_trace(const Scene& s, const WfState& w, const WfQueues& q, int bound, bool shadow,
+                                   unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+cudaError_t launch_wavefront_shade(int vk, const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w,
+                                   const WfQueues& cq, int bound, const WfQueues& nq, float* hdr, uint32_t* dbg,
+                                   unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+
 // rm_denoise.cu
 // stage 0 temporal (in + hist_in -> out), 1 / 2 a-trous step 0 / 1 (in -> out, + RGB8 when rgb != nullptr)
 cudaError_t launch_denoise_stage(int stage, const Params& p, const GBufSoA& gb, const GBufSoA& hg, const float* in,
@@ -94,6 +133,10 @@ struct DevBvhView {
 cudaError_t build_lbvh_into(const rm_triangle* d_tris, int n, int leaf_max, const LbvhScratch& w, DevBvhView& out,
                             cudaStream_t st, std::string& err);
 size_t lbvh_box_bytes();
+// Light records and CDF guide table for light sampling (see Scene in rm_device.cuh).
+cudaError_t prepare_lights(const rm_triangle* d_tris, const int32_t* d_lights, const float* d_cdf, int n_lights,
+                           float light_total, DevBuf& rec, DevBuf& guide, int& guide_n, float& guide_inv,
+                           cudaStream_t st);
 // 64-bit content hash of a device byte range (order-sensitive per 8-byte word).
 cudaError_t device_hash(const void* d_bytes, size_t n_bytes, unsigned long long* d_out, cudaStream_t st);
 

@@ -1,0 +1,590 @@
+// rm_wavefront.cu - ReSTIR shading (reference restir_shade, pathtrace.metal:1056-1258)
+// as wavefront stages over compacted queues.
+//
+// The reference shades with one thread per pixel that loops over all samples
+// of its pixel; on a GPU the 32 threads of a warp are then almost never in the
+// same phase (traversal, RIS candidates, BSDF sampling, next sample).  Here a
+// frame runs in waves of three kernels:
+//   k_wf_extend  closest-hit traversal of every queued extension ray,
+//   k_wf_shadow  any-hit traversal of every queued shadow ray,
+//   k_wf_shade   for every path touched this wave: fold in its shadow result,
+//                shade its hit, sample the next direction, and queue its next
+//                rays (or finish the sample and start the next one),
+// with warp-aggregated atomic appends building the next wave's queues.
+//
+// Results stay bit-identical to the one-thread-per-pixel kernel because
+// (i) each pixel has at most one path in flight, so its random stream is
+// consumed in the same order; (ii) the scene is opaque (ReSTIR requires it,
+// metal.mm:237), so a shadow test consumes no random numbers and only gates
+// the light contribution, which is computed at the vertex and added to the
+// path sum at the start of the next shade, before anything else is added;
+// (iii) every expression keeps the reference's operand order.
+#include <cuda_runtime.h>
+
+#include "rm_device.cuh"
+#include "rm_launch.h"
+
+namespace rmd {
+
+namespace {
+
+// meta bits of a path slot
+constexpr uint32_t kInd = 1u;        // K5 indirect path (kind 1); else camera path (kind 3)
+constexpr uint32_t kDelta = 2u;      // previous vertex was delta (pdel / prev_delta)
+constexpr uint32_t kExt = 4u;        // an extension ray is queued
+constexpr uint32_t kShadow = 8u;     // a shadow ray is queued
+constexpr uint32_t kFinish = 16u;    // path ended; its last shadow ray is still queued
+
+struct PathRegs {
+  float ax, ay, az, tx, ty, tz;
+  float ox, oy, oz, dx, dy, dz;
+  float last_pdf, psumW, pbr, pbg, pbb, pbcos;
+  uint32_t pM;
+  int v;
+  uint32_t meta;
+};
+
+__device__ __forceinline__ void load(const WfState& w, uint32_t i, PathRegs& r, uint32_t& rng, uint32_t& n,
+                                     float& sr, float& sg, float& sb) {
+  const uint4 u = w.u[i];
+  rng = u.x; r.meta = u.y; n = u.z; r.v = int(u.w);
+  const float4 sum = w.sum[i], acc = w.acc[i], thr = w.thr[i], pb = w.pb[i], o = w.o[i], d = w.d[i];
+  sr = sum.x; sg = sum.y; sb = sum.z; r.last_pdf = sum.w;
+  r.ax = acc.x; r.ay = acc.y; r.az = acc.z; r.psumW = acc.w;
+  r.tx = thr.x; r.ty = thr.y; r.tz = thr.z; r.pbcos = thr.w;
+  r.pbr = pb.x; r.pbg = pb.y; r.pbb = pb.z; r.pM = uint32_t(__float_as_int(pb.w));
+  r.ox = o.x; r.oy = o.y; r.oz = o.z; r.dx = d.x; r.dy = d.y; r.dz = d.z;
+}
+
+__device__ __forceinline__ void store(const WfState& w, uint32_t i, const PathRegs& r, uint32_t rng, uint32_t n,
+                                      float sr, float sg, float sb) {
+  w.u[i] = make_uint4(rng, r.meta, n, uint32_t(r.v));
+  w.sum[i] = make_float4(sr, sg, sb, r.last_pdf);
+  w.acc[i] = make_float4(r.ax, r.ay, r.az, r.psumW);
+  w.thr[i] = make_float4(r.tx, r.ty, r.tz, r.pbcos);
+  w.pb[i] = make_float4(r.pbr, r.pbg, r.pbb, __int_as_float(int(r.pM)));
+  w.o[i] = make_float4(r.ox, r.oy, r.oz, 0.f);
+  w.d[i] = make_float4(r.dx, r.dy, r.dz, 0.f);
+}
+
+// Append flagged threads to a queue; the threads of a warp that reach this
+// together share one atomic.
+__device__ __forceinline__ void append(int* q, int* count, bool flag, int value) {
+  const unsigned m = __activemask();
+  const unsigned b = __ballot_sync(m, flag);
+  if (!b) return;
+  const int lane = int(threadIdx.x & 31);
+  const int leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(b));
+  base = __shfl_sync(m, base, leader);
+  if (flag) q[base + __popc(b & ((1u << lane) - 1u))] = value;
+}
+
+__device__ __forceinline__ void warp_add(unsigned long long* ctr, uint32_t v) {
+  unsigned long long s = __reduce_add_sync(0xffffffffu, v);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(ctr, s);
+}
+
+__device__ __forceinline__ void clamp3(const Params& p, float& r, float& g, float& b) {
+  if (p.clamp_value > 0.0f) {
+    r = fminf(r, p.clamp_value); g = fminf(g, p.clamp_value); b = fminf(b, p.clamp_value);
+  }
+}
+
+// Pixel constants of a kind-1 pixel (pathtrace.metal:1086-1128): the primary
+// direct light from the merged reservoir.
+struct Pixel1 {
+  float gpx, gpy, gpz, gnx, gny, gnz, wox, woy, woz, ar, ag, ab, rough, metallic, alpha2, spec_prob;
+};
+
+__device__ __forceinline__ Pixel1 pixel1(const GBufSoA& gb, uint32_t id) {
+  const float4 PK = gb.pos_kind[id], NR = gb.nor_rough[id], AM = gb.alb_met[id], WO = gb.wo_ior[id];
+  Pixel1 q;
+  q.gpx = PK.x; q.gpy = PK.y; q.gpz = PK.z; q.gnx = NR.x; q.gny = NR.y; q.gnz = NR.z;
+  q.wox = WO.x; q.woy = WO.y; q.woz = WO.z; q.ar = AM.x; q.ag = AM.y; q.ab = AM.z;
+  float rough = NR.w; if (rough < 0.0f) rough = 0.0f; if (rough > 1.0f) rough = 1.0f;
+  float metallic = AM.w; if (metallic < 0.0f) metallic = 0.0f; if (metallic > 1.0f) metallic = 1.0f;
+  float r2 = rough; if (r2 < 0.02f) r2 = 0.02f;
+  q.alpha2 = (r2 * r2) * (r2 * r2);
+  float sp = 0.05f + 0.95f * metallic; if (sp > 0.98f) sp = 0.98f;
+  if (metallic >= 0.999f) sp = 1.0f;
+  q.rough = rough; q.metallic = metallic; q.spec_prob = sp;
+  return q;
+}
+
+// Start samples of a pixel until one has a ray to trace or all spp are done.
+// Returns true when an extension ray was produced.
+__device__ bool start_samples(Tracer& pt, const Params& p, const GBufSoA& gb, const WfState& w, uint32_t id,
+                              uint32_t x, uint32_t y, PathRegs& r, uint32_t& n, float& sr, float& sg, float& sb) {
+  const bool ind = (r.meta & kInd) != 0;
+  if (ind) {
+    const Pixel1 q = pixel1(gb, id);
+    const float4 base = w.base[id];
+    const uint32_t m_M = w.mM[id];
+    while (n < uint32_t(p.spp)) {
+      float nx2 = 0, ny2 = 0, nz2 = 0;
+      int pdelta = 0;
+      bool early = false;
+      if (pt.U() < q.spec_prob) {
+        float hx, hy, hz;
+        pt.sample_ggx_half(q.alpha2, q.gnx, q.gny, q.gnz, hx, hy, hz);
+        float md = q.wox * hx + (q.woy * hy + q.woz * hz);
+        if (!(md > 1e-8f)) early = true;
+        else {
+          nx2 = 2.0f * md * hx - q.wox; ny2 = 2.0f * md * hy - q.woy; nz2 = 2.0f * md * hz - q.woz;
+          pdelta = (q.rough <= 0.0201f) ? 1 : 0;
+        }
+      } else {
+        pt.sample_cosine(q.gnx, q.gny, q.gnz, nx2, ny2, nz2);
+        pdelta = 0;
+      }
+      Bsdf e0{0.f, 0.f, 0.f, 0.f};
+      if (!early) {
+        float ncos = nx2 * q.gnx + (ny2 * q.gny + nz2 * q.gnz);
+        if (!(ncos > 1e-8f)) early = true;
+        else {
+          float d = 1.0f / sqrtf(nx2 * nx2 + ny2 * ny2 + nz2 * nz2);
+          nx2 *= d; ny2 *= d; nz2 *= d;
+          e0 = Tracer::eval_bsdf(nx2, ny2, nz2, q.wox, q.woy, q.woz, q.gnx, q.gny, q.gnz, q.alpha2, q.metallic,
+                                 q.spec_prob, q.ar, q.ag, q.ab);
+          if (!(e0.pdf > 1e-12f)) early = true;
+        }
+      }
+      if (early) {
+        float fr = base.x, fg = base.y, fb = base.z;
+        clamp3(p, fr, fg, fb);
+        sr += fr; sg += fg; sb += fb;
+        ++n;
+        continue;
+      }
+      float cos0 = nx2 * q.gnx + (ny2 * q.gny + nz2 * q.gnz);
+      r.tx = e0.r * cos0 / e0.pdf; r.ty = e0.g * cos0 / e0.pdf; r.tz = e0.b * cos0 / e0.pdf;
+      r.ox = q.gpx + q.gnx * 0.001f; r.oy = q.gpy + q.gny * 0.001f; r.oz = q.gpz + q.gnz * 0.001f;
+      r.dx = nx2; r.dy = ny2; r.dz = nz2;
+      r.last_pdf = e0.pdf;
+      r.pbr = e0.r; r.pbg = e0.g; r.pbb = e0.b; r.pbcos = cos0;
+      r.psumW = base.w;
+      r.pM = m_M;
+      r.meta = (r.meta & ~kDelta) | (pdelta ? kDelta : 0u);
+      r.ax = r.ay = r.az = 0.0f;
+      r.v = 1;
+      return true;
+    }
+    return false;
+  }
+  // camera path (kind 3): pathtrace.metal:1073-1079 and sample_sensor :729-737
+  while (n < uint32_t(p.spp)) {
+    float sx, sy;
+    pt.jitter(x, y, sx, sy);
+    const rm_camera& cam = p.camera;
+    float focal2 = cam.focal * cam.focal;
+    float dist = 1.0f / sqrtf(sx * sx + (sy * sy + focal2));
+    float tx = sx * dist, ty = sy * dist, tz = cam.focal * dist;
+    r.dx = tx * cam.m0 + (ty * cam.m1 + tz * cam.m2);
+    r.dy = tx * cam.m3 + (ty * cam.m4 + tz * cam.m5);
+    r.dz = tx * cam.m6 + (ty * cam.m7 + tz * cam.m8);
+    r.ox = cam.x; r.oy = cam.y; r.oz = cam.z;
+    r.ax = r.ay = r.az = 0.0f;
+    r.tx = r.ty = r.tz = 1.0f;
+    r.v = 0;
+    r.meta |= kDelta;
+    r.last_pdf = 0.0f; r.psumW = 0.0f; r.pM = 0;
+    r.pbr = r.pbg = r.pbb = r.pbcos = 0.0f;
+    if (p.bounces > 0) return true;
+    float cr = 0.0f, cg = 0.0f, cb = 0.0f;  // no bounce: the path adds nothing
+    clamp3(p, cr, cg, cb);
+    sr += cr; sg += cg; sb += cb;
+    ++n;
+  }
+  return false;
+}
+
+// One vertex of the path loop (pathtrace.metal:564-726 for camera paths,
+// :1175-1251 for kind-1 indirect paths).  Returns true when the path goes on
+// (a new extension ray is in r.o / r.d).  NEE leaves its shadow ray and the
+// contribution of a visible light in shadow / c.
+template <int MAT>  // 0: opaque surface, 1: dielectric (hit.ior > 1.0001)
+__device__ bool vertex(Tracer& pt, const Params& p, PathRegs& r, const Hit& hit, bool& has_shadow, float4& so,
+                       float4& sd, float4& c) {
+  const bool ind = (r.meta & kInd) != 0;
+  float pnx = hit.nix, pny = hit.niy, pnz = hit.niz;
+  float geom = hit.ngx * pnx + (hit.ngy * pny + hit.ngz * pnz);
+  if (geom < 0.0f) { pnx = -pnx; pny = -pny; pnz = -pnz; }
+  float ndot = r.dx * pnx + (r.dy * pny + r.dz * pnz);
+  bool front = true;
+  if (ndot > 0.0f) { pnx = -pnx; pny = -pny; pnz = -pnz; front = false; }
+  float wox = -r.dx, woy = -r.dy, woz = -r.dz;
+  float rough = hit.rough;
+  if (rough < 0.0f) rough = 0.0f;
+  if (rough > 1.0f) rough = 1.0f;
+  if (rough < 0.02f) rough = 0.02f;
+  float alpha = rough * rough;
+  float alpha2 = alpha * alpha;
+  const rm_triangle& lt = pt.s.tris[hit.tri];
+  float metallic = lt.metallic;
+  if (metallic < 0.0f) metallic = 0.0f;
+  if (metallic > 1.0f) metallic = 1.0f;
+  if (r.v == 0 || (r.meta & kDelta)) {
+    r.ax += hit.er * r.tx; r.ay += hit.eg * r.ty; r.az += hit.eb * r.tz;
+  } else {
+    float lx = hit.px - r.ox, ly = hit.py - r.oy, lz = hit.pz - r.oz;
+    float dist2 = lx * lx + ly * ly + lz * lz;
+    float dist = sqrtf(dist2);
+    float pl = 1e30f;
+    const float lta = lt.alpha;
+    if (dist > 1e-20f && r.last_pdf > 1e-20f && r.pM > 0 && r.psumW > 1e-20f) {
+      float ph = lum3(hit.er * r.pbr * r.pbcos * lta, hit.eg * r.pbg * r.pbcos * lta,
+                      hit.eb * r.pbb * r.pbcos * lta);
+      if (ph > 1e-20f) pl = float(r.pM) * ph / r.psumW;
+      else {
+        float inv = 1.0f / dist;
+        float lxn = lx * inv, lyn = ly * inv, lzn = lz * inv;
+        float cos_l = -(lt.nn.x * lxn + (lt.nn.y * lyn + lt.nn.z * lzn));
+        if (cos_l > 1e-8f) {
+          float lum = lum3(lt.er, lt.eg, lt.eb);
+          if (lum < 1e-6f) lum = 1e-6f;
+          pl = dist2 * lum / (cos_l * p.light_total);
+        }
+      }
+    } else if (dist > 1e-20f && r.last_pdf > 1e-20f) {
+      float inv = 1.0f / dist;
+      lx *= inv; ly *= inv; lz *= inv;
+      float cos_l = -(lt.nn.x * lx + (lt.nn.y * ly + lt.nn.z * lz));
+      if (cos_l > 1e-8f) {
+        float lum = lum3(lt.er, lt.eg, lt.eb);
+        if (lum < 1e-6f) lum = 1e-6f;
+        pl = dist2 * lum / (cos_l * p.light_total);
+      }
+    }
+    float w = p.nomis ? 0.0f : ((r.last_pdf + pl > 1e-20f) ? r.last_pdf / (r.last_pdf + pl) : 0.0f);
+    r.ax += hit.er * r.tx * w; r.ay += hit.eg * r.ty * w; r.az += hit.eb * r.tz * w;
+  }
+  if (MAT == 1) {
+    float nx2, ny2, nz2, es;
+    bool valid = pt.sample_dielectric(wox, woy, woz, pnx, pny, pnz, r.dx, r.dy, r.dz, hit.ior, front, rough, alpha2,
+                                      nx2, ny2, nz2, es);
+    if (!valid) return false;
+    r.tx *= es; r.ty *= es; r.tz *= es;
+    float sg = 1.0f;
+    if (nx2 * pnx + (ny2 * pny + nz2 * pnz) < 0.0f) sg = -1.0f;
+    r.ox = hit.px + pnx * 0.001f * sg;
+    r.oy = hit.py + pny * 0.001f * sg;
+    r.oz = hit.pz + pnz * 0.001f * sg;
+    r.dx = nx2; r.dy = ny2; r.dz = nz2;
+    r.meta |= kDelta;
+    r.psumW = 0.0f; r.pM = 0;
+  } else {
+    float spec_prob = 0.05f + 0.95f * metallic;
+    if (spec_prob > 0.98f) spec_prob = 0.98f;
+    if (metallic >= 0.999f) spec_prob = 1.0f;
+    float dlr, dlg, dlb, cur_sumW, sdist, sox, soy, soz, sdx, sdy, sdz;
+    uint32_t cur_M;
+    bool has_ray;
+    pt.direct_lighting_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob,
+                                hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray, sox, soy, soz, sdx,
+                                sdy, sdz, sdist);
+    if (has_ray) {
+      has_shadow = true;
+      so = make_float4(sox, soy, soz, sdist);
+      sd = make_float4(sdx, sdy, sdz, 0.f);
+      c = make_float4(dlr * r.tx, dlg * r.ty, dlb * r.tz, 0.f);
+    }
+    float nx2, ny2, nz2;
+    if (pt.U() < spec_prob) {
+      float hx, hy, hz;
+      pt.sample_ggx_half(alpha2, pnx, pny, pnz, hx, hy, hz);
+      float md = wox * hx + (woy * hy + woz * hz);
+      if (!(md > 1e-8f)) return false;
+      nx2 = 2.0f * md * hx - wox;
+      ny2 = 2.0f * md * hy - woy;
+      nz2 = 2.0f * md * hz - woz;
+      r.meta = (r.meta & ~kDelta) | ((rough <= 0.0201f) ? kDelta : 0u);
+    } else {
+      pt.sample_cosine(pnx, pny, pnz, nx2, ny2, nz2);
+      r.meta &= ~kDelta;
+    }
+    float ncos = nx2 * pnx + (ny2 * pny + nz2 * pnz);
+    if (!(ncos > 1e-8f)) return false;
+    {
+      float d = 1.0f / sqrtf(nx2 * nx2 + ny2 * ny2 + nz2 * nz2);
+      nx2 *= d; ny2 *= d; nz2 *= d;
+    }
+    Bsdf e = Tracer::eval_bsdf(nx2, ny2, nz2, wox, woy, woz, pnx, pny, pnz, alpha2, metallic, spec_prob, hit.ar,
+                               hit.ag, hit.ab);
+    if (!(e.pdf > 1e-12f)) return false;
+    r.last_pdf = e.pdf;
+    float cos_i = nx2 * pnx + (ny2 * pny + nz2 * pnz);
+    r.tx *= e.r * cos_i / e.pdf;
+    r.ty *= e.g * cos_i / e.pdf;
+    r.tz *= e.b * cos_i / e.pdf;
+    r.psumW = cur_sumW; r.pM = cur_M;
+    r.pbr = e.r; r.pbg = e.g; r.pbb = e.b; r.pbcos = cos_i;
+    r.ox = hit.px + pnx * 0.001f;
+    r.oy = hit.py + pny * 0.001f;
+    r.oz = hit.pz + pnz * 0.001f;
+    r.dx = nx2; r.dy = ny2; r.dz = nz2;
+  }
+  if (!ind) {
+    if (r.tx < 0.0f) r.tx = 0.0f;
+    if (r.ty < 0.0f) r.ty = 0.0f;
+    if (r.tz < 0.0f) r.tz = 0.0f;
+  }
+  float mx = fmaxf(r.tx, r.ty);
+  mx = fmaxf(mx, r.tz);
+  if (!(mx >= 1e-12f)) return false;
+  if (p.rr && r.v >= (ind ? 2 : 1)) {
+    float rr = mx;
+    if (rr < 0.05f) rr = 0.05f;
+    if (rr > 0.9f) rr = 0.9f;
+    if (!(pt.U() <= rr)) return false;
+    float ir = 1.0f / rr;
+    r.tx *= ir; r.ty *= ir; r.tz *= ir;
+  }
+  r.v += 1;
+  return r.v < p.bounces;
+}
+
+// Finish the current sample (pathtrace.metal:1077-1078 camera, :1252-1254 kind 1).
+__device__ __forceinline__ void finish_sample(const Params& p, const WfState& w, uint32_t id, const PathRegs& r,
+                                              uint32_t& n, float& sr, float& sg, float& sb) {
+  float fr, fg, fb;
+  if (r.meta & kInd) {
+    const float4 base = w.base[id];
+    fr = base.x + r.ax; fg = base.y + r.ay; fb = base.z + r.az;
+  } else {
+    fr = r.ax; fg = r.ay; fb = r.az;
+  }
+  clamp3(p, fr, fg, fb);
+  sr += fr; sg += fg; sb += fb;
+  ++n;
+}
+
+__device__ __forceinline__ void write_pixel(const Params& p, uint32_t id, bool ind, uint32_t n, float sr, float sg,
+                                            float sb, uint32_t rng, float* hdr, uint32_t* dbg) {
+  float fn = float(max(int(n), 1));
+  float cr = sr / fn, cg = sg / fn, cb = sb / fn;
+  if (!ind) clamp3(p, cr, cg, cb);
+  hdr[size_t(id) * 3] = cr; hdr[size_t(id) * 3 + 1] = cg; hdr[size_t(id) * 3 + 2] = cb;
+  if (dbg) { dbg[size_t(id) * 2] = rng; dbg[size_t(id) * 2 + 1] = n; }
+}
+
+// Wave 0: per pixel, the kind-1 primary direct light (pathtrace.metal:1097-1128)
+// and the first samples.
+__global__ void __launch_bounds__(256) k_wf_init(Scene s, Params p, uint64_t seed, GBufSoA gb, ResSoA rm,
+                                                 WfState w, WfQueues q, float* __restrict__ hdr,
+                                                 uint32_t* __restrict__ dbg, unsigned long long* ctr, uint32_t* err) {
+  const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t npix = uint32_t(p.width) * uint32_t(p.height);
+  bool push = false, ext = false;
+  uint32_t samples = 0;
+  if (id < npix) {
+    const int kind = __float_as_int(gb.pos_kind[id].w);
+    if (kind == 0) {
+      hdr[size_t(id) * 3] = 0.f; hdr[size_t(id) * 3 + 1] = 0.f; hdr[size_t(id) * 3 + 2] = 0.f;
+      if (dbg) { dbg[size_t(id) * 2] = 0; dbg[size_t(id) * 2 + 1] = 0; }
+    } else {
+      const uint32_t x = id % uint32_t(p.width), y = id / uint32_t(p.width);
+      Tracer pt(s, p, err);
+      pt.rng.seed(seed ^ (uint64_t(id + 1) * 0xBF58476D1CE4E5B9ull) ^ 0x94D049BB133111EBull);
+      PathRegs r{};
+      uint32_t n = 0;
+      float sr = 0, sg = 0, sb = 0;
+      r.meta = kind == 1 ? kInd : 0u;
+      bool done = false;
+      if (kind == 1) {
+        const Pixel1 g = pixel1(gb, id);
+        const float4 EM = gb.emi[id];
+        float pdr = 0, pdg = 0, pdb = 0, m_sumWu = 0;
+        uint32_t m_M = 0;
+        const float4 R3 = rm.sumwu_m_valid[id];
+        const float4 R0 = rm.lp_alpha[id], R1 = rm.ln_phat[id], R2 = rm.le_sumws[id];
+        if (__float_as_int(R3.z) != 0 && __float_as_int(R3.y) != 0 && R3.x > 0.0f && R2.w > 0.0f && R1.w > 0.0f) {
+          m_sumWu = R3.x; m_M = uint32_t(__float_as_int(R3.y));
+          float m_sumWs = R2.w;
+          float ldx = R0.x - g.gpx, ldy = R0.y - g.gpy, ldz = R0.z - g.gpz;
+          float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
+          if (dist > 0.003f) {
+            float inv = 1.0f / dist;
+            float dxn = ldx * inv, dyn = ldy * inv, dzn = ldz * inv;
+            float lcos = -(R1.x * dxn + (R1.y * dyn + R1.z * dzn));
+            float scos = g.gnx * dxn + (g.gny * dyn + g.gnz * dzn);
+            if (lcos > 1e-8f && scos > 1e-8f) {
+              Bsdf e = Tracer::eval_bsdf(dxn, dyn, dzn, g.wox, g.woy, g.woz, g.gnx, g.gny, g.gnz, g.alpha2,
+                                         g.metallic, g.spec_prob, g.ar, g.ag, g.ab);
+              float Fr = R2.x * e.r * scos * R0.w, Fg = R2.y * e.g * scos * R0.w, Fb = R2.z * e.b * scos * R0.w;
+              float ph = lum3(Fr, Fg, Fb);
+              if (ph > 0.0f) {
+                float pdf_ris = float(m_M) * ph / m_sumWu;
+                float wnee = 1.0f;
+                if (!p.nomis && e.pdf > 1e-20f) wnee = pdf_ris / (pdf_ris + e.pdf);
+                float Wt = m_sumWs / (float(m_M) * ph);
+                pdr = Fr * Wt * wnee; pdg = Fg * Wt * wnee; pdb = Fb * Wt * wnee;
+              }
+            }
+          }
+        }
+        const float bsr = EM.x + pdr, bsg = EM.y + pdg, bsb = EM.z + pdb;
+        w.base[id] = make_float4(bsr, bsg, bsb, m_sumWu);
+        w.mM[id] = m_M;
+        if (p.bounces <= 1 || p.spp <= 0) {
+          float cr = bsr, cg = bsg, cb = bsb;
+          clamp3(p, cr, cg, cb);
+          hdr[size_t(id) * 3] = cr; hdr[size_t(id) * 3 + 1] = cg; hdr[size_t(id) * 3 + 2] = cb;
+          if (dbg) { dbg[size_t(id) * 2] = pt.rng.state; dbg[size_t(id) * 2 + 1] = 0; }
+          done = true;
+        }
+      }
+      if (!done) {
+        ext = start_samples(pt, p, gb, w, id, x, y, r, n, sr, sg, sb);
+        if (ext) r.meta |= kExt;
+        else write_pixel(p, id, kind == 1, n, sr, sg, sb, pt.rng.state, hdr, dbg);
+        store(w, id, r, pt.rng.state, n, sr, sg, sb);
+        push = ext;
+        samples = n;
+      }
+    }
+  }
+  (void)push;
+  append(q.ext, q.counts + kCntExt, ext, int(id));
+  warp_add(ctr + 0, samples);
+}
+
+// Traversal of a queue of rays, one thread per ray (closest hit for extension
+// rays, pathtrace.metal:119-163; any hit for shadow rays, :164).  Finished
+// extension rays are sorted into the shading queue of their surface type.
+template <bool kShadowRays>
+__global__ void __launch_bounds__(128) k_wf_trace(Scene s, WfState w, WfQueues q, unsigned long long* ctr,
+                                                  uint32_t* err) {
+  const int n = q.counts[kShadowRays ? kCntShd : kCntExt];
+  const int* queue = kShadowRays ? q.shd : q.ext;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t nodes = 0, tests = 0, rays = 0;
+  int cls = -1;  // 0 opaque, 1 dielectric, 2 miss
+  int id = 0;
+  if (i < n) {
+    id = queue[i];
+    const float4 o = kShadowRays ? w.so[id] : w.o[id];
+    const float4 d = kShadowRays ? w.sd[id] : w.d[id];
+    const TraceResult r = traverse<kShadowRays>(s, o.x, o.y, o.z, d.x, d.y, d.z, kShadowRays ? o.w : kFar, err,
+                                                 nodes, tests);
+    rays = 1;
+    if (kShadowRays) {
+      w.occ[id] = r.tri >= 0 ? 1u : 0u;
+    } else {
+      w.hit[id] = make_float4(r.t, r.u, r.v, __int_as_float(r.tri));
+      cls = 2;
+      if (r.tri >= 0) cls = __ldg(&s.tris[r.tri].ior) > 1.0001f ? 1 : 0;
+    }
+  }
+  if (!kShadowRays) {
+    append(q.qa, q.counts + kCntA, cls == 0, id);
+    append(q.qb, q.counts + kCntB, cls == 1, id);
+    append(q.qc, q.counts + kCntC, cls == 2, id);
+  }
+  __syncwarp();
+  warp_add(ctr + 1, rays);
+  warp_add(ctr + 2, nodes);
+  warp_add(ctr + 3, tests);
+}
+
+// Shade the paths of one queue: VK 0 opaque hits, 1 dielectric hits, 2 paths
+// without a vertex (the ray missed, or the path ended and waited for its last
+// shadow ray).  Specialising on the vertex type keeps the warps' lanes on the
+// same branch.
+template <int VK>
+__global__ void __launch_bounds__(256) k_wf_shade(Scene s, Params p, GBufSoA gb, WfState w, WfQueues cq,
+                                                  WfQueues nq, float* __restrict__ hdr, uint32_t* __restrict__ dbg,
+                                                  unsigned long long* ctr, uint32_t* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int count = cq.counts[VK == 0 ? kCntA : (VK == 1 ? kCntB : kCntC)];
+  const int* queue = VK == 0 ? cq.qa : (VK == 1 ? cq.qb : cq.qc);
+  bool ext = false, shd = false, fin = false;
+  int id = 0;
+  uint32_t samples = 0;
+  if (i < count) {
+    id = queue[i];
+    const uint32_t x = uint32_t(id) % uint32_t(p.width), y = uint32_t(id) / uint32_t(p.width);
+    Tracer pt(s, p, err);
+    PathRegs r;
+    uint32_t n;
+    float sr, sg, sb;
+    load(w, uint32_t(id), r, pt.rng.state, n, sr, sg, sb);
+    const uint32_t n0 = n;
+    if (r.meta & kShadow) {
+      r.meta &= ~kShadow;
+      if (w.occ[id] == 0u) {
+        const float4 c = w.c[id];
+        r.ax += c.x; r.ay += c.y; r.az += c.z;
+      }
+    }
+    bool ended;
+    if (VK == 2) {
+      ended = true;  // a miss ends the path; a finishing path has now folded in its last shadow ray
+      r.meta &= ~(kExt | kFinish);
+    } else {
+      r.meta &= ~kExt;
+      const float4 hh = w.hit[id];
+      const TraceResult tr{hh.x, __float_as_int(hh.w), hh.y, hh.z};
+      const Hit hit = pt.attributes(tr, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz);
+      bool has_shadow = false;
+      float4 so, sd, c;
+      const bool go = vertex<VK>(pt, p, r, hit, has_shadow, so, sd, c);
+      if (has_shadow) {
+        w.so[id] = so; w.sd[id] = sd; w.c[id] = c;
+        r.meta |= kShadow;
+        shd = true;
+      }
+      if (go) { r.meta |= kExt; ext = true; }
+      ended = !go;
+      if (ended && has_shadow) { r.meta |= kFinish; ended = false; fin = true; }  // wait for the shadow ray
+    }
+    if (ended) {
+      finish_sample(p, w, uint32_t(id), r, n, sr, sg, sb);
+      if (start_samples(pt, p, gb, w, uint32_t(id), x, y, r, n, sr, sg, sb)) {
+        r.meta |= kExt;
+        ext = true;
+      } else {
+        write_pixel(p, uint32_t(id), (r.meta & kInd) != 0, n, sr, sg, sb, pt.rng.state, hdr, dbg);
+      }
+    }
+    samples = n - n0;
+    store(w, uint32_t(id), r, pt.rng.state, n, sr, sg, sb);
+  }
+  append(nq.ext, nq.counts + kCntExt, ext, id);
+  append(nq.shd, nq.counts + kCntShd, shd, id);
+  append(nq.qc, nq.counts + kCntC, fin, id);
+  warp_add(ctr + 0, samples);
+}
+
+}  // namespace
+
+cudaError_t launch_wavefront_init(const Scene& s, const Params& p, uint64_t seed, const GBufSoA& gb, const ResSoA& rm,
+                                  const WfState& w, const WfQueues& q, float* hdr, uint32_t* dbg,
+                                  unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
+  const uint32_t npix = uint32_t(p.width) * uint32_t(p.height);
+  k_wf_init<<<(npix + 255) / 256, 256, 0, st>>>(s, p, seed, gb, rm, w, q, hdr, dbg, ctr, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wavefront_trace(const Scene& s, const WfState& w, const WfQueues& q, int bound, bool shadow,
+                                   unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
+  if (bound <= 0) return cudaSuccess;
+  const unsigned g = unsigned((bound + 127) / 128);
+  if (shadow) k_wf_trace<true><<<g, 128, 0, st>>>(s, w, q, ctr, err);
+  else k_wf_trace<false><<<g, 128, 0, st>>>(s, w, q, ctr, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wavefront_shade(int vk, const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w,
+                                   const WfQueues& cq, int bound, const WfQueues& nq, float* hdr, uint32_t* dbg,
+                                   unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
+  if (bound <= 0) return cudaSuccess;
+  const unsigned g = unsigned((bound + 255) / 256);
+  if (vk == 0) k_wf_shade<0><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+  else if (vk == 1) k_wf_shade<1><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+  else k_wf_shade<2><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+  return cudaGetLastError();
+}
+
+}  // namespace rmd

@@ -98,7 +98,9 @@ struct rmcuda_ctx {
   cudaStream_t own = nullptr, stream = nullptr;
   std::mutex mu;
   // resident scene
-  DevBuf tris, lights, cdf, texels;
+  DevBuf tris, lights, cdf, texels, lrec, guide;
+  int guide_n = 0;
+  float guide_inv = 0.0f;
   DevBvh bvh;
   int n_tris = 0, n_lights = 0;
   float light_total = 0;
@@ -125,8 +127,16 @@ struct rmcuda_ctx {
   uint64_t launches = 0;
   float* last_final = nullptr;  // device pointer of the last frame's tonemap input
   int last_w = 0, last_h = 0;
+  // wavefront shading state (rm_wavefront.cu)
+  DevBuf wf[14];
+  DevBuf wq[11];
+  int* h_counts = nullptr;  // pinned: the current wave's queue lengths
+  size_t wf_cap = 0;
+  uint64_t waves = 0;
+  std::vector<int> wave_log;  // last frame: (act, ext, shd) per wave
   // per-stage CUDA-event timing (rmcuda_profile)
-  bool profiling = false;
+  int profiling = 0;
+  bool profiling_any() const { return profiling > 0; }
   struct Pending { int stage; cudaEvent_t a, b; };
   std::vector<Pending> pending;
   double stage_ms[RM_STAGE_COUNT] = {};
@@ -140,7 +150,7 @@ std::string cuda_msg(const char* what, cudaError_t e) { return std::string(what)
 // Launch through `fn`, bracketed by events on the context stream when profiling.
 template <class Fn> cudaError_t staged(rmcuda_ctx* c, int stage, Fn&& fn) {
   cudaEvent_t a = nullptr, b = nullptr;
-  if (c->profiling && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess)
+  if (c->profiling > 0 && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess)
     cudaEventRecord(a, c->stream);
   cudaError_t e = fn();
   if (a && b) {
@@ -149,6 +159,13 @@ template <class Fn> cudaError_t staged(rmcuda_ctx* c, int stage, Fn&& fn) {
   }
   c->launches += 1;
   return e;
+}
+
+// As staged(), but timed only at profiling level 2 (per-launch breakdown).
+template <class Fn> cudaError_t staged2(rmcuda_ctx* c, int stage, Fn&& fn) {
+  if (c->profiling >= 2) return staged(c, stage, fn);
+  c->launches += 1;
+  return fn();
 }
 
 void resolve_pending(rmcuda_ctx* c) {
@@ -175,6 +192,10 @@ Scene scene_view(const rmcuda_ctx* c) {
   s.n_lights = c->n_lights;
   s.light_total = c->light_total;
   s.texels = c->texels.as<rm_vec3>();
+  s.lrec = c->lrec.as<float4>();
+  s.guide = c->guide.as<int32_t>();
+  s.guide_n = c->guide_n;
+  s.guide_inv = c->guide_inv;
   return s;
 }
 
@@ -224,6 +245,11 @@ int upload_scene(rmcuda_ctx* c, const rm_scene_view* sv, std::string& msg) {
   c->n_lights = sv->n_lights;
   c->light_total = sv->light_total;
   c->opaque = opaque;
+  if ((e = prepare_lights(c->tris.as<rm_triangle>(), c->lights.as<int32_t>(), c->cdf.as<float>(), c->n_lights,
+                          c->light_total, c->lrec, c->guide, c->guide_n, c->guide_inv, st)) != cudaSuccess) {
+    msg = cuda_msg("light preparation failed", e);
+    return RM_ERR_CUDA;
+  }
   c->refits = 0;
   c->have_scene = false;
   if (sv->n_tris > 0 && sv->nodes && sv->n_nodes == 0) {
@@ -306,6 +332,97 @@ Plan make_plan(const rmcuda_ctx* c, const rm_camera& cam, const rm_config& cfg) 
   return pl;
 }
 
+bool use_megakernel() {
+  const char* v = std::getenv("RAYMOTION_CUDA_MEGAKERNEL");
+  return v && std::string(v) == "1";
+}
+
+cudaError_t ensure_wavefront(rmcuda_ctx* c, size_t npix) {
+  if (c->wf_cap >= npix && c->h_counts) return cudaSuccess;
+  cudaError_t e;
+  for (int i = 0; i < 14; ++i)
+    if ((e = c->wf[i].reserve(npix * (i < 12 ? sizeof(float4) : sizeof(uint32_t)))) != cudaSuccess) return e;
+  for (int i = 0; i < 10; ++i)
+    if ((e = c->wq[i].reserve(npix * sizeof(int))) != cudaSuccess) return e;
+  if ((e = c->wq[10].reserve(2 * kCntSlots * sizeof(int))) != cudaSuccess) return e;
+  if (!c->h_counts &&
+      (e = cudaMallocHost(reinterpret_cast<void**>(&c->h_counts), kCntSlots * sizeof(int))) != cudaSuccess)
+    return e;
+  c->wf_cap = npix;
+  return cudaSuccess;
+}
+
+// ReSTIR shading as wavefront stages (rm_wavefront.cu): init, then waves of
+// extend / shadow / shade until no path is left.
+cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, uint64_t seed, std::string& msg) {
+  const size_t npix = size_t(p.width) * size_t(p.height);
+  cudaStream_t st = c->stream;
+  cudaError_t e = ensure_wavefront(c, npix);
+  if (e != cudaSuccess) { msg = cuda_msg("wavefront allocation failed", e); return e; }
+  WfState w{c->wf[0].as<uint4>(), c->wf[1].as<float4>(), c->wf[2].as<float4>(), c->wf[3].as<float4>(),
+            c->wf[4].as<float4>(), c->wf[5].as<float4>(), c->wf[6].as<float4>(), c->wf[7].as<float4>(),
+            c->wf[8].as<float4>(), c->wf[9].as<float4>(), c->wf[10].as<float4>(), c->wf[11].as<float4>(),
+            c->wf[12].as<uint32_t>(), c->wf[13].as<uint32_t>()};
+  int* counts = c->wq[10].as<int>();
+  WfQueues q[2];
+  for (int k = 0; k < 2; ++k)
+    q[k] = WfQueues{c->wq[5 * k + 0].as<int>(), c->wq[5 * k + 1].as<int>(), c->wq[5 * k + 2].as<int>(),
+                    c->wq[5 * k + 3].as<int>(), c->wq[5 * k + 4].as<int>(), counts + kCntSlots * k};
+  unsigned long long* ctr = c->ctr.as<unsigned long long>();
+  uint32_t* err = c->err.as<uint32_t>();
+  if ((e = cudaMemsetAsync(counts, 0, 2 * kCntSlots * sizeof(int), st)) != cudaSuccess) {
+    msg = cuda_msg("memset", e);
+    return e;
+  }
+  e = staged2(c, RM_STAGE_WF_SHADE, [&] {
+    return launch_wavefront_init(s, p, seed, c->gb.view(), c->rmerged.view(), w, q[0], c->hdr.as<float>(),
+                                 c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, st);
+  });
+  if (e != cudaSuccess) { msg = cuda_msg("wavefront init failed", e); return e; }
+  int cur = 0;
+  c->wave_log.clear();
+  // Every unfinished pixel has its path either in the extension queue or (if it
+  // only waits for a shadow ray) in queue c, and the number of unfinished
+  // pixels only shrinks: ext + c read every kBatch waves bounds all queues of
+  // the next waves, which size their grids; kernels read exact lengths on the
+  // device.
+  const int kBatch = 4;
+  const uint64_t max_waves = uint64_t(p.spp) * uint64_t(p.bounces + 2) * 4 + 64;
+  for (uint64_t wave = 0;;) {
+    if (wave > max_waves) { msg = "wavefront did not drain"; return cudaErrorLaunchFailure; }
+    if ((e = cudaMemcpyAsync(c->h_counts, counts + kCntSlots * cur, kCntSlots * sizeof(int), cudaMemcpyDeviceToHost,
+                             st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+      msg = cuda_msg("wavefront count read failed", e);
+      return e;
+    }
+    const int bound = c->h_counts[kCntExt] + c->h_counts[kCntC];
+    if (bound == 0) break;
+    c->wave_log.insert(c->wave_log.end(), {bound, c->h_counts[kCntExt], c->h_counts[kCntShd]});
+    for (int k = 0; k < kBatch; ++k, ++wave) {
+      c->waves++;
+      const WfQueues& Q = q[cur];
+      const WfQueues& N = q[cur ^ 1];
+      e = staged2(c, RM_STAGE_WF_EXTEND, [&] {
+        return launch_wavefront_trace(s, w, Q, bound, false, ctr + 4 * RM_STAGE_WF_EXTEND, err, st);
+      });
+      if (e == cudaSuccess)
+        e = staged2(c, RM_STAGE_WF_SHADOW, [&] {
+          return launch_wavefront_trace(s, w, Q, bound, true, ctr + 4 * RM_STAGE_WF_SHADOW, err, st);
+        });
+      if (e == cudaSuccess) e = cudaMemsetAsync(N.counts, 0, kCntSlots * sizeof(int), st);
+      for (int vk = 0; vk < 3 && e == cudaSuccess; ++vk)
+        e = staged2(c, RM_STAGE_WF_SHADE, [&] {
+          return launch_wavefront_shade(vk, s, p, c->gb.view(), w, Q, bound, N, c->hdr.as<float>(),
+                                        c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, st);
+        });
+      if (e != cudaSuccess) { msg = cuda_msg("wavefront launch failed", e); return e; }
+      cur ^= 1;
+    }
+  }
+  return cudaSuccess;
+}
+
 cudaError_t ensure_frame(rmcuda_ctx* c, size_t npix, bool restir) {
   cudaError_t e;
   if ((e = c->hdr.reserve(npix * 12)) != cudaSuccess || (e = c->rgb.reserve(npix * 3)) != cudaSuccess ||
@@ -373,12 +490,27 @@ int enqueue_frame(rmcuda_ctx* c, const rm_camera& cam, const rm_config& cfg, uin
     if (pl.temporal_off) have_hist = false;
     p.hasHistory = have_hist ? 1 : 0;
     p.prevCamera = c->hist_cam;
-    for (int stage = 0; stage < 3 && e == cudaSuccess; ++stage)
+    const bool wavefront = !use_megakernel();  // ReSTIR scenes are opaque (make_plan)
+    for (int stage = 0; stage < 3 && e == cudaSuccess; ++stage) {
+      if (stage == 2 && wavefront) {
+        std::string wmsg;
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (c->profiling == 1 && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess)
+          cudaEventRecord(a, st);
+        e = run_wavefront_shade(c, s, p, seed, wmsg);
+        if (a && b) {
+          cudaEventRecord(b, st);
+          c->pending.push_back({RM_STAGE_SHADE, a, b});
+        }
+        if (e != cudaSuccess) { msg = wmsg; return RM_ERR_CUDA; }
+        continue;
+      }
       e = staged(c, RM_STAGE_GENERATE + stage, [&] {
         return launch_restir_stage(stage, s, p, seed, c->gb.view(), c->rinit.view(), c->rmerged.view(), c->hg.view(),
                                    c->hres.view(), c->hdr.as<float>(), c->dbg.as<uint32_t>(),
                                    ctr + 4 * (RM_STAGE_GENERATE + stage), err, st);
       });
+    }
     if (e != cudaSuccess) { msg = cuda_msg("ReSTIR launch failed", e); return RM_ERR_CUDA; }
     if (pl.denoise) {
       // temporal(hdr, hist_col) -> tmp_a -> a-trous -> tmp_b -> a-trous + tonemap -> tmp_a
@@ -469,11 +601,14 @@ void rmcuda_destroy(rmcuda_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  for (DevBuf* b : {&c->tris, &c->lights, &c->cdf, &c->texels, &c->hdr, &c->tmp_a, &c->tmp_b, &c->hist_col, &c->rgb, &c->dbg,
+  for (DevBuf* b : {&c->tris, &c->lights, &c->cdf, &c->texels, &c->lrec, &c->guide, &c->hdr, &c->tmp_a, &c->tmp_b, &c->hist_col, &c->rgb, &c->dbg,
                     &c->hash_out, &c->ctr, &c->err, &c->bvh.records, &c->bvh.parents, &c->bvh.counters,
                     &c->bvh.order, &c->bvh.tgeo, &c->bvh.keys, &c->bvh.keys_alt, &c->bvh.vals_alt, &c->bvh.knodes,
                     &c->bvh.kbox, &c->bvh.kcount, &c->bvh.ranges, &c->bvh.temp, &c->bvh.bounds, &c->bvh.depth})
     b->release();
+  for (DevBuf& b : c->wf) b.release();
+  for (DevBuf& b : c->wq) b.release();
+  if (c->h_counts) cudaFreeHost(c->h_counts);
   c->gb.release(); c->hg.release();
   c->rinit.release(); c->rmerged.release(); c->hres.release();
   resolve_pending(c);
@@ -519,6 +654,9 @@ int rmcuda_scene_update(rmcuda_ctx* c, const rm_triangle* tris, int32_t n, int32
     if (!(tris[i].alpha >= 1.0f)) { opaque = false; break; }
   c->opaque = opaque;
   if (n == 0) return RM_OK;
+  e = prepare_lights(c->tris.as<rm_triangle>(), c->lights.as<int32_t>(), c->cdf.as<float>(), c->n_lights,
+                     c->light_total, c->lrec, c->guide, c->guide_n, c->guide_inv, c->stream);
+  if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("light preparation failed", e)); return RM_ERR_CUDA; }
   if (rebuild_every > 0 && c->refits + 1 >= rebuild_every) {
     std::string berr;
     e = build_lbvh(c->tris.as<rm_triangle>(), n, kLbvhLeaf, c->bvh, c->stream, berr);
@@ -695,11 +833,19 @@ int rmcuda_stats_get(rmcuda_ctx* c, rm_stats* out) {
   return RM_OK;
 }
 
-int rmcuda_profile(rmcuda_ctx* c, int enable) {
+int rmcuda_profile(rmcuda_ctx* c, int level) {
   if (!c) return RM_ERR_INVALID;
   std::lock_guard<std::mutex> lk(c->mu);
-  c->profiling = enable != 0;
+  c->profiling = level < 0 ? 0 : level;
   return RM_OK;
+}
+
+int rmcuda_wave_log(rmcuda_ctx* c, int32_t* out, int32_t cap) {
+  if (!c || cap < 0) return -1;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const int waves = int(c->wave_log.size() / 3);
+  for (int i = 0; i < waves * 3 && i < cap * 3; ++i) out[i] = c->wave_log[size_t(i)];
+  return waves;
 }
 
 int rmcuda_stage_counters(rmcuda_ctx* c, uint64_t* out, int32_t n) {

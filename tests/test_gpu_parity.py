@@ -109,7 +109,10 @@ def _restir_cfg(flags=0):
                         restir_spatial=4, restir_radius=12.0, flags=flags)
 
 
-def test_restir_chain_matches_oracle(backend, oracle, small_field):
+@pytest.mark.parametrize("shading", ["wavefront", "megakernel"])
+def test_restir_chain_matches_oracle(backend, oracle, small_field, shading, monkeypatch):
+    if shading == "megakernel":
+        monkeypatch.setenv("RAYMOTION_CUDA_MEGAKERNEL", "1")
     sc, cam, _ = small_field
     cfg = _restir_cfg(_abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_DENOISE_OFF)
     o = oracle.Oracle()
@@ -145,3 +148,20 @@ def test_denoiser_within_tolerance(backend, oracle, small_field):
         _, o_hdr, _ = o.render(sc, cam, cfg, seed)
         g_rgb, g_hdr = backend.render(sc, cam, cfg, seed, hdr=True)
         assert rel_close_fraction(g_hdr, o_hdr, 1e-4) >= 0.999
+
+
+@pytest.mark.parametrize("candidates,flags", [(1, 0), (8, _abi.RM_FLAG_NOMIS), (4, _abi.RM_FLAG_NO_RR)])
+def test_wavefront_shading_variants_bit_exact(backend, oracle, candidates, flags):
+    """Wavefront shading vs the oracle with legacy NEE (1 candidate), MIS off and RR off."""
+    sb, cam, _ = icosphere_field(seed=7, n_spheres=24, subdiv=2, n_emitters=48, width=96, height=64, spp=6, depth=7)
+    sc = oracle.with_reference_bvh(sb.pack())
+    cfg = RenderConfig(width=96, height=64, spp=6, max_bounces=7, adapt_min=0, restir_candidates=candidates,
+                       restir_spatial=3, restir_radius=9.0, flags=_abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_DENOISE_OFF | flags)
+    o = oracle.Oracle()
+    backend.reset_history()
+    _, o_hdr, o_st = o.render(sc, cam, cfg, 99)
+    _, g_hdr = backend.render(sc, cam, cfg, 99, hdr=True)
+    assert o_st["chain"] == 2
+    npix = cfg.width * cfg.height
+    assert np.array_equal(backend.debug_read(4, npix), o.debug_read(4, npix))
+    assert exact_fraction(g_hdr, o_hdr) == 1.0
