@@ -17,6 +17,7 @@
 // Triangle boxes come from the caller's fp32 vertices, so every box bounds its
 // float triangle exactly.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -517,6 +518,269 @@ cudaError_t build_lbvh_into(const rm_triangle* d_tris, int n, int leaf_max, cons
 }
 
 size_t lbvh_box_bytes() { return sizeof(Box); }
+
+// ---- PLOC ---------------------------------------------------------------------
+//
+// Meister & Bittner, "Parallel Locally-Ordered Clustering for Bounding Volume
+// Hierarchy Construction" (IEEE TVCG 2018).  Clusters start as the triangles in
+// Morton order; every iteration each cluster finds, within a window of
+// +-kPlocRadius neighbours in that order, the cluster whose union box has the
+// smallest surface area; mutual nearest neighbours merge into a new node, and
+// the survivors are compacted in order.  Node ids: leaves 0..n-1 (Morton
+// position), internal nodes n.. in creation order, so a parent's id is larger
+// than its children's.  The tree is then laid out like the LBVH: leaves in
+// depth-first order, subtrees of at most `leaf_max` triangles as leaves, one
+// child-pair record per remaining internal node (record of node k is
+// 2n-2-k, the root is record 0).
+
+namespace {
+
+constexpr int kPlocRadius = 16;
+
+__device__ __forceinline__ float half_area(const float4& lo, const float4& hi) {
+  const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+  return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void k_ploc_leaves(const rm_triangle* __restrict__ tris, const int* __restrict__ order, int n,
+                              float4* __restrict__ blo, float4* __restrict__ bhi, int* __restrict__ cl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Box b = tri_box(tris[order[i]]);
+  blo[i] = make_float4(b.mn[0], b.mn[1], b.mn[2], __int_as_float(1));
+  bhi[i] = make_float4(b.mx[0], b.mx[1], b.mx[2], __int_as_float(-1));
+  cl[i] = i;
+}
+
+__global__ void k_ploc_nn(const int* __restrict__ cl, int C, const float4* __restrict__ blo,
+                          const float4* __restrict__ bhi, int* __restrict__ nn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C) return;
+  const int a = cl[i];
+  const float4 alo = blo[a], ahi = bhi[a];
+  float best = __int_as_float(0x7f800000);
+  int bj = -1;
+  const int j0 = max(0, i - kPlocRadius), j1 = min(C - 1, i + kPlocRadius);
+  for (int j = j0; j <= j1; ++j) {
+    if (j == i) continue;
+    const int b = cl[j];
+    const float4 l = blo[b], h = bhi[b];
+    const float4 ulo = make_float4(fminf(alo.x, l.x), fminf(alo.y, l.y), fminf(alo.z, l.z), 0.f);
+    const float4 uhi = make_float4(fmaxf(ahi.x, h.x), fmaxf(ahi.y, h.y), fmaxf(ahi.z, h.z), 0.f);
+    const float area = half_area(ulo, uhi);
+    if (area < best) { best = area; bj = j; }  // ties keep the smaller index (scanned in order)
+  }
+  nn[i] = bj;
+}
+
+// flags: x = this cluster creates a node, y = this cluster survives
+__global__ void k_ploc_flags(const int* __restrict__ nn, int C, int force, int* __restrict__ mflag,
+                             int* __restrict__ kflag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C) return;
+  int j = nn[i];
+  bool mutual = j >= 0 && nn[j] == i;
+  if (force) {  // no mutual pair anywhere: merge neighbours (0,1), (2,3), ...
+    j = (i & 1) ? i - 1 : i + 1;
+    mutual = j < C;
+  }
+  mflag[i] = (mutual && i < j) ? 1 : 0;
+  kflag[i] = (!mutual || i < j) ? 1 : 0;
+}
+
+__global__ void k_ploc_apply(const int* __restrict__ cl, const int* __restrict__ nn, int C, int force,
+                             const int* __restrict__ mflag, const int* __restrict__ mscan,
+                             const int* __restrict__ kflag, const int* __restrict__ kscan, int next_node,
+                             float4* __restrict__ blo, float4* __restrict__ bhi, int2* __restrict__ child,
+                             int* __restrict__ ncl, int n_leaves) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C) return;
+  if (!kflag[i]) return;
+  int out = cl[i];
+  if (mflag[i]) {
+    const int j = force ? i + 1 : nn[i];
+    const int a = cl[i], b = cl[j];
+    const int id = next_node + mscan[i];
+    const float4 al = blo[a], ah = bhi[a], bl = blo[b], bh = bhi[b];
+    const int size = __float_as_int(al.w) + __float_as_int(bl.w);
+    blo[id] = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), __int_as_float(size));
+    bhi[id] = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), __int_as_float(-1));
+    child[id - n_leaves] = make_int2(a, b);
+    bhi[a].w = __int_as_float(id);  // parent links
+    bhi[b].w = __int_as_float(id);
+    out = id;
+  }
+  ncl[kscan[i]] = out;
+}
+
+__global__ void k_ploc_totals(const int* __restrict__ mflag, const int* __restrict__ mscan,
+                              const int* __restrict__ kflag, const int* __restrict__ kscan, int C,
+                              int* __restrict__ totals) {
+  totals[0] = mscan[C - 1] + mflag[C - 1];
+  totals[1] = kscan[C - 1] + kflag[C - 1];
+}
+
+// Leaf position in depth-first order and depth: walk to the root adding the
+// sizes of left siblings.  Only the n leaves walk; max depth -> *depth.
+__global__ void k_ploc_layout(int n, int root, const float4* __restrict__ blo, const float4* __restrict__ bhi,
+                              const int2* __restrict__ child, const int* __restrict__ order, int* __restrict__ pos,
+                              int* __restrict__ out_order, int* __restrict__ depth) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int off = 0, d = 1, cur = i;
+  while (cur != root) {
+    const int p = __float_as_int(bhi[cur].w);
+    const int2 c = child[p - n];
+    if (c.y == cur) off += __float_as_int(blo[c.x].w);
+    cur = p;
+    ++d;
+    if (d > 4 * kStack) break;  // a corrupt tree cannot loop forever
+  }
+  pos[i] = off;
+  out_order[off] = order[i];
+  atomicMax(depth, d);
+}
+
+__device__ __forceinline__ int ploc_first(int node, int n, const int2* __restrict__ child,
+                                          const int* __restrict__ pos) {
+  while (node >= n) node = child[node - n].x;
+  return pos[node];
+}
+
+__global__ void k_ploc_emit(int n, int leaf_max, const float4* __restrict__ blo, const float4* __restrict__ bhi,
+                            const int2* __restrict__ child, const int* __restrict__ pos, float4* recs, int* parents) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;  // internal node n + k
+  if (k >= n - 1) return;
+  const int node = n + k;
+  const int rec_id = 2 * n - 2 - node;
+  float4* rec = recs + size_t(rec_id) * 4;
+  if (__float_as_int(blo[node].w) <= leaf_max) {
+    // collapsed into an ancestor's leaf: an unreachable record
+    write_slot(rec, 0, empty_box());
+    write_slot(rec, 1, empty_box());
+    rec[3] = make_float4(__int_as_float(0), __int_as_float(0), __int_as_float(-1), __int_as_float(-1));
+    parents[rec_id] = -1;
+    return;
+  }
+  const int2 ch = child[k];
+  int links[2], counts[2];
+  for (int s = 0; s < 2; ++s) {
+    const int c = s ? ch.y : ch.x;
+    const float4 l = blo[c], h = bhi[c];
+    Box b;
+    b.mn[0] = l.x; b.mn[1] = l.y; b.mn[2] = l.z;
+    b.mx[0] = h.x; b.mx[1] = h.y; b.mx[2] = h.z;
+    write_slot(rec, s, b);
+    const int size = __float_as_int(l.w);
+    if (size <= leaf_max) {
+      links[s] = ploc_first(c, n, child, pos);
+      counts[s] = size;
+    } else {
+      links[s] = 2 * n - 2 - c;
+      counts[s] = 0;
+      parents[links[s]] = (rec_id << 1) | s;
+    }
+  }
+  rec[3] = make_float4(__int_as_float(links[0]), __int_as_float(links[1]), __int_as_float(counts[0]),
+                       __int_as_float(counts[1]));
+  if (rec_id == 0) parents[0] = -1;
+}
+
+}  // namespace
+
+cudaError_t build_ploc(const rm_triangle* d_tris, int n, int leaf_max, DevBvh& b, cudaStream_t st, std::string& err) {
+  b.n_tris = n;
+  b.max_depth = 0;
+  if (n <= 0) { b.n_records = 0; return cudaSuccess; }
+  leaf_max = std::max(1, std::min(leaf_max, kMaxLeaf));
+  if (n <= leaf_max) return build_lbvh(d_tris, n, leaf_max, b, st, err);  // one leaf
+  if (n >= kMaxLink / 2) { err = "scene exceeds 8388607 triangles for the clustering build"; return cudaErrorInvalidValue; }
+  const int total = 2 * n - 1;
+  // Morton order (shared with the LBVH build)
+  RM_TRY(b.order.reserve(size_t(n) * sizeof(int)));
+  RM_TRY(b.bounds.reserve(6 * sizeof(unsigned int)));
+  RM_TRY(b.keys.reserve(size_t(n) * 4 * 2));
+  RM_TRY(b.keys_alt.reserve(size_t(n) * 4));
+  RM_TRY(b.vals_alt.reserve(size_t(n) * 4));
+  unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  RM_TRY(cudaMemcpyAsync(b.bounds.ptr, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  k_centroid_bounds<<<148 * 4, 256, 0, st>>>(d_tris, n, b.bounds.as<unsigned int>());
+  unsigned int* keys = b.keys.as<unsigned int>();
+  int* vals = reinterpret_cast<int*>(keys + n);
+  k_morton<<<(n + 255) / 256, 256, 0, st>>>(d_tris, n, b.bounds.as<unsigned int>(), keys, vals);
+  RM_TRY(cudaGetLastError());
+  cub::DoubleBuffer<unsigned int> dk(keys, b.keys_alt.as<unsigned int>());
+  cub::DoubleBuffer<int> dv(vals, b.vals_alt.as<int>());
+  size_t sort_bytes = 0, scan_bytes = 0;
+  RM_TRY(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, dk, dv, n, 0, 30, st));
+  RM_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, static_cast<int*>(nullptr), static_cast<int*>(nullptr), n,
+                                       st));
+  RM_TRY(b.temp.reserve(std::max(sort_bytes, scan_bytes)));
+  RM_TRY(cub::DeviceRadixSort::SortPairs(b.temp.ptr, sort_bytes, dk, dv, n, 0, 30, st));
+  const int* sorted = dv.Current();
+  // node and cluster arrays (kbox: box lo/hi; knodes: children; ranges: 2 cluster lists + nn + 4 flag arrays)
+  RM_TRY(b.kbox.reserve(size_t(total) * 2 * sizeof(float4)));
+  RM_TRY(b.knodes.reserve(size_t(n) * sizeof(int2)));
+  RM_TRY(b.ranges.reserve(size_t(n) * 7 * sizeof(int) + 2 * sizeof(int)));
+  RM_TRY(b.kcount.reserve(size_t(n) * sizeof(int)));
+  float4* blo = b.kbox.as<float4>();
+  float4* bhi = blo + total;
+  int2* child = b.knodes.as<int2>();
+  int* cl0 = b.ranges.as<int>();
+  int* cl1 = cl0 + n;
+  int* nn = cl1 + n;
+  int* mflag = nn + n;
+  int* mscan = mflag + n;
+  int* kflag = mscan + n;
+  int* kscan = kflag + n;
+  int* totals = kscan + n;
+  k_ploc_leaves<<<(n + 255) / 256, 256, 0, st>>>(d_tris, sorted, n, blo, bhi, cl0);
+  RM_TRY(cudaGetLastError());
+  int C = n, next_node = n, iters = 0;
+  int* cl = cl0;
+  int* ncl = cl1;
+  int h_tot[2];
+  while (C > 1) {
+    if (++iters > 4 * n + 64) { err = "clustering build did not converge"; return cudaErrorInvalidValue; }
+    const unsigned g = unsigned((C + 255) / 256);
+    int force = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      if (!force) k_ploc_nn<<<g, 256, 0, st>>>(cl, C, blo, bhi, nn);
+      k_ploc_flags<<<g, 256, 0, st>>>(nn, C, force, mflag, kflag);
+      RM_TRY(cub::DeviceScan::ExclusiveSum(b.temp.ptr, scan_bytes, mflag, mscan, C, st));
+      RM_TRY(cub::DeviceScan::ExclusiveSum(b.temp.ptr, scan_bytes, kflag, kscan, C, st));
+      k_ploc_totals<<<1, 1, 0, st>>>(mflag, mscan, kflag, kscan, C, totals);
+      RM_TRY(cudaMemcpyAsync(h_tot, totals, sizeof(h_tot), cudaMemcpyDeviceToHost, st));
+      RM_TRY(cudaStreamSynchronize(st));
+      if (h_tot[0] > 0) break;
+      force = 1;  // degenerate input: pair up neighbours
+    }
+    k_ploc_apply<<<g, 256, 0, st>>>(cl, nn, C, force, mflag, mscan, kflag, kscan, next_node, blo, bhi, child, ncl, n);
+    RM_TRY(cudaGetLastError());
+    next_node += h_tot[0];
+    C = h_tot[1];
+    std::swap(cl, ncl);
+  }
+  const int root = next_node - 1;
+  if (root != total - 1) { err = "clustering build produced a malformed tree"; return cudaErrorInvalidValue; }
+  // layout
+  int* pos = b.kcount.as<int>();
+  RM_TRY(b.depth.reserve(sizeof(int)));
+  RM_TRY(cudaMemsetAsync(b.depth.ptr, 0, sizeof(int), st));
+  k_ploc_layout<<<(n + 255) / 256, 256, 0, st>>>(n, root, blo, bhi, child, sorted, pos, b.order.as<int>(),
+                                                 b.depth.as<int>());
+  RM_TRY(b.records.reserve(size_t(n - 1) * 4 * sizeof(float4)));
+  RM_TRY(b.parents.reserve(size_t(n - 1) * sizeof(int)));
+  RM_TRY(b.counters.reserve(size_t(n - 1) * sizeof(int)));
+  k_ploc_emit<<<(n - 1 + 255) / 256, 256, 0, st>>>(n, leaf_max, blo, bhi, child, pos, b.records.as<float4>(),
+                                                   b.parents.as<int>());
+  RM_TRY(cudaGetLastError());
+  RM_TRY(cudaMemcpyAsync(&b.max_depth, b.depth.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  RM_TRY(cudaStreamSynchronize(st));
+  if (b.max_depth > kStack) { err = "device BVH deeper than the traversal stack"; return cudaErrorInvalidValue; }
+  b.n_records = n - 1;
+  return pack_tgeo(d_tris, b, st);
+}
 
 bool convert_caller_bvh(const rm_bvh_node* nodes, int M, const int32_t* bvh_tri, int n_tris, DevBvh& out,
                         cudaStream_t st, std::string& err) {

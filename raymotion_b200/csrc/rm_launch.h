@@ -98,6 +98,9 @@ bool convert_caller_bvh(const rm_bvh_node* nodes, int n_nodes, const int32_t* bv
 // Build an LBVH on the device from the device triangle array.
 cudaError_t build_lbvh(const rm_triangle* d_tris, int n_tris, int leaf_max, DevBvh& out, cudaStream_t st,
                        std::string& err);
+// Build a clustering BVH (PLOC) on the device from the device triangle array.
+cudaError_t build_ploc(const rm_triangle* d_tris, int n_tris, int leaf_max, DevBvh& out, cudaStream_t st,
+                       std::string& err);
 // Write the leaf-ordered Moller-Trumbore records from the triangles.
 cudaError_t pack_tgeo(const rm_triangle* d_tris, DevBvh& bvh, cudaStream_t st);
 // Refit all boxes bottom-up from the current triangle positions.

@@ -34,6 +34,21 @@ constexpr const char* kUnavailable = "Metal backend is not available in this bui
 constexpr const char* kInvalidDims = "Invalid Metal render dimensions or sample count";
 constexpr int kLbvhLeaf = 4;
 
+// Device BVH builder: PLOC clustering (default) or LBVH (RAYMOTION_CUDA_BVH=lbvh);
+// RAYMOTION_CUDA_BVH_LEAF sets the maximum triangles per leaf (default 4).
+cudaError_t build_device_bvh(const rm_triangle* d_tris, int n, rmd::DevBvh& bvh, cudaStream_t st, std::string& err) {
+  int leaf = kLbvhLeaf;
+  if (const char* v = std::getenv("RAYMOTION_CUDA_BVH_LEAF")) leaf = std::max(1, std::min(255, std::atoi(v)));
+  const char* kind = std::getenv("RAYMOTION_CUDA_BVH");
+  if (kind && std::string(kind) == "lbvh") return rmd::build_lbvh(d_tris, n, leaf, bvh, st, err);
+  cudaError_t e = rmd::build_ploc(d_tris, n, leaf, bvh, st, err);
+  if (e != cudaSuccess && err.find("deeper") != std::string::npos) {
+    err.clear();
+    return rmd::build_lbvh(d_tris, n, leaf, bvh, st, err);  // depth fallback
+  }
+  return e;
+}
+
 void set_err(char* err, size_t cap, const std::string& m) {
   if (err && cap) std::snprintf(err, cap, "%s", m.c_str());
 }
@@ -276,7 +291,7 @@ int upload_scene(rmcuda_ctx* c, const rm_scene_view* sv, std::string& msg) {
     c->device_built = !converted;
     if (!converted) {
       std::string berr;
-      if ((e = build_lbvh(c->tris.as<rm_triangle>(), sv->n_tris, kLbvhLeaf, c->bvh, st, berr)) != cudaSuccess) {
+      if ((e = build_device_bvh(c->tris.as<rm_triangle>(), sv->n_tris, c->bvh, st, berr)) != cudaSuccess) {
         msg = berr.empty() ? cuda_msg("device BVH build failed", e) : berr;
         return RM_ERR_CUDA;
       }
@@ -659,7 +674,7 @@ int rmcuda_scene_update(rmcuda_ctx* c, const rm_triangle* tris, int32_t n, int32
   if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("light preparation failed", e)); return RM_ERR_CUDA; }
   if (rebuild_every > 0 && c->refits + 1 >= rebuild_every) {
     std::string berr;
-    e = build_lbvh(c->tris.as<rm_triangle>(), n, kLbvhLeaf, c->bvh, c->stream, berr);
+    e = build_device_bvh(c->tris.as<rm_triangle>(), n, c->bvh, c->stream, berr);
     c->refits = 0;
     c->device_built = true;
     if (e != cudaSuccess) { set_err(err, errcap, berr.empty() ? cuda_msg("rebuild failed", e) : berr); return RM_ERR_CUDA; }

@@ -1,0 +1,75 @@
+"""Device BVH builds (PLOC clustering, LBVH), caller-BVH conversion and device
+refit / rebuild: closest hits stay bit-identical to the oracle's (GPU)."""
+import numpy as np
+import pytest
+
+from raymotion_b200.scene import SceneBuilder
+from raymotion_b200.scenes import icosphere_field
+
+from .gpu_util import random_rays
+from .test_gpu_parity import _trace_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def field(oracle):
+    sb, cam, cfg = icosphere_field(seed=11, n_spheres=20, subdiv=3, n_emitters=32, width=64, height=36)
+    return sb.pack()
+
+
+def _check_hits(backend, oracle, scene, rays):
+    g_tri, g_t, _, _ = _trace_gpu(backend, rays)
+    o_tri, o_t, _, _ = oracle.trace(scene, rays)
+    assert np.array_equal(g_tri, o_tri)
+    hit = o_tri >= 0
+    assert np.array_equal(g_t[hit].view(np.uint32), o_t[hit].view(np.uint32))
+    return hit.mean()
+
+
+@pytest.mark.parametrize("builder,leaf", [("ploc", "4"), ("ploc", "1"), ("ploc", "8"), ("lbvh", "4")])
+def test_device_builders_give_identical_hits(backend, oracle, field, builder, leaf, monkeypatch):
+    monkeypatch.setenv("RAYMOTION_CUDA_BVH", builder)
+    monkeypatch.setenv("RAYMOTION_CUDA_BVH_LEAF", leaf)
+    sc = oracle.with_reference_bvh(field)
+    backend.upload(sc, use_nodes=False)
+    rays = random_rays(30000, [-22, -1, -22], [22, 12, 22], 5)
+    assert _check_hits(backend, oracle, sc, rays) > 0.2
+
+
+def test_degenerate_clusters(backend, oracle):
+    """300 copies of one triangle: no mutual nearest neighbours by area ties; the
+    build must still terminate, and ties resolve to the smallest index."""
+    sb = SceneBuilder()
+    p = np.array([[0.0, 0.0, 3.0]] * 300)
+    sb.add_triangles(p + [-1, -1, 0], p + [1, -1, 0], p + [0, 1, 0])
+    sc = oracle.with_reference_bvh(sb.pack())
+    backend.upload(sc, use_nodes=False)
+    rays = random_rays(2000, [-0.5, -0.5, -1], [0.5, 0.5, 0], 2)
+    rays[:, 3:6] = [0, 0, 1]
+    g_tri, _, _, _ = _trace_gpu(backend, rays)
+    o_tri, _, _, _ = oracle.trace(sc, rays)
+    assert np.array_equal(g_tri, o_tri)
+    assert (o_tri[o_tri >= 0] == 0).all()
+
+
+def _moved(scene, shift):
+    moved = scene.tris.copy()
+    for f in ("v0", "v1", "v2"):
+        moved[f][: len(moved) // 2] += np.float32(shift)
+    return moved
+
+
+@pytest.mark.parametrize("use_nodes", [False, True], ids=["device_bvh", "caller_bvh"])
+def test_refit_and_rebuild_track_moved_geometry(backend, oracle, field, use_nodes):
+    sc = oracle.with_reference_bvh(field)
+    backend.upload(sc, use_nodes=use_nodes)
+    rays = random_rays(30000, [-22, -1, -22], [22, 12, 22], 8)
+    for step, (shift, rebuild_every) in enumerate([((0.7, 0.3, -0.4), 0), ((-1.1, 0.2, 0.9), 0), ((0.2, 2.0, 0.1), 1)]):
+        moved = _moved(sc, shift)
+        backend.update(moved, rebuild_every=rebuild_every)
+        ms = oracle.with_reference_bvh(type(sc)(tris=moved, light_tri=sc.light_tri, light_cdf=sc.light_cdf,
+                                                light_total=sc.light_total, texels=sc.texels,
+                                                verts64=np.concatenate([moved["v0"], moved["v1"], moved["v2"]],
+                                                                       axis=1).astype(np.float64)))
+        assert _check_hits(backend, oracle, ms, rays) > 0.2, step
