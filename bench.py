@@ -317,6 +317,16 @@ def run_b200(args, world, rank, local):
                     peak_source=peak["source"],
                     note="achieved = (64 B x BVH records fetched + 48 B x triangle tests) per launch / average "
                          "launch time; most of these bytes hit L1/L2")
+    # screen-space passes (temporal 92 B/px, two a-trous 64 B/px each, fused tonemap write 3 B/px):
+    # algorithmic bytes per frame against the measured HBM peak
+    ss_ms = sum(kern_t[k][0] for k in ("temporal", "atrous0", "atrous1"))
+    ss_bytes = cfg.width * cfg.height * (92 + 64 + 64 + 3)
+    roofline_ss = None
+    if ss_ms > 0:
+        ach = ss_bytes / (ss_ms / 1e3) / 1e9
+        roofline_ss = dict(bound="hbm", kernels="k_denoise_temporal_tiled + k_denoise_atrous_tiled x2", achieved=ach,
+                           peak=peak["hbm_gbs"], unit="GB/s", frac=ach / peak["hbm_gbs"], us_per_frame=ss_ms * 1e3,
+                           bytes_per_frame=ss_bytes)
     stage_summary = {k: dict(ms_per_frame=v[0] / args.steps, launches_per_frame=v[1] / args.steps)
                      for k, v in stage_t.items() if v[1]}
     kernel_summary = {}
@@ -368,7 +378,7 @@ def run_b200(args, world, rank, local):
                     config=dict(desc, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
                     mrays_per_s=rays_sum / secs_max / 1e6, e2e=e2e, roofline=roofline, cpu_baseline=cpu,
                     gpu_launches=int(st["kernel_launches"]), clocks=clk, stages=stage_summary,
-                    kernels_one_frame=kernel_summary, wavefront=wave_summary)
+                    kernels_one_frame=kernel_summary, wavefront=wave_summary, roofline_screen_space=roofline_ss)
         print(json.dumps(line), flush=True)
     backend.close()
     return 0

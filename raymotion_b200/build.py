@@ -28,7 +28,10 @@ NVFLAGS = ARCH + [
     "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
     f"-I{ROOT / 'include'}", f"-I{CSRC}",
 ]
-CU_SOURCES = ["rm_kernels.cu", "rm_denoise.cu", "rm_bvh.cu", "rmcuda_api.cu", "rm_noalloc.cu", "rm_wavefront.cu"]
+CU_SOURCES = ["rm_kernels.cu", "rm_denoise.cu", "rm_bvh.cu", "rmcuda_api.cu", "rm_noalloc.cu", "rm_wavefront.cu",
+              "rm_atrous.cu"]
+# Tolerance-checked kernels (approximate exp2 / rsqrt anyway) are compiled with FMA contraction.
+FMA_SOURCES = {"rm_atrous.cu"}
 CXX_SOURCES = ["shim_metal.cpp"]
 
 
@@ -66,7 +69,10 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
         if _stale(o, [s] + headers) or ptxas_info:
             extra = ["-Xptxas", "-v"] if (ptxas_info and src.endswith(".cu")) else []
             lang = [] if src.endswith(".cu") else ["-x", "c++"]
-            jobs.append([nvcc, *NVFLAGS, *extra, *lang, "-c", str(s), "-o", str(o)])
+            flags = [f for f in NVFLAGS if not (src in FMA_SOURCES and f == "-fmad=false")]
+            if src in FMA_SOURCES:
+                flags.append("-fmad=true")
+            jobs.append([nvcc, *flags, *extra, *lang, "-c", str(s), "-o", str(o)])
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         for cmd, fut in [(c, ex.submit(_run, c)) for c in jobs]:
             fut.result()

@@ -137,13 +137,86 @@ __global__ void __launch_bounds__(256) k_tonemap(const float* __restrict__ in, u
   rgb[i] = tonemap8(in[i]);
 }
 
+// ---- tiled versions --------------------------------------------------------
+//
+// 32 x 8 pixels per block.  The neighbourhood of the tile (halo 1 for the
+// temporal clamp, 2 * stride for a-trous) is staged once in shared memory with
+// coalesced 128-bit loads, so each G-buffer / colour byte leaves HBM (or L2)
+// about once instead of once per tap.
+
+constexpr int kTX = 32, kTY = 8;
+
+__global__ void __launch_bounds__(kTX* kTY) k_denoise_temporal_tiled(Params p, GBufSoA gb, GBufSoA hg,
+                                                                     const float* __restrict__ cur,
+                                                                     const float* __restrict__ hist,
+                                                                     float* __restrict__ out) {
+  __shared__ float3 sc[kTY + 2][kTX + 2];
+  const int W = p.width, H = p.height;
+  const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
+  const int tid = threadIdx.y * kTX + threadIdx.x;
+  for (int k = tid; k < (kTX + 2) * (kTY + 2); k += kTX * kTY) {
+    const int lx = k % (kTX + 2), ly = k / (kTX + 2);
+    const int gx = x0 + lx - 1, gy = y0 + ly - 1;
+    float3 v = make_float3(0.f, 0.f, 0.f);
+    if (gx >= 0 && gy >= 0 && gx < W && gy < H) v = ld3(cur, uint32_t(gy) * uint32_t(W) + uint32_t(gx));
+    sc[ly][lx] = v;
+  }
+  __syncthreads();
+  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+  if (x >= W || y >= H) return;
+  const uint32_t id = uint32_t(y) * uint32_t(W) + uint32_t(x);
+  const float3 c = sc[threadIdx.y + 1][threadIdx.x + 1];
+  const float4 PK = gb.pos_kind[id];
+  if (p.hasHistory == 0 || __float_as_int(PK.w) != 1) { st3(out, id, c.x, c.y, c.z); return; }
+  float mnx = c.x, mny = c.y, mnz = c.z, mxx = c.x, mxy = c.y, mxz = c.z;
+#pragma unroll
+  for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int nx = x + dx, ny = y + dy;
+      if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;
+      const float3 v = sc[threadIdx.y + 1 + dy][threadIdx.x + 1 + dx];
+      mnx = fminf(mnx, v.x); mny = fminf(mny, v.y); mnz = fminf(mnz, v.z);
+      mxx = fmaxf(mxx, v.x); mxy = fmaxf(mxy, v.y); mxz = fmaxf(mxz, v.z);
+    }
+  float ox = c.x, oy = c.y, oz = c.z;
+  const rm_camera& pc = p.prevCamera;
+  float pdx = PK.x - pc.x, pdy = PK.y - pc.y, pdz = PK.z - pc.z;
+  float ccx = pc.m0 * pdx + pc.m3 * pdy + pc.m6 * pdz;
+  float ccy = pc.m1 * pdx + pc.m4 * pdy + pc.m7 * pdz;
+  float ccz = pc.m2 * pdx + pc.m5 * pdy + pc.m8 * pdz;
+  if (ccz > 1e-6f) {
+    float ppx = pc.focal * ccx / ccz + float(W) * 0.5f;
+    float ppy = float(H) * 0.5f - pc.focal * ccy / ccz;
+    if (ppx >= 0.0f && ppx < float(W) && ppy >= 0.0f && ppy < float(H)) {
+      const uint32_t hidx = uint32_t(int(floorf(ppy))) * uint32_t(W) + uint32_t(int(floorf(ppx)));
+      const float4 HK = hg.pos_kind[hidx];
+      if (__float_as_int(HK.w) == 1) {
+        const float4 HN = hg.nor_rough[hidx];
+        const float4 CN = gb.nor_rough[id];
+        float ddx = PK.x - HK.x, ddy = PK.y - HK.y, ddz = PK.z - HK.z;
+        float dd = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz);
+        float dcx = PK.x - p.camera.x, dcy = PK.y - p.camera.y, dcz = PK.z - p.camera.z;
+        float dc = sqrtf(dcx * dcx + dcy * dcy + dcz * dcz);
+        if (dd < 0.02f * dc + 1e-3f && (CN.x * HN.x + (CN.y * HN.y + CN.z * HN.z)) > 0.9f) {
+          const float3 h = ld3(hist, hidx);
+          float hx = fminf(fmaxf(h.x, mnx), mxx), hy = fminf(fmaxf(h.y, mny), mxy), hz = fminf(fmaxf(h.z, mnz), mxz);
+          ox = hx + (c.x - hx) * 0.2f; oy = hy + (c.y - hy) * 0.2f; oz = hz + (c.z - hz) * 0.2f;
+        }
+      }
+    }
+  }
+  st3(out, id, ox, oy, oz);
+}
+
 cudaError_t launch_denoise_stage(int stage, const Params& p, const GBufSoA& gb, const GBufSoA& hg, const float* in,
                                  const float* hist_in, float* out, uint8_t* rgb, cudaStream_t st) {
-  const uint32_t npix = uint32_t(p.width) * uint32_t(p.height);
-  const unsigned g = (npix + 255) / 256;
-  if (stage == 0) k_denoise_temporal<<<g, 256, 0, st>>>(p, gb, hg, in, hist_in, out);
-  else k_denoise_atrous<<<g, 256, 0, st>>>(p, gb, in, out, stage - 1, rgb);
-  return cudaGetLastError();
+  const dim3 blk(kTX, kTY), grd((p.width + kTX - 1) / kTX, (p.height + kTY - 1) / kTY);
+  if (stage == 0) {
+    k_denoise_temporal_tiled<<<grd, blk, 0, st>>>(p, gb, hg, in, hist_in, out);
+    return cudaGetLastError();
+  }
+  return launch_atrous_tiled(stage - 1, p, gb, in, out, rgb, st);
 }
 
 cudaError_t launch_tonemap(const float* hdr, uint8_t* rgb, uint32_t npix, cudaStream_t st) {

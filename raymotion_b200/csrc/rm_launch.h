@@ -65,6 +65,9 @@ cudaError_t launch_wavefront_shade(int vk, const Scene& s, const Params& p, cons
 cudaError_t launch_denoise_stage(int stage, const Params& p, const GBufSoA& gb, const GBufSoA& hg, const float* in,
                                  const float* hist_in, float* out, uint8_t* rgb, cudaStream_t st);
 cudaError_t launch_tonemap(const float* hdr, uint8_t* rgb, uint32_t npix, cudaStream_t st);
+// rm_atrous.cu: a-trous pass `step` (stride 1 << step), RGB8 written when rgb != nullptr.
+cudaError_t launch_atrous_tiled(int step, const Params& p, const GBufSoA& gb, const float* in, float* out,
+                                uint8_t* rgb, cudaStream_t st);
 
 // rm_bvh.cu ------------------------------------------------------------------
 
