@@ -205,6 +205,62 @@ int rmcuda_trace_noalloc(const rm_triangle* d_tris, int32_t n_tris, const float*
                          int32_t any_hit, int32_t* d_tri, float* d_t, float* d_u, float* d_v,
                          void* cuda_stream, char* err, size_t errcap);
 
+/* ---- Scene objects and batched rendering.  No counterpart in the reference,
+ * which renders one scene per call (metal.mm:95-414). */
+typedef struct rmcuda_scene rmcuda_scene;
+
+/* Upload a scene into device buffers of its own (BVH built or converted as in
+ * rmcuda_render), beside the context's resident scene.  Destroy the scenes of
+ * a context before the context. */
+int rmcuda_scene_create(rmcuda_ctx* ctx, const rm_scene_view* scene, rmcuda_scene** out,
+                        char* err, size_t errcap);
+void rmcuda_scene_destroy(rmcuda_ctx* ctx, rmcuda_scene* scene);
+
+/* One frame of a scene object with the single-frame policy of rmcuda_render
+ * (plain or lane path tracer, or ReSTIR + denoise when the policy picks it),
+ * into DEVICE buffers (either may be NULL); enqueued on the context stream and
+ * not waited for. */
+int rmcuda_render_scene_async(rmcuda_ctx* ctx, const rmcuda_scene* scene, const rm_camera* cam,
+                              const rm_config* cfg, uint64_t seed, uint8_t* d_rgb, float* d_hdr,
+                              char* err, size_t errcap);
+
+/* One image of a batch.  Output pointers are DEVICE pointers or NULL. */
+typedef struct rm_batch_item {
+  const rmcuda_scene* scene;
+  rm_camera camera;
+  rm_config config;
+  uint64_t seed;
+  uint8_t* d_rgb;   /* W*H*3 RGB8 */
+  float* d_hdr;     /* W*H*3 linear radiance */
+  uint32_t* d_aux;  /* W*H*2: xor of the pixel's final lane RNG states, samples taken */
+} rm_batch_item;
+
+/* Launch settings of batched rendering (rmcuda_batch_tune picks them). */
+typedef struct rm_batch_tuning {
+  int32_t pool_chunks;  /* path slots in flight, in chunks of 32 lane slots */
+  int32_t tile_shape;   /* pixels of a chunk: 0 a row segment, 1 a near-square block */
+  int32_t grid_scale;   /* persistent grids: resident blocks per SM x this (1..4) */
+  int32_t graph_waves;  /* waves per CUDA graph launch (even, 2..64); 0: no graph */
+} rm_batch_tuning;
+
+/* Render many images of (possibly different) scenes, views, resolutions,
+ * sample counts and depths together in one pool of path slots.  Each image is
+ * what the plain single-frame chain gives it: render_paths (K1) or the 8/32
+ * lane kernel (K2) of pathtrace.metal:739-815 with the lane rule of
+ * metal.mm:390-394, adaptive sampling and clamp, bit for bit equal to
+ * rmcuda_render_scene_async with the same inputs (radiance, RGB8, samples
+ * and RNG streams).  Items whose policy picks the ReSTIR chain are rejected
+ * (set RM_FLAG_RESTIR_OFF, or restir_spatial 0).  Synchronous. */
+int rmcuda_render_batch(rmcuda_ctx* ctx, const rm_batch_item* items, int32_t n, char* err, size_t errcap);
+
+/* Time candidate launch settings on the first waves of this batch, keep the
+ * fastest for later rmcuda_render_batch calls on this context and return it
+ * in `out` (may be NULL).  Leaves partial images in the items' buffers. */
+int rmcuda_batch_tune(rmcuda_ctx* ctx, const rm_batch_item* items, int32_t n, rm_batch_tuning* out,
+                      char* err, size_t errcap);
+int rmcuda_batch_get_tuning(rmcuda_ctx* ctx, rm_batch_tuning* out);
+int rmcuda_batch_set_tuning(rmcuda_ctx* ctx, const rm_batch_tuning* tuning, char* err, size_t errcap);
+
 /* Read the last frame's ReSTIR buffers back in the reference record layouts
  * (metal_types.h:32-56): which = 0 G-buffer (76 B/px), 1 initial reservoir,
  * 2 merged reservoir (60 B/px), 3 shaded HDR (12 B/px).  Host pointer. */
@@ -233,9 +289,15 @@ int rmcuda_stats_reset(rmcuda_ctx* ctx);
 #define RM_STAGE_WF_EXTEND 9 /* wavefront shading: closest-hit traversal waves */
 #define RM_STAGE_WF_SHADOW 10 /* wavefront shading: shadow-ray traversal waves */
 #define RM_STAGE_WF_SHADE 11 /* wavefront shading: shading waves (incl. the first) */
-#define RM_STAGE_COUNT 12
+#define RM_STAGE_BT_START 12  /* batched rendering: tile refill + sample starts */
+#define RM_STAGE_BT_EXTEND 13 /* batched rendering: closest-hit traversal */
+#define RM_STAGE_BT_SHADOW 14 /* batched rendering: shadow-ray traversal */
+#define RM_STAGE_BT_SHADE 15  /* batched rendering: shading */
+#define RM_STAGE_BATCH 16     /* batched rendering: a whole rmcuda_render_batch call */
+#define RM_STAGE_COUNT 17
 /* level 0: off; 1: one event pair per stage (the wavefront shading loop counts
- * as RM_STAGE_SHADE); 2: also every wavefront launch in its own stage. */
+ * as RM_STAGE_SHADE, a batch as RM_STAGE_BATCH); 2: also every wavefront
+ * launch in its own stage (batches then run without CUDA graphs). */
 int rmcuda_profile(rmcuda_ctx* ctx, int level);
 /* Per-stage device counters since the last reset: n records of
  * {path samples, rays, BVH nodes visited, triangle tests}. */

@@ -16,6 +16,7 @@ library or a sm_100 GPU every call fails loudly.
 from __future__ import annotations
 
 import ctypes as C
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -23,8 +24,8 @@ from . import _abi
 from ._abi import GBUF_DTYPE, RESERVOIR_DTYPE, load_library
 from .scene import Camera, PackedScene, RenderConfig, SceneBuilder, Texture
 
-__all__ = ["Backend", "RenderError", "render_image_metal", "Camera", "RenderConfig", "SceneBuilder", "Texture",
-           "PackedScene", "load_library"]
+__all__ = ["Backend", "BatchItem", "RenderError", "render_image_metal", "Camera", "RenderConfig", "SceneBuilder",
+           "Texture", "PackedScene", "load_library"]
 
 
 class RenderError(RuntimeError):
@@ -35,6 +36,34 @@ class RenderError(RuntimeError):
 
 def _err() -> C.Array:
     return C.create_string_buffer(512)
+
+
+@dataclass
+class BatchItem:
+    """One image of a batch (rm_batch_item): a scene object, its view and config,
+    and DEVICE output pointers (RGB8 W*H*3, radiance W*H*3 floats, and per
+    pixel (xor of the final lane RNG states, samples taken)), any may be None."""
+    scene: int
+    camera: Camera
+    config: RenderConfig
+    seed: int = 12345
+    d_rgb: int | None = None
+    d_hdr: int | None = None
+    d_aux: int | None = None
+
+
+def _batch_array(items) -> C.Array:
+    arr = (_abi.RmBatchItem * max(len(items), 1))()
+    for k, it in enumerate(items):
+        a = arr[k]
+        a.scene = it.scene
+        a.camera = it.camera.packed()
+        a.config = it.config.packed()
+        a.seed = it.seed & 0xFFFFFFFFFFFFFFFF
+        a.d_rgb = it.d_rgb
+        a.d_hdr = it.d_hdr
+        a.d_aux = it.d_aux
+    return arr
 
 
 class Backend:
@@ -116,6 +145,50 @@ class Backend:
         e = _err()
         self._check(self.lib.rmcuda_debug_read(self.h, which, _abi.ptr(out), out.nbytes, e, 512), e)
         return out
+
+    # ---- scene objects and batched rendering
+    def scene_create(self, scene: PackedScene, use_nodes: bool = False) -> int:
+        """Upload a scene into buffers of its own; returns its handle."""
+        v = scene.view(use_nodes)
+        h = C.c_void_p()
+        e = _err()
+        self._check(self.lib.rmcuda_scene_create(self.h, C.byref(v), C.byref(h), e, 512), e)
+        return h.value
+
+    def scene_destroy(self, handle: int) -> None:
+        self.lib.rmcuda_scene_destroy(self.h, handle)
+
+    def render_scene_async(self, handle: int, cam: Camera, cfg: RenderConfig, seed: int, d_rgb: int | None,
+                           d_hdr: int | None = None) -> None:
+        """The single-frame policy on a scene object, into device buffers (not waited for)."""
+        e = _err()
+        self._check(self.lib.rmcuda_render_scene_async(self.h, handle, C.byref(cam.packed()), C.byref(cfg.packed()),
+                                                       C.c_uint64(seed & 0xFFFFFFFFFFFFFFFF), d_rgb, d_hdr, e, 512),
+                    e)
+
+    def render_batch(self, items) -> None:
+        """Render a list of BatchItem together (synchronous)."""
+        arr = _batch_array(items)
+        e = _err()
+        self._check(self.lib.rmcuda_render_batch(self.h, arr, len(items), e, 512), e)
+
+    def batch_tune(self, items) -> dict:
+        """Pick launch settings on the first waves of this batch; returns them."""
+        arr = _batch_array(items)
+        t = _abi.RmBatchTuning()
+        e = _err()
+        self._check(self.lib.rmcuda_batch_tune(self.h, arr, len(items), C.byref(t), e, 512), e)
+        return {f: getattr(t, f) for f, _ in _abi.RmBatchTuning._fields_}
+
+    def batch_tuning(self) -> dict:
+        t = _abi.RmBatchTuning()
+        self.lib.rmcuda_batch_get_tuning(self.h, C.byref(t))
+        return {f: getattr(t, f) for f, _ in _abi.RmBatchTuning._fields_}
+
+    def set_batch_tuning(self, **kw) -> None:
+        t = _abi.RmBatchTuning(**{**self.batch_tuning(), **kw})
+        e = _err()
+        self._check(self.lib.rmcuda_batch_set_tuning(self.h, C.byref(t), e, 512), e)
 
     def reset_history(self) -> None:
         self.lib.rmcuda_reset_history(self.h)

@@ -83,6 +83,16 @@ class RmStats(C.Structure):
                 ("device_error", C.c_uint32), ("kernel_chain", C.c_uint32)]
 
 
+class RmBatchItem(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", RmCamera), ("config", RmConfig), ("seed", C.c_uint64),
+                ("d_rgb", C.c_void_p), ("d_hdr", C.c_void_p), ("d_aux", C.c_void_p)]
+
+
+class RmBatchTuning(C.Structure):
+    _fields_ = [("pool_chunks", C.c_int32), ("tile_shape", C.c_int32), ("grid_scale", C.c_int32),
+                ("graph_waves", C.c_int32)]
+
+
 # (name, restype, argtypes) of every symbol declared in include/rmcuda.h
 _P = C.c_void_p
 _S = C.c_char_p
@@ -109,10 +119,18 @@ EXPORTS = [
     ("rmcuda_wave_log", C.c_int, [_P, C.POINTER(C.c_int32), C.c_int32]),
     ("rmcuda_trace_noalloc", C.c_int, [_P, C.c_int32, _P, C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _S, _Z]),
     ("rmcuda_stage_times", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int32]),
+    ("rmcuda_scene_create", C.c_int, [_P, C.POINTER(RmSceneView), C.POINTER(_P), _S, _Z]),
+    ("rmcuda_scene_destroy", None, [_P, _P]),
+    ("rmcuda_render_scene_async", C.c_int, [_P, _P, C.POINTER(RmCamera), C.POINTER(RmConfig), C.c_uint64, _P, _P,
+                                             _S, _Z]),
+    ("rmcuda_render_batch", C.c_int, [_P, C.POINTER(RmBatchItem), C.c_int32, _S, _Z]),
+    ("rmcuda_batch_tune", C.c_int, [_P, C.POINTER(RmBatchItem), C.c_int32, C.POINTER(RmBatchTuning), _S, _Z]),
+    ("rmcuda_batch_get_tuning", C.c_int, [_P, C.POINTER(RmBatchTuning)]),
+    ("rmcuda_batch_set_tuning", C.c_int, [_P, C.POINTER(RmBatchTuning), _S, _Z]),
 ]
 
 STAGES = ["plain", "hash", "generate", "spatial", "shade", "temporal", "atrous0", "atrous1", "tonemap", "wf_extend",
-          "wf_shadow", "wf_shade"]
+          "wf_shadow", "wf_shade", "bt_start", "bt_extend", "bt_shadow", "bt_shade", "batch"]
 
 _lib = None
 

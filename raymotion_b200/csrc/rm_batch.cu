@@ -1,0 +1,453 @@
+// rm_batch.cu - many plain-path images rendered together by one pool of path
+// slots (wavefront stages over compacted queues, persistent grid-stride
+// kernels whose grids do not depend on queue lengths, so a sequence of waves
+// can be captured in a CUDA graph once and replayed).
+//
+// Each image follows the reference's plain chain: render_paths (K1,
+// pathtrace.metal:739-769) with one lane per pixel, or render_paths_simd (K2,
+// :773-815) with 8 or 32 lanes per pixel that take one sample each per round,
+// are summed with a butterfly reduction, and stop early when the adaptive test
+// (:759-764) passes at the end of a round.  Here every lane is a slot of the
+// pool with its own random stream; a lane that finishes its sample of the
+// round publishes it and the last lane of the pixel to finish sums the round
+// in the butterfly's order (a pairwise tree: every level adds the upper half
+// to the lower half), runs the adaptive test and either starts the next round
+// on all lanes or writes the pixel.  So the images, random streams and sample
+// counts equal those of the one-image lane kernels bit for bit, whatever the
+// mix of images in the pool.
+//
+// Per wave:  refill  chunks that finished their tile take the batch's next tile;
+//            start   lane slots start their sample of the round (camera ray);
+//            trace   closest hit of every extension ray (stochastic alpha
+//                    crossings in partially transparent scenes, with the
+//                    slot's random stream, as pathtrace.metal:536-550),
+//                    then any hit of every deferred shadow ray;
+//            shade   one vertex per path (rm_wf_common.cuh), by surface type.
+#include <cuda_runtime.h>
+
+#include "rm_device.cuh"
+#include "rm_launch.h"
+#include "rm_wf_common.cuh"
+
+namespace rmd {
+
+namespace {
+
+using namespace wf;
+
+__device__ __forceinline__ void tile_pixel(const BtJob& J, int tile, int g, int& x, int& y) {
+  const int tx = tile % J.tiles_x, ty = tile / J.tiles_x;
+  x = tx * J.tile_w + g % J.tile_w;
+  y = ty * J.tile_h + g / J.tile_w;
+}
+
+__device__ __forceinline__ void bload(const BtState& w, int i, PathRegs& r, uint32_t& rng) {
+  const uint4 u = w.u[i];
+  rng = u.x; r.meta = u.y; r.v = int(u.z);
+  const float4 acc = w.acc[i], thr = w.thr[i], pb = w.pb[i], o = w.o[i], d = w.d[i];
+  r.ax = acc.x; r.ay = acc.y; r.az = acc.z; r.psumW = acc.w;
+  r.tx = thr.x; r.ty = thr.y; r.tz = thr.z; r.pbcos = thr.w;
+  r.pbr = pb.x; r.pbg = pb.y; r.pbb = pb.z; r.pM = uint32_t(__float_as_int(pb.w));
+  r.ox = o.x; r.oy = o.y; r.oz = o.z; r.last_pdf = o.w;
+  r.dx = d.x; r.dy = d.y; r.dz = d.z;
+}
+
+__device__ __forceinline__ void bstore(const BtState& w, int i, const PathRegs& r, uint32_t rng) {
+  w.u[i] = make_uint4(rng, r.meta, uint32_t(r.v), 0u);
+  w.acc[i] = make_float4(r.ax, r.ay, r.az, r.psumW);
+  w.thr[i] = make_float4(r.tx, r.ty, r.tz, r.pbcos);
+  w.pb[i] = make_float4(r.pbr, r.pbg, r.pbb, __int_as_float(int(r.pM)));
+  w.o[i] = make_float4(r.ox, r.oy, r.oz, r.last_pdf);
+  w.d[i] = make_float4(r.dx, r.dy, r.dz, 0.f);
+}
+
+// The last lane of a pixel to finish the round: sum the round (K2's butterfly,
+// pathtrace.metal:797-805, which gives every lane the pairwise-tree sum), then
+// the adaptive test (:806-810) and either the next round or the pixel's
+// output (:811-814; K1 :759-768 is the one-lane case).
+__device__ __noinline__ void finish_round(const BtState& w, const BtQueues& nq, const BtJob& J, int chunk, int g0,
+                                          int rbase, int x, int y) {
+  const int L = J.lanes;
+  const int spp = J.p.spp;
+  const int takers = min(L, spp - rbase);
+  float vr[kBtChunk], vg[kBtChunk], vb[kBtChunk], vl[kBtChunk], vl2[kBtChunk];
+  for (int k = 0; k < L; ++k) {
+    float cr = 0.f, cg = 0.f, cb = 0.f;
+    if (k < takers) {
+      const float4 a = w.val[g0 + k];
+      cr = a.x; cg = a.y; cb = a.z;
+    }
+    float lum = cr * 0.2126f + cg * 0.7152f + cb * 0.0722f;
+    vr[k] = cr; vg[k] = cg; vb[k] = cb; vl[k] = lum; vl2[k] = lum * lum;
+  }
+  for (int m = 1; m < L; m <<= 1)
+    for (int k = 0; k < L; k += 2 * m) {
+      vr[k] = vr[k] + vr[k + m];
+      vg[k] = vg[k] + vg[k + m];
+      vb[k] = vb[k] + vb[k + m];
+      vl[k] = vl[k] + vl[k + m];
+      vl2[k] = vl2[k] + vl2[k + m];
+    }
+  float4 gs = w.gsum[g0];
+  float sl2 = w.gsl2[g0];
+  gs.x += vr[0]; gs.y += vg[0]; gs.z += vb[0]; gs.w += vl[0];
+  sl2 += vl2[0];
+  const int n = min(rbase + L, spp);
+  bool stop = n >= spp;
+  const Params& p = J.p;
+  if (!stop && p.adapt_min > 0 && n >= p.adapt_min && n > 1 && n % p.adapt_step == 0) {
+    float mean = gs.w / float(n);
+    float var = fmaxf(0.0f, (sl2 - gs.w * mean) / float(n - 1));
+    float thr = p.adapt_rel * mean + p.adapt_abs;
+    if (var < thr * thr) stop = true;
+  }
+  if (stop) {
+    const size_t pix = size_t(y) * size_t(p.width) + size_t(x);
+    const float cr = gs.x / float(n), cg = gs.y / float(n), cb = gs.z / float(n);
+    if (J.hdr) { J.hdr[pix * 3] = cr; J.hdr[pix * 3 + 1] = cg; J.hdr[pix * 3 + 2] = cb; }
+    if (J.rgb) { J.rgb[pix * 3] = tonemap8(cr); J.rgb[pix * 3 + 1] = tonemap8(cg); J.rgb[pix * 3 + 2] = tonemap8(cb); }
+    if (J.dbg) {
+      uint32_t st = 0;
+      for (int k = 0; k < L; ++k) st ^= w.u[g0 + k].x;
+      J.dbg[pix * 2] = st;
+      J.dbg[pix * 2 + 1] = uint32_t(n);
+    }
+    if (atomicSub(&w.cleft[chunk], 1) == 1) {
+      const int pos = atomicAdd(nq.counts + kBtRf, 1);
+      nq.rf[pos] = chunk;
+    }
+    return;
+  }
+  w.gsum[g0] = gs;
+  w.gsl2[g0] = sl2;
+  w.gbase[g0] = rbase + L;
+  w.garr[g0] = 0;
+  const int m = min(L, spp - (rbase + L));
+  const int pos = atomicAdd(nq.counts + kBtSt, m);
+  for (int k = 0; k < m; ++k) nq.st[pos + k] = g0 + k;
+}
+
+// A lane's sample of the round is done (value already clamped): publish it;
+// the pixel's last lane finishes the round.  The slot's RNG state must be
+// stored before this (the pixel's output XORs the lanes' states).
+__device__ __forceinline__ void arrive(const BtState& w, const BtQueues& nq, const BtJob& J, int i, float fr,
+                                       float fg, float fb) {
+  const int chunk = i >> 5, k = i & 31;
+  const int L = J.lanes, g = k / L;
+  const int g0 = (chunk << 5) + g * L;
+  w.val[i] = make_float4(fr, fg, fb, 0.f);
+  const int rbase = w.gbase[g0];
+  const int takers = min(L, J.p.spp - rbase);
+  __threadfence();
+  const int old = atomicAdd(&w.garr[g0], 1);
+  if (old + 1 != takers) return;
+  __threadfence();
+  int x, y;
+  tile_pixel(J, w.ctile[chunk], g, x, y);
+  finish_round(w, nq, J, chunk, g0, rbase, x, y);
+}
+
+__global__ void k_bt_init(BtState w, BtQueues q0, int chunks, int* next_tile) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < chunks) {
+    q0.rf[i] = i;
+    w.cjob[i] = -1;
+  }
+  if (i < kBtCounts) q0.counts[i] = i == kBtRf ? chunks : 0;
+  if (i == 0) *next_tile = 0;
+}
+
+// Chunks whose tile is done take the next tile of the batch (one warp per
+// chunk) and queue their lane slots to start round 0.
+__global__ void __launch_bounds__(256) k_bt_refill(BtBatch b, BtState w, BtQueues q) {
+  const int n = q.counts[kBtRf];
+  const int k = int(threadIdx.x & 31);
+  const int stride = int(gridDim.x * blockDim.x);
+  for (int base = int(blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); base < n * kBtChunk; base += stride) {
+    const int chunk = q.rf[base >> 5];
+    int t = 0;
+    if (k == 0) t = atomicAdd(b.next_tile, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= b.total_tiles) {
+      if (k == 0) w.cjob[chunk] = -1;
+      continue;
+    }
+    int lo = 0, hi = b.n_jobs - 1;  // last job whose first tile is <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (b.tile_begin[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const BtJob& J = b.jobs[lo];
+    const int tile = t - J.tile_begin;
+    const int L = J.lanes, g = k / L, lane = k % L;
+    int x, y;
+    tile_pixel(J, tile, g, x, y);
+    const bool present = x < J.p.width && y < J.p.height;
+    const int slot = (chunk << 5) + k;
+    if (present && lane == 0) {
+      w.gsum[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+      w.gsl2[slot] = 0.f;
+      w.gbase[slot] = 0;
+      w.garr[slot] = 0;
+    }
+    const unsigned groups = __ballot_sync(0xffffffffu, present && lane == 0);
+    if (k == 0) {
+      w.cjob[chunk] = lo;
+      w.ctile[chunk] = tile;
+      w.cleft[chunk] = __popc(groups);
+    }
+    append(q.st, q.counts + kBtSt, present, slot);
+  }
+}
+
+// Start the round's sample of each queued lane slot: the jitter and camera ray
+// of K1 / K2 (pathtrace.metal:754-756, :792-794; sample_sensor :729-737).
+__global__ void __launch_bounds__(256) k_bt_start(BtBatch b, BtState w, BtQueues q, BtQueues nq,
+                                                  unsigned long long* ctr, uint32_t* err) {
+  const int n = q.counts[kBtSt];
+  const int stride = int(gridDim.x * blockDim.x);
+  uint32_t samples = 0;
+  for (int base = int(blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); base < n; base += stride) {
+    const int qi = base + int(threadIdx.x & 31);
+    bool ext = false;
+    int i = 0;
+    if (qi < n) {
+      i = q.st[qi];
+      const int chunk = i >> 5, k = i & 31;
+      const BtJob& J = b.jobs[w.cjob[chunk]];
+      const int L = J.lanes, g = k / L, lane = k % L;
+      const int g0 = (chunk << 5) + g * L;
+      int x, y;
+      tile_pixel(J, w.ctile[chunk], g, x, y);
+      Tracer pt(J.s, J.p, err);
+      if (w.gbase[g0] == 0) {
+        uint64_t sd = seed_pixel(J.seed, uint32_t(x), uint32_t(y));
+        if (L > 1) sd ^= uint64_t(lane) * 0x94D049BB133111EBull;
+        pt.rng.seed(sd);
+      } else {
+        pt.rng.state = w.u[i].x;
+      }
+      float sx, sy;
+      pt.jitter(uint32_t(x), uint32_t(y), sx, sy);
+      const rm_camera& cam = J.p.camera;
+      const float focal2 = cam.focal * cam.focal;
+      const float dist = 1.0f / sqrtf(sx * sx + (sy * sy + focal2));
+      const float tx = sx * dist, ty = sy * dist, tz = cam.focal * dist;
+      PathRegs r;
+      r.dx = tx * cam.m0 + (ty * cam.m1 + tz * cam.m2);
+      r.dy = tx * cam.m3 + (ty * cam.m4 + tz * cam.m5);
+      r.dz = tx * cam.m6 + (ty * cam.m7 + tz * cam.m8);
+      r.ox = cam.x; r.oy = cam.y; r.oz = cam.z;
+      r.ax = r.ay = r.az = 0.0f;
+      r.tx = r.ty = r.tz = 1.0f;
+      r.v = 0;
+      r.meta = kDelta;
+      r.last_pdf = 0.0f; r.psumW = 0.0f; r.pM = 0;
+      r.pbr = r.pbg = r.pbb = r.pbcos = 0.0f;
+      if (J.p.bounces > 0) {
+        r.meta |= kExt;
+        bstore(w, i, r, pt.rng.state);
+        ext = true;
+      } else {  // no bounce: the sample is zero
+        w.u[i] = make_uint4(pt.rng.state, 0u, 0u, 0u);
+        float fr = 0.f, fg = 0.f, fb = 0.f;
+        clamp3(J.p, fr, fg, fb);
+        ++samples;
+        arrive(w, nq, J, i, fr, fg, fb);
+      }
+    }
+    append(q.ext, q.counts + kBtExt, ext, i);
+  }
+  __syncwarp();
+  warp_add(ctr + 0, samples);
+}
+
+// Traversal of a queue of rays, one thread per ray (closest hit for extension
+// rays, pathtrace.metal:119-163 and :536-550; any hit for shadow rays, :164).
+// Finished extension rays are sorted into the shading queue of their surface
+// type.
+template <bool kShadowRays>
+__global__ void __launch_bounds__(128) k_bt_trace(BtBatch b, BtState w, BtQueues q, unsigned long long* ctr,
+                                                  uint32_t* err) {
+  const int n = q.counts[kShadowRays ? kBtShd : kBtExt];
+  const int* queue = kShadowRays ? q.shd : q.ext;
+  const int stride = int(gridDim.x * blockDim.x);
+  uint32_t nodes = 0, tests = 0, rays = 0;
+  for (int base = int(blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); base < n; base += stride) {
+    const int qi = base + int(threadIdx.x & 31);
+    int cls = -1;  // 0 opaque, 1 dielectric, 2 miss
+    int i = 0;
+    if (qi < n) {
+      i = queue[qi];
+      const BtJob& J = b.jobs[w.cjob[i >> 5]];
+      const Scene& s = J.s;
+      if (kShadowRays) {
+        const float4 o = w.so[i], d = w.sd[i];
+        const TraceResult r = traverse<true>(s, o.x, o.y, o.z, d.x, d.y, d.z, o.w, err, nodes, tests);
+        ++rays;
+        w.occ[i] = r.tri >= 0 ? 1u : 0u;
+      } else {
+        const float4 o = w.o[i], d = w.d[i];
+        TraceResult r;
+        if (J.p.opaque) {
+          r = traverse<false>(s, o.x, o.y, o.z, d.x, d.y, d.z, kFar, err, nodes, tests);
+          ++rays;
+        } else {
+          // stochastic coverage: step through transparent crossings
+          Rng rng;
+          rng.state = w.u[i].x;
+          r.tri = -1;
+          r.t = kFar;
+          float traveled = 0.0f;
+          float hx = o.x, hy = o.y, hz = o.z;
+          for (int it = 0; it < kMaxAlphaCrossings && traveled < kFar; ++it) {
+            const float qx = o.x + d.x * traveled, qy = o.y + d.y * traveled, qz = o.z + d.z * traveled;
+            const TraceResult h = traverse<false>(s, qx, qy, qz, d.x, d.y, d.z, kFar - traveled, err, nodes, tests);
+            ++rays;
+            if (h.tri < 0) break;
+            const float opacity = s.tris[h.tri].alpha;
+            if (opacity >= 1.0f || (opacity > 0.0f && rng.uniform01() < opacity)) {
+              r = h;
+              hx = qx; hy = qy; hz = qz;
+              break;
+            }
+            traveled += h.t + 0.0001f;
+          }
+          w.u[i].x = rng.state;
+          w.hoff[i] = make_float4(hx, hy, hz, 0.f);
+        }
+        w.hit[i] = make_float4(r.t, r.u, r.v, __int_as_float(r.tri));
+        cls = 2;
+        if (r.tri >= 0) cls = __ldg(&s.tris[r.tri].ior) > 1.0001f ? 1 : 0;
+      }
+    }
+    if (!kShadowRays) {
+      append(q.qa, q.counts + kBtA, cls == 0, i);
+      append(q.qb, q.counts + kBtB, cls == 1, i);
+      append(q.qc, q.counts + kBtC, cls == 2, i);
+    }
+  }
+  __syncwarp();
+  warp_add(ctr + 1, rays);
+  warp_add(ctr + 2, nodes);
+  warp_add(ctr + 3, tests);
+}
+
+// Shade the paths of one queue: VK 0 opaque hits, 1 dielectric hits, 2 paths
+// without a vertex (the ray missed, or the path ended and waited for its last
+// shadow ray).  A path that ends finishes its lane's sample of the round.
+template <int VK>
+__global__ void __launch_bounds__(256) k_bt_shade(BtBatch b, BtState w, BtQueues cq, BtQueues nq,
+                                                  unsigned long long* ctr, uint32_t* err) {
+  const int count = cq.counts[VK == 0 ? kBtA : (VK == 1 ? kBtB : kBtC)];
+  const int* queue = VK == 0 ? cq.qa : (VK == 1 ? cq.qb : cq.qc);
+  const int stride = int(gridDim.x * blockDim.x);
+  uint32_t samples = 0, rays = 0, nodes = 0, tests = 0;
+  for (int base = int(blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); base < count; base += stride) {
+    const int qi = base + int(threadIdx.x & 31);
+    bool ext = false, shd = false, fin = false;
+    int i = 0;
+    if (qi < count) {
+      i = queue[qi];
+      const BtJob& J = b.jobs[w.cjob[i >> 5]];
+      Tracer pt(J.s, J.p, err);
+      PathRegs r;
+      bload(w, i, r, pt.rng.state);
+      if (r.meta & kShadow) {
+        r.meta &= ~kShadow;
+        if (w.occ[i] == 0u) {
+          const float4 c = w.c[i];
+          r.ax += c.x; r.ay += c.y; r.az += c.z;
+        }
+      }
+      bool ended;
+      if (VK == 2) {
+        ended = true;  // a miss ends the path; a finishing path has now folded in its last shadow ray
+        r.meta &= ~(kExt | kFinish);
+      } else {
+        r.meta &= ~kExt;
+        const float4 hh = w.hit[i];
+        const TraceResult tr{hh.x, __float_as_int(hh.w), hh.y, hh.z};
+        Hit hit;
+        if (J.p.opaque) {
+          hit = pt.attributes(tr, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz);
+        } else {
+          const float4 ho = w.hoff[i];
+          hit = pt.attributes(tr, ho.x, ho.y, ho.z, r.dx, r.dy, r.dz);
+        }
+        bool has_shadow = false;
+        float4 so, sd, c;
+        const bool go = vertex<VK>(pt, J.p, r, hit, has_shadow, so, sd, c);
+        if (has_shadow) {
+          w.so[i] = so; w.sd[i] = sd; w.c[i] = c;
+          r.meta |= kShadow;
+          shd = true;
+        }
+        if (go) { r.meta |= kExt; ext = true; }
+        ended = !go;
+        if (ended && has_shadow) { r.meta |= kFinish; ended = false; fin = true; }  // wait for the shadow ray
+      }
+      bstore(w, i, r, pt.rng.state);
+      if (ended) {
+        float fr = r.ax, fg = r.ay, fb = r.az;
+        clamp3(J.p, fr, fg, fb);
+        ++samples;
+        arrive(w, nq, J, i, fr, fg, fb);
+      }
+      rays += pt.rays; nodes += pt.nodes; tests += pt.tests;
+    }
+    append(nq.ext, nq.counts + kBtExt, ext, i);
+    append(nq.shd, nq.counts + kBtShd, shd, i);
+    append(nq.qc, nq.counts + kBtC, fin, i);
+  }
+  __syncwarp();
+  warp_add(ctr + 0, samples);
+  warp_add(ctr + 1, rays);
+  warp_add(ctr + 2, nodes);
+  warp_add(ctr + 3, tests);
+}
+
+}  // namespace
+
+cudaError_t launch_batch_init(const BtState& w, const BtQueues& q0, int chunks, int* next_tile, cudaStream_t st) {
+  const int n = chunks > kBtCounts ? chunks : kBtCounts;
+  k_bt_init<<<(n + 255) / 256, 256, 0, st>>>(w, q0, chunks, next_tile);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_refill(const BtBatch& b, const BtState& w, const BtQueues& q, int grid, cudaStream_t st) {
+  k_bt_refill<<<grid, 256, 0, st>>>(b, w, q);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_start(const BtBatch& b, const BtState& w, const BtQueues& q, const BtQueues& nq, int grid,
+                               unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
+  k_bt_start<<<grid, 256, 0, st>>>(b, w, q, nq, ctr, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_trace(const BtBatch& b, const BtState& w, const BtQueues& q, bool shadow, int grid,
+                               unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
+  if (shadow) k_bt_trace<true><<<grid, 128, 0, st>>>(b, w, q, ctr, err);
+  else k_bt_trace<false><<<grid, 128, 0, st>>>(b, w, q, ctr, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_shade(int vk, const BtBatch& b, const BtState& w, const BtQueues& q, const BtQueues& nq,
+                               int grid, unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
+  if (vk == 0) k_bt_shade<0><<<grid, 256, 0, st>>>(b, w, q, nq, ctr, err);
+  else if (vk == 1) k_bt_shade<1><<<grid, 256, 0, st>>>(b, w, q, nq, ctr, err);
+  else k_bt_shade<2><<<grid, 256, 0, st>>>(b, w, q, nq, ctr, err);
+  return cudaGetLastError();
+}
+
+void batch_occupancy(int& aux, int& trace, int& shade) {
+  aux = trace = shade = 1;
+  int v = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_bt_start, 256, 0) == cudaSuccess && v > 0) aux = v;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_bt_trace<false>, 128, 0) == cudaSuccess && v > 0) trace = v;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_bt_shade<0>, 256, 0) == cudaSuccess && v > 0) shade = v;
+}
+
+}  // namespace rmd

@@ -1,0 +1,179 @@
+// rm_ctx.h - the library context and device-resident scenes, shared by the
+// translation units of the C ABI (rmcuda_api.cu, rmcuda_batch.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "rm_launch.h"
+#include "rmcuda.h"
+
+namespace rmapi {
+
+using rmd::DevBuf;
+using rmd::DevBvh;
+using rmd::GBufSoA;
+using rmd::ResSoA;
+
+struct GBufSet {
+  DevBuf pos_kind, nor_rough, alb_met, wo_ior, emi;
+  cudaError_t reserve(size_t npix) {
+    cudaError_t e;
+    for (DevBuf* b : {&pos_kind, &nor_rough, &alb_met, &wo_ior, &emi})
+      if ((e = b->reserve(npix * sizeof(float4))) != cudaSuccess) return e;
+    return cudaSuccess;
+  }
+  GBufSoA view() const {
+    return GBufSoA{pos_kind.as<float4>(), nor_rough.as<float4>(), alb_met.as<float4>(), wo_ior.as<float4>(),
+                   emi.as<float4>()};
+  }
+  void release() { for (DevBuf* b : {&pos_kind, &nor_rough, &alb_met, &wo_ior, &emi}) b->release(); }
+};
+struct ResSet {
+  DevBuf lp, ln, le, wm;
+  cudaError_t reserve(size_t npix) {
+    cudaError_t e;
+    for (DevBuf* b : {&lp, &ln, &le, &wm})
+      if ((e = b->reserve(npix * sizeof(float4))) != cudaSuccess) return e;
+    return cudaSuccess;
+  }
+  ResSoA view() const { return ResSoA{lp.as<float4>(), ln.as<float4>(), le.as<float4>(), wm.as<float4>()}; }
+  void release() { for (DevBuf* b : {&lp, &ln, &le, &wm}) b->release(); }
+};
+
+// One device-resident scene: the uploaded triangles, lights, textures, the
+// light-sampling tables and the BVH.
+struct DevScene {
+  DevBuf tris, lights, cdf, texels, lrec, guide;
+  int guide_n = 0;
+  float guide_inv = 0.0f;
+  DevBvh bvh;
+  int n_tris = 0, n_lights = 0;
+  float light_total = 0;
+  bool opaque = true;
+  bool have_scene = false;
+  int refits = 0;
+  bool device_built = false;
+  void release() {
+    for (DevBuf* b : {&tris, &lights, &cdf, &texels, &lrec, &guide, &bvh.records, &bvh.parents, &bvh.counters,
+                      &bvh.order, &bvh.tgeo, &bvh.keys, &bvh.keys_alt, &bvh.vals_alt, &bvh.knodes, &bvh.kbox,
+                      &bvh.kcount, &bvh.ranges, &bvh.temp, &bvh.bounds, &bvh.depth})
+      b->release();
+  }
+};
+
+// Buffers of batched rendering: the pool of lane slots (rmd::BtState), the
+// queues of two waves, the job table and the captured wave graph.
+struct BatchPool {
+  DevBuf slot[17];   // per lane slot and per group arrays of BtState
+  DevBuf chunk[3];   // per chunk arrays of BtState
+  DevBuf queue[15];  // 7 queues x 2 waves + the counts of both waves
+  DevBuf jobs, tile_begin, next_tile;
+  rm_batch_tuning tuning{65536, 0, 1, 8};
+  int chunks = 0;    // pool size the buffers hold, in chunks of 32 lane slots
+  int occ[3] = {0, 0, 0};  // resident blocks per SM of the batch kernels
+  int* h_counts = nullptr;  // pinned: queue lengths read back between graph launches (2 x kBtCounts)
+  cudaGraphExec_t exec = nullptr;
+  uint64_t waves = 0;
+  std::vector<int> wave_log;  // last batch: (live slots, extension rays) per check
+  void release();
+};
+
+// Frame policy of one image (metal.mm:146-170, :236-237, :390-394).
+struct Plan {
+  rmd::Params p;
+  int lanes = 1;
+  bool use_spatial = false;
+  bool denoise = true;
+  bool temporal_off = false;
+};
+
+}  // namespace rmapi
+
+struct rmcuda_scene {
+  rmapi::DevScene d;
+  int device = 0;
+};
+
+struct rmcuda_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  std::mutex mu;
+  rmapi::DevScene sc;  // the resident scene
+  // frame buffers
+  rmapi::GBufSet gb, hg;
+  rmapi::ResSet rinit, rmerged, hres;
+  rmd::DevBuf hdr, tmp_a, tmp_b, hist_col, rgb, dbg, hash_out;
+  rmd::DevBuf ctr, err;
+  // temporal history (metal.mm:35-40)
+  rm_camera hist_cam{};
+  int hist_w = 0, hist_h = 0;
+  uint64_t hist_seed = 0;
+  unsigned long long hist_hash = 0;
+  bool hist_valid = false, have_hist_bufs = false;
+  // last frame
+  int last_chain = 0;
+  uint64_t frames = 0;
+  uint64_t launches = 0;
+  float* last_final = nullptr;  // device pointer of the last frame's tonemap input
+  int last_w = 0, last_h = 0;
+  // wavefront shading state (rm_wavefront.cu)
+  rmd::DevBuf wf[14];
+  rmd::DevBuf wq[11];
+  int* h_counts = nullptr;  // pinned: the current wave's queue lengths
+  size_t wf_cap = 0;
+  uint64_t waves = 0;
+  std::vector<int> wave_log;  // last frame: (act, ext, shd) per wave
+  // batched rendering (rmcuda_batch.cu)
+  rmapi::BatchPool batch;
+  // per-stage CUDA-event timing (rmcuda_profile)
+  int profiling = 0;
+  struct Pending { int stage; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  double stage_ms[RM_STAGE_COUNT] = {};
+  uint64_t stage_n[RM_STAGE_COUNT] = {};
+};
+
+namespace rmapi {
+
+extern const char* const kUnavailable;
+extern const char* const kInvalidDims;
+
+void set_err(char* err, size_t cap, const std::string& m);
+std::string cuda_msg(const char* what, cudaError_t e);
+
+// Launch through `fn`, bracketed by events on the context stream when profiling.
+template <class Fn> cudaError_t staged(rmcuda_ctx* c, int stage, Fn&& fn) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (c->profiling > 0 && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess)
+    cudaEventRecord(a, c->stream);
+  cudaError_t e = fn();
+  if (a && b) {
+    cudaEventRecord(b, c->stream);
+    c->pending.push_back({stage, a, b});
+  }
+  c->launches += 1;
+  return e;
+}
+
+// As staged(), but timed only at profiling level 2 (per-launch breakdown).
+template <class Fn> cudaError_t staged2(rmcuda_ctx* c, int stage, Fn&& fn) {
+  if (c->profiling >= 2) return staged(c, stage, fn);
+  c->launches += 1;
+  return fn();
+}
+
+void resolve_pending(rmcuda_ctx* c);
+rmd::Scene scene_view(const DevScene& sc);
+// Validate and upload one scene into `sc`; build or convert its BVH.
+int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::string& msg);
+Plan make_plan(const DevScene& sc, const rm_camera& cam, const rm_config& cfg);
+// Enqueue one frame of `sc` with the single-frame policy.
+int enqueue_frame(rmcuda_ctx* c, DevScene& sc, const rm_camera& cam, const rm_config& cfg, uint64_t seed,
+                  uint8_t* d_rgb, std::string& msg);
+int check_device_error(rmcuda_ctx* c, std::string& msg);
+
+}  // namespace rmapi

@@ -60,6 +60,79 @@ cudaError_t launch_wavefront_shade(int vk, const Scene& s, const Params& p, cons
                                    const WfQueues& cq, int bound, const WfQueues& nq, float* hdr, uint32_t* dbg,
                                    unsigned long long* ctr, uint32_t* err, cudaStream_t st);
 
+// rm_batch.cu: many plain-path images (reference K1 / K2) rendered together
+// by one pool of path slots.  A pixel owns `lanes` consecutive lane slots (its
+// K2 lanes); 32 lane slots form a chunk, which renders one tile of one image
+// (tile_w x tile_h pixels, tile_w * tile_h * lanes == 32) and is refilled with
+// the next tile of the batch when all its pixels are done.
+constexpr int kBtChunk = 32;
+struct BtJob {
+  Scene s;
+  Params p;
+  uint64_t seed;
+  float* hdr;      // W*H*3 floats, or null
+  uint8_t* rgb;    // W*H*3 bytes, or null
+  uint32_t* dbg;   // W*H*2 words (xor of the lanes' final RNG states, samples), or null
+  int lanes;       // 1, 8 or 32
+  int tile_w, tile_h, tiles_x, tiles;
+  int tile_begin;  // first tile of the job in the batch's tile sequence
+};
+struct BtBatch {
+  const BtJob* jobs;
+  const int* tile_begin;  // per job, ascending
+  int n_jobs, total_tiles;
+  int* next_tile;         // device counter: next tile to hand out
+};
+struct BtState {
+  // per lane slot
+  uint4* u;      // rng, meta, vertex index, -
+  float4* acc;   // path radiance, psumW
+  float4* thr;   // throughput, previous BSDF cosine
+  float4* pb;    // previous BSDF value, previous M
+  float4* o;     // extension ray origin, last_pdf
+  float4* d;     // extension ray direction
+  float4* c;     // contribution of the pending shadow ray if visible
+  float4* so;    // shadow ray origin, length
+  float4* sd;    // shadow ray direction
+  float4* hit;   // t, u, v, triangle (t from hoff's origin in partially transparent scenes)
+  float4* hoff;  // partially transparent scenes: origin of the ray that made the hit
+  float4* val;   // the slot's sample of the current round
+  uint32_t* occ;
+  // per pixel group, at the index of its first lane slot
+  float4* gsum;  // radiance sums, luminance sum
+  float* gsl2;   // squared-luminance sum
+  int* gbase;    // first sample index of the current round
+  int* garr;     // lanes of the round that have finished their sample
+  // per chunk
+  int* cjob;     // job, or -1 when idle
+  int* ctile;    // tile within the job
+  int* cleft;    // pixels of the tile still rendering
+};
+// Queues of one wave: extension rays, shadow rays, paths to shade by vertex
+// type (a opaque, b dielectric, c none), lane slots to start a sample, chunks
+// to refill.
+constexpr int kBtExt = 0, kBtShd = 1, kBtA = 2, kBtB = 3, kBtC = 4, kBtSt = 5, kBtRf = 6, kBtCounts = 8;
+struct BtQueues {
+  int *ext, *shd, *qa, *qb, *qc, *st, *rf;
+  int* counts;  // kBtCounts ints
+};
+// Grid sizes of the persistent (grid-stride) batch kernels.
+struct BtGrid {
+  int aux;    // refill / start, 256 threads per block
+  int trace;  // 128 threads per block
+  int shade;  // 256 threads per block
+};
+cudaError_t launch_batch_init(const BtState& w, const BtQueues& q0, int chunks, int* next_tile, cudaStream_t st);
+cudaError_t launch_batch_refill(const BtBatch& b, const BtState& w, const BtQueues& q, int grid, cudaStream_t st);
+cudaError_t launch_batch_start(const BtBatch& b, const BtState& w, const BtQueues& q, const BtQueues& nq, int grid,
+                               unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+cudaError_t launch_batch_trace(const BtBatch& b, const BtState& w, const BtQueues& q, bool shadow, int grid,
+                               unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+cudaError_t launch_batch_shade(int vk, const BtBatch& b, const BtState& w, const BtQueues& q, const BtQueues& nq,
+                               int grid, unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+// Resident blocks per SM of each batch kernel (aux, trace, shade).
+void batch_occupancy(int& aux, int& trace, int& shade);
+
 // rm_denoise.cu
 // stage 0 temporal (in + hist_in -> out), 1 / 2 a-trous step 0 / 1 (in -> out, + RGB8 when rgb != nullptr)
 cudaError_t launch_denoise_stage(int stage, const Params& p, const GBufSoA& gb, const GBufSoA& hg, const float* in,

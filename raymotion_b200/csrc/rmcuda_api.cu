@@ -23,15 +23,28 @@
 #include <utility>
 #include <vector>
 
+#include "rm_ctx.h"
 #include "rm_launch.h"
 #include "rmcuda.h"
 
 using namespace rmd;
+using namespace rmapi;
+
+namespace rmapi {
+
+const char* const kUnavailable = "Metal backend is not available in this build";
+const char* const kInvalidDims = "Invalid Metal render dimensions or sample count";
+
+void set_err(char* err, size_t cap, const std::string& m) {
+  if (err && cap) std::snprintf(err, cap, "%s", m.c_str());
+}
+
+std::string cuda_msg(const char* what, cudaError_t e) { return std::string(what) + ": " + cudaGetErrorString(e); }
+
+}  // namespace rmapi
 
 namespace {
 
-constexpr const char* kUnavailable = "Metal backend is not available in this build";
-constexpr const char* kInvalidDims = "Invalid Metal render dimensions or sample count";
 constexpr int kLbvhLeaf = 4;
 
 // Device BVH builder: PLOC clustering (default) or LBVH (RAYMOTION_CUDA_BVH=lbvh);
@@ -48,36 +61,6 @@ cudaError_t build_device_bvh(const rm_triangle* d_tris, int n, rmd::DevBvh& bvh,
   }
   return e;
 }
-
-void set_err(char* err, size_t cap, const std::string& m) {
-  if (err && cap) std::snprintf(err, cap, "%s", m.c_str());
-}
-
-struct GBufSet {
-  DevBuf pos_kind, nor_rough, alb_met, wo_ior, emi;
-  cudaError_t reserve(size_t npix) {
-    cudaError_t e;
-    for (DevBuf* b : {&pos_kind, &nor_rough, &alb_met, &wo_ior, &emi})
-      if ((e = b->reserve(npix * sizeof(float4))) != cudaSuccess) return e;
-    return cudaSuccess;
-  }
-  GBufSoA view() const {
-    return GBufSoA{pos_kind.as<float4>(), nor_rough.as<float4>(), alb_met.as<float4>(), wo_ior.as<float4>(),
-                   emi.as<float4>()};
-  }
-  void release() { for (DevBuf* b : {&pos_kind, &nor_rough, &alb_met, &wo_ior, &emi}) b->release(); }
-};
-struct ResSet {
-  DevBuf lp, ln, le, wm;
-  cudaError_t reserve(size_t npix) {
-    cudaError_t e;
-    for (DevBuf* b : {&lp, &ln, &le, &wm})
-      if ((e = b->reserve(npix * sizeof(float4))) != cudaSuccess) return e;
-    return cudaSuccess;
-  }
-  ResSoA view() const { return ResSoA{lp.as<float4>(), ln.as<float4>(), le.as<float4>(), wm.as<float4>()}; }
-  void release() { for (DevBuf* b : {&lp, &ln, &le, &wm}) b->release(); }
-};
 
 struct Env {
   bool noadapt = false, nomis = false, restir_off = false, denoise_off = false, temporal_off = false;
@@ -108,80 +91,7 @@ Env read_env(uint32_t flags) {
 
 }  // namespace
 
-struct rmcuda_ctx {
-  int device = 0;
-  cudaStream_t own = nullptr, stream = nullptr;
-  std::mutex mu;
-  // resident scene
-  DevBuf tris, lights, cdf, texels, lrec, guide;
-  int guide_n = 0;
-  float guide_inv = 0.0f;
-  DevBvh bvh;
-  int n_tris = 0, n_lights = 0;
-  float light_total = 0;
-  bool opaque = true;
-  bool have_scene = false;
-  int refits = 0;
-  bool device_built = false;
-  unsigned long long scene_hash = 0;
-  // frame buffers
-  GBufSet gb, hg;
-  ResSet rinit, rmerged, hres;
-  DevBuf hdr, tmp_a, tmp_b, hist_col, rgb, dbg, hash_out;
-  DevBuf ctr, err;
-  size_t npix_cap = 0;
-  // temporal history (metal.mm:35-40)
-  rm_camera hist_cam{};
-  int hist_w = 0, hist_h = 0;
-  uint64_t hist_seed = 0;
-  unsigned long long hist_hash = 0;
-  bool hist_valid = false, have_hist_bufs = false;
-  // last frame
-  int last_chain = 0;
-  uint64_t frames = 0;
-  uint64_t launches = 0;
-  float* last_final = nullptr;  // device pointer of the last frame's tonemap input
-  int last_w = 0, last_h = 0;
-  // wavefront shading state (rm_wavefront.cu)
-  DevBuf wf[14];
-  DevBuf wq[11];
-  int* h_counts = nullptr;  // pinned: the current wave's queue lengths
-  size_t wf_cap = 0;
-  uint64_t waves = 0;
-  std::vector<int> wave_log;  // last frame: (act, ext, shd) per wave
-  // per-stage CUDA-event timing (rmcuda_profile)
-  int profiling = 0;
-  bool profiling_any() const { return profiling > 0; }
-  struct Pending { int stage; cudaEvent_t a, b; };
-  std::vector<Pending> pending;
-  double stage_ms[RM_STAGE_COUNT] = {};
-  uint64_t stage_n[RM_STAGE_COUNT] = {};
-};
-
-namespace {
-
-std::string cuda_msg(const char* what, cudaError_t e) { return std::string(what) + ": " + cudaGetErrorString(e); }
-
-// Launch through `fn`, bracketed by events on the context stream when profiling.
-template <class Fn> cudaError_t staged(rmcuda_ctx* c, int stage, Fn&& fn) {
-  cudaEvent_t a = nullptr, b = nullptr;
-  if (c->profiling > 0 && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess)
-    cudaEventRecord(a, c->stream);
-  cudaError_t e = fn();
-  if (a && b) {
-    cudaEventRecord(b, c->stream);
-    c->pending.push_back({stage, a, b});
-  }
-  c->launches += 1;
-  return e;
-}
-
-// As staged(), but timed only at profiling level 2 (per-launch breakdown).
-template <class Fn> cudaError_t staged2(rmcuda_ctx* c, int stage, Fn&& fn) {
-  if (c->profiling >= 2) return staged(c, stage, fn);
-  c->launches += 1;
-  return fn();
-}
+namespace rmapi {
 
 void resolve_pending(rmcuda_ctx* c) {
   for (auto& pe : c->pending) {
@@ -196,26 +106,26 @@ void resolve_pending(rmcuda_ctx* c) {
   c->pending.clear();
 }
 
-Scene scene_view(const rmcuda_ctx* c) {
+Scene scene_view(const DevScene& sc) {
   Scene s;
-  s.tris = c->tris.as<rm_triangle>();
-  s.tgeo = c->bvh.tgeo.as<float4>();
-  s.nodes = c->bvh.records.as<float4>();
-  s.n_nodes = c->n_tris > 0 ? c->bvh.n_records : 0;
-  s.lights = c->lights.as<int32_t>();
-  s.cdf = c->cdf.as<float>();
-  s.n_lights = c->n_lights;
-  s.light_total = c->light_total;
-  s.texels = c->texels.as<rm_vec3>();
-  s.lrec = c->lrec.as<float4>();
-  s.guide = c->guide.as<int32_t>();
-  s.guide_n = c->guide_n;
-  s.guide_inv = c->guide_inv;
+  s.tris = sc.tris.as<rm_triangle>();
+  s.tgeo = sc.bvh.tgeo.as<float4>();
+  s.nodes = sc.bvh.records.as<float4>();
+  s.n_nodes = sc.n_tris > 0 ? sc.bvh.n_records : 0;
+  s.lights = sc.lights.as<int32_t>();
+  s.cdf = sc.cdf.as<float>();
+  s.n_lights = sc.n_lights;
+  s.light_total = sc.light_total;
+  s.texels = sc.texels.as<rm_vec3>();
+  s.lrec = sc.lrec.as<float4>();
+  s.guide = sc.guide.as<int32_t>();
+  s.guide_n = sc.guide_n;
+  s.guide_inv = sc.guide_inv;
   return s;
 }
 
 // Validate and upload one scene; build or convert its BVH.
-int upload_scene(rmcuda_ctx* c, const rm_scene_view* sv, std::string& msg) {
+int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::string& msg) {
   if (!sv || sv->n_tris < 0 || sv->n_lights < 0 || sv->n_texels < 0 || (sv->n_tris > 0 && !sv->tris) ||
       (sv->n_lights > 0 && (!sv->light_tri || !sv->light_cdf)) || (sv->n_texels > 0 && !sv->texels)) {
     msg = "invalid scene view";
@@ -238,94 +148,86 @@ int upload_scene(rmcuda_ctx* c, const rm_scene_view* sv, std::string& msg) {
   cudaStream_t st = c->stream;
   cudaError_t e;
   const size_t tb = size_t(sv->n_tris) * sizeof(rm_triangle);
-  if ((e = c->tris.reserve(tb)) != cudaSuccess || (e = c->lights.reserve(size_t(sv->n_lights) * 4)) != cudaSuccess ||
-      (e = c->cdf.reserve(size_t(sv->n_lights) * 4)) != cudaSuccess ||
-      (e = c->texels.reserve(size_t(sv->n_texels) * sizeof(rm_vec3))) != cudaSuccess) {
+  if ((e = sc.tris.reserve(tb)) != cudaSuccess || (e = sc.lights.reserve(size_t(sv->n_lights) * 4)) != cudaSuccess ||
+      (e = sc.cdf.reserve(size_t(sv->n_lights) * 4)) != cudaSuccess ||
+      (e = sc.texels.reserve(size_t(sv->n_texels) * sizeof(rm_vec3))) != cudaSuccess) {
     msg = cuda_msg("Metal scene buffer allocation failed", e);
     return RM_ERR_ALLOC;
   }
-  if ((tb && (e = cudaMemcpyAsync(c->tris.ptr, sv->tris, tb, cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+  if ((tb && (e = cudaMemcpyAsync(sc.tris.ptr, sv->tris, tb, cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
       (sv->n_lights &&
-       (e = cudaMemcpyAsync(c->lights.ptr, sv->light_tri, size_t(sv->n_lights) * 4, cudaMemcpyHostToDevice, st)) !=
+       (e = cudaMemcpyAsync(sc.lights.ptr, sv->light_tri, size_t(sv->n_lights) * 4, cudaMemcpyHostToDevice, st)) !=
            cudaSuccess) ||
       (sv->n_lights &&
-       (e = cudaMemcpyAsync(c->cdf.ptr, sv->light_cdf, size_t(sv->n_lights) * 4, cudaMemcpyHostToDevice, st)) !=
+       (e = cudaMemcpyAsync(sc.cdf.ptr, sv->light_cdf, size_t(sv->n_lights) * 4, cudaMemcpyHostToDevice, st)) !=
            cudaSuccess) ||
-      (sv->n_texels && (e = cudaMemcpyAsync(c->texels.ptr, sv->texels, size_t(sv->n_texels) * sizeof(rm_vec3),
+      (sv->n_texels && (e = cudaMemcpyAsync(sc.texels.ptr, sv->texels, size_t(sv->n_texels) * sizeof(rm_vec3),
                                             cudaMemcpyHostToDevice, st)) != cudaSuccess)) {
     msg = cuda_msg("scene upload failed", e);
     return RM_ERR_CUDA;
   }
-  c->n_tris = sv->n_tris;
-  c->n_lights = sv->n_lights;
-  c->light_total = sv->light_total;
-  c->opaque = opaque;
-  if ((e = prepare_lights(c->tris.as<rm_triangle>(), c->lights.as<int32_t>(), c->cdf.as<float>(), c->n_lights,
-                          c->light_total, c->lrec, c->guide, c->guide_n, c->guide_inv, st)) != cudaSuccess) {
+  sc.n_tris = sv->n_tris;
+  sc.n_lights = sv->n_lights;
+  sc.light_total = sv->light_total;
+  sc.opaque = opaque;
+  if ((e = prepare_lights(sc.tris.as<rm_triangle>(), sc.lights.as<int32_t>(), sc.cdf.as<float>(), sc.n_lights,
+                          sc.light_total, sc.lrec, sc.guide, sc.guide_n, sc.guide_inv, st)) != cudaSuccess) {
     msg = cuda_msg("light preparation failed", e);
     return RM_ERR_CUDA;
   }
-  c->refits = 0;
-  c->have_scene = false;
+  sc.refits = 0;
+  sc.have_scene = false;
   if (sv->n_tris > 0 && sv->nodes && sv->n_nodes == 0) {
     // caller passed an empty BVH: every ray misses, as with params.nodes == 0
     // in the reference (pathtrace.metal:121)
-    c->bvh.n_records = 0;
-    c->bvh.n_tris = 0;
-    c->device_built = false;
+    sc.bvh.n_records = 0;
+    sc.bvh.n_tris = 0;
+    sc.device_built = false;
   } else if (sv->n_tris > 0) {
     bool converted = false;
     if (sv->nodes && sv->n_nodes > 0) {
       std::string berr;
-      if (convert_caller_bvh(sv->nodes, sv->n_nodes, sv->bvh_tri, sv->n_tris, c->bvh, st, berr)) {
+      if (convert_caller_bvh(sv->nodes, sv->n_nodes, sv->bvh_tri, sv->n_tris, sc.bvh, st, berr)) {
         converted = true;
       } else if (berr.find("deeper") == std::string::npos) {
         msg = berr;
         return RM_ERR_BVH;
       }
-      if (converted && (e = pack_tgeo(c->tris.as<rm_triangle>(), c->bvh, st)) != cudaSuccess) {
+      if (converted && (e = pack_tgeo(sc.tris.as<rm_triangle>(), sc.bvh, st)) != cudaSuccess) {
         msg = cuda_msg("BVH packing failed", e);
         return RM_ERR_CUDA;
       }
     }
-    c->device_built = !converted;
+    sc.device_built = !converted;
     if (!converted) {
       std::string berr;
-      if ((e = build_device_bvh(c->tris.as<rm_triangle>(), sv->n_tris, c->bvh, st, berr)) != cudaSuccess) {
+      if ((e = build_device_bvh(sc.tris.as<rm_triangle>(), sv->n_tris, sc.bvh, st, berr)) != cudaSuccess) {
         msg = berr.empty() ? cuda_msg("device BVH build failed", e) : berr;
         return RM_ERR_CUDA;
       }
     }
   } else {
-    c->bvh.n_records = 0;
-    c->bvh.n_tris = 0;
+    sc.bvh.n_records = 0;
+    sc.bvh.n_tris = 0;
   }
-  c->have_scene = true;
+  sc.have_scene = true;
   return RM_OK;
 }
 
-struct Plan {
-  Params p;
-  int lanes = 1;
-  bool use_spatial = false;
-  bool denoise = true;
-  bool temporal_off = false;
-};
-
 // metal.mm:146-170, :236-237, :390-394
-Plan make_plan(const rmcuda_ctx* c, const rm_camera& cam, const rm_config& cfg) {
+Plan make_plan(const DevScene& sc, const rm_camera& cam, const rm_config& cfg) {
   Env env = read_env(cfg.flags);
   Plan pl;
   Params& p = pl.p;
   std::memset(&p, 0, sizeof(p));
   p.camera = cam;
   p.width = cfg.width; p.height = cfg.height; p.spp = cfg.spp; p.bounces = cfg.max_bounces;
-  p.nodes = c->n_tris > 0 ? c->bvh.n_records : 0;
-  p.lights = c->n_lights; p.light_total = c->light_total;
+  p.nodes = sc.n_tris > 0 ? sc.bvh.n_records : 0;
+  p.lights = sc.n_lights; p.light_total = sc.light_total;
   p.resolution = cfg.resolution; p.clamp_value = cfg.clamp; p.adapt_rel = cfg.adapt_rel; p.adapt_abs = cfg.adapt_abs;
   p.adapt_min = env.noadapt ? 0 : cfg.adapt_min;
   p.adapt_step = cfg.adapt_step > 0 ? cfg.adapt_step : 8;
-  p.opaque = c->opaque ? 1 : 0;
+  p.opaque = sc.opaque ? 1 : 0;
   p.nomis = env.nomis ? 1 : 0;
   p.restir_candidates = env.restir_off ? 1 : (cfg.restir_candidates > 0 ? cfg.restir_candidates : 1);
   p.restir_candidates = std::min(32, std::max(1, p.restir_candidates));
@@ -456,15 +358,15 @@ cudaError_t ensure_frame(rmcuda_ctx* c, size_t npix, bool restir) {
 
 // Enqueue one frame of the resident scene.  d_rgb (device) receives the
 // image; the final linear radiance stays in c->last_final.
-int enqueue_frame(rmcuda_ctx* c, const rm_camera& cam, const rm_config& cfg, uint64_t seed, uint8_t* d_rgb,
+int enqueue_frame(rmcuda_ctx* c, DevScene& sc, const rm_camera& cam, const rm_config& cfg, uint64_t seed, uint8_t* d_rgb,
                   std::string& msg) {
   if (cfg.width <= 0 || cfg.height <= 0 || cfg.spp <= 0 || cfg.max_bounces < 0 ||
       size_t(cfg.width) * size_t(cfg.height) > 100000000) {
     msg = kInvalidDims;
     return RM_ERR_INVALID;
   }
-  if (!c->have_scene) { msg = "no resident scene"; return RM_ERR_INVALID; }
-  Plan pl = make_plan(c, cam, cfg);
+  if (!sc.have_scene) { msg = "no resident scene"; return RM_ERR_INVALID; }
+  Plan pl = make_plan(sc, cam, cfg);
   Params& p = pl.p;
   const size_t npix = size_t(cfg.width) * size_t(cfg.height);
   cudaStream_t st = c->stream;
@@ -473,7 +375,7 @@ int enqueue_frame(rmcuda_ctx* c, const rm_camera& cam, const rm_config& cfg, uin
     msg = cuda_msg(pl.use_spatial ? "Metal ReSTIR buffer allocation failed" : "Metal image buffer allocation failed", e);
     return RM_ERR_ALLOC;
   }
-  Scene s = scene_view(c);
+  Scene s = scene_view(sc);
   unsigned long long* ctr = c->ctr.as<unsigned long long>();
   uint32_t* err = c->err.as<uint32_t>();
   if (!pl.use_spatial) {
@@ -489,15 +391,15 @@ int enqueue_frame(rmcuda_ctx* c, const rm_camera& cam, const rm_config& cfg, uin
     // scene hash over the uploaded triangle bytes (metal.mm:241-248)
     if ((e = c->hash_out.reserve(8)) != cudaSuccess) { msg = cuda_msg("hash buffer", e); return RM_ERR_ALLOC; }
     e = staged(c, RM_STAGE_HASH, [&] {
-      return device_hash(c->tris.ptr, size_t(c->n_tris) * sizeof(rm_triangle), c->hash_out.as<unsigned long long>(), st);
+      return device_hash(sc.tris.ptr, size_t(sc.n_tris) * sizeof(rm_triangle), c->hash_out.as<unsigned long long>(), st);
     });
     unsigned long long h = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, c->hash_out.ptr, 8, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { msg = cuda_msg("scene hash failed", e); return RM_ERR_CUDA; }
     uint32_t lt_bits;
-    std::memcpy(&lt_bits, &c->light_total, 4);
-    h ^= uint64_t(c->n_tris) * 0x9E3779B97F4A7C15ull ^ uint64_t(c->n_lights) * 0xBF58476D1CE4E5B9ull ^
+    std::memcpy(&lt_bits, &sc.light_total, 4);
+    h ^= uint64_t(sc.n_tris) * 0x9E3779B97F4A7C15ull ^ uint64_t(sc.n_lights) * 0xBF58476D1CE4E5B9ull ^
          uint64_t(lt_bits) * 0x94D049BB133111EBull;
     const bool animated = (cfg.flags & RM_FLAG_ANIMATED_HISTORY) != 0;
     bool have_hist = c->hist_valid && c->hist_w == cfg.width && c->hist_h == cfg.height && c->have_hist_bufs &&
@@ -574,7 +476,7 @@ int check_device_error(rmcuda_ctx* c, std::string& msg) {
   return RM_OK;
 }
 
-}  // namespace
+}  // namespace rmapi
 
 extern "C" {
 
@@ -616,10 +518,9 @@ void rmcuda_destroy(rmcuda_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  for (DevBuf* b : {&c->tris, &c->lights, &c->cdf, &c->texels, &c->lrec, &c->guide, &c->hdr, &c->tmp_a, &c->tmp_b, &c->hist_col, &c->rgb, &c->dbg,
-                    &c->hash_out, &c->ctr, &c->err, &c->bvh.records, &c->bvh.parents, &c->bvh.counters,
-                    &c->bvh.order, &c->bvh.tgeo, &c->bvh.keys, &c->bvh.keys_alt, &c->bvh.vals_alt, &c->bvh.knodes,
-                    &c->bvh.kbox, &c->bvh.kcount, &c->bvh.ranges, &c->bvh.temp, &c->bvh.bounds, &c->bvh.depth})
+  c->sc.release();
+  c->batch.release();
+  for (DevBuf* b : {&c->hdr, &c->tmp_a, &c->tmp_b, &c->hist_col, &c->rgb, &c->dbg, &c->hash_out, &c->ctr, &c->err})
     b->release();
   for (DevBuf& b : c->wf) b.release();
   for (DevBuf& b : c->wq) b.release();
@@ -644,7 +545,7 @@ int rmcuda_scene_upload(rmcuda_ctx* c, const rm_scene_view* sv, char* err, size_
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   std::string msg;
-  int rc = upload_scene(c, sv, msg);
+  int rc = upload_scene(c, c->sc, sv, msg);
   if (rc == RM_OK) {
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { msg = cuda_msg("scene upload failed", e); rc = RM_ERR_CUDA; }
@@ -658,29 +559,29 @@ int rmcuda_scene_update(rmcuda_ctx* c, const rm_triangle* tris, int32_t n, int32
   if (!c) { set_err(err, errcap, "null context"); return RM_ERR_INVALID; }
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
-  if (!c->have_scene || n != c->n_tris || (n > 0 && !tris)) {
+  if (!c->sc.have_scene || n != c->sc.n_tris || (n > 0 && !tris)) {
     set_err(err, errcap, "scene update needs a resident scene with the same triangle count");
     return RM_ERR_INVALID;
   }
-  cudaError_t e = cudaMemcpyAsync(c->tris.ptr, tris, size_t(n) * sizeof(rm_triangle), cudaMemcpyHostToDevice, c->stream);
+  cudaError_t e = cudaMemcpyAsync(c->sc.tris.ptr, tris, size_t(n) * sizeof(rm_triangle), cudaMemcpyHostToDevice, c->stream);
   if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("scene update upload failed", e)); return RM_ERR_CUDA; }
   bool opaque = true;
   for (int i = 0; i < n; ++i)
     if (!(tris[i].alpha >= 1.0f)) { opaque = false; break; }
-  c->opaque = opaque;
+  c->sc.opaque = opaque;
   if (n == 0) return RM_OK;
-  e = prepare_lights(c->tris.as<rm_triangle>(), c->lights.as<int32_t>(), c->cdf.as<float>(), c->n_lights,
-                     c->light_total, c->lrec, c->guide, c->guide_n, c->guide_inv, c->stream);
+  e = prepare_lights(c->sc.tris.as<rm_triangle>(), c->sc.lights.as<int32_t>(), c->sc.cdf.as<float>(), c->sc.n_lights,
+                     c->sc.light_total, c->sc.lrec, c->sc.guide, c->sc.guide_n, c->sc.guide_inv, c->stream);
   if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("light preparation failed", e)); return RM_ERR_CUDA; }
-  if (rebuild_every > 0 && c->refits + 1 >= rebuild_every) {
+  if (rebuild_every > 0 && c->sc.refits + 1 >= rebuild_every) {
     std::string berr;
-    e = build_device_bvh(c->tris.as<rm_triangle>(), n, c->bvh, c->stream, berr);
-    c->refits = 0;
-    c->device_built = true;
+    e = build_device_bvh(c->sc.tris.as<rm_triangle>(), n, c->sc.bvh, c->stream, berr);
+    c->sc.refits = 0;
+    c->sc.device_built = true;
     if (e != cudaSuccess) { set_err(err, errcap, berr.empty() ? cuda_msg("rebuild failed", e) : berr); return RM_ERR_CUDA; }
   } else {
-    e = refit_bvh(c->tris.as<rm_triangle>(), c->bvh, c->stream);
-    c->refits++;
+    e = refit_bvh(c->sc.tris.as<rm_triangle>(), c->sc.bvh, c->stream);
+    c->sc.refits++;
     if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("refit failed", e)); return RM_ERR_CUDA; }
   }
   return RM_OK;
@@ -692,7 +593,7 @@ int rmcuda_render_resident_async(rmcuda_ctx* c, const rm_camera* cam, const rm_c
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   std::string msg;
-  int rc = enqueue_frame(c, *cam, *cfg, seed, d_rgb, msg);
+  int rc = enqueue_frame(c, c->sc, *cam, *cfg, seed, d_rgb, msg);
   if (rc == RM_OK && d_hdr) {
     const size_t bytes = size_t(cfg->width) * size_t(cfg->height) * 12;
     cudaError_t e = cudaMemcpyAsync(d_hdr, c->last_final, bytes, cudaMemcpyDeviceToDevice, c->stream);
@@ -725,12 +626,12 @@ int rmcuda_render(rmcuda_ctx* c, const rm_scene_view* sv, const rm_camera* cam, 
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   std::string msg;
-  int rc = upload_scene(c, sv, msg);
+  int rc = upload_scene(c, c->sc, sv, msg);
   if (rc == RM_OK) {
     cudaError_t e = c->rgb.reserve(npix * 3);
     if (e != cudaSuccess) { msg = cuda_msg("Metal image buffer allocation failed", e); rc = RM_ERR_ALLOC; }
   }
-  if (rc == RM_OK) rc = enqueue_frame(c, *cam, *cfg, seed, c->rgb.as<uint8_t>(), msg);
+  if (rc == RM_OK) rc = enqueue_frame(c, c->sc, *cam, *cfg, seed, c->rgb.as<uint8_t>(), msg);
   if (rc == RM_OK) {
     cudaError_t e = cudaSuccess;
     if (rgb) e = cudaMemcpyAsync(rgb, c->rgb.ptr, npix * 3, cudaMemcpyDeviceToHost, c->stream);
@@ -751,8 +652,8 @@ int rmcuda_trace(rmcuda_ctx* c, const float* d_rays, int32_t n, int32_t any_hit,
   if (!c || (n > 0 && (!d_rays || !d_tri)) || n < 0) { set_err(err, errcap, "invalid trace arguments"); return RM_ERR_INVALID; }
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
-  if (!c->have_scene) { set_err(err, errcap, "no resident scene"); return RM_ERR_INVALID; }
-  cudaError_t e = launch_trace(scene_view(c), d_rays, n, any_hit, d_tri, d_t, d_u, d_v, c->err.as<uint32_t>(), c->stream);
+  if (!c->sc.have_scene) { set_err(err, errcap, "no resident scene"); return RM_ERR_INVALID; }
+  cudaError_t e = launch_trace(scene_view(c->sc), d_rays, n, any_hit, d_tri, d_t, d_u, d_v, c->err.as<uint32_t>(), c->stream);
   if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("trace launch failed", e)); return RM_ERR_CUDA; }
   std::string msg;
   int rc = check_device_error(c, msg);

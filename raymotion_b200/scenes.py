@@ -11,6 +11,10 @@
   (roughness U[0.05, 1]) / 20 % dielectric (IOR 1.5, roughness 0 or 0.2), and
   small emissive triangles with log-uniform radiance in [1, 100].  The default
   arguments give 200 spheres + 2 + 4096 = 1,028,098 triangles.
+* ``batch_workload(...)``: many such scenes of uneven size for batched
+  rendering: triangle counts log-uniform over [1k, 2M], resolutions from
+  {256x256, 640x360, 1280x720, 1920x1080}, spp from {4, 16, 64}, depth 8-12,
+  all on the plain path (ReSTIR and the denoiser off).
 """
 from __future__ import annotations
 
@@ -18,6 +22,7 @@ import math
 
 import numpy as np
 
+from . import _abi
 from .scene import Camera, RenderConfig, SceneBuilder
 
 
@@ -167,3 +172,43 @@ def icosphere_field(seed: int = 1, n_spheres: int = 200, subdiv: int = 4, n_emit
     cfg = RenderConfig(width=width, height=height, spp=spp, max_bounces=depth, restir_candidates=32,
                        restir_spatial=5, restir_radius=30.0)
     return sb, cam, cfg
+
+
+PLAIN_FLAGS = _abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_RESTIR_OFF | _abi.RM_FLAG_DENOISE_OFF
+BATCH_RESOLUTIONS = ((256, 256), (640, 360), (1280, 720), (1920, 1080))
+
+
+def sized_field(seed: int, n_tris: int, width: int, height: int, spp: int, depth: int):
+    """An icosphere field of about ``n_tris`` triangles on the plain path.
+
+    Emitters: n_tris / 64 clamped to [16, 4096]; the rest are icospheres of the
+    finest subdivision (<= 4) that still gives at least three spheres, plus the
+    two ground triangles."""
+    n_emit = int(min(4096, max(16, n_tris // 64)))
+    rest = max(20, n_tris - n_emit - 2)
+    subdiv = 0
+    for k in (4, 3, 2, 1, 0):
+        if rest // (20 * 4 ** k) >= 3:
+            subdiv = k
+            break
+    n_spheres = max(1, int(round(rest / (20 * 4 ** subdiv))))
+    sb, cam, cfg = icosphere_field(seed, n_spheres=n_spheres, subdiv=subdiv, n_emitters=n_emit, width=width,
+                                   height=height, spp=spp, depth=depth)
+    cfg.flags = PLAIN_FLAGS
+    return sb, cam, cfg
+
+
+def batch_workload(seed: int = 3, n_scenes: int = 64, tri_range=(1000, 2_000_000), resolutions=BATCH_RESOLUTIONS,
+                   spps=(4, 16, 64), depths=(8, 12)):
+    """Specs of a batch of uneven scenes: a list of dicts (seed, n_tris, width,
+    height, spp, depth) drawn from ``seed``; ``sized_field(**spec)`` builds one."""
+    rng = np.random.default_rng(seed)
+    out = []
+    lo, hi = math.log(tri_range[0]), math.log(tri_range[1])
+    for i in range(n_scenes):
+        n_tris = int(round(math.exp(rng.uniform(lo, hi))))
+        w, h = resolutions[int(rng.integers(len(resolutions)))]
+        spp = int(spps[int(rng.integers(len(spps)))])
+        depth = int(rng.integers(depths[0], depths[1] + 1))
+        out.append(dict(seed=seed * 1000 + i, n_tris=n_tris, width=w, height=h, spp=spp, depth=depth))
+    return out
