@@ -258,6 +258,11 @@ int rmcuda_render_batch(rmcuda_ctx* ctx, const rm_batch_item* items, int32_t n, 
  * in `out` (may be NULL).  Leaves partial images in the items' buffers. */
 int rmcuda_batch_tune(rmcuda_ctx* ctx, const rm_batch_item* items, int32_t n, rm_batch_tuning* out,
                       char* err, size_t errcap);
+/* Progress of the last batch: for each check between graph replays (every
+ * graph_waves waves, or 8 without a graph) the live lane slots (queued to
+ * start, trace or finish) and the extension rays queued, at most `cap`
+ * records (2 ints each) written.  Returns the number of records. */
+int rmcuda_batch_log(rmcuda_ctx* ctx, int32_t* out, int32_t cap);
 int rmcuda_batch_get_tuning(rmcuda_ctx* ctx, rm_batch_tuning* out);
 int rmcuda_batch_set_tuning(rmcuda_ctx* ctx, const rm_batch_tuning* tuning, char* err, size_t errcap);
 

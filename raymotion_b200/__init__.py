@@ -180,6 +180,14 @@ class Backend:
         self._check(self.lib.rmcuda_batch_tune(self.h, arr, len(items), C.byref(t), e, 512), e)
         return {f: getattr(t, f) for f, _ in _abi.RmBatchTuning._fields_}
 
+    def batch_log(self) -> np.ndarray:
+        """(live lane slots, extension rays) at each progress check of the last batch."""
+        n = self.lib.rmcuda_batch_log(self.h, None, 0)
+        out = np.zeros((max(n, 0), 2), np.int32)
+        if n > 0:
+            self.lib.rmcuda_batch_log(self.h, out.ctypes.data_as(C.POINTER(C.c_int32)), n)
+        return out
+
     def batch_tuning(self) -> dict:
         t = _abi.RmBatchTuning()
         self.lib.rmcuda_batch_get_tuning(self.h, C.byref(t))

@@ -125,6 +125,7 @@ EXPORTS = [
                                              _S, _Z]),
     ("rmcuda_render_batch", C.c_int, [_P, C.POINTER(RmBatchItem), C.c_int32, _S, _Z]),
     ("rmcuda_batch_tune", C.c_int, [_P, C.POINTER(RmBatchItem), C.c_int32, C.POINTER(RmBatchTuning), _S, _Z]),
+    ("rmcuda_batch_log", C.c_int, [_P, C.POINTER(C.c_int32), C.c_int32]),
     ("rmcuda_batch_get_tuning", C.c_int, [_P, C.POINTER(RmBatchTuning)]),
     ("rmcuda_batch_set_tuning", C.c_int, [_P, C.POINTER(RmBatchTuning), _S, _Z]),
 ]

@@ -9,12 +9,12 @@
 // are summed with a butterfly reduction, and stop early when the adaptive test
 // (:759-764) passes at the end of a round.  Here every lane is a slot of the
 // pool with its own random stream; a lane that finishes its sample of the
-// round publishes it and the last lane of the pixel to finish sums the round
-// in the butterfly's order (a pairwise tree: every level adds the upper half
-// to the lower half), runs the adaptive test and either starts the next round
-// on all lanes or writes the pixel.  So the images, random streams and sample
-// counts equal those of the one-image lane kernels bit for bit, whatever the
-// mix of images in the pool.
+// round publishes it, and the last lane of the pixel to finish queues the
+// pixel; a combine pass then gives each queued pixel L lanes of a warp, which
+// sum the round with the same shuffles as K2, run the adaptive test and either
+// queue the next round's lane slots or write the pixel.  So the images, random
+// streams and sample counts equal those of the one-image lane kernels bit for
+// bit, whatever the mix of images in the pool.
 //
 // Per wave:  refill  chunks that finished their tile take the batch's next tile;
 //            start   lane slots start their sample of the round (camera ray);
@@ -22,7 +22,9 @@
 //                    crossings in partially transparent scenes, with the
 //                    slot's random stream, as pathtrace.metal:536-550),
 //                    then any hit of every deferred shadow ray;
-//            shade   one vertex per path (rm_wf_common.cuh), by surface type.
+//            shade   one vertex per path (rm_wf_common.cuh), by surface type;
+//            combine the pixels whose round is complete, one warp lane per
+//                    pixel lane, with K2's own shuffles.
 #include <cuda_runtime.h>
 
 #include "rm_device.cuh"
@@ -61,90 +63,30 @@ __device__ __forceinline__ void bstore(const BtState& w, int i, const PathRegs& 
   w.d[i] = make_float4(r.dx, r.dy, r.dz, 0.f);
 }
 
-// The last lane of a pixel to finish the round: sum the round (K2's butterfly,
-// pathtrace.metal:797-805, which gives every lane the pairwise-tree sum), then
-// the adaptive test (:806-810) and either the next round or the pixel's
-// output (:811-814; K1 :759-768 is the one-lane case).
-__device__ __noinline__ void finish_round(const BtState& w, const BtQueues& nq, const BtJob& J, int chunk, int g0,
-                                          int rbase, int x, int y) {
-  const int L = J.lanes;
-  const int spp = J.p.spp;
-  const int takers = min(L, spp - rbase);
-  float vr[kBtChunk], vg[kBtChunk], vb[kBtChunk], vl[kBtChunk], vl2[kBtChunk];
-  for (int k = 0; k < L; ++k) {
-    float cr = 0.f, cg = 0.f, cb = 0.f;
-    if (k < takers) {
-      const float4 a = w.val[g0 + k];
-      cr = a.x; cg = a.y; cb = a.z;
-    }
-    float lum = cr * 0.2126f + cg * 0.7152f + cb * 0.0722f;
-    vr[k] = cr; vg[k] = cg; vb[k] = cb; vl[k] = lum; vl2[k] = lum * lum;
-  }
-  for (int m = 1; m < L; m <<= 1)
-    for (int k = 0; k < L; k += 2 * m) {
-      vr[k] = vr[k] + vr[k + m];
-      vg[k] = vg[k] + vg[k + m];
-      vb[k] = vb[k] + vb[k + m];
-      vl[k] = vl[k] + vl[k + m];
-      vl2[k] = vl2[k] + vl2[k + m];
-    }
-  float4 gs = w.gsum[g0];
-  float sl2 = w.gsl2[g0];
-  gs.x += vr[0]; gs.y += vg[0]; gs.z += vb[0]; gs.w += vl[0];
-  sl2 += vl2[0];
-  const int n = min(rbase + L, spp);
-  bool stop = n >= spp;
-  const Params& p = J.p;
-  if (!stop && p.adapt_min > 0 && n >= p.adapt_min && n > 1 && n % p.adapt_step == 0) {
-    float mean = gs.w / float(n);
-    float var = fmaxf(0.0f, (sl2 - gs.w * mean) / float(n - 1));
-    float thr = p.adapt_rel * mean + p.adapt_abs;
-    if (var < thr * thr) stop = true;
-  }
-  if (stop) {
-    const size_t pix = size_t(y) * size_t(p.width) + size_t(x);
-    const float cr = gs.x / float(n), cg = gs.y / float(n), cb = gs.z / float(n);
-    if (J.hdr) { J.hdr[pix * 3] = cr; J.hdr[pix * 3 + 1] = cg; J.hdr[pix * 3 + 2] = cb; }
-    if (J.rgb) { J.rgb[pix * 3] = tonemap8(cr); J.rgb[pix * 3 + 1] = tonemap8(cg); J.rgb[pix * 3 + 2] = tonemap8(cb); }
-    if (J.dbg) {
-      uint32_t st = 0;
-      for (int k = 0; k < L; ++k) st ^= w.u[g0 + k].x;
-      J.dbg[pix * 2] = st;
-      J.dbg[pix * 2 + 1] = uint32_t(n);
-    }
-    if (atomicSub(&w.cleft[chunk], 1) == 1) {
-      const int pos = atomicAdd(nq.counts + kBtRf, 1);
-      nq.rf[pos] = chunk;
-    }
-    return;
-  }
-  w.gsum[g0] = gs;
-  w.gsl2[g0] = sl2;
-  w.gbase[g0] = rbase + L;
-  w.garr[g0] = 0;
-  const int m = min(L, spp - (rbase + L));
-  const int pos = atomicAdd(nq.counts + kBtSt, m);
-  for (int k = 0; k < m; ++k) nq.st[pos + k] = g0 + k;
-}
-
-// A lane's sample of the round is done (value already clamped): publish it;
-// the pixel's last lane finishes the round.  The slot's RNG state must be
-// stored before this (the pixel's output XORs the lanes' states).
-__device__ __forceinline__ void arrive(const BtState& w, const BtQueues& nq, const BtJob& J, int i, float fr,
-                                       float fg, float fb) {
+// A lane's sample of the round is done (value already clamped): publish it.
+// Returns true for the pixel's last lane of the round, which queues the pixel
+// for k_bt_combine.  The slot's RNG state must be stored before this (the
+// pixel's output XORs the lanes' states).
+__device__ __forceinline__ bool arrive(const BtState& w, const BtJob& J, int i, float fr, float fg, float fb,
+                                       int& g0) {
   const int chunk = i >> 5, k = i & 31;
   const int L = J.lanes, g = k / L;
-  const int g0 = (chunk << 5) + g * L;
+  g0 = (chunk << 5) + g * L;
   w.val[i] = make_float4(fr, fg, fb, 0.f);
-  const int rbase = w.gbase[g0];
-  const int takers = min(L, J.p.spp - rbase);
+  const int takers = min(L, J.p.spp - w.gbase[g0]);
   __threadfence();
   const int old = atomicAdd(&w.garr[g0], 1);
-  if (old + 1 != takers) return;
+  if (old + 1 != takers) return false;
   __threadfence();
-  int x, y;
-  tile_pixel(J, w.ctile[chunk], g, x, y);
-  finish_round(w, nq, J, chunk, g0, rbase, x, y);
+  return true;
+}
+
+// Queue a pixel whose round is complete by its lane count; every thread of the
+// warp must reach this.
+__device__ __forceinline__ void queue_round(const BtQueues& q, int lanes, int g0) {
+  append(q.cm1, q.counts + kBtCm1, lanes == 1, g0);
+  append(q.cm8, q.counts + kBtCm8, lanes == 8, g0);
+  append(q.cm32, q.counts + kBtCm32, lanes == 32, g0);
 }
 
 __global__ void k_bt_init(BtState w, BtQueues q0, int chunks, int* next_tile) {
@@ -203,21 +145,21 @@ __global__ void __launch_bounds__(256) k_bt_refill(BtBatch b, BtState w, BtQueue
 
 // Start the round's sample of each queued lane slot: the jitter and camera ray
 // of K1 / K2 (pathtrace.metal:754-756, :792-794; sample_sensor :729-737).
-__global__ void __launch_bounds__(256) k_bt_start(BtBatch b, BtState w, BtQueues q, BtQueues nq,
-                                                  unsigned long long* ctr, uint32_t* err) {
+__global__ void __launch_bounds__(256) k_bt_start(BtBatch b, BtState w, BtQueues q, unsigned long long* ctr,
+                                                  uint32_t* err) {
   const int n = q.counts[kBtSt];
   const int stride = int(gridDim.x * blockDim.x);
   uint32_t samples = 0;
   for (int base = int(blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); base < n; base += stride) {
     const int qi = base + int(threadIdx.x & 31);
     bool ext = false;
-    int i = 0;
+    int i = 0, g0 = 0, round_lanes = 0;
     if (qi < n) {
       i = q.st[qi];
       const int chunk = i >> 5, k = i & 31;
       const BtJob& J = b.jobs[w.cjob[chunk]];
       const int L = J.lanes, g = k / L, lane = k % L;
-      const int g0 = (chunk << 5) + g * L;
+      g0 = (chunk << 5) + g * L;
       int x, y;
       tile_pixel(J, w.ctile[chunk], g, x, y);
       Tracer pt(J.s, J.p, err);
@@ -254,10 +196,11 @@ __global__ void __launch_bounds__(256) k_bt_start(BtBatch b, BtState w, BtQueues
         float fr = 0.f, fg = 0.f, fb = 0.f;
         clamp3(J.p, fr, fg, fb);
         ++samples;
-        arrive(w, nq, J, i, fr, fg, fb);
+        if (arrive(w, J, i, fr, fg, fb, g0)) round_lanes = L;
       }
     }
     append(q.ext, q.counts + kBtExt, ext, i);
+    queue_round(q, round_lanes, g0);
   }
   __syncwarp();
   warp_add(ctr + 0, samples);
@@ -276,7 +219,7 @@ __global__ void __launch_bounds__(128) k_bt_trace(BtBatch b, BtState w, BtQueues
   uint32_t nodes = 0, tests = 0, rays = 0;
   for (int base = int(blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); base < n; base += stride) {
     const int qi = base + int(threadIdx.x & 31);
-    int cls = -1;  // 0 opaque, 1 dielectric, 2 miss
+    int cls = -1;  // the shading queue: 0 a, 1 b (dielectric), 2 c (miss), 3 d
     int i = 0;
     if (qi < n) {
       i = queue[qi];
@@ -319,13 +262,15 @@ __global__ void __launch_bounds__(128) k_bt_trace(BtBatch b, BtState w, BtQueues
         }
         w.hit[i] = make_float4(r.t, r.u, r.v, __int_as_float(r.tri));
         cls = 2;
-        if (r.tri >= 0) cls = __ldg(&s.tris[r.tri].ior) > 1.0001f ? 1 : 0;
+        if (r.tri >= 0)
+          cls = __ldg(&s.tris[r.tri].ior) > 1.0001f ? 1 : ((J.p.opaque && J.p.restir_candidates <= 1) ? 0 : 3);
       }
     }
     if (!kShadowRays) {
       append(q.qa, q.counts + kBtA, cls == 0, i);
       append(q.qb, q.counts + kBtB, cls == 1, i);
       append(q.qc, q.counts + kBtC, cls == 2, i);
+      append(q.qd, q.counts + kBtD, cls == 3, i);
     }
   }
   __syncwarp();
@@ -334,20 +279,21 @@ __global__ void __launch_bounds__(128) k_bt_trace(BtBatch b, BtState w, BtQueues
   warp_add(ctr + 3, tests);
 }
 
-// Shade the paths of one queue: VK 0 opaque hits, 1 dielectric hits, 2 paths
-// without a vertex (the ray missed, or the path ended and waited for its last
-// shadow ray).  A path that ends finishes its lane's sample of the round.
+// Shade the paths of one queue: VK 0 opaque hits in opaque scenes with
+// single-candidate NEE, 1 dielectric hits, 2 paths without a vertex (the ray
+// missed, or the path ended and waited for its last shadow ray), 3 other
+// opaque hits.  A path that ends finishes its lane's sample of the round.
 template <int VK>
 __global__ void __launch_bounds__(256) k_bt_shade(BtBatch b, BtState w, BtQueues cq, BtQueues nq,
                                                   unsigned long long* ctr, uint32_t* err) {
-  const int count = cq.counts[VK == 0 ? kBtA : (VK == 1 ? kBtB : kBtC)];
-  const int* queue = VK == 0 ? cq.qa : (VK == 1 ? cq.qb : cq.qc);
+  const int count = cq.counts[VK == 0 ? kBtA : VK == 1 ? kBtB : VK == 2 ? kBtC : kBtD];
+  const int* queue = VK == 0 ? cq.qa : VK == 1 ? cq.qb : VK == 2 ? cq.qc : cq.qd;
   const int stride = int(gridDim.x * blockDim.x);
   uint32_t samples = 0, rays = 0, nodes = 0, tests = 0;
   for (int base = int(blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); base < count; base += stride) {
     const int qi = base + int(threadIdx.x & 31);
     bool ext = false, shd = false, fin = false;
-    int i = 0;
+    int i = 0, g0 = 0, round_lanes = 0;
     if (qi < count) {
       i = queue[qi];
       const BtJob& J = b.jobs[w.cjob[i >> 5]];
@@ -378,7 +324,8 @@ __global__ void __launch_bounds__(256) k_bt_shade(BtBatch b, BtState w, BtQueues
         }
         bool has_shadow = false;
         float4 so, sd, c;
-        const bool go = vertex<VK>(pt, J.p, r, hit, has_shadow, so, sd, c);
+        const bool go = VK == 3 ? vertex<0, 1>(pt, J.p, r, hit, has_shadow, so, sd, c)
+                                : vertex<VK == 1 ? 1 : 0, VK == 0 ? 0 : 1>(pt, J.p, r, hit, has_shadow, so, sd, c);
         if (has_shadow) {
           w.so[i] = so; w.sd[i] = sd; w.c[i] = c;
           r.meta |= kShadow;
@@ -393,19 +340,107 @@ __global__ void __launch_bounds__(256) k_bt_shade(BtBatch b, BtState w, BtQueues
         float fr = r.ax, fg = r.ay, fb = r.az;
         clamp3(J.p, fr, fg, fb);
         ++samples;
-        arrive(w, nq, J, i, fr, fg, fb);
+        if (arrive(w, J, i, fr, fg, fb, g0)) round_lanes = J.lanes;
       }
       rays += pt.rays; nodes += pt.nodes; tests += pt.tests;
     }
     append(nq.ext, nq.counts + kBtExt, ext, i);
     append(nq.shd, nq.counts + kBtShd, shd, i);
     append(nq.qc, nq.counts + kBtC, fin, i);
+    queue_round(cq, round_lanes, g0);
   }
   __syncwarp();
   warp_add(ctr + 0, samples);
   warp_add(ctr + 1, rays);
   warp_add(ctr + 2, nodes);
   warp_add(ctr + 3, tests);
+}
+
+// Pixels whose round is complete, `L` lanes each, L lanes of a warp per pixel:
+// the round's butterfly sum exactly as K2 does it (pathtrace.metal:797-805,
+// shuffles of width L), then the adaptive test (:806-810) and either the next
+// round's lane slots queued to start or the pixel's output (:811-814; K1
+// :759-768 is the one-lane case).
+template <int L>
+__global__ void __launch_bounds__(256) k_bt_combine(BtBatch b, BtState w, BtQueues q, BtQueues nq) {
+  const int n = q.counts[L == 1 ? kBtCm1 : L == 8 ? kBtCm8 : kBtCm32];
+  const int* queue = L == 1 ? q.cm1 : L == 8 ? q.cm8 : q.cm32;
+  const int lane = int(threadIdx.x & 31), k = lane % L;
+  const int stride = int(gridDim.x * blockDim.x) / L;  // pixels per sweep of the grid
+  for (int base = int(blockIdx.x * blockDim.x + (threadIdx.x & ~31u)) / L; base < n; base += stride) {
+    const int e = base + lane / L;
+    const bool valid = e < n;
+    int g0 = 0, m = 0;
+    float cr = 0.f, cg = 0.f, cb = 0.f;
+    uint32_t st = 0;
+    const BtJob* J = nullptr;
+    int rbase = 0;
+    if (valid) {
+      g0 = queue[e];
+      J = &b.jobs[w.cjob[g0 >> 5]];
+      rbase = w.gbase[g0];
+      if (k < J->p.spp - rbase) {
+        const float4 a = w.val[g0 + k];
+        cr = a.x; cg = a.y; cb = a.z;
+      }
+      st = w.u[g0 + k].x;
+    }
+    float lum = cr * 0.2126f + cg * 0.7152f + cb * 0.0722f;
+    float lum2 = lum * lum;
+#pragma unroll
+    for (int mm = 1; mm < L; mm <<= 1) {
+      cr += __shfl_xor_sync(0xffffffffu, cr, mm, L);
+      cg += __shfl_xor_sync(0xffffffffu, cg, mm, L);
+      cb += __shfl_xor_sync(0xffffffffu, cb, mm, L);
+      lum += __shfl_xor_sync(0xffffffffu, lum, mm, L);
+      lum2 += __shfl_xor_sync(0xffffffffu, lum2, mm, L);
+      st ^= __shfl_xor_sync(0xffffffffu, st, mm, L);
+    }
+    if (valid) {
+      // every lane of the pixel holds the same sums and takes the same decision
+      const Params& p = J->p;
+      float4 gs = w.gsum[g0];
+      float sl2 = w.gsl2[g0];
+      gs.x += cr; gs.y += cg; gs.z += cb; gs.w += lum;
+      sl2 += lum2;
+      const int nn = min(rbase + L, p.spp);
+      bool stop = nn >= p.spp;
+      if (!stop && p.adapt_min > 0 && nn >= p.adapt_min && nn > 1 && nn % p.adapt_step == 0) {
+        float mean = gs.w / float(nn);
+        float var = fmaxf(0.0f, (sl2 - gs.w * mean) / float(nn - 1));
+        float thr = p.adapt_rel * mean + p.adapt_abs;
+        if (var < thr * thr) stop = true;
+      }
+      if (stop) {
+        if (k == 0) {
+          const int chunk = g0 >> 5;
+          int x, y;
+          tile_pixel(*J, w.ctile[chunk], (g0 & 31) / L, x, y);
+          const size_t pix = size_t(y) * size_t(p.width) + size_t(x);
+          const float fr = gs.x / float(nn), fg = gs.y / float(nn), fb = gs.z / float(nn);
+          if (J->hdr) { J->hdr[pix * 3] = fr; J->hdr[pix * 3 + 1] = fg; J->hdr[pix * 3 + 2] = fb; }
+          if (J->rgb) {
+            J->rgb[pix * 3] = tonemap8(fr); J->rgb[pix * 3 + 1] = tonemap8(fg); J->rgb[pix * 3 + 2] = tonemap8(fb);
+          }
+          if (J->dbg) { J->dbg[pix * 2] = st; J->dbg[pix * 2 + 1] = uint32_t(nn); }
+          if (atomicSub(&w.cleft[chunk], 1) == 1) {
+            const int pos = atomicAdd(nq.counts + kBtRf, 1);
+            nq.rf[pos] = chunk;
+          }
+        }
+      } else {
+        __syncwarp(0xffffffffu >> (32 - L) << (lane & ~(L - 1)));  // the group's reads of the old sums are done
+        if (k == 0) {
+          w.gsum[g0] = gs;
+          w.gsl2[g0] = sl2;
+          w.gbase[g0] = rbase + L;
+          w.garr[g0] = 0;
+        }
+        m = min(L, p.spp - (rbase + L));
+      }
+    }
+    append(nq.st, nq.counts + kBtSt, k < m, g0 + k);
+  }
 }
 
 }  // namespace
@@ -423,7 +458,16 @@ cudaError_t launch_batch_refill(const BtBatch& b, const BtState& w, const BtQueu
 
 cudaError_t launch_batch_start(const BtBatch& b, const BtState& w, const BtQueues& q, const BtQueues& nq, int grid,
                                unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
-  k_bt_start<<<grid, 256, 0, st>>>(b, w, q, nq, ctr, err);
+  (void)nq;
+  k_bt_start<<<grid, 256, 0, st>>>(b, w, q, ctr, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_combine(int lanes, const BtBatch& b, const BtState& w, const BtQueues& q,
+                                 const BtQueues& nq, int grid, cudaStream_t st) {
+  if (lanes == 1) k_bt_combine<1><<<grid, 256, 0, st>>>(b, w, q, nq);
+  else if (lanes == 8) k_bt_combine<8><<<grid, 256, 0, st>>>(b, w, q, nq);
+  else k_bt_combine<32><<<grid, 256, 0, st>>>(b, w, q, nq);
   return cudaGetLastError();
 }
 
@@ -438,7 +482,8 @@ cudaError_t launch_batch_shade(int vk, const BtBatch& b, const BtState& w, const
                                int grid, unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
   if (vk == 0) k_bt_shade<0><<<grid, 256, 0, st>>>(b, w, q, nq, ctr, err);
   else if (vk == 1) k_bt_shade<1><<<grid, 256, 0, st>>>(b, w, q, nq, ctr, err);
-  else k_bt_shade<2><<<grid, 256, 0, st>>>(b, w, q, nq, ctr, err);
+  else if (vk == 2) k_bt_shade<2><<<grid, 256, 0, st>>>(b, w, q, nq, ctr, err);
+  else k_bt_shade<3><<<grid, 256, 0, st>>>(b, w, q, nq, ctr, err);
   return cudaGetLastError();
 }
 

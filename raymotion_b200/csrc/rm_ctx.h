@@ -70,7 +70,7 @@ struct DevScene {
 struct BatchPool {
   DevBuf slot[17];   // per lane slot and per group arrays of BtState
   DevBuf chunk[3];   // per chunk arrays of BtState
-  DevBuf queue[15];  // 7 queues x 2 waves + the counts of both waves
+  DevBuf queue[2 * rmd::kBtQueues + 1];  // the queues of two waves + the counts of both
   DevBuf jobs, tile_begin, next_tile;
   rm_batch_tuning tuning{65536, 0, 1, 8};
   int chunks = 0;    // pool size the buffers hold, in chunks of 32 lane slots

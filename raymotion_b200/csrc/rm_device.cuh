@@ -604,6 +604,62 @@ struct Tracer {
     o_b = sel_Fb * W * wnee;
   }
 
+  // The single-candidate branch (Mc <= 1, pathtrace.metal:319-384) of
+  // direct_lighting_deferred, inlined where a caller knows Mc <= 1.
+  __device__ __forceinline__ void nee_single_deferred(float px, float py, float pz, float nx, float ny, float nz,
+                                                      float wox, float woy, float woz, float rough, float metallic,
+                                                      float spec_prob, float ar, float ag, float ab, float& o_r,
+                                                      float& o_g, float& o_b, float& out_sumW, uint32_t& out_M,
+                                                      bool& has_ray, float& sox, float& soy, float& soz,
+                                                      float& sdx, float& sdy, float& sdz, float& sdist) {
+    o_r = o_g = o_b = 0.0f;
+    out_sumW = 0.0f;
+    out_M = 0;
+    has_ray = false;
+    if (p.lights == 0 || !(p.light_total > 1e-12f)) return;
+    float r2 = rough;
+    if (r2 < 0.0f) r2 = 0.0f;
+    if (r2 > 1.0f) r2 = 1.0f;
+    if (r2 < 0.02f) r2 = 0.02f;
+    float alpha2 = (r2 * r2) * (r2 * r2);
+    const float LT = p.light_total;
+    float pick = U() * LT;
+    const LightRec t = load_light(s, pick_light(pick));
+    float lu = U(), lv = U();
+    if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
+    float lw = 1.0f - lu - lv;
+    float ldx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x) - px;
+    float ldy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y) - py;
+    float ldz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z) - pz;
+    float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
+    if (!(dist > 0.003f)) { out_M = 1; return; }
+    float inv = 1.0f / dist;
+    ldx *= inv; ldy *= inv; ldz *= inv;
+    float lcos = -(t.nn.x * ldx + (t.nn.y * ldy + t.nn.z * ldz));
+    float scos = nx * ldx + (ny * ldy + nz * ldz);
+    if (!(lcos > 1e-8f && scos > 1e-8f)) { out_M = 1; return; }
+    float lt_lum = lum3(t.er, t.eg, t.eb);
+    if (lt_lum < 1e-6f) lt_lum = 1e-6f;
+    float pdf = dist * dist * lt_lum / (lcos * LT);
+    has_ray = true;
+    sox = px + nx * 0.002f; soy = py + ny * 0.002f; soz = pz + nz * 0.002f;
+    sdx = ldx; sdy = ldy; sdz = ldz; sdist = dist - 0.003f;
+    Bsdf e = eval_bsdf(ldx, ldy, ldz, wox, woy, woz, nx, ny, nz, alpha2, metallic, spec_prob, ar, ag, ab);
+    out_M = 1;
+    if (!(pdf > 1e-12f)) return;
+    float Fr = t.er * e.r * scos * t.alpha;
+    float Fg = t.eg * e.g * scos * t.alpha;
+    float Fb = t.eb * e.b * scos * t.alpha;
+    float ph = lum3(Fr, Fg, Fb);
+    out_sumW = (ph > 0.0f) ? ph / pdf : 0.0f;
+    float wnee = 1.0f;
+    if (!p.nomis && e.pdf > 1e-20f) wnee = pdf / (pdf + e.pdf);
+    float k = scos * wnee * t.alpha / pdf;
+    o_r = t.er * e.r * k;
+    o_g = t.eg * e.g * k;
+    o_b = t.eb * e.b * k;
+  }
+
   // direct_lighting for opaque scenes with the visibility test left to the
   // caller: the same draws and arithmetic, returning the contribution a
   // visible light would add (o_*) and the shadow ray to test (has_ray).  In an
@@ -631,41 +687,8 @@ struct Tracer {
     float alpha2 = (r2 * r2) * (r2 * r2);
     const float LT = p.light_total;
     if (Mc <= 1) {
-      float pick = U() * LT;
-      const LightRec t = load_light(s, pick_light(pick));
-      float lu = U(), lv = U();
-      if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
-      float lw = 1.0f - lu - lv;
-      float ldx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x) - px;
-      float ldy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y) - py;
-      float ldz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z) - pz;
-      float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
-      if (!(dist > 0.003f)) { out_M = 1; return; }
-      float inv = 1.0f / dist;
-      ldx *= inv; ldy *= inv; ldz *= inv;
-      float lcos = -(t.nn.x * ldx + (t.nn.y * ldy + t.nn.z * ldz));
-      float scos = nx * ldx + (ny * ldy + nz * ldz);
-      if (!(lcos > 1e-8f && scos > 1e-8f)) { out_M = 1; return; }
-      float lt_lum = lum3(t.er, t.eg, t.eb);
-      if (lt_lum < 1e-6f) lt_lum = 1e-6f;
-      float pdf = dist * dist * lt_lum / (lcos * LT);
-      has_ray = true;
-      sox = px + nx * 0.002f; soy = py + ny * 0.002f; soz = pz + nz * 0.002f;
-      sdx = ldx; sdy = ldy; sdz = ldz; sdist = dist - 0.003f;
-      Bsdf e = eval_bsdf(ldx, ldy, ldz, wox, woy, woz, nx, ny, nz, alpha2, metallic, spec_prob, ar, ag, ab);
-      out_M = 1;
-      if (!(pdf > 1e-12f)) return;
-      float Fr = t.er * e.r * scos * t.alpha;
-      float Fg = t.eg * e.g * scos * t.alpha;
-      float Fb = t.eb * e.b * scos * t.alpha;
-      float ph = lum3(Fr, Fg, Fb);
-      out_sumW = (ph > 0.0f) ? ph / pdf : 0.0f;
-      float wnee = 1.0f;
-      if (!p.nomis && e.pdf > 1e-20f) wnee = pdf / (pdf + e.pdf);
-      float k = scos * wnee * t.alpha / pdf;
-      o_r = t.er * e.r * k;
-      o_g = t.eg * e.g * k;
-      o_b = t.eb * e.b * k;
+      nee_single_deferred(px, py, pz, nx, ny, nz, wox, woy, woz, rough, metallic, spec_prob, ar, ag, ab, o_r, o_g,
+                          o_b, out_sumW, out_M, has_ray, sox, soy, soz, sdx, sdy, sdz, sdist);
       return;
     }
     float sumW = 0.0f;

@@ -109,18 +109,16 @@ struct BtState {
   int* cleft;    // pixels of the tile still rendering
 };
 // Queues of one wave: extension rays, shadow rays, paths to shade by vertex
-// type (a opaque, b dielectric, c none), lane slots to start a sample, chunks
-// to refill.
-constexpr int kBtExt = 0, kBtShd = 1, kBtA = 2, kBtB = 3, kBtC = 4, kBtSt = 5, kBtRf = 6, kBtCounts = 8;
+// type (a opaque surface of an opaque scene with single-candidate NEE, b
+// dielectric, c none, d any other opaque surface), lane slots to start a
+// sample, chunks to refill, and pixels whose round is complete by lane count
+// (1, 8, 32).
+constexpr int kBtExt = 0, kBtShd = 1, kBtA = 2, kBtB = 3, kBtC = 4, kBtD = 5, kBtSt = 6, kBtRf = 7;
+constexpr int kBtCm1 = 8, kBtCm8 = 9, kBtCm32 = 10;
+constexpr int kBtQueues = 11, kBtCounts = 16;
 struct BtQueues {
-  int *ext, *shd, *qa, *qb, *qc, *st, *rf;
+  int *ext, *shd, *qa, *qb, *qc, *qd, *st, *rf, *cm1, *cm8, *cm32;
   int* counts;  // kBtCounts ints
-};
-// Grid sizes of the persistent (grid-stride) batch kernels.
-struct BtGrid {
-  int aux;    // refill / start, 256 threads per block
-  int trace;  // 128 threads per block
-  int shade;  // 256 threads per block
 };
 cudaError_t launch_batch_init(const BtState& w, const BtQueues& q0, int chunks, int* next_tile, cudaStream_t st);
 cudaError_t launch_batch_refill(const BtBatch& b, const BtState& w, const BtQueues& q, int grid, cudaStream_t st);
@@ -130,6 +128,9 @@ cudaError_t launch_batch_trace(const BtBatch& b, const BtState& w, const BtQueue
                                unsigned long long* ctr, uint32_t* err, cudaStream_t st);
 cudaError_t launch_batch_shade(int vk, const BtBatch& b, const BtState& w, const BtQueues& q, const BtQueues& nq,
                                int grid, unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+// Sum the completed rounds of the pixels with `lanes` lanes (1, 8, 32).
+cudaError_t launch_batch_combine(int lanes, const BtBatch& b, const BtState& w, const BtQueues& q,
+                                 const BtQueues& nq, int grid, cudaStream_t st);
 // Resident blocks per SM of each batch kernel (aux, trace, shade).
 void batch_occupancy(int& aux, int& trace, int& shade);
 

@@ -56,7 +56,10 @@ __device__ __forceinline__ void clamp3(const Params& p, float& r, float& g, floa
 // (a new extension ray is in r.o / r.d).  In an opaque scene NEE leaves its
 // shadow ray and the contribution of a visible light in so / sd / c; otherwise
 // it tests visibility itself and adds the light at once.
-template <int MAT>  // 0: opaque surface, 1: dielectric (hit.ior > 1.0001)
+// MAT 0: opaque surface, 1: dielectric (hit.ior > 1.0001).  NEE 0: the scene
+// is opaque and NEE takes one candidate (the single-candidate branch inlined);
+// 1: any scene and candidate count.
+template <int MAT, int NEE = 1>
 __device__ bool vertex(Tracer& pt, const Params& p, PathRegs& r, const Hit& hit, bool& has_shadow, float4& so,
                        float4& sd, float4& c) {
   const bool ind = (r.meta & kInd) != 0;
@@ -132,10 +135,15 @@ __device__ bool vertex(Tracer& pt, const Params& p, PathRegs& r, const Hit& hit,
     if (metallic >= 0.999f) spec_prob = 1.0f;
     float dlr, dlg, dlb, cur_sumW;
     uint32_t cur_M;
-    if (p.opaque) {
+    if (NEE == 0 || p.opaque) {
       float sdist, sox, soy, soz, sdx, sdy, sdz;
       bool has_ray;
-      pt.direct_lighting_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob,
+      if (NEE == 0)
+        pt.nee_single_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob,
+                               hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray, sox, soy, soz, sdx,
+                               sdy, sdz, sdist);
+      else
+        pt.direct_lighting_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob,
                                   hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray, sox, soy, soz,
                                   sdx, sdy, sdz, sdist);
       if (has_ray) {

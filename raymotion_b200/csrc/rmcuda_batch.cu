@@ -50,12 +50,12 @@ cudaError_t ensure_pool(BatchPool& bp, int chunks) {
     if ((e = bp.slot[i].reserve(slots * size_t(kSlotBytes[i]))) != cudaSuccess) return e;
   for (DevBuf& b : bp.chunk)
     if ((e = b.reserve(size_t(chunks) * sizeof(int))) != cudaSuccess) return e;
-  for (int k = 0; k < 2; ++k) {
-    for (int i = 0; i < 6; ++i)
-      if ((e = bp.queue[7 * k + i].reserve(slots * sizeof(int))) != cudaSuccess) return e;
-    if ((e = bp.queue[7 * k + 6].reserve(size_t(chunks) * sizeof(int))) != cudaSuccess) return e;
-  }
-  if ((e = bp.queue[14].reserve(2 * kBtCounts * sizeof(int))) != cudaSuccess) return e;
+  for (int k = 0; k < 2; ++k)
+    for (int i = 0; i < kBtQueues; ++i)  // the refill queue holds chunks, the others lane slots or pixels
+      if ((e = bp.queue[kBtQueues * k + i].reserve((i == kBtRf ? size_t(chunks) : slots) * sizeof(int))) !=
+          cudaSuccess)
+        return e;
+  if ((e = bp.queue[2 * kBtQueues].reserve(2 * kBtCounts * sizeof(int))) != cudaSuccess) return e;
   if ((e = bp.next_tile.reserve(sizeof(int))) != cudaSuccess) return e;
   if (!bp.h_counts &&
       (e = cudaMallocHost(reinterpret_cast<void**>(&bp.h_counts), 2 * kBtCounts * sizeof(int))) != cudaSuccess)
@@ -82,9 +82,9 @@ BtState state_view(const BatchPool& bp) {
 
 BtQueues queue_view(const BatchPool& bp, int k) {
   BtQueues q;
-  int** qs[] = {&q.ext, &q.shd, &q.qa, &q.qb, &q.qc, &q.st, &q.rf};
-  for (int i = 0; i < 7; ++i) *qs[i] = bp.queue[7 * k + i].as<int>();
-  q.counts = bp.queue[14].as<int>() + kBtCounts * k;
+  int** qs[kBtQueues] = {&q.ext, &q.shd, &q.qa, &q.qb, &q.qc, &q.qd, &q.st, &q.rf, &q.cm1, &q.cm8, &q.cm32};
+  for (int i = 0; i < kBtQueues; ++i) *qs[i] = bp.queue[kBtQueues * k + i].as<int>();
+  q.counts = bp.queue[2 * kBtQueues].as<int>() + kBtCounts * k;
   return q;
 }
 
@@ -186,6 +186,9 @@ Grids grids(rmcuda_ctx* c, int scale) {
   return Grids{sms * occ[0] * scale, sms * occ[1] * scale, sms * occ[2] * scale};
 }
 
+// Kernels of a wave: refill, start, 2 traversals, 4 shades, 3 round sums.
+constexpr int kWaveKernels = 11;
+
 // Enqueue one wave on the context stream (cur: this wave's queues).
 cudaError_t enqueue_wave(rmcuda_ctx* c, const BtBatch& b, const BtState& w, const BtQueues* q, int cur,
                          const Grids& g) {
@@ -206,9 +209,12 @@ cudaError_t enqueue_wave(rmcuda_ctx* c, const BtBatch& b, const BtState& w, cons
   if (e == cudaSuccess)
     e = staged2(c, RM_STAGE_BT_SHADOW,
                 [&] { return launch_batch_trace(b, w, Q, true, g.trace, ctr + 4 * RM_STAGE_BT_SHADOW, err, st); });
-  for (int vk = 0; vk < 3 && e == cudaSuccess; ++vk)
+  for (int vk = 0; vk < 4 && e == cudaSuccess; ++vk)
     e = staged2(c, RM_STAGE_BT_SHADE,
                 [&] { return launch_batch_shade(vk, b, w, Q, N, g.shade, ctr + 4 * RM_STAGE_BT_SHADE, err, st); });
+  for (int lanes : {1, 8, 32})
+    if (e == cudaSuccess)
+      e = staged2(c, RM_STAGE_BT_START, [&] { return launch_batch_combine(lanes, b, w, Q, N, g.aux, st); });
   return e;
 }
 
@@ -265,7 +271,7 @@ int run_batch(rmcuda_ctx* c, const Prepared& P, const rm_batch_tuning& tune, Win
     c->launches = launches0;  // counted per replay below
     if (e != cudaSuccess) { msg = cuda_msg("batch graph capture failed", e); return RM_ERR_CUDA; }
   }
-  const uint64_t graph_kernels = uint64_t(per_launch) * 7;
+  const uint64_t graph_kernels = uint64_t(per_launch) * kWaveKernels;
   bp.wave_log.clear();
   cudaEvent_t ev[2] = {nullptr, nullptr};
   if ((e = cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming)) != cudaSuccess ||
@@ -441,6 +447,14 @@ int rmcuda_batch_tune(rmcuda_ctx* c, const rm_batch_item* items, int32_t n, rm_b
   if (rc != RM_OK) { set_err(err, errcap, msg); return rc; }
   if (out) *out = best;
   return RM_OK;
+}
+
+int rmcuda_batch_log(rmcuda_ctx* c, int32_t* out, int32_t cap) {
+  if (!c || cap < 0 || (cap > 0 && !out)) return -1;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const int recs = int(c->batch.wave_log.size() / 2);
+  for (int i = 0; i < recs * 2 && i < cap * 2; ++i) out[i] = c->batch.wave_log[size_t(i)];
+  return recs;
 }
 
 int rmcuda_batch_get_tuning(rmcuda_ctx* c, rm_batch_tuning* out) {
