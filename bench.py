@@ -22,7 +22,9 @@ Reported on one JSON line (rank 0):
             against the measured HBM copy bandwidth;
   cpu_baseline - the CPU oracle (a restatement of the reference's Metal
             kernels; the reference itself runs only on Apple GPUs) timed on a
-            band of rows of the same frame with every host core.
+            band of rows of the same frame with every host core;
+  batch   - batched vs one-at-a-time path samples/s over 64 uneven scenes
+            (see batch_compare), with the images checked identical.
 --impl reference times that CPU implementation alone.
 """
 from __future__ import annotations
@@ -59,6 +61,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-breakdown", action="store_true", help="skip the per-kernel timing frame")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-serial measurement")
+    ap.add_argument("--batch-scenes", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=2)
     return ap.parse_args()
 
 
@@ -232,6 +237,79 @@ def run_reference(args, world, rank):
 
 # ---------------------------------------------------------------- GPU
 
+def batch_compare(args, backend, torch, stream, dev, world):
+    """Batched vs one-at-a-time rendering of the uneven multi-scene workload.
+
+    Scenes as raymotion_b200.scenes.batch_workload (seed 3): triangle counts
+    log-uniform over [1k, 2M], resolutions from {256x256, 640x360, 1280x720,
+    1920x1080}, spp from {4, 16, 64}, depth 8-12, plain path.  Serial: the
+    single-frame policy per scene object (rmcuda_render_scene_async), all
+    enqueued back to back; batched: rmcuda_render_batch with the settings
+    rmcuda_batch_tune picked (tuning is untimed).  Both produce the same
+    images bit for bit (checked), so their relMSE is equal."""
+    from raymotion_b200 import BatchItem
+    from raymotion_b200.scenes import batch_workload, sized_field
+    specs = batch_workload(seed=3, n_scenes=args.batch_scenes)
+    t0 = time.time()
+    items, hdrs, handles = [], [], []
+    for sp in specs:
+        sb, cam, cfg = sized_field(**sp)
+        h = backend.scene_create(sb.pack())
+        handles.append(h)
+        npix = cfg.width * cfg.height
+        rgb = torch.empty(npix * 3, dtype=torch.uint8, device=dev)
+        hdr = torch.empty(npix * 3, dtype=torch.float32, device=dev)
+        hdrs.append((rgb, hdr))
+        items.append(BatchItem(h, cam, cfg, 777, rgb.data_ptr(), hdr.data_ptr(), None))
+    build_s = time.time() - t0
+
+    def serial():
+        for it in items:
+            backend.render_scene_async(it.scene, it.camera, it.config, it.seed, it.d_rgb, it.d_hdr)
+
+    def batched():
+        backend.render_batch(items)
+
+    def timed(fn):
+        backend.stats_reset()
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.batch_steps):
+            fn()
+        e1.record(stream)
+        backend.sync()
+        torch.cuda.synchronize()
+        sec, = allreduce([e0.elapsed_time(e1) / 1e3], "max", world, dev)
+        samples, = allreduce([float(backend.stats()["path_samples"])], "sum", world, dev)
+        return sec, samples
+
+    serial()
+    backend.sync()
+    ref = [h.clone() for _, h in hdrs]
+    t1 = time.time()
+    tuning = backend.batch_tune(items)
+    tune_s = time.time() - t1
+    batched()
+    identical = all(torch.equal(h.view(torch.int32), r.view(torch.int32)) for (_, h), r in zip(hdrs, ref))
+    s_sec, s_samples = timed(serial)
+    b_sec, b_samples = timed(batched)
+    log = backend.batch_log()
+    for h in handles:
+        backend.scene_destroy(h)
+    return dict(
+        workload=f"{len(specs)} seeded icosphere-field scenes, triangles log-uniform in [1k, 2M], resolutions "
+                 "{256x256, 640x360, 1280x720, 1920x1080}, spp {4, 16, 64}, depth 8-12, plain path",
+        triangles=int(sum(sp["n_tris"] for sp in specs)), pixels=int(sum(sp["width"] * sp["height"] for sp in specs)),
+        steps=args.batch_steps, path_samples_per_step=int(b_samples / args.batch_steps),
+        serial=dict(value=s_samples / s_sec, unit=UNIT, ms_per_step=1e3 * s_sec / args.batch_steps),
+        batched=dict(value=b_samples / b_sec, unit=UNIT, ms_per_step=1e3 * b_sec / args.batch_steps,
+                     tuning=tuning, progress_checks=int(len(log))),
+        speedup=(b_samples / b_sec) / (s_samples / s_sec), identical_images=bool(identical),
+        equal_samples=bool(s_samples == b_samples), scene_build_s=build_s, tune_s=tune_s)
+
+
 def run_b200(args, world, rank, local):
     import torch
 
@@ -366,6 +444,8 @@ def run_b200(args, world, rank, local):
         h2d = sum(pinned[k].nbytes for k in pinned)
         e2e = dict(value=es / esec, unit=UNIT, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(npix * 3),
                    ms_per_step=1e3 * esec / args.steps)
+    # ---- batched vs serial rendering of many uneven scenes
+    batch = None if args.no_batch else batch_compare(args, backend, torch, stream, dev, world)
     # ---- CPU baseline (rank 0, N=1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -378,7 +458,8 @@ def run_b200(args, world, rank, local):
                     config=dict(desc, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
                     mrays_per_s=rays_sum / secs_max / 1e6, e2e=e2e, roofline=roofline, cpu_baseline=cpu,
                     gpu_launches=int(st["kernel_launches"]), clocks=clk, stages=stage_summary,
-                    kernels_one_frame=kernel_summary, wavefront=wave_summary, roofline_screen_space=roofline_ss)
+                    kernels_one_frame=kernel_summary, wavefront=wave_summary, roofline_screen_space=roofline_ss,
+                    batch=batch)
         print(json.dumps(line), flush=True)
     backend.close()
     return 0
