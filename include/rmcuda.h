@@ -266,6 +266,42 @@ int rmcuda_batch_log(rmcuda_ctx* ctx, int32_t* out, int32_t cap);
 int rmcuda_batch_get_tuning(rmcuda_ctx* ctx, rm_batch_tuning* out);
 int rmcuda_batch_set_tuning(rmcuda_ctx* ctx, const rm_batch_tuning* tuning, char* err, size_t errcap);
 
+/* ---- Differentiable rendering.  No counterpart in the reference, whose
+ * triangles carry their material inline (metal_types.h:5-11). */
+
+/* The differentiable parameters of a material, in gradient order. */
+typedef struct rm_material {
+  float albedo[3];
+  float rough;
+  float emission[3];
+  float ior;
+} rm_material;
+#define RM_MATERIAL_PARAMS 8
+
+/* Give a scene object materials: triangle i takes the parameters of
+ * mats[tri_material[i]] (albedo, rough, emission, ior written into the
+ * triangle on the device; -1 keeps the triangle's own values).  tri_material
+ * (host, n_tris entries) may be NULL after the first call to keep the
+ * mapping; n_materials must then stay the same.  light_cdf (host, the scene's
+ * n_lights entries) and light_total replace the light-selection table when
+ * light_cdf is not NULL (the caller recomputes them from the new emission, as
+ * it built them for the scene view).  Synchronous. */
+int rmcuda_scene_set_materials(rmcuda_ctx* ctx, rmcuda_scene* scene, const int32_t* tri_material,
+                               const rm_material* mats, int32_t n_materials, const float* light_cdf,
+                               float light_total, char* err, size_t errcap);
+
+/* Path-replay adjoint of the frame rmcuda_render_scene_async renders for the
+ * same arguments: adds dL/dparams into d_grad (DEVICE, n_materials x
+ * RM_MATERIAL_PARAMS floats) given d_dL_dimage (DEVICE, W*H*3 floats, the
+ * loss gradient with respect to the linear radiance image).  Sampling is held
+ * fixed (random decisions, directions, pdfs, MIS weights, Russian-roulette
+ * probabilities); the material-dependent factors of each path are
+ * differentiated; each sample is replayed from its random state instead of
+ * being stored.  Needs the plain chain with single-candidate NEE and a fixed
+ * sample count (adapt_min 0 or RM_FLAG_NOADAPT).  Enqueued, not waited for. */
+int rmcuda_backward(rmcuda_ctx* ctx, const rmcuda_scene* scene, const rm_camera* cam, const rm_config* cfg,
+                    uint64_t seed, const float* d_dL_dimage, float* d_grad, char* err, size_t errcap);
+
 /* Read the last frame's ReSTIR buffers back in the reference record layouts
  * (metal_types.h:32-56): which = 0 G-buffer (76 B/px), 1 initial reservoir,
  * 2 merged reservoir (60 B/px), 3 shaded HDR (12 B/px).  Host pointer. */
@@ -299,7 +335,8 @@ int rmcuda_stats_reset(rmcuda_ctx* ctx);
 #define RM_STAGE_BT_SHADOW 14 /* batched rendering: shadow-ray traversal */
 #define RM_STAGE_BT_SHADE 15  /* batched rendering: shading */
 #define RM_STAGE_BATCH 16     /* batched rendering: a whole rmcuda_render_batch call */
-#define RM_STAGE_COUNT 17
+#define RM_STAGE_ADJOINT 17   /* path-replay adjoint (rmcuda_backward) */
+#define RM_STAGE_COUNT 18
 /* level 0: off; 1: one event pair per stage (the wavefront shading loop counts
  * as RM_STAGE_SHADE, a batch as RM_STAGE_BATCH); 2: also every wavefront
  * launch in its own stage (batches then run without CUDA graphs). */

@@ -859,6 +859,342 @@ static void k_atrous(const Params& p, const GBuf* gb, const float* in, float* ou
 // ---------------------------------------------------------------- C API
 using namespace orc;
 
+namespace orc {
+namespace {
+
+// ---- frozen-path evaluation: the finite-difference side of the adjoint check
+//
+// The adjoint (raymotion_b200/csrc/rm_adjoint.cu) differentiates the plain
+// frame with its sampling held at the current parameters: every random
+// decision, direction, pdf, MIS weight and Russian-roulette probability stays
+// as the fp32 path made it, and only the material-dependent factors of the
+// path integrand move.  frozen_path() walks the fp32 path exactly as
+// Tracer<float>::pathtrace does (pathtrace.metal:552-728, single-candidate
+// NEE :319-384, dielectric :470-534), taking every decision from it, and
+// evaluates alongside in double the sample's value with the material factors
+// at parameters `prm`: the opaque BSDF value (albedo x texel, alpha2 from the
+// roughness), the emission of hit and sampled lights, and for a dielectric
+// the Fresnel / (eta_i/eta_t)^2 and microfacet D, G factors relative to their
+// value at the scene's own (fp32) parameters.  At the scene's parameters it is
+// the fp32 sample in double; its central differences are what the adjoint's
+// gradient must match.
+struct MatTable {
+  const int32_t* tri_mat = nullptr;  // per triangle, -1: the triangle's own values
+  const double* prm = nullptr;       // n x 8: albedo rgb, rough, emission rgb, ior
+  double get(const rm_triangle* tris, int tri, int k) const {
+    const int m = tri_mat ? tri_mat[tri] : -1;
+    if (m >= 0) return prm[size_t(m) * 8 + size_t(k)];
+    const rm_triangle& t = tris[tri];
+    switch (k) {
+      case 0: return t.ar;
+      case 1: return t.ag;
+      case 2: return t.ab;
+      case 3: return t.rough;
+      case 4: return t.er;
+      case 5: return t.eg;
+      case 6: return t.eb;
+      default: return t.ior;
+    }
+  }
+};
+
+double alpha2_of(double rough) {
+  double r = rough;
+  if (r < 0) r = 0;
+  if (r > 1) r = 1;
+  if (r < 0.02) r = 0.02;
+  return (r * r) * (r * r);
+}
+
+V3<double> bsdf64(const MatTable& mt, const SceneRef& s, const Hit<float>& hit, double wix, double wiy, double wiz,
+                  double wox, double woy, double woz, double nx, double ny, double nz, double metallic,
+                  double spec_prob) {
+  double a[3];
+  const double tx[3] = {double(hit.txr), double(hit.txg), double(hit.txb)};
+  const double own[3] = {double(hit.ar), double(hit.ag), double(hit.ab)};
+  for (int c = 0; c < 3; ++c) a[c] = hit.shader == 1 ? own[c] : mt.get(s.tris, hit.tri, c) * tx[c];
+  const auto e = Tracer<double>::eval_bsdf(wix, wiy, wiz, wox, woy, woz, nx, ny, nz,
+                                           alpha2_of(mt.get(s.tris, hit.tri, 3)), metallic, spec_prob, a[0], a[1],
+                                           a[2]);
+  return mk(e.r, e.g, e.b);
+}
+
+// The dielectric factor that depends on the material: event 0 reflection
+// (Fresnel), 1 refraction ((1 - Fresnel) (eta_i/eta_t)^2), 2 total internal
+// reflection (1); for a rough surface, whatever the event, times D and the
+// clamped G weight (pathtrace.metal:520-532 weights every rough event).
+double diel_value(double ior, bool front, int event, double cos_m, bool rough_branch, double alpha2, double cos_i,
+                  double cos_o, double cos_h, double vo_h) {
+  double v = 1.0;
+  if (event != 2) {
+    const double ei = front ? 1.0 : ior, et = front ? ior : 1.0;
+    const double F = Tracer<double>::fresnel(cos_m, ei, et);
+    v = event == 0 ? F : (1.0 - F) * (ei / et) * (ei / et);
+  }
+  if (rough_branch) {
+    const double dd = cos_h * cos_h * (alpha2 - 1.0) + 1.0;
+    const double D = alpha2 / (3.141592653589793 * dd * dd);
+    const double g1 = 2.0 * cos_o / (cos_o + std::sqrt(cos_o * cos_o + alpha2 * (1.0 - cos_o * cos_o)));
+    const double g2 = 2.0 * cos_i / (cos_i + std::sqrt(cos_i * cos_i + alpha2 * (1.0 - cos_i * cos_i)));
+    double w = g1 * g2 * vo_h / (cos_o * cos_h);
+    if (w > 10.0) w = 10.0;
+    v *= D * w;
+  }
+  return v;
+}
+
+V3<double> frozen_path(Tracer<float>& pt, const MatTable& mt, V3<float> ro, V3<float> rd, int max_bounces) {
+  const SceneRef& S = *pt.s;
+  const Params& P = *pt.p;
+  float ox = ro.x, oy = ro.y, oz = ro.z, dx = rd.x, dy = rd.y, dz = rd.z;
+  float thr_r = 1, thr_g = 1, thr_b = 1;
+  double t64[3] = {1, 1, 1}, a64[3] = {0, 0, 0};
+  int bounce = 0, prev_delta = 1;
+  float last_pdf = 0, prev_sumW = 0;
+  uint32_t prev_M = 0;
+  float prev_br = 0, prev_bg = 0, prev_bb = 0, prev_cos = 0;
+  const float LT = float(P.light_total);
+  for (int b = 0; b < max_bounces; ++b) {
+    Hit<float> hit = pt.cast_alpha_ray(mk(ox, oy, oz), mk(dx, dy, dz), 1e30f);
+    if (hit.tri < 0) break;
+    float pnx = hit.n_interp.x, pny = hit.n_interp.y, pnz = hit.n_interp.z;
+    float geom = hit.n_geom.x * pnx + (hit.n_geom.y * pny + hit.n_geom.z * pnz);
+    if (geom < 0) { pnx = -pnx; pny = -pny; pnz = -pnz; }
+    float ndot = dx * pnx + (dy * pny + dz * pnz);
+    bool front = true;
+    if (ndot > 0) { pnx = -pnx; pny = -pny; pnz = -pnz; front = false; }
+    float wox = -dx, woy = -dy, woz = -dz;
+    float rough = hit.rough;
+    if (rough < 0) rough = 0;
+    if (rough > 1) rough = 1;
+    if (rough < 0.02f) rough = 0.02f;
+    float alpha = rough * rough;
+    float alpha2 = alpha * alpha;
+    const rm_triangle& lt = S.tris[hit.tri];
+    float metallic = lt.metallic;
+    if (metallic < 0) metallic = 0;
+    if (metallic > 1) metallic = 1;
+    float we = 1.0f;
+    if (!(bounce == 0 || prev_delta == 1)) {
+      float lx = hit.p.x - ox, ly = hit.p.y - oy, lz = hit.p.z - oz;
+      float dist2 = lx * lx + ly * ly + lz * lz;
+      float dist = std::sqrt(dist2);
+      float pl = 1e30f;
+      if (dist > 1e-20f && last_pdf > 1e-20f && prev_M > 0 && prev_sumW > 1e-20f) {
+        float ph = lum3(hit.er * prev_br * prev_cos * lt.alpha, hit.eg * prev_bg * prev_cos * lt.alpha,
+                        hit.eb * prev_bb * prev_cos * lt.alpha);
+        if (ph > 1e-20f) pl = float(prev_M) * ph / prev_sumW;
+        else {
+          float inv = 1.0f / dist;
+          float lxn = lx * inv, lyn = ly * inv, lzn = lz * inv;
+          float cos_l = -(lt.nn.x * lxn + (lt.nn.y * lyn + lt.nn.z * lzn));
+          if (cos_l > 1e-8f) {
+            float lum = lum3(lt.er, lt.eg, lt.eb);
+            if (lum < 1e-6f) lum = 1e-6f;
+            pl = dist2 * lum / (cos_l * LT);
+          }
+        }
+      } else if (dist > 1e-20f && last_pdf > 1e-20f) {
+        float inv = 1.0f / dist;
+        lx *= inv; ly *= inv; lz *= inv;
+        float cos_l = -(lt.nn.x * lx + (lt.nn.y * ly + lt.nn.z * lz));
+        if (cos_l > 1e-8f) {
+          float lum = lum3(lt.er, lt.eg, lt.eb);
+          if (lum < 1e-6f) lum = 1e-6f;
+          pl = dist2 * lum / (cos_l * LT);
+        }
+      }
+      we = P.nomis ? 0.0f : ((last_pdf + pl > 1e-20f) ? last_pdf / (last_pdf + pl) : 0.0f);
+    }
+    for (int c = 0; c < 3; ++c) a64[c] += mt.get(S.tris, hit.tri, 4 + c) * t64[c] * double(we);
+    if (hit.ior > 1.0001f) {
+      // sample_dielectric (pathtrace.metal:470-534) with its pieces kept
+      float eta_i = 1.0f, eta_t = hit.ior;
+      if (!front) { eta_i = hit.ior; eta_t = 1.0f; }
+      float hx, hy, hz;
+      bool valid = true;
+      if (rough <= 0.0201f) { hx = pnx; hy = pny; hz = pnz; }
+      else {
+        pt.sample_ggx_half(alpha2, pnx, pny, pnz, hx, hy, hz);
+        float md = wox * hx + (woy * hy + woz * hz);
+        if (!(md > 1e-8f)) valid = false;
+      }
+      float cos_m = wox * hx + (woy * hy + woz * hz);
+      if (cos_m < 0) { hx = -hx; hy = -hy; hz = -hz; cos_m = -cos_m; }
+      if (cos_m > 1) cos_m = 1;
+      float fres = Tracer<float>::fresnel(cos_m, eta_i, eta_t);
+      float eta = eta_i / eta_t;
+      float s2 = eta * eta * (1.0f - cos_m * cos_m);
+      float n_x, n_y, n_z, es;
+      int event;
+      if (s2 >= 1.0f || pt.U() < fres) {
+        n_x = 2.0f * cos_m * hx - wox;
+        n_y = 2.0f * cos_m * hy - woy;
+        n_z = 2.0f * cos_m * hz - woz;
+        es = 1.0f;
+        event = s2 >= 1.0f ? 2 : 0;
+      } else {
+        float cos_t = std::sqrt(1.0f - s2);
+        n_x = eta * dx + hx * (eta * cos_m - cos_t);
+        n_y = eta * dy + hy * (eta * cos_m - cos_t);
+        n_z = eta * dz + hz * (eta * cos_m - cos_t);
+        es = eta * eta;
+        event = 1;
+      }
+      {
+        float d = 1.0f / std::sqrt(n_x * n_x + n_y * n_y + n_z * n_z);
+        n_x *= d; n_y *= d; n_z *= d;
+      }
+      float ci = 0, co = 0, chh = 0, voh = 0;
+      const bool rb = rough > 0.0201f;
+      if (rb) {
+        ci = std::fabs(n_x * pnx + (n_y * pny + n_z * pnz));
+        co = std::fabs(wox * pnx + (woy * pny + woz * pnz));
+        chh = std::fabs(hx * pnx + (hy * pny + hz * pnz));
+        voh = std::fabs(wox * hx + (woy * hy + woz * hz));
+        if (ci > 1e-8f && co > 1e-8f && chh > 1e-8f && voh > 1e-8f) {
+          float g1 = 2.0f * co / (co + std::sqrt(co * co + alpha2 * (1.0f - co * co)));
+          float g2 = 2.0f * ci / (ci + std::sqrt(ci * ci + alpha2 * (1.0f - ci * ci)));
+          float w = g1 * g2 * voh / (co * chh);
+          if (w > 10.0f) w = 10.0f;
+          es *= w;
+        } else {
+          valid = false;
+        }
+      }
+      if (!valid) break;
+      const double v0 = diel_value(lt.ior, front, event, cos_m, rb, alpha2_of(lt.rough), ci, co, chh, voh);
+      const double v1 = diel_value(mt.get(S.tris, hit.tri, 7), front, event, cos_m, rb,
+                                   alpha2_of(mt.get(S.tris, hit.tri, 3)), ci, co, chh, voh);
+      const double ratio = v0 > 0 ? v1 / v0 : 1.0;
+      for (int c = 0; c < 3; ++c) t64[c] *= double(es) * ratio;
+      thr_r *= es; thr_g *= es; thr_b *= es;
+      float sg = 1.0f;
+      if (n_x * pnx + (n_y * pny + n_z * pnz) < 0.0f) sg = -1.0f;
+      ox = hit.p.x + pnx * 0.001f * sg;
+      oy = hit.p.y + pny * 0.001f * sg;
+      oz = hit.p.z + pnz * 0.001f * sg;
+      dx = n_x; dy = n_y; dz = n_z;
+      prev_delta = 1;
+      prev_sumW = 0; prev_M = 0;
+    } else {
+      float spec_prob = 0.05f + 0.95f * metallic;
+      if (spec_prob > 0.98f) spec_prob = 0.98f;
+      if (metallic >= 0.999f) spec_prob = 1.0f;
+      float cur_sumW = 0;
+      uint32_t cur_M = 0;
+      // direct_lighting, single candidate (pathtrace.metal:319-384)
+      if (P.lights != 0 && LT > 1e-12f) {
+        float r2 = rough;
+        if (r2 < 0.02f) r2 = 0.02f;
+        float al2 = (r2 * r2) * (r2 * r2);
+        float pick = pt.U() * LT;
+        const int ltri = pt.pick_light(pick);
+        const rm_triangle& t = S.tris[ltri];
+        float lu = pt.U(), lv = pt.U();
+        if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
+        float lw = 1.0f - lu - lv;
+        float ldx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x) - hit.p.x;
+        float ldy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y) - hit.p.y;
+        float ldz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z) - hit.p.z;
+        float dist = std::sqrt(ldx * ldx + ldy * ldy + ldz * ldz);
+        cur_M = 1;
+        if (dist > 0.003f) {
+          float inv = 1.0f / dist;
+          ldx *= inv; ldy *= inv; ldz *= inv;
+          float lcos = -(t.nn.x * ldx + (t.nn.y * ldy + t.nn.z * ldz));
+          float scos = pnx * ldx + (pny * ldy + pnz * ldz);
+          if (lcos > 1e-8f && scos > 1e-8f) {
+            float lt_lum = lum3(t.er, t.eg, t.eb);
+            if (lt_lum < 1e-6f) lt_lum = 1e-6f;
+            float pdf = dist * dist * lt_lum / (lcos * LT);
+            V3<float> so = mk(hit.p.x + pnx * 0.002f, hit.p.y + pny * 0.002f, hit.p.z + pnz * 0.002f);
+            const bool occ = pt.occluded(so, mk(ldx, ldy, ldz), dist - 0.003f);
+            auto e = Tracer<float>::eval_bsdf(ldx, ldy, ldz, wox, woy, woz, pnx, pny, pnz, al2, metallic, spec_prob,
+                                              hit.ar, hit.ag, hit.ab);
+            if (pdf > 1e-12f) {
+              float Fr = t.er * e.r * scos * t.alpha;
+              float Fg = t.eg * e.g * scos * t.alpha;
+              float Fb = t.eb * e.b * scos * t.alpha;
+              float ph = lum3(Fr, Fg, Fb);
+              cur_sumW = ph > 0 ? ph / pdf : 0.0f;
+              if (!occ) {
+                float wnee = 1.0f;
+                if (!P.nomis && e.pdf > 1e-20f) wnee = pdf / (pdf + e.pdf);
+                const float k = scos * wnee * t.alpha / pdf;
+                const V3<double> f = bsdf64(mt, S, hit, ldx, ldy, ldz, wox, woy, woz, pnx, pny, pnz, metallic,
+                                            spec_prob);
+                const double fv[3] = {f.x, f.y, f.z};
+                for (int c = 0; c < 3; ++c) a64[c] += t64[c] * mt.get(S.tris, ltri, 4 + c) * fv[c] * double(k);
+              }
+            }
+          }
+        }
+      }
+      float nx2, ny2, nz2;
+      if (pt.U() < spec_prob) {
+        float hx, hy, hz;
+        pt.sample_ggx_half(alpha2, pnx, pny, pnz, hx, hy, hz);
+        float md = wox * hx + (woy * hy + woz * hz);
+        if (!(md > 1e-8f)) break;
+        nx2 = 2.0f * md * hx - wox;
+        ny2 = 2.0f * md * hy - woy;
+        nz2 = 2.0f * md * hz - woz;
+        prev_delta = (rough <= 0.0201f) ? 1 : 0;
+      } else {
+        pt.sample_cosine(pnx, pny, pnz, nx2, ny2, nz2);
+        prev_delta = 0;
+      }
+      float ncos = nx2 * pnx + (ny2 * pny + nz2 * pnz);
+      if (!(ncos > 1e-8f)) break;
+      {
+        float d = 1.0f / std::sqrt(nx2 * nx2 + ny2 * ny2 + nz2 * nz2);
+        nx2 *= d; ny2 *= d; nz2 *= d;
+      }
+      auto e = Tracer<float>::eval_bsdf(nx2, ny2, nz2, wox, woy, woz, pnx, pny, pnz, alpha2, metallic, spec_prob,
+                                        hit.ar, hit.ag, hit.ab);
+      if (!(e.pdf > 1e-12f)) break;
+      last_pdf = e.pdf;
+      float cos_i = nx2 * pnx + (ny2 * pny + nz2 * pnz);
+      const V3<double> f = bsdf64(mt, S, hit, nx2, ny2, nz2, wox, woy, woz, pnx, pny, pnz, metallic, spec_prob);
+      t64[0] *= f.x * double(cos_i) / double(e.pdf);
+      t64[1] *= f.y * double(cos_i) / double(e.pdf);
+      t64[2] *= f.z * double(cos_i) / double(e.pdf);
+      thr_r *= e.r * cos_i / e.pdf;
+      thr_g *= e.g * cos_i / e.pdf;
+      thr_b *= e.b * cos_i / e.pdf;
+      prev_sumW = cur_sumW; prev_M = cur_M;
+      prev_br = e.r; prev_bg = e.g; prev_bb = e.b; prev_cos = cos_i;
+      ox = hit.p.x + pnx * 0.001f;
+      oy = hit.p.y + pny * 0.001f;
+      oz = hit.p.z + pnz * 0.001f;
+      dx = nx2; dy = ny2; dz = nz2;
+    }
+    if (thr_r < 0) thr_r = 0;
+    if (thr_g < 0) thr_g = 0;
+    if (thr_b < 0) thr_b = 0;
+    for (int c = 0; c < 3; ++c)
+      if (t64[c] < 0) t64[c] = 0;
+    float mx = std::max(thr_r, thr_g);
+    mx = std::max(mx, thr_b);
+    if (!(mx >= 1e-12f)) break;
+    if (P.rr && bounce >= 1) {
+      float rr = mx;
+      if (rr < 0.05f) rr = 0.05f;
+      if (rr > 0.9f) rr = 0.9f;
+      if (!(pt.U() <= rr)) break;
+      float ir = 1.0f / rr;
+      thr_r *= ir; thr_g *= ir; thr_b *= ir;
+      for (int c = 0; c < 3; ++c) t64[c] *= double(ir);
+    }
+    bounce++;
+  }
+  return mk(a64[0], a64[1], a64[2]);
+}
+
+}  // namespace
+}  // namespace orc
+
 extern "C" {
 
 orc::Ctx* orc_create(void) { return new orc::Ctx(); }
@@ -1226,6 +1562,67 @@ void orc_detmath(int which, const float* x, float* y0, float* y1, int n) {
     else if (which == 1) y0[i] = rm_atanf(x[i]);
     else if (which == 2) y0[i] = rm_expf(x[i]);
   }
+}
+
+// Frozen-path evaluation of the plain frame (see frozen_path): out receives
+// W*H*3 doubles, the mean over spp samples of each pixel's clamped sample
+// values with material parameters prm (n_materials x 8 doubles) applied
+// through tri_material; every decision comes from the fp32 path of the scene
+// as given.  The frame must have a fixed sample count and single-candidate
+// NEE.  Returns 0, or RM_ERR_INVALID.
+int orc_render_frozen(const rm_scene_view* sv, const rm_camera* cam, const rm_config* cfg, uint64_t seed,
+                      const int32_t* tri_material, const double* prm, int n_materials, double* out, int nthreads) {
+  using namespace orc;
+  if (cfg->width <= 0 || cfg->height <= 0 || cfg->spp <= 0 || cfg->max_bounces < 0 || n_materials < 0)
+    return RM_ERR_INVALID;
+  SceneRef s;
+  s.tris = sv->tris; s.n_tris = sv->n_tris;
+  s.nodes = to_preorder(sv->nodes, sv->n_nodes);
+  s.indices = sv->bvh_tri; s.lights = sv->light_tri; s.cdf = sv->light_cdf;
+  s.n_lights = sv->n_lights; s.light_total = sv->light_total; s.texels = sv->texels;
+  bool opaque = true;
+  for (int i = 0; i < sv->n_tris; ++i)
+    if (!(sv->tris[i].alpha >= 1)) { opaque = false; break; }
+  Env env = read_env(cfg->flags);
+  Params p = resolve(*cfg, *cam, int(s.nodes.size()), sv->n_lights, sv->light_total, opaque, env);
+  if (p.adapt_min > 0 || p.restir_candidates > 1) return RM_ERR_INVALID;
+  int lanes = 1;
+  if (p.spp >= 8) lanes = 8;
+  if (p.spp >= 32) lanes = 32;
+  MatTable mt;
+  mt.tri_mat = tri_material;
+  mt.prm = prm;
+  const int W = p.width;
+  parallel_for(p.height, nthreads, [&](int y) {
+    Counters ctr;
+    for (int x = 0; x < W; ++x) {
+      double sum[3] = {0, 0, 0};
+      for (int l = 0; l < lanes; ++l) {
+        Tracer<float> pt{&s, &p, Rng{}, &ctr};
+        pt.rng.seed(lanes == 1 ? seed_pixel(seed, uint32_t(x), uint32_t(y))
+                               : seed_lane(seed, uint32_t(x), uint32_t(y), uint32_t(l)));
+        for (int si = l; si < p.spp; si += lanes) {
+          float sx, sy;
+          pt.jitter(uint32_t(x), uint32_t(y), sx, sy);
+          const rm_camera& c = p.camera;
+          float focal2 = c.focal * c.focal;
+          float dist = 1.0f / std::sqrt(sx * sx + (sy * sy + focal2));
+          float tx = sx * dist, ty = sy * dist, tz = c.focal * dist;
+          V3<float> rd = mk(tx * c.m0 + (ty * c.m1 + tz * c.m2), tx * c.m3 + (ty * c.m4 + tz * c.m5),
+                            tx * c.m6 + (ty * c.m7 + tz * c.m8));
+          V3<double> v = frozen_path(pt, mt, mk(c.x, c.y, c.z), rd, p.bounces);
+          if (p.clamp_value > 0) {
+            const double cl = p.clamp_value;
+            v.x = std::fmin(v.x, cl); v.y = std::fmin(v.y, cl); v.z = std::fmin(v.z, cl);
+          }
+          sum[0] += v.x; sum[1] += v.y; sum[2] += v.z;
+        }
+      }
+      double* o = out + (size_t(y) * size_t(W) + size_t(x)) * 3;
+      for (int k = 0; k < 3; ++k) o[k] = sum[k] / double(p.spp);
+    }
+  });
+  return RM_OK;
 }
 
 }  // extern "C"

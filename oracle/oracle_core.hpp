@@ -125,6 +125,7 @@ template <class F> struct Hit {
   F ar = 0, ag = 0, ab = 0, er = 0, eg = 0, eb = 0, ior = 0, rough = 0;
   int shader = 0;
   V3<F> n_geom{0, 0, 0};
+  F txr = 1, txg = 1, txb = 1;  // texel colour the albedo was multiplied by
 };
 
 struct Counters {
@@ -235,6 +236,7 @@ template <class F> struct Tracer {
         int y = t.texture_height - 1 - std::min(int(tv * F(t.texture_height)), t.texture_height - 1);
         const rm_vec3& c = s->texels[size_t(t.texture_offset) + size_t(y) * size_t(t.texture_width) + size_t(x)];
         h.ar *= F(c.x); h.ag *= F(c.y); h.ab *= F(c.z);
+        h.txr = F(c.x); h.txg = F(c.y); h.txb = F(c.z);
       }
       h.er = F(t.er); h.eg = F(t.eg); h.eb = F(t.eb);
       h.ior = F(t.ior); h.rough = F(t.rough); h.shader = t.shader;

@@ -198,6 +198,25 @@ class Backend:
         e = _err()
         self._check(self.lib.rmcuda_batch_set_tuning(self.h, C.byref(t), e, 512), e)
 
+    # ---- differentiable rendering
+    def scene_set_materials(self, handle: int, params: np.ndarray, tri_material: np.ndarray | None = None,
+                            light_cdf: np.ndarray | None = None, light_total: float = 0.0) -> None:
+        """Per-triangle materials of a scene object (params: n x 8 float32)."""
+        prm = np.ascontiguousarray(params, np.float32)
+        assert prm.ndim == 2 and prm.shape[1] == 8
+        tm = None if tri_material is None else np.ascontiguousarray(tri_material, np.int32)
+        cdf = None if light_cdf is None else np.ascontiguousarray(light_cdf, np.float32)
+        e = _err()
+        self._check(self.lib.rmcuda_scene_set_materials(self.h, handle, _abi.ptr(tm), _abi.ptr(prm), len(prm),
+                                                         _abi.ptr(cdf), float(light_total), e, 512), e)
+
+    def backward(self, handle: int, cam: Camera, cfg: RenderConfig, seed: int, d_dl_dimage: int,
+                 d_grad: int) -> None:
+        """Path-replay adjoint: adds dL/dparams (device, n x 8 floats) given dL/dimage (device)."""
+        e = _err()
+        self._check(self.lib.rmcuda_backward(self.h, handle, C.byref(cam.packed()), C.byref(cfg.packed()),
+                                             C.c_uint64(seed & 0xFFFFFFFFFFFFFFFF), d_dl_dimage, d_grad, e, 512), e)
+
     def reset_history(self) -> None:
         self.lib.rmcuda_reset_history(self.h)
 

@@ -126,12 +126,14 @@ EXPORTS = [
     ("rmcuda_render_batch", C.c_int, [_P, C.POINTER(RmBatchItem), C.c_int32, _S, _Z]),
     ("rmcuda_batch_tune", C.c_int, [_P, C.POINTER(RmBatchItem), C.c_int32, C.POINTER(RmBatchTuning), _S, _Z]),
     ("rmcuda_batch_log", C.c_int, [_P, C.POINTER(C.c_int32), C.c_int32]),
+    ("rmcuda_scene_set_materials", C.c_int, [_P, _P, _P, _P, C.c_int32, _P, C.c_float, _S, _Z]),
+    ("rmcuda_backward", C.c_int, [_P, _P, C.POINTER(RmCamera), C.POINTER(RmConfig), C.c_uint64, _P, _P, _S, _Z]),
     ("rmcuda_batch_get_tuning", C.c_int, [_P, C.POINTER(RmBatchTuning)]),
     ("rmcuda_batch_set_tuning", C.c_int, [_P, C.POINTER(RmBatchTuning), _S, _Z]),
 ]
 
 STAGES = ["plain", "hash", "generate", "spatial", "shade", "temporal", "atrous0", "atrous1", "tonemap", "wf_extend",
-          "wf_shadow", "wf_shade", "bt_start", "bt_extend", "bt_shadow", "bt_shade", "batch"]
+          "wf_shadow", "wf_shade", "bt_start", "bt_extend", "bt_shadow", "bt_shade", "batch", "adjoint"]
 
 _lib = None
 

@@ -1,0 +1,454 @@
+// rm_adjoint.cu - path-replay adjoint of the plain single-frame chain:
+// gradients of an image loss with respect to per-material albedo, roughness,
+// emission and index of refraction.
+//
+// The differentiated estimator is the frame of render_paths (K1) or the lane
+// kernel (K2) (pathtrace.metal:739-815) with its sampling held fixed: every
+// random decision, sampled direction, pdf, MIS weight and Russian-roulette
+// probability keeps its value at the current parameters, and only the
+// factors of the path integrand that depend on the materials are
+// differentiated - the opaque BSDF value (albedo, roughness), the emission of
+// hit and sampled lights, and for a dielectric the Fresnel and (eta_i/eta_t)^2
+// factors (index of refraction) and the microfacet D and G terms (roughness),
+// each as a ratio to its value at the current parameters (path replay
+// backpropagation with detached sampling, Vicini, Speierer and Jakob,
+// SIGGRAPH 2021).  With the sample's radiance C and the radiance S_k that the
+// path gathers after vertex k, the derivative of a sample is
+//     sum_k thr_k * d(E_k + N_k) + sum_k (dB_k / B_k) * S_k
+// (E_k emission at vertex k, N_k its light sample, B_k the throughput factor
+// of its scattering).  Each thread owns a pixel lane, as the forward kernels
+// do, and replays each of its samples twice from the sample's RNG state:
+// once to get C, once to walk the path again accumulating the derivative
+// with S_k = C - (radiance gathered up to vertex k).  The refracted direction
+// is held fixed when the index of refraction changes; its motion would need a
+// reparameterised sampler and is not part of the estimator.
+#include <cuda_runtime.h>
+
+#include "rm_device.cuh"
+#include "rm_launch.h"
+
+namespace rmd {
+
+namespace {
+
+constexpr int kMatParams = 8;  // albedo rgb, rough, emission rgb, ior
+
+struct GradSink {
+  float* sh;  // per-block accumulators, or null
+  float* gl;  // the caller's gradient
+  __device__ __forceinline__ void add(int m, int k, float v) const {
+    if (m < 0 || v == 0.0f) return;
+    atomicAdd((sh ? sh : gl) + m * kMatParams + k, v);
+  }
+};
+
+struct Dual {
+  float v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return Dual{a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return Dual{a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return Dual{a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+  return Dual{a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)};
+}
+__device__ __forceinline__ Dual dsqrt(Dual a) {
+  const float r = sqrtf(a.v);
+  return Dual{r, r > 0.0f ? a.d / (2.0f * r) : 0.0f};
+}
+__device__ __forceinline__ Dual dc(float v) { return Dual{v, 0.0f}; }
+
+// Fresnel (pathtrace.metal:80-91) and its derivative along the dual parts of
+// the two indices.
+__device__ Dual fresnel_dual(float ci, Dual eta_in, Dual eta_out) {
+  if (ci < 0.0f) ci = 0.0f;
+  if (ci > 1.0f) ci = 1.0f;
+  const Dual eta = eta_in / eta_out;
+  const Dual s2 = eta * eta * dc(1.0f - ci * ci);
+  if (s2.v >= 1.0f) return dc(1.0f);
+  const Dual ct = dsqrt(dc(1.0f) - s2);
+  const Dual c = dc(ci);
+  const Dual rp = (eta_out * c - eta_in * ct) / (eta_out * c + eta_in * ct);
+  const Dual rs = (eta_in * c - eta_out * ct) / (eta_in * c + eta_out * ct);
+  return dc(0.5f) * (rp * rp + rs * rs);
+}
+
+// |h x n|^2: the squared sine between two unit vectors, accurate near 0.
+__device__ __forceinline__ float sin2(float hx, float hy, float hz, float nx, float ny, float nz) {
+  const float cx = hy * nz - hz * ny, cy = hz * nx - hx * nz, cz = hx * ny - hy * nx;
+  return cx * cx + cy * cy + cz * cz;
+}
+
+// d/dalpha2 of log G1 for one direction (Smith G1 of pathtrace.metal:270-276).
+__device__ __forceinline__ float dlog_g1(float c, float alpha2) {
+  const float sq = sqrtf(c * c + alpha2 * (1.0f - c * c));
+  return -(1.0f - c * c) / (2.0f * sq * (c + sq));
+}
+
+// The opaque BSDF value (pathtrace.metal:243-295) with its derivatives with
+// respect to each albedo channel and alpha2.
+struct BsdfGrad {
+  float f[3], da[3], dal2[3];
+};
+
+__device__ BsdfGrad bsdf_grad(float wix, float wiy, float wiz, float wox, float woy, float woz, float nx, float ny,
+                              float nz, float alpha2, float metallic, float ar, float ag, float ab) {
+  BsdfGrad out;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out.f[c] = out.da[c] = out.dal2[c] = 0.0f;
+  const float cos_i = wix * nx + (wiy * ny + wiz * nz);
+  const float cos_o = wox * nx + (woy * ny + woz * nz);
+  if (!(cos_i > 1e-8f && cos_o > 1e-8f)) return out;
+  float hx = wix + wox, hy = wiy + woy, hz = wiz + woz;
+  const float hl = sqrtf(hx * hx + hy * hy + hz * hz);
+  if (!(hl > 1e-8f)) return out;
+  const float inv = 1.0f / hl;
+  hx *= inv; hy *= inv; hz *= inv;
+  float cos_h = hx * nx + (hy * ny + hz * nz);
+  float vo_h = wox * hx + (woy * hy + woz * hz);
+  if (cos_h < 0.0f) { cos_h = -cos_h; vo_h = -vo_h; }
+  if (!(vo_h > 1e-8f)) return out;
+  // cos_h^2 (alpha2 - 1) + 1 = |h x n|^2 + alpha2 cos_h^2, without the
+  // cancellation near the lobe's peak (alpha2 can be 6e-6)
+  const float dd = sin2(hx, hy, hz, nx, ny, nz) + alpha2 * cos_h * cos_h;
+  const float D = alpha2 / (kPi * dd * dd);
+  const float g1 = 2.0f * cos_o / (cos_o + sqrtf(cos_o * cos_o + alpha2 * (1.0f - cos_o * cos_o)));
+  const float g2 = 2.0f * cos_i / (cos_i + sqrtf(cos_i * cos_i + alpha2 * (1.0f - cos_i * cos_i)));
+  const float G = g1 * g2;
+  float om = 1.0f - vo_h;
+  om *= om; om *= om; om *= 1.0f - vo_h;
+  const float di = 1.0f - metallic;
+  const float base = D * G / (4.0f * cos_i * cos_o);
+  const float dlog = 1.0f / alpha2 - 2.0f * cos_h * cos_h / dd + dlog_g1(cos_o, alpha2) + dlog_g1(cos_i, alpha2);
+  const float alb[3] = {ar, ag, ab};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float f0 = 0.04f * di + alb[c] * metallic;
+    const float F = f0 + (1.0f - f0) * om;
+    out.f[c] = alb[c] * di * (1.0f - F) / kPi + base * F;
+    out.da[c] = (di * (1.0f - F) - alb[c] * di * metallic * (1.0f - om)) / kPi + base * metallic * (1.0f - om);
+    out.dal2[c] = base * dlog * F;
+  }
+  return out;
+}
+
+// d alpha2 / d rough for alpha2 = r^4, r = max(clamp(rough, 0, 1), 0.02).
+__device__ __forceinline__ float dalpha2(float rough) {
+  if (!(rough > 0.02f && rough < 1.0f)) return 0.0f;
+  return 4.0f * rough * rough * rough;
+}
+
+// One sample's path again (pathtrace.metal:552-728, the same arithmetic and
+// random draws as Tracer::pathtrace), accumulating g . dC/dparams.
+__device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict__ tri_mat, float ox, float oy,
+                                          float oz, float dx, float dy, float dz, int max_bounces, float Cr, float Cg,
+                                          float Cb, float gr, float gg, float gb, const GradSink& sink) {
+  const Scene& s = pt.s;
+  const Params& p = pt.p;
+  float accr = 0, accg = 0, accb = 0, thr_r = 1, thr_g = 1, thr_b = 1;
+  int bounce = 0, prev_delta = 1;
+  float last_pdf = 0, prev_sumW = 0;
+  uint32_t prev_M = 0;
+  float prev_br = 0, prev_bg = 0, prev_bb = 0, prev_cos = 0;
+  const float LT = p.light_total;
+  for (int b = 0; b < max_bounces; ++b) {
+    Hit hit = pt.cast_alpha_ray(ox, oy, oz, dx, dy, dz, kFar);
+    if (hit.tri < 0) break;
+    const int m = tri_mat[hit.tri];
+    float pnx = hit.nix, pny = hit.niy, pnz = hit.niz;
+    float geom = hit.ngx * pnx + (hit.ngy * pny + hit.ngz * pnz);
+    if (geom < 0.0f) { pnx = -pnx; pny = -pny; pnz = -pnz; }
+    float ndot = dx * pnx + (dy * pny + dz * pnz);
+    bool front = true;
+    if (ndot > 0.0f) { pnx = -pnx; pny = -pny; pnz = -pnz; front = false; }
+    float wox = -dx, woy = -dy, woz = -dz;
+    float rough = hit.rough;
+    if (rough < 0.0f) rough = 0.0f;
+    if (rough > 1.0f) rough = 1.0f;
+    if (rough < 0.02f) rough = 0.02f;
+    float alpha = rough * rough;
+    float alpha2 = alpha * alpha;
+    const float dal2 = dalpha2(hit.rough);
+    const rm_triangle& lt = s.tris[hit.tri];
+    float metallic = lt.metallic;
+    if (metallic < 0.0f) metallic = 0.0f;
+    if (metallic > 1.0f) metallic = 1.0f;
+    float we = 1.0f;  // MIS weight of the emission term (held fixed)
+    if (bounce == 0 || prev_delta == 1) {
+      accr += hit.er * thr_r; accg += hit.eg * thr_g; accb += hit.eb * thr_b;
+    } else {
+      float lx = hit.px - ox, ly = hit.py - oy, lz = hit.pz - oz;
+      float dist2 = lx * lx + ly * ly + lz * lz;
+      float dist = sqrtf(dist2);
+      float pl = 1e30f;
+      float lta = lt.alpha;
+      if (dist > 1e-20f && last_pdf > 1e-20f && prev_M > 0 && prev_sumW > 1e-20f) {
+        float ph = lum3(hit.er * prev_br * prev_cos * lta, hit.eg * prev_bg * prev_cos * lta,
+                        hit.eb * prev_bb * prev_cos * lta);
+        if (ph > 1e-20f) pl = float(prev_M) * ph / prev_sumW;
+        else {
+          float inv = 1.0f / dist;
+          float lxn = lx * inv, lyn = ly * inv, lzn = lz * inv;
+          float cos_l = -(lt.nn.x * lxn + (lt.nn.y * lyn + lt.nn.z * lzn));
+          if (cos_l > 1e-8f) {
+            float lum = lum3(lt.er, lt.eg, lt.eb);
+            if (lum < 1e-6f) lum = 1e-6f;
+            pl = dist2 * lum / (cos_l * LT);
+          }
+        }
+      } else if (dist > 1e-20f && last_pdf > 1e-20f) {
+        float inv = 1.0f / dist;
+        lx *= inv; ly *= inv; lz *= inv;
+        float cos_l = -(lt.nn.x * lx + (lt.nn.y * ly + lt.nn.z * lz));
+        if (cos_l > 1e-8f) {
+          float lum = lum3(lt.er, lt.eg, lt.eb);
+          if (lum < 1e-6f) lum = 1e-6f;
+          pl = dist2 * lum / (cos_l * LT);
+        }
+      }
+      we = p.nomis ? 0.0f : ((last_pdf + pl > 1e-20f) ? last_pdf / (last_pdf + pl) : 0.0f);
+      accr += hit.er * thr_r * we; accg += hit.eg * thr_g * we; accb += hit.eb * thr_b * we;
+    }
+    sink.add(m, 4, gr * thr_r * we);
+    sink.add(m, 5, gg * thr_g * we);
+    sink.add(m, 6, gb * thr_b * we);
+    if (hit.ior > 1.0001f) {
+      float nx2, ny2, nz2, es;
+      float dp[7];
+      bool valid = pt.sample_dielectric(wox, woy, woz, pnx, pny, pnz, dx, dy, dz, hit.ior, front, rough, alpha2, nx2,
+                                        ny2, nz2, es, dp);
+      if (!valid) break;
+      // B_k = es: d log B_k, times g . S_k
+      const float gS = gr * (Cr - accr) + gg * (Cg - accg) + gb * (Cb - accb);
+      if (gS != 0.0f) {
+        const int event = int(dp[0]);
+        if (event != 2) {
+          const Dual ior{hit.ior, 1.0f};
+          const Dual ei = front ? dc(1.0f) : ior, et = front ? ior : dc(1.0f);
+          const Dual F = fresnel_dual(dp[1], ei, et);
+          float dlog = 0.0f;
+          if (event == 0) dlog = F.v > 0.0f ? F.d / F.v : 0.0f;
+          else {
+            dlog = F.v < 1.0f ? -F.d / (1.0f - F.v) : 0.0f;
+            dlog += front ? -2.0f / hit.ior : 2.0f / hit.ior;  // (eta_i / eta_t)^2
+          }
+          sink.add(m, 7, gS * dlog);
+        }
+        if (rough > 0.0201f && dal2 != 0.0f) {
+          const float ch = dp[4];
+          const float dd = dp[6] + alpha2 * ch * ch;
+          float dlog = 1.0f / alpha2 - 2.0f * ch * ch / dd;  // D
+          if (dp[5] == 0.0f) dlog += dlog_g1(dp[3], alpha2) + dlog_g1(dp[2], alpha2);  // G, unless clamped
+          sink.add(m, 3, gS * dlog * dal2);
+        }
+      }
+      thr_r *= es; thr_g *= es; thr_b *= es;
+      float sg = 1.0f;
+      if (nx2 * pnx + (ny2 * pny + nz2 * pnz) < 0.0f) sg = -1.0f;
+      ox = hit.px + pnx * 0.001f * sg;
+      oy = hit.py + pny * 0.001f * sg;
+      oz = hit.pz + pnz * 0.001f * sg;
+      dx = nx2; dy = ny2; dz = nz2;
+      prev_delta = 1;
+      prev_sumW = 0; prev_M = 0;
+    } else {
+      float spec_prob = 0.05f + 0.95f * metallic;
+      if (spec_prob > 0.98f) spec_prob = 0.98f;
+      if (metallic >= 0.999f) spec_prob = 1.0f;
+      const bool alb_grad = hit.shader != 1;
+      const float tx[3] = {hit.txr, hit.txg, hit.txb};
+      const float gv[3] = {gr, gg, gb};
+      float cur_sumW = 0;
+      uint32_t cur_M = 0;
+      {
+        float dlr, dlg, dlb, sdist, sox, soy, soz, sdx, sdy, sdz;
+        bool has_ray;
+        float parts[2];
+        pt.nee_single_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob,
+                               hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray, sox, soy, soz, sdx,
+                               sdy, sdz, sdist, parts);
+        if (has_ray && !pt.occluded(sox, soy, soz, sdx, sdy, sdz, sdist)) {
+          accr += dlr * thr_r; accg += dlg * thr_g; accb += dlb * thr_b;
+          // N_k = Le * f * k: derivative in the light's emission and this surface's BSDF
+          const int li = __float_as_int(parts[0]);
+          const float k = parts[1];
+          const LightRec L = load_light(s, li);
+          const int ml = tri_mat[s.lights[li]];
+          const BsdfGrad bg = bsdf_grad(sdx, sdy, sdz, wox, woy, woz, pnx, pny, pnz, alpha2, metallic, hit.ar, hit.ag,
+                                        hit.ab);
+          const float thr[3] = {thr_r, thr_g, thr_b};
+          const float le[3] = {L.er, L.eg, L.eb};
+          float drough = 0.0f;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const float gt = gv[c] * thr[c] * k;
+            sink.add(ml, 4 + c, gt * bg.f[c]);
+            if (alb_grad) sink.add(m, c, gt * le[c] * bg.da[c] * tx[c]);
+            drough += gt * le[c] * bg.dal2[c];
+          }
+          sink.add(m, 3, drough * dal2);
+        }
+      }
+      float nx2, ny2, nz2;
+      if (pt.U() < spec_prob) {
+        float hx, hy, hz;
+        pt.sample_ggx_half(alpha2, pnx, pny, pnz, hx, hy, hz);
+        float md = wox * hx + (woy * hy + woz * hz);
+        if (!(md > 1e-8f)) break;
+        nx2 = 2.0f * md * hx - wox;
+        ny2 = 2.0f * md * hy - woy;
+        nz2 = 2.0f * md * hz - woz;
+        prev_delta = (rough <= 0.0201f) ? 1 : 0;
+      } else {
+        pt.sample_cosine(pnx, pny, pnz, nx2, ny2, nz2);
+        prev_delta = 0;
+      }
+      float ncos = nx2 * pnx + (ny2 * pny + nz2 * pnz);
+      if (!(ncos > 1e-8f)) break;
+      {
+        float d = 1.0f / sqrtf(nx2 * nx2 + ny2 * ny2 + nz2 * nz2);
+        nx2 *= d; ny2 *= d; nz2 *= d;
+      }
+      Bsdf e = Tracer::eval_bsdf(nx2, ny2, nz2, wox, woy, woz, pnx, pny, pnz, alpha2, metallic, spec_prob, hit.ar,
+                                 hit.ag, hit.ab);
+      if (!(e.pdf > 1e-12f)) break;
+      {
+        // B_k = f * cos / pdf: d log B_k = df / f, times g . S_k per channel
+        const BsdfGrad bg = bsdf_grad(nx2, ny2, nz2, wox, woy, woz, pnx, pny, pnz, alpha2, metallic, hit.ar, hit.ag,
+                                      hit.ab);
+        const float S[3] = {Cr - accr, Cg - accg, Cb - accb};
+        float drough = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (!(bg.f[c] > 0.0f)) continue;
+          const float gs = gv[c] * S[c] / bg.f[c];
+          if (alb_grad) sink.add(m, c, gs * bg.da[c] * tx[c]);
+          drough += gs * bg.dal2[c];
+        }
+        sink.add(m, 3, drough * dal2);
+      }
+      last_pdf = e.pdf;
+      float cos_i = nx2 * pnx + (ny2 * pny + nz2 * pnz);
+      thr_r *= e.r * cos_i / e.pdf;
+      thr_g *= e.g * cos_i / e.pdf;
+      thr_b *= e.b * cos_i / e.pdf;
+      prev_sumW = cur_sumW; prev_M = cur_M;
+      prev_br = e.r; prev_bg = e.g; prev_bb = e.b; prev_cos = cos_i;
+      ox = hit.px + pnx * 0.001f;
+      oy = hit.py + pny * 0.001f;
+      oz = hit.pz + pnz * 0.001f;
+      dx = nx2; dy = ny2; dz = nz2;
+    }
+    if (thr_r < 0.0f) thr_r = 0.0f;
+    if (thr_g < 0.0f) thr_g = 0.0f;
+    if (thr_b < 0.0f) thr_b = 0.0f;
+    float mx = fmaxf(thr_r, thr_g);
+    mx = fmaxf(mx, thr_b);
+    if (!(mx >= 1e-12f)) break;
+    if (p.rr && bounce >= 1) {
+      float rr = mx;
+      if (rr < 0.05f) rr = 0.05f;
+      if (rr > 0.9f) rr = 0.9f;
+      if (!(pt.U() <= rr)) break;
+      float ir = 1.0f / rr;
+      thr_r *= ir; thr_g *= ir; thr_b *= ir;
+    }
+    bounce++;
+  }
+}
+
+// One pixel lane per thread, the samples of K1 (LANES 1) or of one lane of K2,
+// in the forward kernels' order (pathtrace.metal:749-758, :787-796).
+template <int LANES>
+__global__ void __launch_bounds__(256) k_adjoint(Scene s, Params p, uint64_t seed, const int32_t* __restrict__ tri_mat,
+                                                 int n_mat, const float* __restrict__ dLdI, float* __restrict__ grad,
+                                                 int use_shared, unsigned long long* ctr, uint32_t* err) {
+  extern __shared__ float sh[];
+  if (use_shared) {
+    for (int i = threadIdx.x; i < n_mat * kMatParams; i += blockDim.x) sh[i] = 0.0f;
+    __syncthreads();
+  }
+  const GradSink sink{use_shared ? sh : nullptr, grad};
+  const uint64_t gid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint32_t npix = uint32_t(p.width) * uint32_t(p.height);
+  const uint32_t pixel = uint32_t(gid / LANES), lane = uint32_t(gid % LANES);
+  uint32_t samples = 0;
+  if (pixel < npix) {
+    const uint32_t x = pixel % uint32_t(p.width), y = pixel / uint32_t(p.width);
+    Tracer pt(s, p, err);
+    uint64_t sd = seed_pixel(seed, x, y);
+    if (LANES > 1) sd ^= uint64_t(lane) * 0x94D049BB133111EBull;
+    pt.rng.seed(sd);
+    const float inv_n = 1.0f / float(p.spp);
+    const float d0 = dLdI[size_t(pixel) * 3] * inv_n, d1 = dLdI[size_t(pixel) * 3 + 1] * inv_n,
+                d2 = dLdI[size_t(pixel) * 3 + 2] * inv_n;
+    for (uint32_t si = lane; si < uint32_t(p.spp); si += LANES) {
+      float sx, sy;
+      pt.jitter(x, y, sx, sy);
+      const uint32_t st0 = pt.rng.state;
+      float cr, cg, cb;
+      pt.sample_sensor(sx, sy, p.bounces, cr, cg, cb);
+      pt.rng.state = st0;
+      // the sample enters the pixel mean clamped (pathtrace.metal:757)
+      const bool cl = p.clamp_value > 0.0f;
+      const float gr = (cl && !(cr < p.clamp_value)) ? 0.0f : d0;
+      const float gg = (cl && !(cg < p.clamp_value)) ? 0.0f : d1;
+      const float gb = (cl && !(cb < p.clamp_value)) ? 0.0f : d2;
+      const rm_camera& cam = p.camera;
+      const float focal2 = cam.focal * cam.focal;
+      const float dist = 1.0f / sqrtf(sx * sx + (sy * sy + focal2));
+      const float tx = sx * dist, ty = sy * dist, tz = cam.focal * dist;
+      const float dx = tx * cam.m0 + (ty * cam.m1 + tz * cam.m2);
+      const float dy = tx * cam.m3 + (ty * cam.m4 + tz * cam.m5);
+      const float dz = tx * cam.m6 + (ty * cam.m7 + tz * cam.m8);
+      adjoint_path(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, cr, cg, cb, gr, gg, gb, sink);
+      ++samples;
+    }
+  }
+  const unsigned long long tot = __reduce_add_sync(0xffffffffu, samples);
+  if ((threadIdx.x & 31) == 0 && tot) atomicAdd(ctr, tot);
+  if (use_shared) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < n_mat * kMatParams; i += blockDim.x)
+      if (sh[i] != 0.0f) atomicAdd(grad + i, sh[i]);
+  }
+}
+
+// Copy per-material parameters into the triangles (albedo, rough, emission, ior).
+__global__ void k_apply_materials(rm_triangle* tris, const int32_t* __restrict__ tri_mat,
+                                  const float* __restrict__ mats, int n_tris) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_tris) return;
+  const int m = tri_mat[i];
+  if (m < 0) return;
+  const float* q = mats + size_t(m) * kMatParams;
+  rm_triangle& t = tris[i];
+  t.ar = q[0]; t.ag = q[1]; t.ab = q[2];
+  t.rough = q[3];
+  t.er = q[4]; t.eg = q[5]; t.eb = q[6];
+  t.ior = q[7];
+}
+
+}  // namespace
+
+cudaError_t launch_adjoint(int lanes, const Scene& s, const Params& p, uint64_t seed, const int32_t* tri_mat,
+                           int n_mat, const float* dLdI, float* grad, unsigned long long* ctr, uint32_t* err,
+                           cudaStream_t st) {
+  const size_t shmem = size_t(n_mat) * kMatParams * sizeof(float);
+  const int use_shared = shmem <= 32 * 1024 ? 1 : 0;
+  const size_t threads = size_t(p.width) * size_t(p.height) * size_t(lanes);
+  const unsigned grid = unsigned((threads + 255) / 256);
+  const size_t sm = use_shared ? shmem : 0;
+  if (lanes == 32) k_adjoint<32><<<grid, 256, sm, st>>>(s, p, seed, tri_mat, n_mat, dLdI, grad, use_shared, ctr, err);
+  else if (lanes == 8) k_adjoint<8><<<grid, 256, sm, st>>>(s, p, seed, tri_mat, n_mat, dLdI, grad, use_shared, ctr, err);
+  else k_adjoint<1><<<grid, 256, sm, st>>>(s, p, seed, tri_mat, n_mat, dLdI, grad, use_shared, ctr, err);
+  return cudaGetLastError();
+}
+
+cudaError_t apply_materials(rm_triangle* tris, const int32_t* tri_mat, const float* mats, int n_tris,
+                            cudaStream_t st) {
+  if (n_tris <= 0) return cudaSuccess;
+  k_apply_materials<<<(n_tris + 255) / 256, 256, 0, st>>>(tris, tri_mat, mats, n_tris);
+  return cudaGetLastError();
+}
+
+}  // namespace rmd

@@ -57,8 +57,12 @@ struct DevScene {
   bool have_scene = false;
   int refits = 0;
   bool device_built = false;
+  // per-triangle materials (rmcuda_scene_set_materials): index per triangle,
+  // 8 parameters per material
+  DevBuf tri_mat, mats;
+  int n_materials = 0;
   void release() {
-    for (DevBuf* b : {&tris, &lights, &cdf, &texels, &lrec, &guide, &bvh.records, &bvh.parents, &bvh.counters,
+    for (DevBuf* b : {&tri_mat, &mats, &tris, &lights, &cdf, &texels, &lrec, &guide, &bvh.records, &bvh.parents, &bvh.counters,
                       &bvh.order, &bvh.tgeo, &bvh.keys, &bvh.keys_alt, &bvh.vals_alt, &bvh.knodes, &bvh.kbox,
                       &bvh.kcount, &bvh.ranges, &bvh.temp, &bvh.bounds, &bvh.depth})
       b->release();

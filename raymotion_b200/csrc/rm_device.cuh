@@ -137,6 +137,7 @@ struct Hit {
   float ar, ag, ab, er, eg, eb, ior, rough;
   int shader;
   float ngx, ngy, ngz;
+  float txr, txg, txb;  // texel colour the albedo was multiplied by (1 untextured)
 };
 
 struct Bsdf { float r, g, b, pdf; };
@@ -330,6 +331,7 @@ struct Tracer {
       float d = 1.0f / sqrtf(nx * nx + (ny * ny + nz * nz));
       h.nix = nx * d; h.niy = ny * d; h.niz = nz * d;
       h.ar = t.ar; h.ag = t.ag; h.ab = t.ab;
+      h.txr = h.txg = h.txb = 1.0f;
       if (t.texture_offset >= 0) {
         float tu = w * t.tu0 + h.u * t.tu1 + h.v * t.tu2;
         float tv = w * t.tv0 + h.u * t.tv1 + h.v * t.tv2;
@@ -339,6 +341,7 @@ struct Tracer {
         int y = t.texture_height - 1 - min(int(tv * float(t.texture_height)), t.texture_height - 1);
         const rm_vec3 c = s.texels[size_t(t.texture_offset) + size_t(y) * size_t(t.texture_width) + size_t(x)];
         h.ar *= c.x; h.ag *= c.y; h.ab *= c.z;
+        h.txr = c.x; h.txg = c.y; h.txb = c.z;
       }
       h.er = t.er; h.eg = t.eg; h.eb = t.eb;
       h.ior = t.ior; h.rough = t.rough; h.shader = t.shader;
@@ -606,12 +609,15 @@ struct Tracer {
 
   // The single-candidate branch (Mc <= 1, pathtrace.metal:319-384) of
   // direct_lighting_deferred, inlined where a caller knows Mc <= 1.
+  // `parts`, when given, receives the light's list index and the factor k of
+  // the contribution o = emission * bsdf * k (the adjoint differentiates it).
   __device__ __forceinline__ void nee_single_deferred(float px, float py, float pz, float nx, float ny, float nz,
                                                       float wox, float woy, float woz, float rough, float metallic,
                                                       float spec_prob, float ar, float ag, float ab, float& o_r,
                                                       float& o_g, float& o_b, float& out_sumW, uint32_t& out_M,
                                                       bool& has_ray, float& sox, float& soy, float& soz,
-                                                      float& sdx, float& sdy, float& sdz, float& sdist) {
+                                                      float& sdx, float& sdy, float& sdz, float& sdist,
+                                                      float* parts = nullptr) {
     o_r = o_g = o_b = 0.0f;
     out_sumW = 0.0f;
     out_M = 0;
@@ -624,7 +630,9 @@ struct Tracer {
     float alpha2 = (r2 * r2) * (r2 * r2);
     const float LT = p.light_total;
     float pick = U() * LT;
-    const LightRec t = load_light(s, pick_light(pick));
+    const int li = pick_light(pick);
+    const LightRec t = load_light(s, li);
+    if (parts) { parts[0] = __int_as_float(li); parts[1] = 0.0f; }
     float lu = U(), lv = U();
     if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
     float lw = 1.0f - lu - lv;
@@ -658,6 +666,7 @@ struct Tracer {
     o_r = t.er * e.r * k;
     o_g = t.eg * e.g * k;
     o_b = t.eb * e.b * k;
+    if (parts) parts[1] = k;
   }
 
   // direct_lighting for opaque scenes with the visibility test left to the
@@ -769,9 +778,14 @@ struct Tracer {
   }
 
   // pathtrace.metal:470-534; returns valid, writes direction and eta scale.
+  // `parts`, when given, receives what the adjoint differentiates: the event
+  // (0 reflection, 1 refraction, 2 total internal reflection), cos_m, for a
+  // rough surface cos_i, cos_o, cos_h and whether the weight was clamped, and
+  // |h x n|^2.
   __device__ __noinline__ bool sample_dielectric(float wox, float woy, float woz, float nx, float ny, float nz,
                                                  float cdx, float cdy, float cdz, float ior, bool front, float rough,
-                                                 float alpha2, float& o_x, float& o_y, float& o_z, float& eta_scale) {
+                                                 float alpha2, float& o_x, float& o_y, float& o_z, float& eta_scale,
+                                                 float* parts = nullptr) {
     bool valid = true;
     float eta_i = 1.0f, eta_t = ior;
     if (!front) { eta_i = ior; eta_t = 1.0f; }
@@ -793,12 +807,20 @@ struct Tracer {
       o_y = 2.0f * cos_m * hy - woy;
       o_z = 2.0f * cos_m * hz - woz;
       eta_scale = 1.0f;
+      if (parts) parts[0] = s2 >= 1.0f ? 2.0f : 0.0f;
     } else {
       float cos_t = sqrtf(1.0f - s2);
       o_x = eta * cdx + hx * (eta * cos_m - cos_t);
       o_y = eta * cdy + hy * (eta * cos_m - cos_t);
       o_z = eta * cdz + hz * (eta * cos_m - cos_t);
       eta_scale = eta * eta;
+      if (parts) parts[0] = 1.0f;
+    }
+    if (parts) {
+      parts[1] = cos_m;
+      parts[2] = parts[3] = parts[4] = parts[5] = 0.0f;
+      const float cx = hy * nz - hz * ny, cy = hz * nx - hx * nz, cz = hx * ny - hy * nx;
+      parts[6] = cx * cx + cy * cy + cz * cz;  // |h x n|^2
     }
     {
       float d = 1.0f / sqrtf(o_x * o_x + o_y * o_y + o_z * o_z);
@@ -813,6 +835,7 @@ struct Tracer {
         float g1 = 2.0f * cos_o / (cos_o + sqrtf(cos_o * cos_o + alpha2 * (1.0f - cos_o * cos_o)));
         float g2 = 2.0f * cos_i / (cos_i + sqrtf(cos_i * cos_i + alpha2 * (1.0f - cos_i * cos_i)));
         float w = g1 * g2 * vo_h / (cos_o * cos_h);
+        if (parts) { parts[2] = cos_i; parts[3] = cos_o; parts[4] = cos_h; parts[5] = w > 10.0f ? 1.0f : 0.0f; }
         if (w > 10.0f) w = 10.0f;
         eta_scale *= w;
       } else {

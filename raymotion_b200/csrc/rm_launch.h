@@ -134,6 +134,15 @@ cudaError_t launch_batch_combine(int lanes, const BtBatch& b, const BtState& w, 
 // Resident blocks per SM of each batch kernel (aux, trace, shade).
 void batch_occupancy(int& aux, int& trace, int& shade);
 
+// rm_adjoint.cu: path-replay adjoint of the plain frame (adds g . dC/dparams
+// into grad, n_mat x 8 floats: albedo rgb, rough, emission rgb, ior).
+cudaError_t launch_adjoint(int lanes, const Scene& s, const Params& p, uint64_t seed, const int32_t* tri_mat,
+                           int n_mat, const float* dLdI, float* grad, unsigned long long* ctr, uint32_t* err,
+                           cudaStream_t st);
+// Write per-material parameters (8 floats each) into the triangles with tri_mat >= 0.
+cudaError_t apply_materials(rm_triangle* tris, const int32_t* tri_mat, const float* mats, int n_tris,
+                            cudaStream_t st);
+
 // rm_denoise.cu
 // stage 0 temporal (in + hist_in -> out), 1 / 2 a-trous step 0 / 1 (in -> out, + RGB8 when rgb != nullptr)
 cudaError_t launch_denoise_stage(int stage, const Params& p, const GBufSoA& gb, const GBufSoA& hg, const float* in,

@@ -87,6 +87,46 @@ class PackedScene:
         return v
 
 
+MATERIAL_PARAMS = 8  # albedo rgb, rough, emission rgb, ior (rm_material)
+
+
+def light_table(scene: PackedScene, emission: np.ndarray) -> tuple[np.ndarray, float]:
+    """Light-selection CDF over scene.light_tri by area x luminance (scene.cpp:73-85)
+    for per-triangle emission (n_tris x 3); returns (cdf float32, total)."""
+    lt = scene.light_tri
+    if not len(lt):
+        return np.zeros(0, np.float32), 0.0
+    v = scene.verts64[lt]
+    e1 = v[:, 3:6] - v[:, 0:3]
+    e2 = v[:, 6:9] - v[:, 0:3]
+    d00 = np.einsum("ij,ij->i", e1, e1)
+    d01 = np.einsum("ij,ij->i", e1, e2)
+    d11 = np.einsum("ij,ij->i", e2, e2)
+    area = 0.5 * np.sqrt(np.maximum(d00 * d11 - d01 * d01, 0.0))
+    em = np.asarray(emission, np.float64)[lt]
+    lum = np.maximum(0.2126 * em[:, 0] + 0.7152 * em[:, 1] + 0.0722 * em[:, 2], 1e-6)
+    cdf = np.add.accumulate(area * lum)
+    return cdf.astype(np.float32), float(np.float32(cdf[-1]))
+
+
+def with_materials(scene: PackedScene, tri_material: np.ndarray, params: np.ndarray) -> PackedScene:
+    """A copy of ``scene`` whose triangles take their material's albedo, rough,
+    emission and ior (params: n_materials x 8 float32; tri_material -1 keeps a
+    triangle's own values), with the light table recomputed from the new
+    emission; the host-side twin of rmcuda_scene_set_materials."""
+    tm = np.asarray(tri_material, np.int32)
+    prm = np.asarray(params, np.float32)
+    t = scene.tris.copy()
+    sel = tm >= 0
+    m = tm[sel]
+    for k, name in enumerate(("ar", "ag", "ab", "rough", "er", "eg", "eb", "ior")):
+        t[name][sel] = prm[m, k]
+    emission = np.stack([t["er"], t["eg"], t["eb"]], axis=1).astype(np.float64)
+    cdf, total = light_table(scene, emission)
+    return PackedScene(tris=t, light_tri=scene.light_tri, light_cdf=cdf, light_total=np.float32(total),
+                       texels=scene.texels, verts64=scene.verts64, nodes=scene.nodes, bvh_tri=scene.bvh_tri)
+
+
 class SceneBuilder:
     """fp64 scene with the reference's add_triangle precompute, vectorised."""
 

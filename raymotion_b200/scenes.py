@@ -127,6 +127,21 @@ def _value_noise(p: np.ndarray, seed: int) -> np.ndarray:
     return out
 
 
+def _displaced_sphere(unit_v, faces, center, r, noise_seed):
+    """Corners and smooth vertex normals of an icosphere of radius r displaced by
+    value noise of amplitude 0.05 r."""
+    world = center + unit_v * r
+    disp = 0.05 * r * _value_noise(world * (2.0 / r), noise_seed)
+    pos = center + unit_v * (r + disp)[:, None]
+    fa, fb, fc = pos[faces[:, 0]], pos[faces[:, 1]], pos[faces[:, 2]]
+    fn = np.cross(fb - fa, fc - fa)
+    vn = np.zeros_like(pos)
+    for k in range(3):
+        np.add.at(vn, faces[:, k], fn)
+    vn /= np.linalg.norm(vn, axis=1, keepdims=True)
+    return fa, fb, fc, vn[faces[:, 0]], vn[faces[:, 1]], vn[faces[:, 2]]
+
+
 def icosphere_field(seed: int = 1, n_spheres: int = 200, subdiv: int = 4, n_emitters: int = 4096,
                     width: int = 1280, height: int = 720, spp: int = 64, depth: int = 12):
     """Returns (SceneBuilder, Camera, RenderConfig) of the instanced icosphere workload."""
@@ -138,23 +153,14 @@ def icosphere_field(seed: int = 1, n_spheres: int = 200, subdiv: int = 4, n_emit
                         rng.uniform(-20, 20, n_spheres)], axis=1)
     kind = rng.choice(3, size=n_spheres, p=[0.5, 0.3, 0.2])
     for i in range(n_spheres):
-        r = radii[i]
-        world = centers[i] + unit_v * r
-        disp = 0.05 * r * _value_noise(world * (2.0 / r), seed * 1000 + i)
-        pos = centers[i] + unit_v * (r + disp)[:, None]
-        fa, fb, fc = pos[faces[:, 0]], pos[faces[:, 1]], pos[faces[:, 2]]
-        fn = np.cross(fb - fa, fc - fa)
-        vn = np.zeros_like(pos)
-        for k in range(3):
-            np.add.at(vn, faces[:, k], fn)
-        vn /= np.linalg.norm(vn, axis=1, keepdims=True)
+        fa, fb, fc, na, nb, nc = _displaced_sphere(unit_v, faces, centers[i], radii[i], seed * 1000 + i)
         if kind[i] == 0:
             mat = dict(albedo=tuple(rng.uniform(0.1, 0.9, 3)), rough=0.5)
         elif kind[i] == 1:
             mat = dict(albedo=tuple(rng.uniform(0.5, 0.95, 3)), metallic=1.0, rough=float(rng.uniform(0.05, 1.0)))
         else:
             mat = dict(albedo=(1.0, 1.0, 1.0), ior=1.5, rough=float(rng.choice([0.0, 0.2])))
-        sb.add_triangles(fa, fb, fc, vn[faces[:, 0]], vn[faces[:, 1]], vn[faces[:, 2]], **mat)
+        sb.add_triangles(fa, fb, fc, na, nb, nc, **mat)
     g = 100.0
     _quad(sb, (-g, 0, -g), (-g, 0, g), (g, 0, g), (g, 0, -g), normal=(0, 1, 0), albedo=(0.5, 0.5, 0.5), rough=0.8)
     # small emitters facing down, scattered above the spheres
@@ -212,3 +218,86 @@ def batch_workload(seed: int = 3, n_scenes: int = 64, tri_range=(1000, 2_000_000
         depth = int(rng.integers(depths[0], depths[1] + 1))
         out.append(dict(seed=seed * 1000 + i, n_tris=n_tris, width=w, height=h, spp=spp, depth=depth))
     return out
+
+
+# parameter ranges of the inverse-rendering materials (albedo rgb, rough, emission rgb, ior)
+INVERSE_LO = np.array([0.05, 0.05, 0.05, 0.05, 0.0, 0.0, 0.0, 1.3], np.float32)
+INVERSE_HI = np.array([0.95, 0.95, 0.95, 1.0, 20.0, 20.0, 20.0, 1.7], np.float32)
+
+
+def inverse_scene(seed: int = 4, n_spheres: int = 100, subdiv: int = 3, ground: int = 190, patches=(10, 14),
+                  n_emitters: int = 16, n_dielectric: int = 32, width: int = 512, height: int = 512, spp: int = 32,
+                  depth: int = 8):
+    """The differentiable-rendering scene: displaced icospheres (20 * 4**subdiv
+    triangles each) over a tessellated ground of ground x ground quads split
+    into patches[0] x patches[1] material patches, and n_emitters small quad
+    lights.  Materials: one per sphere, per ground patch and per light
+    (100 + 140 + 16 = 256 by default), parameters uniform in INVERSE_LO..HI
+    (emission only for the lights, ior only for n_dielectric spheres; the
+    others keep emission 0 and ior 1).  The defaults give 100 * 1280 + 72,200 +
+    32 = 200,232 triangles.  Returns a dict: scene (PackedScene with the
+    materials applied), tri_material, params (n x 8 float32), mask (n x 8 bool,
+    the parameters a fit may change), camera, config (plain path, fixed spp)."""
+    rng = np.random.default_rng(seed)
+    sb = SceneBuilder()
+    unit_v, faces = _icosphere(subdiv)
+    n_patch = patches[0] * patches[1]
+    n_mat = n_spheres + n_patch + n_emitters
+    params = np.zeros((n_mat, 8), np.float32)
+    params[:, 0:3] = rng.uniform(INVERSE_LO[0], INVERSE_HI[0], (n_mat, 3))
+    params[:, 3] = rng.uniform(INVERSE_LO[3], INVERSE_HI[3], n_mat)
+    params[:, 7] = 1.0
+    mask = np.zeros((n_mat, 8), bool)
+    mask[:, 0:4] = True
+    diel = rng.choice(n_spheres, size=min(n_dielectric, n_spheres), replace=False)
+    params[diel, 7] = rng.uniform(INVERSE_LO[7], INVERSE_HI[7], len(diel))
+    mask[diel, 7] = True
+    lights = np.arange(n_spheres + n_patch, n_mat)
+    params[lights, 4:7] = rng.uniform(INVERSE_LO[4], INVERSE_HI[4], (len(lights), 3))
+    mask[lights, 4:7] = True
+    metal = rng.uniform(size=n_spheres) < 0.3
+    tri_mat = []
+    radii = rng.uniform(0.5, 1.5, n_spheres)
+    centers = np.stack([rng.uniform(-12, 12, n_spheres), rng.uniform(0.5, 4, n_spheres),
+                        rng.uniform(-12, 12, n_spheres)], axis=1)
+    for i in range(n_spheres):
+        fa, fb, fc, na, nb, nc = _displaced_sphere(unit_v, faces, centers[i], radii[i], seed * 1000 + i)
+        is_diel = params[i, 7] > 1.0001
+        idx = sb.add_triangles(fa, fb, fc, na, nb, nc, albedo=tuple(params[i, 0:3]), rough=float(params[i, 3]),
+                               metallic=1.0 if (metal[i] and not is_diel) else 0.0, ior=float(params[i, 7]))
+        tri_mat.append(np.full(len(idx), i, np.int32))
+    g = 20.0
+    xs = np.linspace(-g, g, ground + 1)
+    ix, iz = np.meshgrid(np.arange(ground), np.arange(ground), indexing="ij")
+    ix, iz = ix.ravel(), iz.ravel()
+    y0 = np.zeros(len(ix))
+    a = np.stack([xs[ix], y0, xs[iz]], axis=1)
+    b = np.stack([xs[ix], y0, xs[iz + 1]], axis=1)
+    c = np.stack([xs[ix + 1], y0, xs[iz + 1]], axis=1)
+    d = np.stack([xs[ix + 1], y0, xs[iz]], axis=1)
+    pm = n_spheres + (ix * patches[0] // ground) * patches[1] + (iz * patches[1] // ground)
+    up = np.broadcast_to(np.asarray([0.0, 1.0, 0.0]), (len(ix), 3))
+    for tri in ((a, b, c), (a, c, d)):
+        sb.add_triangles(tri[0], tri[1], tri[2], up, up, up, albedo=params[pm, 0:3], rough=params[pm, 3])
+        tri_mat.append(pm.astype(np.int32))
+    lc = np.stack([rng.uniform(-10, 10, n_emitters), rng.uniform(8, 11, n_emitters),
+                   rng.uniform(-10, 10, n_emitters)], axis=1)
+    h = 0.6
+    down = np.broadcast_to(np.asarray([0.0, -1.0, 0.0]), (n_emitters, 3))
+    p0 = lc + [-h, 0, -h]
+    p1 = lc + [h, 0, -h]
+    p2 = lc + [h, 0, h]
+    p3 = lc + [-h, 0, h]
+    for tri in ((p0, p1, p2), (p0, p2, p3)):
+        sb.add_triangles(tri[0], tri[1], tri[2], down, down, down, albedo=params[lights, 0:3],
+                         rough=params[lights, 3], emission=params[lights, 4:7])
+        tri_mat.append(lights.astype(np.int32))
+    tri_mat = np.concatenate(tri_mat)
+    packed = sb.pack()
+    assert len(tri_mat) == packed.n_tris
+    from .scene import with_materials
+    packed = with_materials(packed, tri_mat, params)
+    cam = Camera().set((0.0, 12.0, -27.0), (22.0, 0.0, 0.0), 58)
+    cfg = RenderConfig(width=width, height=height, spp=spp, max_bounces=depth, adapt_min=0, restir_candidates=1,
+                       restir_spatial=0, flags=PLAIN_FLAGS | _abi.RM_FLAG_NOADAPT)
+    return dict(scene=packed, tri_material=tri_mat, params=params, mask=mask, camera=cam, config=cfg)

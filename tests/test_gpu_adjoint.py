@@ -1,0 +1,215 @@
+"""Path-replay adjoint (rmcuda_backward) against FP64 central differences (GPU).
+
+The loss is L = mean((I - T)^2) over a W x H x 3 radiance image I of the
+plain frame, T a fixed target.  The adjoint's dL/dparams (given dL/dI at the
+current parameters) is compared with central differences of L (h = 1e-3,
+Richardson-extrapolated with h/2) evaluated by the oracle's frozen-path
+renderer in double: the same paths as
+the fp32 frame (sampling held at the current parameters), material factors at
+the perturbed parameters.  For each parameter kind (albedo r/g/b, roughness,
+emission r/g/b, ior) the check takes the materials with the largest gradients
+and one more; gradients above 1 % of the kind's largest must agree within
+1e-3 relative, the rest within 1e-5 of that largest.
+
+The torch.autograd.Function below exists only in this test harness: it wraps
+rmcuda_render_scene_async / rmcuda_backward so that torch's optimiser can
+drive them.
+"""
+import numpy as np
+import pytest
+
+from raymotion_b200 import RenderError
+from raymotion_b200.scene import with_materials
+from raymotion_b200.scenes import inverse_scene
+
+pytestmark = pytest.mark.gpu
+
+H = 1e-3
+
+
+def _torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _scene(oracle, spp, depth=6):
+    # 8 of the 10 spheres dielectric, so that several are in view
+    d = inverse_scene(seed=7, n_spheres=10, subdiv=2, ground=20, patches=(3, 3), n_emitters=3, n_dielectric=8,
+                      width=48, height=40, spp=spp, depth=depth)
+    oracle.with_reference_bvh(d["scene"])
+    return d
+
+
+def _set(backend, h, d, params):
+    s = with_materials(d["scene"], d["tri_material"], params)
+    backend.scene_set_materials(h, params, d["tri_material"], s.light_cdf, s.light_total)
+
+
+def _render(backend, h, d, seed):
+    torch = _torch()
+    cfg = d["config"]
+    img = torch.empty(cfg.width * cfg.height * 3, dtype=torch.float32, device="cuda")
+    backend.render_scene_async(h, d["camera"], cfg, seed, None, img.data_ptr())
+    backend.sync()
+    return img
+
+
+def _grad(backend, h, d, seed, dl):
+    torch = _torch()
+    g = torch.zeros(d["params"].size, dtype=torch.float32, device="cuda")
+    backend.backward(h, d["camera"], d["config"], seed, dl.data_ptr(), g.data_ptr())
+    backend.sync()
+    return g.cpu().numpy().reshape(-1, 8)
+
+
+def central_difference(loss, prm, m, col):
+    """Central differences at H and H/2, Richardson-extrapolated: the plain
+    H-difference carries an H^2 error of up to a few percent on the peaks of
+    glossy lobes and near a dielectric's critical angle, where the frame's
+    third derivative is large."""
+    def d(h):
+        qp, qm = prm.copy(), prm.copy()
+        qp[m, col] += h
+        qm[m, col] -= h
+        return (loss(qp) - loss(qm)) / (2 * h)
+    return (4.0 * d(H / 2) - d(H)) / 3.0
+
+
+@pytest.mark.parametrize("spp", [4, 8], ids=["one_lane", "eight_lanes"])
+def test_adjoint_matches_fp64_central_differences(backend, oracle, spp):
+    torch = _torch()
+    d = _scene(oracle, spp)
+    seed = 2024
+    sc, cam, cfg, tm = d["scene"], d["camera"], d["config"], d["tri_material"]
+    prm = d["params"].astype(np.float64)
+    h = backend.scene_create(sc)
+    try:
+        _set(backend, h, d, d["params"])
+        img = _render(backend, h, d, seed)
+        T = (img.cpu().numpy() * np.float32(0.75) + np.float32(0.01)).reshape(-1, 3).astype(np.float64)
+        # dL/dI of the loss on the FP64 image (the fp32 frame differs from it by
+        # rounding, up to ~3e-4 near the peaks of smooth GGX lobes)
+        i64 = oracle.render_frozen(sc, cam, cfg, seed, tm, prm)
+        dl = torch.from_numpy(((2.0 / i64.size) * (i64 - T)).astype(np.float32).ravel()).cuda()
+        g = _grad(backend, h, d, seed, dl)
+    finally:
+        backend.scene_destroy(h)
+
+    def loss(q):
+        return np.mean((oracle.render_frozen(sc, cam, cfg, seed, tm, q) - T) ** 2)
+
+    rng = np.random.default_rng(0)
+    checks = []
+    for col in range(8):
+        cand = np.nonzero(d["mask"][:, col])[0]
+        top = cand[np.argsort(-np.abs(g[cand, col]))][:3]
+        extra = rng.choice(cand, 1)
+        for m in sorted(set(top.tolist()) | set(extra.tolist())):
+            checks.append((m, col, central_difference(loss, prm, m, col), float(g[m, col])))
+    significant = 0
+    for col in range(8):
+        rows = [c for c in checks if c[1] == col]
+        big = max(abs(c[2]) for c in rows)
+        assert big > 0, f"param {col}: no gradient"
+        for (m, _, f, a) in rows:
+            if abs(f) >= 1e-2 * big:
+                significant += 1
+                assert abs(a - f) <= 1e-3 * abs(f), f"material {m} param {col}: adjoint {a} vs FD {f}"
+            else:
+                assert abs(a - f) <= 1e-5 * big, f"material {m} param {col}: adjoint {a} vs FD {f}"
+    assert significant >= 16
+
+
+def test_backward_rejects_what_it_does_not_differentiate(backend, oracle):
+    torch = _torch()
+    d = _scene(oracle, 4)
+    h = backend.scene_create(d["scene"])
+    try:
+        dl = torch.zeros(d["config"].width * d["config"].height * 3, device="cuda")
+        g = torch.zeros(d["params"].size, device="cuda")
+        with pytest.raises(RenderError, match="no materials"):
+            backend.backward(h, d["camera"], d["config"], 1, dl.data_ptr(), g.data_ptr())
+        _set(backend, h, d, d["params"])
+        adaptive = d["config"]
+        adaptive.flags &= ~0x2  # RM_FLAG_NOADAPT off
+        adaptive.adapt_min = 16
+        with pytest.raises(RenderError, match="fixed sample count"):
+            backend.backward(h, d["camera"], adaptive, 1, dl.data_ptr(), g.data_ptr())
+    finally:
+        backend.scene_destroy(h)
+
+
+def _render_function():
+    torch = _torch()
+
+    class RenderMaterials(torch.autograd.Function):
+        """image = plain frame of the scene object with material parameters `params` (n x 8)."""
+
+        @staticmethod
+        def forward(ctx, params, backend, h, d, seed, adjoint_seed):
+            p = params.detach().cpu().numpy().astype(np.float32)
+            _set(backend, h, d, p)
+            img = _render(backend, h, d, seed)
+            ctx.backend, ctx.h, ctx.d, ctx.seed = backend, h, d, adjoint_seed
+            return img
+
+        @staticmethod
+        def backward(ctx, grad_img):
+            # adjoint_seed == seed differentiates this frame's own paths; another
+            # seed gives an unbiased gradient of the expected loss for a
+            # stochastic fit (the same paths bias it towards lower variance)
+            g = _grad(ctx.backend, ctx.h, ctx.d, ctx.seed, grad_img.contiguous())
+            return torch.from_numpy(g).to(grad_img.device), None, None, None, None, None
+
+    return RenderMaterials
+
+
+def test_autograd_function_and_a_short_fit(backend, oracle):
+    """Fit the ground patches' albedo back from a +-30 % start.  Russian
+    roulette off and one seed for the target and every step: the paths then
+    do not depend on albedo, so the loss is a smooth function of it with its
+    minimum, zero, at the true values."""
+    torch = _torch()
+    Fn = _render_function()
+    d = _scene(oracle, 4)
+    d["config"].flags |= 0x40  # RM_FLAG_NO_RR
+    lo = torch.tensor([0.05, 0.05, 0.05, 0.05, 0.0, 0.0, 0.0, 1.3], device="cuda")
+    hi = torch.tensor([0.95, 0.95, 0.95, 1.0, 20.0, 20.0, 20.0, 1.7], device="cuda")
+    fit = np.zeros_like(d["mask"])
+    fit[10:19, 0:3] = True  # the ground patches, in view everywhere
+    mask = torch.from_numpy(fit & d["mask"]).cuda()
+    true = torch.from_numpy(d["params"]).cuda()
+    seed = 99
+    h = backend.scene_create(d["scene"])
+    try:
+        target = Fn.apply(true, backend, h, d, seed, seed).detach()
+        gen = torch.Generator(device="cuda").manual_seed(3)
+        noise = (torch.rand(true.shape, device="cuda", generator=gen) * 2 - 1) * 0.3
+        start = torch.where(mask, torch.clamp(true * (1 + noise), lo, hi), true)
+        u = ((start - lo) / (hi - lo)).clone().requires_grad_(True)
+        opt = torch.optim.Adam([u], lr=1e-2)
+        # the gradient through the Function equals a direct rmcuda_backward call
+        params = torch.where(mask, lo + (hi - lo) * u, true)
+        img = Fn.apply(params, backend, h, d, seed, seed)
+        loss = ((img - target) ** 2).mean()
+        loss.backward()
+        dl = (2.0 / img.numel()) * (img - target)
+        direct = torch.from_numpy(_grad(backend, h, d, seed, dl.detach())).cuda()
+        expect = torch.where(mask, direct * (hi - lo), torch.zeros_like(direct))
+        assert torch.allclose(u.grad, expect, rtol=1e-4, atol=1e-9)
+        err0 = ((params - true).abs() / (hi - lo))[mask].mean().item()
+        loss0 = loss.item()
+        for it in range(100):
+            opt.zero_grad()
+            params = torch.where(mask, lo + (hi - lo) * u.clamp(0, 1), true)
+            img = Fn.apply(params, backend, h, d, seed, seed)
+            loss = ((img - target) ** 2).mean()
+            loss.backward()
+            opt.step()
+        params = torch.where(mask, lo + (hi - lo) * u.detach().clamp(0, 1), true)
+        err1 = ((params - true).abs() / (hi - lo))[mask].mean().item()
+        assert loss.item() < 0.05 * loss0, (loss0, loss.item())
+        assert err1 < 0.5 * err0, (err0, err1)
+    finally:
+        backend.scene_destroy(h)
