@@ -24,7 +24,9 @@ Reported on one JSON line (rank 0):
             kernels; the reference itself runs only on Apple GPUs) timed on a
             band of rows of the same frame with every host core;
   batch   - batched vs one-at-a-time path samples/s over 64 uneven scenes
-            (see batch_compare), with the images checked identical.
+            (see batch_compare), with the images checked identical;
+  adjoint - the path-replay adjoint's cost relative to the forward frame and
+            a 200-step material fit (see adjoint_measure).
 --impl reference times that CPU implementation alone.
 """
 from __future__ import annotations
@@ -64,6 +66,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-serial measurement")
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-rendering measurement")
+    ap.add_argument("--fit-iters", type=int, default=200)
     return ap.parse_args()
 
 
@@ -310,6 +314,147 @@ def batch_compare(args, backend, torch, stream, dev, world):
         equal_samples=bool(s_samples == b_samples), scene_build_s=build_s, tune_s=tune_s)
 
 
+def adjoint_measure(args, backend, torch, stream, dev):
+    """Differentiable rendering on raymotion_b200.scenes.inverse_scene: 100
+    displaced icospheres (subdivision 3) + a 190 x 190-quad ground + 16 quad
+    lights = 200,232 triangles, 256 materials, 512 x 512, 32 spp, depth 8.
+
+    (1) forward frame vs rmcuda_backward, each timed with CUDA events over 3
+    calls after 2 warm-ups: the adjoint/forward time ratio;  (2) the fit: a
+    1024-spp target at the true materials, a start with +-30 % uniform noise on
+    every fitted parameter (albedo and roughness of all materials, emission of
+    the 16 lights, IOR of the 32 dielectrics), 200 Adam steps (lr 1e-2 on
+    parameters normalised to their ranges) of an L2 loss at 32 spp, the adjoint
+    replaying an independent frame each step (an unbiased gradient of the
+    expected loss).  Reports the mean normalised parameter error before and
+    after, over all fitted parameters and over those of materials the camera
+    sees directly on at least 256 pixels."""
+    import raymotion_b200 as rb
+    from raymotion_b200.scene import with_materials
+    from raymotion_b200.scenes import INVERSE_HI, INVERSE_LO, inverse_scene
+    d = inverse_scene()
+    sc, cam, cfg, tm = d["scene"], d["camera"], d["config"], d["tri_material"]
+    n_mat = len(d["params"])
+    h = backend.scene_create(sc)
+    npix = cfg.width * cfg.height
+
+    def set_params(p):
+        s2 = with_materials(sc, tm, p)
+        backend.scene_set_materials(h, p, tm, s2.light_cdf, s2.light_total)
+
+    set_params(d["params"])
+    img = torch.empty(npix * 3, dtype=torch.float32, device=dev)
+    dl = torch.full((npix * 3,), 1e-6, dtype=torch.float32, device=dev)
+    grad = torch.zeros(n_mat * 8, dtype=torch.float32, device=dev)
+
+    def fwd(seed):
+        backend.render_scene_async(h, cam, cfg, seed, None, img.data_ptr())
+
+    def bwd(seed):
+        backend.backward(h, cam, cfg, seed, dl.data_ptr(), grad.data_ptr())
+
+    def timed(fn, k=3):
+        for i in range(2):
+            fn(100 + i)
+        backend.sync()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(k):
+            fn(200 + i)
+        e1.record(stream)
+        backend.sync()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    backend.stats_reset()
+    fwd_ms = timed(fwd)
+    bwd_ms = timed(bwd)
+    st = backend.stage_counters()
+    # which materials the camera sees: primary hits of the pixel centres
+    backend.upload(sc, use_nodes=False)
+    ys, xs = np.mgrid[0:cfg.height, 0:cfg.width]
+    sx = (xs + 0.5 - cfg.width * 0.5).astype(np.float32).ravel()
+    sy = (cfg.height * 0.5 - (ys + 0.5)).astype(np.float32).ravel()
+    f = np.float32(cam.focal)
+    inv = np.float32(1) / np.sqrt(sx * sx + (sy * sy + f * f))
+    m = np.asarray(cam.m, np.float32)
+    tx, ty, tz = sx * inv, sy * inv, f * inv
+    rays = np.zeros((npix, 7), np.float32)
+    rays[:, 0:3] = (cam.x, cam.y, cam.z)
+    rays[:, 3] = tx * m[0] + (ty * m[1] + tz * m[2])
+    rays[:, 4] = tx * m[3] + (ty * m[4] + tz * m[5])
+    rays[:, 5] = tx * m[6] + (ty * m[7] + tz * m[8])
+    rays[:, 6] = 1e30
+    d_rays = torch.from_numpy(rays).to(dev)
+    d_tri = torch.empty(npix, dtype=torch.int32, device=dev)
+    backend.trace(d_rays.data_ptr(), npix, False, d_tri.data_ptr())
+    tri = d_tri.cpu().numpy()
+    seen = np.bincount(tm[tri[tri >= 0]], minlength=n_mat) >= 256
+    # the fit
+    lo = torch.from_numpy(INVERSE_LO).to(dev)
+    hi = torch.from_numpy(INVERSE_HI).to(dev)
+    mask = torch.from_numpy(d["mask"]).to(dev)
+    true = torch.from_numpy(d["params"]).to(dev)
+    cfg_t = rb.RenderConfig(**{k: getattr(cfg, k) for k in cfg.__dataclass_fields__})
+    cfg_t.spp = 1024
+    backend.render_scene_async(h, cam, cfg_t, 1, None, img.data_ptr())
+    backend.sync()
+    target = img.clone()
+    gen = torch.Generator(device=dev).manual_seed(4)
+    noise = (torch.rand(true.shape, device=dev, generator=gen) * 2 - 1) * 0.3
+    start = torch.where(mask, torch.minimum(torch.maximum(true * (1 + noise), lo), hi), true)
+    u = ((start - lo) / (hi - lo)).clone()
+    opt = torch.optim.Adam([u.requires_grad_(True)], lr=1e-2)
+    seen_t = torch.from_numpy(seen).to(dev)[:, None] & mask
+
+    def errors(p):
+        e = (p - true).abs() / (hi - lo)
+        out = dict(all=e[mask].mean().item(), seen=e[seen_t].mean().item() if seen_t.any() else None)
+        for name, cols in (("albedo", slice(0, 3)), ("rough", slice(3, 4)), ("emission", slice(4, 7)),
+                           ("ior", slice(7, 8))):
+            mk = mask[:, cols]
+            out[name] = e[:, cols][mk].mean().item() if mk.any() else None
+        return out
+
+    err0 = errors(start)
+    t0 = time.time()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    losses = []
+    for it in range(args.fit_iters):
+        p = torch.where(mask, lo + (hi - lo) * u.detach().clamp(0, 1), true)
+        set_params(p.cpu().numpy())
+        backend.render_scene_async(h, cam, cfg, 10000 + it, None, img.data_ptr())
+        dl.copy_((2.0 / img.numel()) * (img - target))
+        losses.append(((img - target) ** 2).mean())
+        grad.zero_()
+        backend.backward(h, cam, cfg, 20000 + it, dl.data_ptr(), grad.data_ptr())
+        opt.zero_grad()
+        u.grad = torch.where(mask, grad.view(n_mat, 8) * (hi - lo), torch.zeros_like(u))
+        opt.step()
+        with torch.no_grad():
+            u.clamp_(0, 1)
+    f1.record(stream)
+    backend.sync()
+    torch.cuda.synchronize()
+    fit_s = time.time() - t0
+    p = torch.where(mask, lo + (hi - lo) * u.detach(), true)
+    err1 = errors(p)
+    backend.scene_destroy(h)
+    loss_curve = [float(x) for x in torch.stack(losses).cpu().numpy()]
+    return dict(
+        workload="inverse_scene: 200,232 triangles, 256 materials, 512x512, 32 spp, depth 8, plain path, "
+                 "fixed spp, Russian roulette on",
+        forward_ms=fwd_ms, adjoint_ms=bwd_ms, adjoint_over_forward=bwd_ms / fwd_ms,
+        adjoint_samples_per_call=int(st["adjoint"]["path_samples"] / 5),
+        fit=dict(iterations=args.fit_iters, lr=1e-2, optimiser="Adam on normalised parameters",
+                 target_spp=1024, fit_spp=cfg.spp, wall_s=fit_s, gpu_ms=f0.elapsed_time(f1),
+                 param_error_start=err0, param_error_end=err1, materials_seen=int(seen.sum()),
+                 loss_first10=float(np.mean(loss_curve[:10])), loss_last10=float(np.mean(loss_curve[-10:]))))
+
+
 def run_b200(args, world, rank, local):
     import torch
 
@@ -446,6 +591,8 @@ def run_b200(args, world, rank, local):
                    ms_per_step=1e3 * esec / args.steps)
     # ---- batched vs serial rendering of many uneven scenes
     batch = None if args.no_batch else batch_compare(args, backend, torch, stream, dev, world)
+    # ---- differentiable rendering: adjoint cost and a 200-step fit
+    adjoint = None if args.no_adjoint else adjoint_measure(args, backend, torch, stream, dev)
     # ---- CPU baseline (rank 0, N=1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -459,7 +606,7 @@ def run_b200(args, world, rank, local):
                     mrays_per_s=rays_sum / secs_max / 1e6, e2e=e2e, roofline=roofline, cpu_baseline=cpu,
                     gpu_launches=int(st["kernel_launches"]), clocks=clk, stages=stage_summary,
                     kernels_one_frame=kernel_summary, wavefront=wave_summary, roofline_screen_space=roofline_ss,
-                    batch=batch)
+                    batch=batch, adjoint=adjoint)
         print(json.dumps(line), flush=True)
     backend.close()
     return 0

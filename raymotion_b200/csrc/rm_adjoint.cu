@@ -17,9 +17,11 @@
 //     sum_k thr_k * d(E_k + N_k) + sum_k (dB_k / B_k) * S_k
 // (E_k emission at vertex k, N_k its light sample, B_k the throughput factor
 // of its scattering).  Each thread owns a pixel lane, as the forward kernels
-// do, and replays each of its samples twice from the sample's RNG state:
-// once to get C, once to walk the path again accumulating the derivative
-// with S_k = C - (radiance gathered up to vertex k).  The refracted direction
+// do, and replays each of its samples from the sample's RNG state, in one
+// walk: the terms independent of C at once, the C-proportional halves of
+// g . dlogB_k . (C - acc_k) kept per vertex until the path ends (see
+// adjoint_path); paths longer than the kept list walk twice (first for C).
+// The refracted direction
 // is held fixed when the index of refraction changes; its motion would need a
 // reparameterised sampler and is not part of the estimator.
 #include <cuda_runtime.h>
@@ -137,11 +139,28 @@ __device__ __forceinline__ float dalpha2(float rough) {
   return 4.0f * rough * rough * rough;
 }
 
+// The terms of a sample's derivative that multiply its radiance C, one per
+// scattering vertex, kept until C is known (single-pass adjoint).
+struct Deferred {
+  static constexpr int kMax = 24;
+  int n;
+  int m[kMax];
+  int kind[kMax];    // 0 opaque surface, 1 dielectric
+  float v[kMax][6];  // opaque: albedo r, g, b; rough per channel.  dielectric: ior, rough
+};
+
 // One sample's path again (pathtrace.metal:552-728, the same arithmetic and
-// random draws as Tracer::pathtrace), accumulating g . dC/dparams.
+// random draws as Tracer::pathtrace), accumulating g . dC/dparams.  With
+// `dfr` null the sample's radiance C is given (a second walk after one that
+// computed it); with `dfr` the walk computes C itself, adds at once every
+// term that does not depend on it - the emission and light-sample terms and
+// the -(g . acc) halves of the scattering terms g . dlogB_k . (C - acc_k) -
+// and the g . dlogB_k . C halves when the path ends, returning C in C_out.
 __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict__ tri_mat, float ox, float oy,
                                           float oz, float dx, float dy, float dz, int max_bounces, float Cr, float Cg,
-                                          float Cb, float gr, float gg, float gb, const GradSink& sink) {
+                                          float Cb, float gr, float gg, float gb, const GradSink& sink,
+                                          Deferred* dfr, float* C_out) {
+  if (dfr) dfr->n = 0;
   const Scene& s = pt.s;
   const Params& p = pt.p;
   float accr = 0, accg = 0, accb = 0, thr_r = 1, thr_g = 1, thr_b = 1;
@@ -217,29 +236,36 @@ __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict_
       bool valid = pt.sample_dielectric(wox, woy, woz, pnx, pny, pnz, dx, dy, dz, hit.ior, front, rough, alpha2, nx2,
                                         ny2, nz2, es, dp);
       if (!valid) break;
-      // B_k = es: d log B_k, times g . S_k
-      const float gS = gr * (Cr - accr) + gg * (Cg - accg) + gb * (Cb - accb);
-      if (gS != 0.0f) {
-        const int event = int(dp[0]);
-        if (event != 2) {
-          const Dual ior{hit.ior, 1.0f};
-          const Dual ei = front ? dc(1.0f) : ior, et = front ? ior : dc(1.0f);
-          const Dual F = fresnel_dual(dp[1], ei, et);
-          float dlog = 0.0f;
-          if (event == 0) dlog = F.v > 0.0f ? F.d / F.v : 0.0f;
-          else {
-            dlog = F.v < 1.0f ? -F.d / (1.0f - F.v) : 0.0f;
-            dlog += front ? -2.0f / hit.ior : 2.0f / hit.ior;  // (eta_i / eta_t)^2
-          }
-          sink.add(m, 7, gS * dlog);
+      // B_k = es: d log B_k (ior, rough), times g . S_k
+      float dlog_ior = 0.0f, dlog_r = 0.0f;
+      const int event = int(dp[0]);
+      if (event != 2) {
+        const Dual ior{hit.ior, 1.0f};
+        const Dual ei = front ? dc(1.0f) : ior, et = front ? ior : dc(1.0f);
+        const Dual F = fresnel_dual(dp[1], ei, et);
+        if (event == 0) dlog_ior = F.v > 0.0f ? F.d / F.v : 0.0f;
+        else {
+          dlog_ior = F.v < 1.0f ? -F.d / (1.0f - F.v) : 0.0f;
+          dlog_ior += front ? -2.0f / hit.ior : 2.0f / hit.ior;  // (eta_i / eta_t)^2
         }
-        if (rough > 0.0201f && dal2 != 0.0f) {
-          const float ch = dp[4];
-          const float dd = dp[6] + alpha2 * ch * ch;
-          float dlog = 1.0f / alpha2 - 2.0f * ch * ch / dd;  // D
-          if (dp[5] == 0.0f) dlog += dlog_g1(dp[3], alpha2) + dlog_g1(dp[2], alpha2);  // G, unless clamped
-          sink.add(m, 3, gS * dlog * dal2);
-        }
+      }
+      if (rough > 0.0201f && dal2 != 0.0f) {
+        const float ch = dp[4];
+        const float dd = dp[6] + alpha2 * ch * ch;
+        dlog_r = 1.0f / alpha2 - 2.0f * ch * ch / dd;  // D
+        if (dp[5] == 0.0f) dlog_r += dlog_g1(dp[3], alpha2) + dlog_g1(dp[2], alpha2);  // G, unless clamped
+        dlog_r *= dal2;
+      }
+      if (dfr) {
+        const float gA = gr * accr + gg * accg + gb * accb;
+        sink.add(m, 7, -gA * dlog_ior);
+        sink.add(m, 3, -gA * dlog_r);
+        const int k = dfr->n++;
+        dfr->m[k] = m; dfr->kind[k] = 1; dfr->v[k][0] = dlog_ior; dfr->v[k][1] = dlog_r;
+      } else {
+        const float gS = gr * (Cr - accr) + gg * (Cg - accg) + gb * (Cb - accb);
+        sink.add(m, 7, gS * dlog_ior);
+        sink.add(m, 3, gS * dlog_r);
       }
       thr_r *= es; thr_g *= es; thr_b *= es;
       float sg = 1.0f;
@@ -315,16 +341,29 @@ __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict_
         // B_k = f * cos / pdf: d log B_k = df / f, times g . S_k per channel
         const BsdfGrad bg = bsdf_grad(nx2, ny2, nz2, wox, woy, woz, pnx, pny, pnz, alpha2, metallic, hit.ar, hit.ag,
                                       hit.ab);
+        float qa[3], qr[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const bool ok = bg.f[c] > 0.0f;
+          qa[c] = (ok && alb_grad) ? gv[c] * bg.da[c] * tx[c] / bg.f[c] : 0.0f;
+          qr[c] = ok ? gv[c] * bg.dal2[c] * dal2 / bg.f[c] : 0.0f;
+        }
+        const float acc[3] = {accr, accg, accb};
         const float S[3] = {Cr - accr, Cg - accg, Cb - accb};
         float drough = 0.0f;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          if (!(bg.f[c] > 0.0f)) continue;
-          const float gs = gv[c] * S[c] / bg.f[c];
-          if (alb_grad) sink.add(m, c, gs * bg.da[c] * tx[c]);
-          drough += gs * bg.dal2[c];
+          const float w = dfr ? -acc[c] : S[c];
+          if (alb_grad) sink.add(m, c, qa[c] * w);
+          drough += qr[c] * w;
         }
-        sink.add(m, 3, drough * dal2);
+        sink.add(m, 3, drough);
+        if (dfr) {
+          const int k = dfr->n++;
+          dfr->m[k] = m; dfr->kind[k] = 0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) { dfr->v[k][c] = qa[c]; dfr->v[k][3 + c] = qr[c]; }
+        }
       }
       last_pdf = e.pdf;
       float cos_i = nx2 * pnx + (ny2 * pny + nz2 * pnz);
@@ -354,6 +393,27 @@ __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict_
     }
     bounce++;
   }
+  if (dfr) {
+    // the path is complete: acc is its radiance C
+    const float C[3] = {accr, accg, accb};
+    const float gC = gr * accr + gg * accg + gb * accb;
+    for (int k = 0; k < dfr->n; ++k) {
+      const int m = dfr->m[k];
+      if (dfr->kind[k] == 0) {
+        float dr = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          sink.add(m, c, dfr->v[k][c] * C[c]);
+          dr += dfr->v[k][3 + c] * C[c];
+        }
+        sink.add(m, 3, dr);
+      } else {
+        sink.add(m, 7, dfr->v[k][0] * gC);
+        sink.add(m, 3, dfr->v[k][1] * gC);
+      }
+    }
+    C_out[0] = accr; C_out[1] = accg; C_out[2] = accb;
+  }
 }
 
 // One pixel lane per thread, the samples of K1 (LANES 1) or of one lane of K2,
@@ -381,18 +441,14 @@ __global__ void __launch_bounds__(256) k_adjoint(Scene s, Params p, uint64_t see
     const float inv_n = 1.0f / float(p.spp);
     const float d0 = dLdI[size_t(pixel) * 3] * inv_n, d1 = dLdI[size_t(pixel) * 3 + 1] * inv_n,
                 d2 = dLdI[size_t(pixel) * 3 + 2] * inv_n;
+    // one walk per sample when its vertices fit the deferred list, else a
+    // first walk for C (Tracer::pathtrace) and a second for the derivative
+    const bool one_walk = p.bounces <= Deferred::kMax;
+    const bool cl = p.clamp_value > 0.0f;
     for (uint32_t si = lane; si < uint32_t(p.spp); si += LANES) {
       float sx, sy;
       pt.jitter(x, y, sx, sy);
       const uint32_t st0 = pt.rng.state;
-      float cr, cg, cb;
-      pt.sample_sensor(sx, sy, p.bounces, cr, cg, cb);
-      pt.rng.state = st0;
-      // the sample enters the pixel mean clamped (pathtrace.metal:757)
-      const bool cl = p.clamp_value > 0.0f;
-      const float gr = (cl && !(cr < p.clamp_value)) ? 0.0f : d0;
-      const float gg = (cl && !(cg < p.clamp_value)) ? 0.0f : d1;
-      const float gb = (cl && !(cb < p.clamp_value)) ? 0.0f : d2;
       const rm_camera& cam = p.camera;
       const float focal2 = cam.focal * cam.focal;
       const float dist = 1.0f / sqrtf(sx * sx + (sy * sy + focal2));
@@ -400,7 +456,31 @@ __global__ void __launch_bounds__(256) k_adjoint(Scene s, Params p, uint64_t see
       const float dx = tx * cam.m0 + (ty * cam.m1 + tz * cam.m2);
       const float dy = tx * cam.m3 + (ty * cam.m4 + tz * cam.m5);
       const float dz = tx * cam.m6 + (ty * cam.m7 + tz * cam.m8);
-      adjoint_path(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, cr, cg, cb, gr, gg, gb, sink);
+      float C[3];
+      if (one_walk) {
+        // derivative as if no channel were clamped; a clamped channel (rare)
+        // is taken back out by a second walk with -g on that channel
+        Deferred dfr;
+        adjoint_path(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, 0.f, 0.f, 0.f, d0, d1, d2, sink, &dfr,
+                     C);
+        if (cl && !(C[0] < p.clamp_value && C[1] < p.clamp_value && C[2] < p.clamp_value)) {
+          const uint32_t st1 = pt.rng.state;
+          pt.rng.state = st0;
+          adjoint_path(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, C[0], C[1], C[2],
+                       C[0] < p.clamp_value ? 0.f : -d0, C[1] < p.clamp_value ? 0.f : -d1,
+                       C[2] < p.clamp_value ? 0.f : -d2, sink, nullptr, nullptr);
+          pt.rng.state = st1;
+        }
+      } else {
+        pt.sample_sensor(sx, sy, p.bounces, C[0], C[1], C[2]);
+        pt.rng.state = st0;
+        // the sample enters the pixel mean clamped (pathtrace.metal:757)
+        const float gr = (cl && !(C[0] < p.clamp_value)) ? 0.0f : d0;
+        const float gg = (cl && !(C[1] < p.clamp_value)) ? 0.0f : d1;
+        const float gb = (cl && !(C[2] < p.clamp_value)) ? 0.0f : d2;
+        adjoint_path(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, C[0], C[1], C[2], gr, gg, gb, sink,
+                     nullptr, nullptr);
+      }
       ++samples;
     }
   }
