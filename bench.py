@@ -498,6 +498,7 @@ def run_b200(args, world, rank, local):
     backend.sync()
     secs = ev0.elapsed_time(ev1) / 1e3
     st = backend.stats()
+    wlog = backend.wave_log()  # of the last timed frame (the breakdown frame below runs with per-launch events)
     stage_t = backend.stage_times()
     stage_c = backend.stage_counters()
     secs_max, = allreduce([secs], "max", world, dev)
@@ -513,13 +514,17 @@ def run_b200(args, world, rank, local):
     kern_c = backend.stage_counters()
     kern_st = backend.stats()
     backend.profile(0)
-    wlog = backend.wave_log()
     wave_summary = None
     if len(wlog):
-        act = wlog[:, 0]
+        act, us = wlog[:, 0], wlog[:, 3]
         first = int(act[0])
-        marks = {f"batches_until_{int(f * 100)}pct": int(np.argmax(act < f * first)) for f in (0.5, 0.1, 0.01)}
-        wave_summary = dict(batches=int(len(act)), waves_per_batch=4, first_act=first, **marks)
+        marks = {}
+        for f in (0.5, 0.1, 0.01):
+            b = int(np.argmax(act < f * first))
+            marks[f"batches_until_{int(f * 100)}pct"] = b
+            marks[f"ms_until_{int(f * 100)}pct"] = float(us[b]) / 1e3
+        wave_summary = dict(batches=int(len(act)), waves_per_batch=4, first_act=first, ms_loop=float(us[-1]) / 1e3,
+                            **marks)
     # ---- roofline of the dominant kernel (the wavefront loop counts as its kernels)
     if args.no_breakdown:
         kern_t, kern_c = stage_t, stage_c
@@ -532,20 +537,21 @@ def run_b200(args, world, rank, local):
         # stage; its traversal counters sit with its traversal kernels
         c = {k: kern_c["wf_extend"][k] + kern_c["wf_shadow"][k] for k in c}
         dom = "wavefront shading loop"
-    alg_bytes = (c["nodes_visited"] * 64 + c["tris_tested"] * 48) / max(launches, 1)
+    node_bytes = st.get("bvh_node_bytes", 64) or 64
+    alg_bytes = (c["nodes_visited"] * node_bytes + c["tris_tested"] * 48) / max(launches, 1)
     avg_s = ms_total / 1e3 / max(launches, 1)
     peak = measured_peaks()
     achieved = alg_bytes / avg_s / 1e9 if avg_s > 0 else 0.0
     kernel_names = dict(plain="k_render_paths", shade="k_restir_shade", generate="k_restir_generate",
                         spatial="k_restir_spatial", temporal="k_denoise_temporal", atrous0="k_denoise_atrous",
                         atrous1="k_denoise_atrous", hash="k_hash", tonemap="k_tonemap", wf_extend="k_wf_extend",
-                        wf_shadow="k_wf_shadow", wf_shade="k_wf_shade",
+                        wf_shadow="k_wf_shadow", wf_shade="k_wf_shade", wf_tail="k_wf_tail",
                         **{"wavefront shading loop": "k_wf_init + k_wf_trace + k_wf_shade (one stage)"})
     roofline = dict(bound="hbm", kernel=kernel_names.get(dom, dom), achieved=achieved, peak=peak["hbm_gbs"],
                     unit="GB/s", frac=achieved / peak["hbm_gbs"], traffic=ncu_traffic(kernel_names.get(dom, dom)),
                     peak_source=peak["source"],
-                    note="achieved = (64 B x BVH records fetched + 48 B x triangle tests) per launch / average "
-                         "launch time; most of these bytes hit L1/L2")
+                    note=f"achieved = ({node_bytes} B x BVH nodes fetched + 48 B x triangle tests) per launch / "
+                         "average launch time; most of these bytes hit L1/L2")
     # screen-space passes (temporal 92 B/px, two a-trous 64 B/px each, fused tonemap write 3 B/px):
     # algorithmic bytes per frame against the measured HBM peak
     ss_ms = sum(kern_t[k][0] for k in ("temporal", "atrous0", "atrous1"))

@@ -130,6 +130,7 @@ typedef struct rm_stats {
   uint64_t kernel_launches; /* this library's kernels launched by frame calls */
   uint32_t device_error;    /* last nonzero device error word, 0 if none */
   uint32_t kernel_chain;    /* 1 = render_paths, 8/32 = lane kernels, 2 = ReSTIR chain */
+  uint32_t bvh_node_bytes;  /* bytes of one node visit: 80 (8-wide compressed BVH) or 64 (binary) */
 } rm_stats;
 
 typedef struct rmcuda_ctx rmcuda_ctx;
@@ -336,7 +337,8 @@ int rmcuda_stats_reset(rmcuda_ctx* ctx);
 #define RM_STAGE_BT_SHADE 15  /* batched rendering: shading */
 #define RM_STAGE_BATCH 16     /* batched rendering: a whole rmcuda_render_batch call */
 #define RM_STAGE_ADJOINT 17   /* path-replay adjoint (rmcuda_backward) */
-#define RM_STAGE_COUNT 18
+#define RM_STAGE_WF_TAIL 18   /* wavefront shading: the last paths, one thread per pixel */
+#define RM_STAGE_COUNT 19
 /* level 0: off; 1: one event pair per stage (the wavefront shading loop counts
  * as RM_STAGE_SHADE, a batch as RM_STAGE_BATCH); 2: also every wavefront
  * launch in its own stage (batches then run without CUDA graphs). */
@@ -344,9 +346,11 @@ int rmcuda_profile(rmcuda_ctx* ctx, int level);
 /* Per-stage device counters since the last reset: n records of
  * {path samples, rays, BVH nodes visited, triangle tests}. */
 int rmcuda_stage_counters(rmcuda_ctx* ctx, uint64_t* out, int32_t n);
-/* Queue lengths of the last frame's wavefront shading: for each wave
- * (paths shaded, extension rays, shadow rays), at most `cap` waves written
- * to `out` (3 ints each).  Returns the number of waves of that frame. */
+/* Queue lengths of the last frame's wavefront shading, read every 4 waves:
+ * for each read (unfinished paths, extension rays, shadow rays, microseconds
+ * from the first read of the frame to this one), at most `cap` records
+ * written to `out` (4 ints each); the last record has empty queues (the
+ * loop's end, or the end of its tail launch).  Returns the number of records. */
 int rmcuda_wave_log(rmcuda_ctx* ctx, int32_t* out, int32_t cap);
 int rmcuda_stage_times(rmcuda_ctx* ctx, double* ms, uint64_t* launches, int32_t n);
 

@@ -41,6 +41,15 @@ def build_ref(ref_root: str = "/root/reference") -> Path | None:
     return REF_SO
 
 
+def build_dropin(ref_root: str = "/root/reference") -> bool:
+    """Build the reference's own test_metal / test_alpha against librmcuda.so
+    (the drop-in check) when the reference checkout is present."""
+    if not Path(ref_root, "tests/test_metal.cpp").exists():
+        return False
+    subprocess.run(["make", "-s", "-f", str(HERE / "Makefile.ref"), f"REF={ref_root}", "dropin"], check=True)
+    return True
+
+
 _orc = None
 _ref = None
 

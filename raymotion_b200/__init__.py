@@ -227,7 +227,7 @@ class Backend:
             raise RenderError(rc, "stats read failed")
         return dict(path_samples=s.path_samples, rays=s.rays, nodes_visited=s.nodes_visited,
                     tris_tested=s.tris_tested, frames=s.frames, kernel_launches=s.kernel_launches,
-                    device_error=s.device_error, kernel_chain=s.kernel_chain)
+                    device_error=s.device_error, kernel_chain=s.kernel_chain, bvh_node_bytes=s.bvh_node_bytes)
 
     def stats_reset(self) -> None:
         self.lib.rmcuda_stats_reset(self.h)
@@ -243,9 +243,9 @@ class Backend:
         return {name: (ms[i], int(cnt[i])) for i, name in enumerate(_abi.STAGES)}
 
     def wave_log(self) -> np.ndarray:
-        """(act, ext, shd) queue lengths per wave of the last wavefront frame."""
+        """(act, ext, shd, us) per count read (every 4 waves) of the last wavefront frame."""
         n = self.lib.rmcuda_wave_log(self.h, None, 0)
-        out = np.zeros((max(n, 0), 3), np.int32)
+        out = np.zeros((max(n, 0), 4), np.int32)
         if n > 0:
             self.lib.rmcuda_wave_log(self.h, out.ctypes.data_as(C.POINTER(C.c_int32)), n)
         return out

@@ -80,7 +80,7 @@ class RmConfig(C.Structure):
 class RmStats(C.Structure):
     _fields_ = [("path_samples", C.c_uint64), ("rays", C.c_uint64), ("nodes_visited", C.c_uint64),
                 ("tris_tested", C.c_uint64), ("frames", C.c_uint64), ("kernel_launches", C.c_uint64),
-                ("device_error", C.c_uint32), ("kernel_chain", C.c_uint32)]
+                ("device_error", C.c_uint32), ("kernel_chain", C.c_uint32), ("bvh_node_bytes", C.c_uint32)]
 
 
 class RmBatchItem(C.Structure):
@@ -133,7 +133,8 @@ EXPORTS = [
 ]
 
 STAGES = ["plain", "hash", "generate", "spatial", "shade", "temporal", "atrous0", "atrous1", "tonemap", "wf_extend",
-          "wf_shadow", "wf_shade", "bt_start", "bt_extend", "bt_shadow", "bt_shade", "batch", "adjoint"]
+          "wf_shadow", "wf_shade", "bt_start", "bt_extend", "bt_shadow", "bt_shade", "batch", "adjoint",
+          "wf_tail"]
 
 _lib = None
 

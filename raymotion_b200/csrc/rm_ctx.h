@@ -64,8 +64,11 @@ struct DevScene {
   void release() {
     for (DevBuf* b : {&tri_mat, &mats, &tris, &lights, &cdf, &texels, &lrec, &guide, &bvh.records, &bvh.parents, &bvh.counters,
                       &bvh.order, &bvh.tgeo, &bvh.keys, &bvh.keys_alt, &bvh.vals_alt, &bvh.knodes, &bvh.kbox,
-                      &bvh.kcount, &bvh.ranges, &bvh.temp, &bvh.bounds, &bvh.depth})
+                      &bvh.kcount, &bvh.ranges, &bvh.temp, &bvh.bounds, &bvh.depth, &bvh.wnodes, &bvh.wtgeo,
+                      &bvh.wq})
       b->release();
+    if (bvh.h_wcnt) cudaFreeHost(bvh.h_wcnt);
+    bvh.h_wcnt = nullptr;
   }
 };
 
@@ -130,7 +133,7 @@ struct rmcuda_ctx {
   int* h_counts = nullptr;  // pinned: the current wave's queue lengths
   size_t wf_cap = 0;
   uint64_t waves = 0;
-  std::vector<int> wave_log;  // last frame: (act, ext, shd) per wave
+  std::vector<int> wave_log;  // last frame: (act, ext, shd, us) per count read
   // batched rendering (rmcuda_batch.cu)
   rmapi::BatchPool batch;
   // per-stage CUDA-event timing (rmcuda_profile)

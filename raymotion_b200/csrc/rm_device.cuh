@@ -57,6 +57,10 @@ struct Scene {
   const int32_t* __restrict__ guide;
   int guide_n;
   float guide_inv;  // guide_n / light_total
+  // 8-wide compressed BVH (rm_wide.cu), used instead of `nodes` when set:
+  // 5 x float4 per node, and the triangle records (as tgeo) in its leaf order
+  const float4* __restrict__ wnodes = nullptr;
+  const float4* __restrict__ wtgeo = nullptr;
 };
 
 // One emissive triangle as light sampling reads it (the fields of
@@ -151,6 +155,35 @@ struct Bsdf { float r, g, b, pdf; };
 // the Moller-Trumbore test would accept: the hit is independent of the BVH.
 struct TraceResult { float t; int tri; float u, v; };
 
+// Moller-Trumbore against one triangle record (pathtrace.metal:150-158) with
+// the (t, triangle index) order of the header; true when it became the hit.
+__device__ __forceinline__ bool test_triangle(const float4* __restrict__ g, float ox, float oy, float oz, float dx,
+                                              float dy, float dz, TraceResult& r) {
+  const float4 q0 = __ldg(g + 0);
+  const float4 q1 = __ldg(g + 1);
+  const float4 q2 = __ldg(g + 2);
+  const int j = __float_as_int(q0.w);
+  float px = dy * q2.z - dz * q2.y;
+  float py = dz * q2.x - dx * q2.z;
+  float pz = dx * q2.y - dy * q2.x;
+  float det = q1.x * px + q1.y * py + q1.z * pz;
+  if (fabsf(det) < 1e-12f) return false;
+  float tx = ox - q0.x, ty = oy - q0.y, tz = oz - q0.z;
+  float u = (tx * px + ty * py + tz * pz) / det;
+  if (u < 0.0f || u > 1.0f) return false;
+  float qx = ty * q1.z - tz * q1.y;
+  float qy = tz * q1.x - tx * q1.z;
+  float qz = tx * q1.y - ty * q1.x;
+  float v = (dx * qx + dy * qy + dz * qz) / det;
+  if (v < 0.0f || u + v > 1.0f) return false;
+  float dd = (q2.x * qx + q2.y * qy + q2.z * qz) / det;
+  if (dd > 1e-8f && (dd < r.t || (dd == r.t && r.tri >= 0 && j < r.tri))) {
+    r.t = dd; r.tri = j; r.u = u; r.v = v;
+    return true;
+  }
+  return false;
+}
+
 // Resumable traversal of one ray: init() then step() until it returns true.
 // A step visits child-pair records until a leaf is pending (descending into
 // the nearer child, pushing the farther one as an 8-bit count / 24-bit link
@@ -174,6 +207,59 @@ struct Trav {
     leaf_count = 0;
   }
 
+  // Pop the next pending subtree (8-bit leaf count / 24-bit link word); true
+  // when none is left.
+  __device__ __forceinline__ bool pop(const int* stack) {
+    if (sp == 0) return true;
+    const int e = stack[--sp];
+    const int cnt = int(uint32_t(e) >> 24), link = e & 0xFFFFFF;
+    if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
+    else node = link;
+    return false;
+  }
+
+  // Box-test the two children of record `node` and move on: into the nearer
+  // hit child (pushing the farther one), else to the next pending subtree.
+  // True when nothing is left (or the stack overflowed, flagged in err).
+  __device__ __forceinline__ bool visit(const Scene& s, int* stack, uint32_t* err, uint32_t& n_nodes) {
+    ++n_nodes;
+    const float4* n = s.nodes + size_t(node) * 4;
+    const float4 a = __ldg(n + 0);
+    const float4 b = __ldg(n + 1);
+    const float4 c = __ldg(n + 2);
+    const int4 d = __ldg(reinterpret_cast<const int4*>(n + 3));
+    // child 0
+    float l0x = (a.x - ox) * ix, h0x = (a.y - ox) * ix;
+    float l0y = (a.z - oy) * iy, h0y = (a.w - oy) * iy;
+    float l0z = (c.x - oz) * iz, h0z = (c.y - oz) * iz;
+    float n0 = fmaxf(0.0f, fmaxf(fminf(l0x, h0x), fmaxf(fminf(l0y, h0y), fminf(l0z, h0z))));
+    float f0 = fminf(r.t, fminf(fmaxf(l0x, h0x), fminf(fmaxf(l0y, h0y), fmaxf(l0z, h0z))));
+    // child 1
+    float l1x = (b.x - ox) * ix, h1x = (b.y - ox) * ix;
+    float l1y = (b.z - oy) * iy, h1y = (b.w - oy) * iy;
+    float l1z = (c.z - oz) * iz, h1z = (c.w - oz) * iz;
+    float n1 = fmaxf(0.0f, fmaxf(fminf(l1x, h1x), fmaxf(fminf(l1y, h1y), fminf(l1z, h1z))));
+    float f1 = fminf(r.t, fminf(fmaxf(l1x, h1x), fminf(fmaxf(l1y, h1y), fmaxf(l1z, h1z))));
+    bool hit0 = d.z >= 0 && !(n0 > f0 * kBoxSlack);
+    bool hit1 = d.w >= 0 && !(n1 > f1 * kBoxSlack);
+    // a child record: link d.x/d.y, count d.z/d.w (>0 leaf, 0 internal, <0 empty)
+    if (hit0 && hit1) {
+      int first = d.x, firstc = d.z, second = d.y, secondc = d.w;
+      if (n1 < n0) { first = d.y; firstc = d.w; second = d.x; secondc = d.z; }
+      if (sp >= kStack) { atomicOr(err, kErrStack); return true; }
+      stack[sp++] = int((uint32_t(secondc) << 24) | uint32_t(second));  // far child: 8-bit count, 24-bit link
+      if (firstc > 0) { leaf_first = first; leaf_count = firstc; node = -1; }
+      else node = first;
+    } else if (hit0 || hit1) {
+      int link = hit0 ? d.x : d.y, cnt = hit0 ? d.z : d.w;
+      if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
+      else node = link;
+    } else {
+      return pop(stack);
+    }
+    return false;
+  }
+
   // Returns true when the ray is finished (r holds the result).  `stack` is
   // the caller's kStack-entry array (kept out of the struct so that the scalar
   // state stays in registers).
@@ -181,82 +267,134 @@ struct Trav {
   __device__ __forceinline__ bool step(const Scene& s, int* stack, uint32_t* err, uint32_t& n_nodes,
                                        uint32_t& n_tests) {
     if (s.n_nodes == 0) return true;
-    while (node >= 0 && leaf_count == 0) {
-      ++n_nodes;
-      const float4* n = s.nodes + size_t(node) * 4;
-      const float4 a = __ldg(n + 0);
-      const float4 b = __ldg(n + 1);
-      const float4 c = __ldg(n + 2);
-      const int4 d = __ldg(reinterpret_cast<const int4*>(n + 3));
-      // child 0
-      float l0x = (a.x - ox) * ix, h0x = (a.y - ox) * ix;
-      float l0y = (a.z - oy) * iy, h0y = (a.w - oy) * iy;
-      float l0z = (c.x - oz) * iz, h0z = (c.y - oz) * iz;
-      float n0 = fmaxf(0.0f, fmaxf(fminf(l0x, h0x), fmaxf(fminf(l0y, h0y), fminf(l0z, h0z))));
-      float f0 = fminf(r.t, fminf(fmaxf(l0x, h0x), fminf(fmaxf(l0y, h0y), fmaxf(l0z, h0z))));
-      // child 1
-      float l1x = (b.x - ox) * ix, h1x = (b.y - ox) * ix;
-      float l1y = (b.z - oy) * iy, h1y = (b.w - oy) * iy;
-      float l1z = (c.z - oz) * iz, h1z = (c.w - oz) * iz;
-      float n1 = fmaxf(0.0f, fmaxf(fminf(l1x, h1x), fmaxf(fminf(l1y, h1y), fminf(l1z, h1z))));
-      float f1 = fminf(r.t, fminf(fmaxf(l1x, h1x), fminf(fmaxf(l1y, h1y), fmaxf(l1z, h1z))));
-      bool hit0 = d.z >= 0 && !(n0 > f0 * kBoxSlack);
-      bool hit1 = d.w >= 0 && !(n1 > f1 * kBoxSlack);
-      // a child record: link d.x/d.y, count d.z/d.w (>0 leaf, 0 internal, <0 empty)
-      if (hit0 && hit1) {
-        int first = d.x, firstc = d.z, second = d.y, secondc = d.w;
-        if (n1 < n0) { first = d.y; firstc = d.w; second = d.x; secondc = d.z; }
-        if (sp >= kStack) { atomicOr(err, kErrStack); return true; }
-        stack[sp++] = int((uint32_t(secondc) << 24) | uint32_t(second));  // far child: 8-bit count, 24-bit link
-        if (firstc > 0) { leaf_first = first; leaf_count = firstc; node = -1; }
-        else node = first;
-      } else if (hit0 || hit1) {
-        int link = hit0 ? d.x : d.y, cnt = hit0 ? d.z : d.w;
-        if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
-        else node = link;
-      } else {
-        if (sp == 0) return true;
-        const int e = stack[--sp];
-        const int cnt = int(uint32_t(e) >> 24), link = e & 0xFFFFFF;
-        if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
-        else node = link;
-      }
-    }
+    while (node >= 0 && leaf_count == 0)
+      if (visit(s, stack, err, n_nodes)) return true;
     // leaf: Moller-Trumbore, pathtrace.metal:150-158
     n_tests += uint32_t(leaf_count);
-    for (int k = 0; k < leaf_count; ++k) {
-      const float4* g = s.tgeo + size_t(leaf_first + k) * 3;
-      const float4 q0 = __ldg(g + 0);
-      const float4 q1 = __ldg(g + 1);
-      const float4 q2 = __ldg(g + 2);
-      const int j = __float_as_int(q0.w);
-      // p = cross(rd, e2)
-      float px = dy * q2.z - dz * q2.y;
-      float py = dz * q2.x - dx * q2.z;
-      float pz = dx * q2.y - dy * q2.x;
-      float det = q1.x * px + q1.y * py + q1.z * pz;
-      if (fabsf(det) < 1e-12f) continue;
-      float tx = ox - q0.x, ty = oy - q0.y, tz = oz - q0.z;
-      float u = (tx * px + ty * py + tz * pz) / det;
-      if (u < 0.0f || u > 1.0f) continue;
-      // q = cross(tv, e1)
-      float qx = ty * q1.z - tz * q1.y;
-      float qy = tz * q1.x - tx * q1.z;
-      float qz = tx * q1.y - ty * q1.x;
-      float v = (dx * qx + dy * qy + dz * qz) / det;
-      if (v < 0.0f || u + v > 1.0f) continue;
-      float dd = (q2.x * qx + q2.y * qy + q2.z * qz) / det;
-      if (dd > 1e-8f && (dd < r.t || (dd == r.t && r.tri >= 0 && j < r.tri))) {
-        r.t = dd; r.tri = j; r.u = u; r.v = v;
-        if (kAnyHit) return true;
-      }
-    }
+    for (int k = 0; k < leaf_count; ++k)
+      if (test_triangle(s.tgeo + size_t(leaf_first + k) * 3, ox, oy, oz, dx, dy, dz, r) && kAnyHit) return true;
     leaf_count = 0;
-    if (sp == 0) return true;
-    const int e = stack[--sp];
-    const int cnt = int(uint32_t(e) >> 24), link = e & 0xFFFFFF;
-    if (cnt > 0) { leaf_first = link; leaf_count = cnt; node = -1; }
-    else node = link;
+    return pop(stack);
+  }
+};
+
+// Traversal of the 8-wide compressed BVH built by rm_wide.cu.  A node is 5 x
+// float4: origin p (3 floats), the three scale exponents and the mask of
+// internal children (4 bytes), the index of its first internal child node and
+// of its first triangle record, one byte per child slot (0xFF empty, 0xFE
+// internal, else a leaf: bits 5-6 triangle count - 1, bits 0-4 offset from the
+// node's first triangle), and each child's box as 8-bit lo / hi per axis on the
+// grid p + q 2^e.  Boxes are dequantized with the same float expression the
+// builder checked to contain the true boxes, and culled with the slack rule of
+// the binary traversal, so the hits are the same as with any other BVH.
+// Child slots follow the octant of the child's centre in its parent: visiting
+// keys slot ^ octant(ray) in increasing order is near to far.  The stack holds
+// groups (first child node, remaining keys | internal mask << 8).
+constexpr int kWideStack = 32;
+
+// p + float(q) * scale for an 8-bit q, computed as one fused multiply-add: the
+// product of an integer below 256 and a power of two is exact, so the single
+// rounding of the fma equals the rounding of the separate add.  float(q) is
+// formed without a conversion instruction: 0x4B000000 | q is the float 2^23 + q.
+__device__ __forceinline__ float dequant(float p, uint32_t q, float scale) {
+  return __fmaf_rn(__uint_as_float(0x4B000000u | q) - 8388608.0f, scale, p);
+}
+
+// Byte b of `word` on the grid p + q scale (one byte permute, one add, one fma).
+template <int b>
+__device__ __forceinline__ float dequant_byte(uint32_t word, float p, float scale) {
+  return __fmaf_rn(__uint_as_float(__byte_perm(word, 0x4B000000u, 0x7540u | b)) - 8388608.0f, scale, p);
+}
+
+// Resumable traversal of the wide BVH: init() then step() until it returns
+// true.  A step visits one node (boxes of its 8 child slots) and tests the
+// triangles of the leaves it hit, popping a group first when the current one
+// is exhausted.
+struct WTrav {
+  float ox, oy, oz, dx, dy, dz, ix, iy, iz;
+  TraceResult r;
+  uint32_t oct, gbase, gbits;
+  int sp;
+
+  __device__ __forceinline__ void init(float ox_, float oy_, float oz_, float dx_, float dy_, float dz_, float tmax) {
+    ox = ox_; oy = oy_; oz = oz_; dx = dx_; dy = dy_; dz = dz_;
+    ix = 1.0f / (dx == 0.0f ? 1e-30f : dx);
+    iy = 1.0f / (dy == 0.0f ? 1e-30f : dy);
+    iz = 1.0f / (dz == 0.0f ? 1e-30f : dz);
+    r = TraceResult{tmax, -1, 0.f, 0.f};
+    oct = (dx < 0.0f ? 1u : 0u) | (dy < 0.0f ? 2u : 0u) | (dz < 0.0f ? 4u : 0u);
+    gbase = 0;
+    gbits = (1u << oct) | (1u << 8);  // the root: slot 0 of a virtual parent
+    sp = 0;
+  }
+
+  template <bool kAnyHit>
+  __device__ __forceinline__ bool step(const Scene& s, uint2* stack, uint32_t* err, uint32_t& n_nodes,
+                                       uint32_t& n_tests) {
+    if (s.n_nodes == 0) return true;
+    while (!(gbits & 0xFFu)) {
+      if (sp == 0) return true;
+      const uint2 e = stack[--sp];
+      gbase = e.x;
+      gbits = e.y;
+    }
+    const uint32_t k = __ffs(gbits & 0xFFu) - 1;
+    gbits &= ~(1u << k);
+    const uint32_t slot = k ^ oct;
+    const uint32_t node = gbase + __popc((gbits >> 8) & ((1u << slot) - 1u));
+    ++n_nodes;
+    const float4* nd = s.wnodes + size_t(node) * 5;
+    const float4 n0 = __ldg(nd + 0);
+    const uint4 n1 = __ldg(reinterpret_cast<const uint4*>(nd + 1));
+    const uint4 n2 = __ldg(reinterpret_cast<const uint4*>(nd + 2));
+    const uint4 n3 = __ldg(reinterpret_cast<const uint4*>(nd + 3));
+    const uint4 n4 = __ldg(reinterpret_cast<const uint4*>(nd + 4));
+    const uint32_t ew = __float_as_uint(n0.w);
+    const float sx = __uint_as_float((ew & 0xFFu) << 23);
+    const float sy = __uint_as_float(((ew >> 8) & 0xFFu) << 23);
+    const float sz = __uint_as_float(((ew >> 16) & 0xFFu) << 23);
+    // n1: child_base, tri_base, meta 0-3, meta 4-7; n2: qlo_x (8), qlo_y (8);
+    // n3: qlo_z (8), qhi_x (8); n4: qhi_y (8), qhi_z (8)
+    uint32_t ikeys = 0, tmask = 0;
+#define RM_WIDE_SLOT(J, H, B)                                                                              \
+  {                                                                                                        \
+    const uint32_t meta = (n1.H >> (8 * B)) & 0xFFu;                                                       \
+    if (meta != 0xFFu) {                                                                                   \
+      const float lx = (dequant_byte<B>(J < 4 ? n2.x : n2.y, n0.x, sx) - ox) * ix;                         \
+      const float hx = (dequant_byte<B>(J < 4 ? n3.z : n3.w, n0.x, sx) - ox) * ix;                         \
+      const float ly = (dequant_byte<B>(J < 4 ? n2.z : n2.w, n0.y, sy) - oy) * iy;                         \
+      const float hy = (dequant_byte<B>(J < 4 ? n4.x : n4.y, n0.y, sy) - oy) * iy;                         \
+      const float lz = (dequant_byte<B>(J < 4 ? n3.x : n3.y, n0.z, sz) - oz) * iz;                         \
+      const float hz = (dequant_byte<B>(J < 4 ? n4.z : n4.w, n0.z, sz) - oz) * iz;                         \
+      const float tn = fmaxf(0.0f, fmaxf(fminf(lx, hx), fmaxf(fminf(ly, hy), fminf(lz, hz))));            \
+      const float tf = fminf(r.t, fminf(fmaxf(lx, hx), fminf(fmaxf(ly, hy), fmaxf(lz, hz))));             \
+      if (!(tn > tf * kBoxSlack)) {                                                                        \
+        if (meta == 0xFEu) ikeys |= 1u << (uint32_t(J) ^ oct);                                             \
+        else tmask |= ((1u << ((meta >> 5) + 1u)) - 1u) << (meta & 31u);                                   \
+      }                                                                                                    \
+    }                                                                                                      \
+  }
+    RM_WIDE_SLOT(0, z, 0) RM_WIDE_SLOT(1, z, 1) RM_WIDE_SLOT(2, z, 2) RM_WIDE_SLOT(3, z, 3)
+    RM_WIDE_SLOT(4, w, 0) RM_WIDE_SLOT(5, w, 1) RM_WIDE_SLOT(6, w, 2) RM_WIDE_SLOT(7, w, 3)
+#undef RM_WIDE_SLOT
+    if (ikeys) {
+      // descend; the node's remaining siblings wait on the stack
+      if (gbits & 0xFFu) {
+        if (sp >= kWideStack) { atomicOr(err, kErrStack); return true; }
+        stack[sp++] = make_uint2(gbase, gbits);
+      }
+      gbase = n1.x;
+      gbits = ikeys | ((ew >> 24) << 8);
+    }
+    if (tmask) {
+      n_tests += uint32_t(__popc(tmask));
+      const float4* tg = s.wtgeo + size_t(n1.y) * 3;
+      do {
+        const uint32_t i = __ffs(tmask) - 1;
+        tmask &= tmask - 1u;
+        if (test_triangle(tg + size_t(i) * 3, ox, oy, oz, dx, dy, dz, r) && kAnyHit) return true;
+      } while (tmask);
+    }
     return false;
   }
 };
@@ -265,6 +403,14 @@ template <bool kAnyHit>
 __device__ __forceinline__ TraceResult traverse(const Scene& s, float ox, float oy, float oz, float dx, float dy,
                                                 float dz, float tmax, uint32_t* err, uint32_t& n_nodes,
                                                 uint32_t& n_tests) {
+  if (s.wnodes) {
+    WTrav t;
+    uint2 stack[kWideStack];
+    t.init(ox, oy, oz, dx, dy, dz, tmax);
+    while (!t.step<kAnyHit>(s, stack, err, n_nodes, n_tests)) {
+    }
+    return t.r;
+  }
   Trav t;
   int stack[kStack];
   t.init(ox, oy, oz, dx, dy, dz, tmax);

@@ -41,7 +41,7 @@ struct WfState {
 };
 // Queue slots of one wave: extension rays, shadow rays, then the paths to
 // shade sorted by vertex type (a: opaque hit, b: dielectric hit, c: no vertex).
-constexpr int kCntExt = 0, kCntShd = 1, kCntA = 2, kCntB = 3, kCntC = 4, kCntFetchExt = 5, kCntFetchShd = 6;
+constexpr int kCntExt = 0, kCntShd = 1, kCntA = 2, kCntB = 3, kCntC = 4;
 constexpr int kCntSlots = 8;
 struct WfQueues {
   int* ext;
@@ -59,6 +59,11 @@ cudaError_t launch_wavefront_trace(const Scene& s, const WfState& w, const WfQue
 cudaError_t launch_wavefront_shade(int vk, const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w,
                                    const WfQueues& cq, int bound, const WfQueues& nq, float* hdr, uint32_t* dbg,
                                    unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+// Run every path left in q (extension queue + queue c) to the end of its pixel.
+cudaError_t launch_wavefront_tail(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w,
+                                  const WfQueues& q, int bound, float* hdr, uint32_t* dbg, unsigned long long* ctr,
+                                  unsigned long long* ctr_ext, unsigned long long* ctr_shd, uint32_t* err,
+                                  cudaStream_t st);
 
 // rm_batch.cu: many plain-path images (reference K1 / K2) rendered together
 // by one pool of path slots.  A pixel owns `lanes` consecutive lane slots (its
@@ -175,6 +180,12 @@ struct DevBvh {
   int n_records = 0;
   int n_tris = 0;
   int max_depth = 0;
+  // 8-wide compressed BVH collapsed from the records (rm_wide.cu): 5 float4 per
+  // node, triangle records in its leaf order, frontier queues; n_wide 0: none
+  DevBuf wnodes, wtgeo, wq;
+  int* h_wcnt = nullptr;  // pinned counters read back per level
+  int n_wide = 0;
+  int wide_levels = 0;
 };
 
 // Convert and validate a caller BVH (reference Scene::nodes layout) on the
@@ -191,6 +202,10 @@ cudaError_t build_ploc(const rm_triangle* d_tris, int n_tris, int leaf_max, DevB
 cudaError_t pack_tgeo(const rm_triangle* d_tris, DevBvh& bvh, cudaStream_t st);
 // Refit all boxes bottom-up from the current triangle positions.
 cudaError_t refit_bvh(const rm_triangle* d_tris, DevBvh& bvh, cudaStream_t st);
+// Collapse the binary records into the 8-wide compressed BVH (rm_wide.cu).
+// Leaves n_wide at 0 (the binary BVH stays in use) when a node cannot be
+// encoded or the wide tree would be deeper than the traversal stack.
+cudaError_t build_wide(DevBvh& bvh, cudaStream_t st);
 // Caller-provided scratch of an LBVH build (device pointers; see rm_noalloc.cu).
 struct LbvhScratch {
   float4* records;        // (n-1) x 4 float4

@@ -268,30 +268,36 @@ __global__ void __launch_bounds__(256) k_wf_init(Scene s, Params p, uint64_t see
 }
 
 // Traversal of a queue of rays, one thread per ray (closest hit for extension
-// rays, pathtrace.metal:119-163; any hit for shadow rays, :164).  Finished
-// extension rays are sorted into the shading queue of their surface type.
-template <bool kShadowRays>
+// rays, pathtrace.metal:119-163; any hit for shadow rays, :164).  T is the
+// traversal (Trav: binary BVH, WTrav: wide BVH) and E / kDepth its stack.
+// Finished extension rays are sorted into the shading queue of their surface
+// type.  (Persistent grids whose idle lanes claim new rays, per leaf-to-leaf
+// step or per node / triangle, measured 7-70 % slower on the 720p frame.)
+template <bool kShadowRays, class T, class E, int kDepth>
 __global__ void __launch_bounds__(128) k_wf_trace(Scene s, WfState w, WfQueues q, unsigned long long* ctr,
                                                   uint32_t* err) {
   const int n = q.counts[kShadowRays ? kCntShd : kCntExt];
   const int* queue = kShadowRays ? q.shd : q.ext;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t nodes = 0, tests = 0, rays = 0;
-  int cls = -1;  // 0 opaque, 1 dielectric, 2 miss
+  int cls = -1;
   int id = 0;
   if (i < n) {
     id = queue[i];
     const float4 o = kShadowRays ? w.so[id] : w.o[id];
     const float4 d = kShadowRays ? w.sd[id] : w.d[id];
-    const TraceResult r = traverse<kShadowRays>(s, o.x, o.y, o.z, d.x, d.y, d.z, kShadowRays ? o.w : kFar, err,
-                                                 nodes, tests);
+    T t;
+    E stack[kDepth];
+    t.init(o.x, o.y, o.z, d.x, d.y, d.z, kShadowRays ? o.w : kFar);
+    while (!t.template step<kShadowRays>(s, stack, err, nodes, tests)) {
+    }
     rays = 1;
     if (kShadowRays) {
-      w.occ[id] = r.tri >= 0 ? 1u : 0u;
+      w.occ[id] = t.r.tri >= 0 ? 1u : 0u;
     } else {
-      w.hit[id] = make_float4(r.t, r.u, r.v, __int_as_float(r.tri));
+      w.hit[id] = make_float4(t.r.t, t.r.u, t.r.v, __int_as_float(t.r.tri));
       cls = 2;
-      if (r.tri >= 0) cls = __ldg(&s.tris[r.tri].ior) > 1.0001f ? 1 : 0;
+      if (t.r.tri >= 0) cls = __ldg(&s.tris[t.r.tri].ior) > 1.0001f ? 1 : 0;
     }
   }
   if (!kShadowRays) {
@@ -303,6 +309,61 @@ __global__ void __launch_bounds__(128) k_wf_trace(Scene s, WfState w, WfQueues q
   warp_add(ctr + 1, rays);
   warp_add(ctr + 2, nodes);
   warp_add(ctr + 3, tests);
+}
+
+// One path of a shading queue: fold in its shadow ray, shade the vertex its
+// extension ray found (VK 0 opaque, 1 dielectric) or end it (VK 2), finish and
+// restart samples; ext / shd / fin tell which queues of the next wave take it.
+template <int VK>
+__device__ __forceinline__ void shade_path(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w, int id,
+                                           float* __restrict__ hdr, uint32_t* __restrict__ dbg, uint32_t* err,
+                                           bool& ext, bool& shd, bool& fin, uint32_t& samples) {
+  const uint32_t x = uint32_t(id) % uint32_t(p.width), y = uint32_t(id) / uint32_t(p.width);
+  Tracer pt(s, p, err);
+  PathRegs r;
+  uint32_t n;
+  float sr, sg, sb;
+  load(w, uint32_t(id), r, pt.rng.state, n, sr, sg, sb);
+  const uint32_t n0 = n;
+  if (r.meta & kShadow) {
+    r.meta &= ~kShadow;
+    if (w.occ[id] == 0u) {
+      const float4 c = w.c[id];
+      r.ax += c.x; r.ay += c.y; r.az += c.z;
+    }
+  }
+  bool ended;
+  if (VK == 2) {
+    ended = true;  // a miss ends the path; a finishing path has now folded in its last shadow ray
+    r.meta &= ~(kExt | kFinish);
+  } else {
+    r.meta &= ~kExt;
+    const float4 hh = w.hit[id];
+    const TraceResult tr{hh.x, __float_as_int(hh.w), hh.y, hh.z};
+    const Hit hit = pt.attributes(tr, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz);
+    bool has_shadow = false;
+    float4 so, sd, c;
+    const bool go = vertex<VK>(pt, p, r, hit, has_shadow, so, sd, c);
+    if (has_shadow) {
+      w.so[id] = so; w.sd[id] = sd; w.c[id] = c;
+      r.meta |= kShadow;
+      shd = true;
+    }
+    if (go) { r.meta |= kExt; ext = true; }
+    ended = !go;
+    if (ended && has_shadow) { r.meta |= kFinish; ended = false; fin = true; }  // wait for the shadow ray
+  }
+  if (ended) {
+    finish_sample(p, w, uint32_t(id), r, n, sr, sg, sb);
+    if (start_samples(pt, p, gb, w, uint32_t(id), x, y, r, n, sr, sg, sb)) {
+      r.meta |= kExt;
+      ext = true;
+    } else {
+      write_pixel(p, uint32_t(id), (r.meta & kInd) != 0, n, sr, sg, sb, pt.rng.state, hdr, dbg);
+    }
+  }
+  samples += n - n0;
+  store(w, uint32_t(id), r, pt.rng.state, n, sr, sg, sb);
 }
 
 // Shade the paths of one queue: VK 0 opaque hits, 1 dielectric hits, 2 paths
@@ -321,57 +382,63 @@ __global__ void __launch_bounds__(256) k_wf_shade(Scene s, Params p, GBufSoA gb,
   uint32_t samples = 0;
   if (i < count) {
     id = queue[i];
-    const uint32_t x = uint32_t(id) % uint32_t(p.width), y = uint32_t(id) / uint32_t(p.width);
-    Tracer pt(s, p, err);
-    PathRegs r;
-    uint32_t n;
-    float sr, sg, sb;
-    load(w, uint32_t(id), r, pt.rng.state, n, sr, sg, sb);
-    const uint32_t n0 = n;
-    if (r.meta & kShadow) {
-      r.meta &= ~kShadow;
-      if (w.occ[id] == 0u) {
-        const float4 c = w.c[id];
-        r.ax += c.x; r.ay += c.y; r.az += c.z;
-      }
-    }
-    bool ended;
-    if (VK == 2) {
-      ended = true;  // a miss ends the path; a finishing path has now folded in its last shadow ray
-      r.meta &= ~(kExt | kFinish);
-    } else {
-      r.meta &= ~kExt;
-      const float4 hh = w.hit[id];
-      const TraceResult tr{hh.x, __float_as_int(hh.w), hh.y, hh.z};
-      const Hit hit = pt.attributes(tr, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz);
-      bool has_shadow = false;
-      float4 so, sd, c;
-      const bool go = vertex<VK>(pt, p, r, hit, has_shadow, so, sd, c);
-      if (has_shadow) {
-        w.so[id] = so; w.sd[id] = sd; w.c[id] = c;
-        r.meta |= kShadow;
-        shd = true;
-      }
-      if (go) { r.meta |= kExt; ext = true; }
-      ended = !go;
-      if (ended && has_shadow) { r.meta |= kFinish; ended = false; fin = true; }  // wait for the shadow ray
-    }
-    if (ended) {
-      finish_sample(p, w, uint32_t(id), r, n, sr, sg, sb);
-      if (start_samples(pt, p, gb, w, uint32_t(id), x, y, r, n, sr, sg, sb)) {
-        r.meta |= kExt;
-        ext = true;
-      } else {
-        write_pixel(p, uint32_t(id), (r.meta & kInd) != 0, n, sr, sg, sb, pt.rng.state, hdr, dbg);
-      }
-    }
-    samples = n - n0;
-    store(w, uint32_t(id), r, pt.rng.state, n, sr, sg, sb);
+    shade_path<VK>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
   }
   append(nq.ext, nq.counts + kCntExt, ext, id);
   append(nq.shd, nq.counts + kCntShd, shd, id);
   append(nq.qc, nq.counts + kCntC, fin, id);
   warp_add(ctr + 0, samples);
+}
+
+// The end of the wavefront loop, once few paths remain: one thread per
+// unfinished pixel runs its path to the end with the steps of the waves, in
+// their order (extension ray, pending shadow ray, shade_path of the vertex
+// type), so the pixel comes out the same, without a launch and a queue round
+// trip per vertex.  ctr: the stage counters of the tail, extension and
+// shadow traversal.
+__global__ void __launch_bounds__(128) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
+                                                 float* __restrict__ hdr, uint32_t* __restrict__ dbg,
+                                                 unsigned long long* ctr, unsigned long long* ctr_ext,
+                                                 unsigned long long* ctr_shd, uint32_t* err) {
+  const int n_ext = q.counts[kCntExt], n_c = q.counts[kCntC];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t samples = 0, rays_e = 0, nodes_e = 0, tests_e = 0, rays_s = 0, nodes_s = 0, tests_s = 0;
+  if (i < n_ext + n_c) {
+    const int id = i < n_ext ? q.ext[i] : q.qc[i - n_ext];
+    bool ext = i < n_ext;
+    for (;;) {
+      int vk = 2;
+      if (ext) {
+        const float4 o = w.o[id];
+        const float4 d = w.d[id];
+        const TraceResult r = traverse<false>(s, o.x, o.y, o.z, d.x, d.y, d.z, kFar, err, nodes_e, tests_e);
+        ++rays_e;
+        w.hit[id] = make_float4(r.t, r.u, r.v, __int_as_float(r.tri));
+        if (r.tri >= 0) vk = __ldg(&s.tris[r.tri].ior) > 1.0001f ? 1 : 0;
+      }
+      if (w.u[id].y & kShadow) {
+        const float4 o = w.so[id];
+        const float4 d = w.sd[id];
+        const TraceResult r = traverse<true>(s, o.x, o.y, o.z, d.x, d.y, d.z, o.w, err, nodes_s, tests_s);
+        ++rays_s;
+        w.occ[id] = r.tri >= 0 ? 1u : 0u;
+      }
+      bool shd = false, fin = false;
+      ext = false;
+      if (vk == 0) shade_path<0>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+      else if (vk == 1) shade_path<1>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+      else shade_path<2>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+      if (!ext && !fin) break;  // the pixel is written
+    }
+  }
+  __syncwarp();
+  warp_add(ctr + 0, samples);
+  warp_add(ctr_ext + 1, rays_e);
+  warp_add(ctr_ext + 2, nodes_e);
+  warp_add(ctr_ext + 3, tests_e);
+  warp_add(ctr_shd + 1, rays_s);
+  warp_add(ctr_shd + 2, nodes_s);
+  warp_add(ctr_shd + 3, tests_s);
 }
 
 }  // namespace
@@ -384,12 +451,30 @@ cudaError_t launch_wavefront_init(const Scene& s, const Params& p, uint64_t seed
   return cudaGetLastError();
 }
 
+template <bool kShadowRays, class T, class E, int kDepth>
+static cudaError_t trace_grid(const Scene& s, const WfState& w, const WfQueues& q, int bound, unsigned long long* ctr,
+                              uint32_t* err, cudaStream_t st) {
+  k_wf_trace<kShadowRays, T, E, kDepth><<<unsigned((bound + 127) / 128), 128, 0, st>>>(s, w, q, ctr, err);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_wavefront_trace(const Scene& s, const WfState& w, const WfQueues& q, int bound, bool shadow,
                                    unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
   if (bound <= 0) return cudaSuccess;
-  const unsigned g = unsigned((bound + 127) / 128);
-  if (shadow) k_wf_trace<true><<<g, 128, 0, st>>>(s, w, q, ctr, err);
-  else k_wf_trace<false><<<g, 128, 0, st>>>(s, w, q, ctr, err);
+  if (s.wnodes) {
+    if (shadow) return trace_grid<true, WTrav, uint2, kWideStack>(s, w, q, bound, ctr, err, st);
+    return trace_grid<false, WTrav, uint2, kWideStack>(s, w, q, bound, ctr, err, st);
+  }
+  if (shadow) return trace_grid<true, Trav, int, kStack>(s, w, q, bound, ctr, err, st);
+  return trace_grid<false, Trav, int, kStack>(s, w, q, bound, ctr, err, st);
+}
+
+cudaError_t launch_wavefront_tail(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w,
+                                  const WfQueues& q, int bound, float* hdr, uint32_t* dbg, unsigned long long* ctr,
+                                  unsigned long long* ctr_ext, unsigned long long* ctr_shd, uint32_t* err,
+                                  cudaStream_t st) {
+  if (bound <= 0) return cudaSuccess;
+  k_wf_tail<<<unsigned((bound + 127) / 128), 128, 0, st>>>(s, p, gb, w, q, hdr, dbg, ctr, ctr_ext, ctr_shd, err);
   return cudaGetLastError();
 }
 

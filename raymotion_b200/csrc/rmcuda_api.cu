@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -46,6 +47,17 @@ std::string cuda_msg(const char* what, cudaError_t e) { return std::string(what)
 namespace {
 
 constexpr int kLbvhLeaf = 4;
+
+// The 8-wide compressed BVH, collapsed from the binary one (rm_wide.cu), when
+// RAYMOTION_CUDA_WIDE=1: traversal then uses it instead of the binary BVH.  It
+// visits a third of the nodes, but its exact box decoding costs more per ray
+// than the binary BVH's fetches on the bench scene, so the binary BVH is the
+// default.
+cudaError_t finish_wide(rmd::DevBvh& bvh, cudaStream_t st) {
+  const char* v = std::getenv("RAYMOTION_CUDA_WIDE");
+  if (!v || std::string(v) != "1") { bvh.n_wide = 0; return cudaSuccess; }
+  return rmd::build_wide(bvh, st);
+}
 
 // Device BVH builder: PLOC clustering (default) or LBVH (RAYMOTION_CUDA_BVH=lbvh);
 // RAYMOTION_CUDA_BVH_LEAF sets the maximum triangles per leaf (default 4).
@@ -121,6 +133,10 @@ Scene scene_view(const DevScene& sc) {
   s.guide = sc.guide.as<int32_t>();
   s.guide_n = sc.guide_n;
   s.guide_inv = sc.guide_inv;
+  if (sc.n_tris > 0 && sc.bvh.n_wide > 0) {
+    s.wnodes = sc.bvh.wnodes.as<float4>();
+    s.wtgeo = sc.bvh.wtgeo.as<float4>();
+  }
   return s;
 }
 
@@ -210,6 +226,10 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
     sc.bvh.n_records = 0;
     sc.bvh.n_tris = 0;
   }
+  if ((e = finish_wide(sc.bvh, st)) != cudaSuccess) {
+    msg = cuda_msg("wide BVH build failed", e);
+    return RM_ERR_CUDA;
+  }
   sc.have_scene = true;
   return RM_OK;
 }
@@ -271,6 +291,18 @@ cudaError_t ensure_wavefront(rmcuda_ctx* c, size_t npix) {
 
 // ReSTIR shading as wavefront stages (rm_wavefront.cu): init, then waves of
 // extend / shadow / shade until no path is left.
+// Unfinished paths at or below which the wavefront loop hands its last paths
+// to one tail launch: a tenth of the paths of the first wave (on the 720p bench
+// frame a tenth to a twentieth measured best; below it the waves run with
+// the GPU mostly idle, above it the tail's one-thread-per-pixel loop is slower
+// than the waves).  RAYMOTION_CUDA_TAIL sets a fixed count; 0 keeps the waves
+// to the end.
+static int tail_paths(int first_bound) {
+  const char* v = std::getenv("RAYMOTION_CUDA_TAIL");
+  if (v) return std::max(0, std::atoi(v));
+  return first_bound / 10;
+}
+
 cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, uint64_t seed, std::string& msg) {
   const size_t npix = size_t(p.width) * size_t(p.height);
   cudaStream_t st = c->stream;
@@ -305,6 +337,8 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
   // device.
   const int kBatch = 4;
   const uint64_t max_waves = uint64_t(p.spp) * uint64_t(p.bounces + 2) * 4 + 64;
+  std::chrono::steady_clock::time_point t0;
+  int tail = 0;
   for (uint64_t wave = 0;;) {
     if (wave > max_waves) { msg = "wavefront did not drain"; return cudaErrorLaunchFailure; }
     if ((e = cudaMemcpyAsync(c->h_counts, counts + kCntSlots * cur, kCntSlots * sizeof(int), cudaMemcpyDeviceToHost,
@@ -314,8 +348,27 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
       return e;
     }
     const int bound = c->h_counts[kCntExt] + c->h_counts[kCntC];
+    const auto now = std::chrono::steady_clock::now();
+    if (wave == 0) {
+      t0 = now;
+      tail = tail_paths(bound);
+    }
+    c->wave_log.insert(c->wave_log.end(), {bound, c->h_counts[kCntExt], c->h_counts[kCntShd],
+                                           int(std::chrono::duration_cast<std::chrono::microseconds>(now - t0).count())});
     if (bound == 0) break;
-    c->wave_log.insert(c->wave_log.end(), {bound, c->h_counts[kCntExt], c->h_counts[kCntShd]});
+    if (bound <= tail) {
+      e = staged2(c, RM_STAGE_WF_TAIL, [&] {
+        return launch_wavefront_tail(s, p, c->gb.view(), w, q[cur], bound, c->hdr.as<float>(), c->dbg.as<uint32_t>(),
+                                     ctr + 4 * RM_STAGE_WF_SHADE, ctr + 4 * RM_STAGE_WF_EXTEND,
+                                     ctr + 4 * RM_STAGE_WF_SHADOW, err, st);
+      });
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) { msg = cuda_msg("wavefront tail failed", e); return e; }
+      // the end of the tail, as a last record with empty queues
+      c->wave_log.insert(c->wave_log.end(), {0, 0, 0, int(std::chrono::duration_cast<std::chrono::microseconds>(
+                                                              std::chrono::steady_clock::now() - t0).count())});
+      break;
+    }
     for (int k = 0; k < kBatch; ++k, ++wave) {
       c->waves++;
       const WfQueues& Q = q[cur];
@@ -584,6 +637,11 @@ int rmcuda_scene_update(rmcuda_ctx* c, const rm_triangle* tris, int32_t n, int32
     c->sc.refits++;
     if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("refit failed", e)); return RM_ERR_CUDA; }
   }
+  // the wide nodes are collapsed again from the refitted or rebuilt records
+  if ((e = finish_wide(c->sc.bvh, c->stream)) != cudaSuccess) {
+    set_err(err, errcap, cuda_msg("wide BVH build failed", e));
+    return RM_ERR_CUDA;
+  }
   return RM_OK;
 }
 
@@ -746,6 +804,7 @@ int rmcuda_stats_get(rmcuda_ctx* c, rm_stats* out) {
   out->kernel_launches = c->launches;
   out->device_error = e32;
   out->kernel_chain = uint32_t(c->last_chain);
+  out->bvh_node_bytes = c->sc.bvh.n_wide > 0 ? 80u : 64u;
   return RM_OK;
 }
 
@@ -759,8 +818,8 @@ int rmcuda_profile(rmcuda_ctx* c, int level) {
 int rmcuda_wave_log(rmcuda_ctx* c, int32_t* out, int32_t cap) {
   if (!c || cap < 0) return -1;
   std::lock_guard<std::mutex> lk(c->mu);
-  const int waves = int(c->wave_log.size() / 3);
-  for (int i = 0; i < waves * 3 && i < cap * 3; ++i) out[i] = c->wave_log[size_t(i)];
+  const int waves = int(c->wave_log.size() / 4);
+  for (int i = 0; i < waves * 4 && i < cap * 4; ++i) out[i] = c->wave_log[size_t(i)];
   return waves;
 }
 

@@ -73,3 +73,49 @@ def test_refit_and_rebuild_track_moved_geometry(backend, oracle, field, use_node
                                                 verts64=np.concatenate([moved["v0"], moved["v1"], moved["v2"]],
                                                                        axis=1).astype(np.float64)))
         assert _check_hits(backend, oracle, ms, rays) > 0.2, step
+
+
+@pytest.mark.parametrize("builder", ["ploc", "lbvh"])
+def test_wide_bvh_hits_equal_binary_and_oracle(backend, oracle, field, builder, monkeypatch):
+    """The 8-wide compressed BVH (collapsed from the device build) answers
+    closest-hit and any-hit queries exactly as the binary BVH and the oracle,
+    also after a refit, whose records it is collapsed again from."""
+    monkeypatch.setenv("RAYMOTION_CUDA_BVH", builder)
+    sc = oracle.with_reference_bvh(field)
+    rays = np.concatenate([random_rays(30000, [-22, -1, -22], [22, 12, 22], 7),
+                           random_rays(5000, [-22, -1, -22], [22, 12, 22], 8, tmax=3.0)])
+    out = {}
+    for wide in ("1", "0"):
+        monkeypatch.setenv("RAYMOTION_CUDA_WIDE", wide)
+        backend.upload(sc, use_nodes=False)
+        backend.render(sc, *_tiny_view(), use_nodes=False)  # stats come from the resident scene
+        assert backend.stats()["bvh_node_bytes"] == (80 if wide == "1" else 64)
+        out[wide] = (_trace_gpu(backend, rays), _trace_gpu(backend, rays, any_hit=True))
+    (w_tri, w_t, w_u, w_v), (w_any, _, _, _) = out["1"]
+    (b_tri, b_t, b_u, b_v), (b_any, _, _, _) = out["0"]
+    hit = b_tri >= 0
+    assert hit.mean() > 0.2
+    assert np.array_equal(w_tri, b_tri)
+    for a, b in ((w_t, b_t), (w_u, b_u), (w_v, b_v)):
+        assert np.array_equal(a[hit].view(np.uint32), b[hit].view(np.uint32))
+    assert np.array_equal(w_any >= 0, b_any >= 0)
+    assert _check_hits(backend, oracle, sc, rays) > 0.2
+    # moved geometry: refit, then the wide nodes are collapsed again
+    monkeypatch.setenv("RAYMOTION_CUDA_WIDE", "1")
+    backend.upload(sc, use_nodes=False)
+    moved = _moved(sc, 0.37)
+    backend.update(moved, rebuild_every=0)
+    msc = oracle.with_reference_bvh(type(sc)(tris=moved, light_tri=sc.light_tri, light_cdf=sc.light_cdf,
+                                              light_total=sc.light_total, texels=sc.texels,
+                                              verts64=_verts64(moved)))
+    assert _check_hits(backend, oracle, msc, rays) > 0.2
+
+
+def _tiny_view():
+    from raymotion_b200.scene import Camera, RenderConfig
+    cam = Camera().set((0.0, 9.0, -34.0), (14.0, 0.0, 0.0), 60)
+    return cam, RenderConfig(width=8, height=8, spp=1, max_bounces=1)
+
+
+def _verts64(tris):
+    return np.concatenate([tris["v0"], tris["v1"], tris["v2"]], axis=1).astype(np.float64)

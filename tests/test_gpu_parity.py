@@ -109,10 +109,19 @@ def _restir_cfg(flags=0):
                         restir_spatial=4, restir_radius=12.0, flags=flags)
 
 
-@pytest.mark.parametrize("shading", ["wavefront", "megakernel"])
+@pytest.mark.parametrize("shading", ["wavefront", "wavefront-no-tail", "wavefront-all-tail", "wavefront-wide",
+                                     "megakernel"])
 def test_restir_chain_matches_oracle(backend, oracle, small_field, shading, monkeypatch):
     if shading == "megakernel":
         monkeypatch.setenv("RAYMOTION_CUDA_MEGAKERNEL", "1")
+    if shading == "wavefront-wide":
+        monkeypatch.setenv("RAYMOTION_CUDA_WIDE", "1")  # every traversal on the 8-wide BVH
+    # the wavefront loop hands its last paths to one tail launch; "no-tail"
+    # runs waves to the end, "all-tail" hands over every path at the first read
+    if shading == "wavefront-no-tail":
+        monkeypatch.setenv("RAYMOTION_CUDA_TAIL", "0")
+    if shading == "wavefront-all-tail":
+        monkeypatch.setenv("RAYMOTION_CUDA_TAIL", "1000000000")
     sc, cam, _ = small_field
     cfg = _restir_cfg(_abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_DENOISE_OFF)
     o = oracle.Oracle()
