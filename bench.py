@@ -87,7 +87,7 @@ def workload(name: str):
     scene = sb.pack()
     desc.update(triangles=int(scene.n_tris), width=cfg.width, height=cfg.height, spp=cfg.spp,
                 max_depth=cfg.max_bounces, l2="inputs larger than L2 (scene 181 MB + 49 MB BVH leaf records)",
-                bvh="device LBVH (4-triangle leaves)")
+                bvh="device PLOC BVH (leaves of at most 4 triangles)")
     return scene, cam, cfg, desc
 
 

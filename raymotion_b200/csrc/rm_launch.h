@@ -60,6 +60,8 @@ cudaError_t launch_wavefront_shade(int vk, const Scene& s, const Params& p, cons
                                    const WfQueues& cq, int bound, const WfQueues& nq, float* hdr, uint32_t* dbg,
                                    unsigned long long* ctr, uint32_t* err, cudaStream_t st);
 // Run every path left in q (extension queue + queue c) to the end of its pixel.
+// wavefront_tail_capacity: the paths one wave of resident tail blocks holds.
+int wavefront_tail_capacity(bool opaque);
 cudaError_t launch_wavefront_tail(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w,
                                   const WfQueues& q, int bound, float* hdr, uint32_t* dbg, unsigned long long* ctr,
                                   unsigned long long* ctr_ext, unsigned long long* ctr_shd, uint32_t* err,

@@ -314,7 +314,8 @@ __global__ void __launch_bounds__(128) k_wf_trace(Scene s, WfState w, WfQueues q
 // One path of a shading queue: fold in its shadow ray, shade the vertex its
 // extension ray found (VK 0 opaque, 1 dielectric) or end it (VK 2), finish and
 // restart samples; ext / shd / fin tell which queues of the next wave take it.
-template <int VK>
+// NEE: the NEE variant of vertex() (2 in opaque scenes, 1 otherwise).
+template <int VK, int NEE>
 __device__ __forceinline__ void shade_path(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w, int id,
                                            float* __restrict__ hdr, uint32_t* __restrict__ dbg, uint32_t* err,
                                            bool& ext, bool& shd, bool& fin, uint32_t& samples) {
@@ -343,7 +344,7 @@ __device__ __forceinline__ void shade_path(const Scene& s, const Params& p, cons
     const Hit hit = pt.attributes(tr, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz);
     bool has_shadow = false;
     float4 so, sd, c;
-    const bool go = vertex<VK>(pt, p, r, hit, has_shadow, so, sd, c);
+    const bool go = vertex<VK, NEE>(pt, p, r, hit, has_shadow, so, sd, c);
     if (has_shadow) {
       w.so[id] = so; w.sd[id] = sd; w.c[id] = c;
       r.meta |= kShadow;
@@ -370,7 +371,7 @@ __device__ __forceinline__ void shade_path(const Scene& s, const Params& p, cons
 // without a vertex (the ray missed, or the path ended and waited for its last
 // shadow ray).  Specialising on the vertex type keeps the warps' lanes on the
 // same branch.
-template <int VK>
+template <int VK, int NEE>
 __global__ void __launch_bounds__(256) k_wf_shade(Scene s, Params p, GBufSoA gb, WfState w, WfQueues cq,
                                                   WfQueues nq, float* __restrict__ hdr, uint32_t* __restrict__ dbg,
                                                   unsigned long long* ctr, uint32_t* err) {
@@ -382,7 +383,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(Scene s, Params p, GBufSoA gb,
   uint32_t samples = 0;
   if (i < count) {
     id = queue[i];
-    shade_path<VK>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+    shade_path<VK, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
   }
   append(nq.ext, nq.counts + kCntExt, ext, id);
   append(nq.shd, nq.counts + kCntShd, shd, id);
@@ -396,7 +397,8 @@ __global__ void __launch_bounds__(256) k_wf_shade(Scene s, Params p, GBufSoA gb,
 // type), so the pixel comes out the same, without a launch and a queue round
 // trip per vertex.  ctr: the stage counters of the tail, extension and
 // shadow traversal.
-__global__ void __launch_bounds__(128) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
+template <int NEE>
+__global__ void __launch_bounds__(128, 4) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
                                                  float* __restrict__ hdr, uint32_t* __restrict__ dbg,
                                                  unsigned long long* ctr, unsigned long long* ctr_ext,
                                                  unsigned long long* ctr_shd, uint32_t* err) {
@@ -425,9 +427,9 @@ __global__ void __launch_bounds__(128) k_wf_tail(Scene s, Params p, GBufSoA gb, 
       }
       bool shd = false, fin = false;
       ext = false;
-      if (vk == 0) shade_path<0>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
-      else if (vk == 1) shade_path<1>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
-      else shade_path<2>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+      if (vk == 0) shade_path<0, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+      else if (vk == 1) shade_path<1, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+      else shade_path<2, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
       if (!ext && !fin) break;  // the pixel is written
     }
   }
@@ -469,12 +471,29 @@ cudaError_t launch_wavefront_trace(const Scene& s, const WfState& w, const WfQue
   return trace_grid<false, Trav, int, kStack>(s, w, q, bound, ctr, err, st);
 }
 
+int wavefront_tail_capacity(bool opaque) {
+  static int cap[2] = {0, 0};
+  int& c = cap[opaque ? 1 : 0];
+  if (c == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, opaque ? k_wf_tail<2> : k_wf_tail<1>, 128, 0) !=
+            cudaSuccess)
+      return 0;
+    c = sms * per_sm * 128;
+  }
+  return c;
+}
+
 cudaError_t launch_wavefront_tail(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w,
                                   const WfQueues& q, int bound, float* hdr, uint32_t* dbg, unsigned long long* ctr,
                                   unsigned long long* ctr_ext, unsigned long long* ctr_shd, uint32_t* err,
                                   cudaStream_t st) {
   if (bound <= 0) return cudaSuccess;
-  k_wf_tail<<<unsigned((bound + 127) / 128), 128, 0, st>>>(s, p, gb, w, q, hdr, dbg, ctr, ctr_ext, ctr_shd, err);
+  const unsigned g = unsigned((bound + 127) / 128);
+  if (p.opaque) k_wf_tail<2><<<g, 128, 0, st>>>(s, p, gb, w, q, hdr, dbg, ctr, ctr_ext, ctr_shd, err);
+  else k_wf_tail<1><<<g, 128, 0, st>>>(s, p, gb, w, q, hdr, dbg, ctr, ctr_ext, ctr_shd, err);
   return cudaGetLastError();
 }
 
@@ -483,9 +502,15 @@ cudaError_t launch_wavefront_shade(int vk, const Scene& s, const Params& p, cons
                                    unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
   if (bound <= 0) return cudaSuccess;
   const unsigned g = unsigned((bound + 255) / 256);
-  if (vk == 0) k_wf_shade<0><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
-  else if (vk == 1) k_wf_shade<1><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
-  else k_wf_shade<2><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+  if (p.opaque) {
+    if (vk == 0) k_wf_shade<0, 2><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+    else if (vk == 1) k_wf_shade<1, 2><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+    else k_wf_shade<2, 2><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+  } else {
+    if (vk == 0) k_wf_shade<0, 1><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+    else if (vk == 1) k_wf_shade<1, 1><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+    else k_wf_shade<2, 1><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+  }
   return cudaGetLastError();
 }
 

@@ -58,7 +58,8 @@ __device__ __forceinline__ void clamp3(const Params& p, float& r, float& g, floa
 // it tests visibility itself and adds the light at once.
 // MAT 0: opaque surface, 1: dielectric (hit.ior > 1.0001).  NEE 0: the scene
 // is opaque and NEE takes one candidate (the single-candidate branch inlined);
-// 1: any scene and candidate count.
+// 1: any scene and candidate count; 2: an opaque scene, any candidate count
+// (without the in-place shadow test of partially transparent scenes).
 template <int MAT, int NEE = 1>
 __device__ bool vertex(Tracer& pt, const Params& p, PathRegs& r, const Hit& hit, bool& has_shadow, float4& so,
                        float4& sd, float4& c) {
@@ -135,7 +136,7 @@ __device__ bool vertex(Tracer& pt, const Params& p, PathRegs& r, const Hit& hit,
     if (metallic >= 0.999f) spec_prob = 1.0f;
     float dlr, dlg, dlb, cur_sumW;
     uint32_t cur_M;
-    if (NEE == 0 || p.opaque) {
+    if (NEE != 1 || p.opaque) {
       float sdist, sox, soy, soz, sdx, sdy, sdz;
       bool has_ray;
       if (NEE == 0)
@@ -152,7 +153,7 @@ __device__ bool vertex(Tracer& pt, const Params& p, PathRegs& r, const Hit& hit,
         sd = make_float4(sdx, sdy, sdz, 0.f);
         c = make_float4(dlr * r.tx, dlg * r.ty, dlb * r.tz, 0.f);
       }
-    } else {
+    } else if (NEE == 1) {
       // partially transparent scene: the shadow test draws random numbers
       // (pathtrace.metal:536-550), so it runs here, in stream order
       pt.direct_lighting(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob, hit.ar,

@@ -295,12 +295,13 @@ cudaError_t ensure_wavefront(rmcuda_ctx* c, size_t npix) {
 // to one tail launch: a tenth of the paths of the first wave (on the 720p bench
 // frame a tenth to a twentieth measured best; below it the waves run with
 // the GPU mostly idle, above it the tail's one-thread-per-pixel loop is slower
-// than the waves).  RAYMOTION_CUDA_TAIL sets a fixed count; 0 keeps the waves
-// to the end.
-static int tail_paths(int first_bound) {
+// than the waves), and no more than one wave of resident tail blocks holds (a
+// second wave of blocks would run after the first, doubling the tail).
+// RAYMOTION_CUDA_TAIL sets a fixed count; 0 keeps the waves to the end.
+static int tail_paths(int first_bound, bool opaque) {
   const char* v = std::getenv("RAYMOTION_CUDA_TAIL");
   if (v) return std::max(0, std::atoi(v));
-  return first_bound / 10;
+  return std::min(first_bound / 10, rmd::wavefront_tail_capacity(opaque));
 }
 
 cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, uint64_t seed, std::string& msg) {
@@ -351,7 +352,7 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
     const auto now = std::chrono::steady_clock::now();
     if (wave == 0) {
       t0 = now;
-      tail = tail_paths(bound);
+      tail = tail_paths(bound, p.opaque != 0);
     }
     c->wave_log.insert(c->wave_log.end(), {bound, c->h_counts[kCntExt], c->h_counts[kCntShd],
                                            int(std::chrono::duration_cast<std::chrono::microseconds>(now - t0).count())});
