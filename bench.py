@@ -32,6 +32,7 @@ Reported on one JSON line (rank 0):
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import datetime
 import json
 import os
@@ -66,6 +67,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-serial measurement")
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--no-sequence", action="store_true", help="skip the animated-sequence measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-rendering measurement")
     ap.add_argument("--fit-iters", type=int, default=200)
     return ap.parse_args()
@@ -455,6 +457,104 @@ def adjoint_measure(args, backend, torch, stream, dev):
                  loss_first10=float(np.mean(loss_curve[:10])), loss_last10=float(np.mean(loss_curve[-10:]))))
 
 
+def sequence_measure(args, backend, torch, stream, dev):
+    """The animated sequence: 34 frames at 1280x720, 16 spp, temporal ReSTIR and
+    denoise on animated geometry (RM_FLAG_ANIMATED_HISTORY).  Per frame: the
+    cloth model's new triangles uploaded (rmcuda_model_update, 36 MB from host
+    memory), the world of 203 instances built on the device with the BVH
+    refitted, or rebuilt every 32nd commit (rmcuda_instances_commit), and the
+    frame rendered (rmcuda_render_resident_async).  The cloth frames are
+    generated before the timed loop (the animation itself is the caller's).
+    value = path samples over the sequence / its wall time, measured with CUDA
+    events around the whole loop on the rendering stream.
+    """
+    import raymotion_b200 as rb
+    from raymotion_b200 import objects
+    from raymotion_b200.scenes import AnimatedSequence
+    seq = AnimatedSequence()
+    cfg = seq.cfg
+    cloth = [seq.cloth(f) for f in range(seq.frames)]
+    recs = [objects.instance_records(seq.instances(f)) for f in range(seq.frames)]
+    cams = [seq.camera(f) for f in range(seq.frames)]
+    ids = [backend.model_create(m) for m in seq.models]
+    for r in recs:
+        r["model"] = np.asarray(ids, np.int32)[r["model"]]
+    npix = cfg.width * cfg.height
+    d_rgb = torch.empty(npix * 3, dtype=torch.uint8, device=dev)
+    # warm-up: the first frames of the sequence, once
+    backend.reset_history()
+    for f in range(2):
+        backend.model_update(ids[seq.CLOTH], cloth[f])
+        backend.instances_commit(recs[f], rebuild_every=32)
+        backend.render_resident_async(cams[f], cfg, 12345 + f, d_rgb.data_ptr())
+    backend.sync()
+    backend.reset_history()
+    backend.stats_reset()
+    backend.profile(1)
+    st0 = backend.stats()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for f in range(seq.frames):
+        backend.model_update(ids[seq.CLOTH], cloth[f])
+        backend.instances_commit(recs[f], rebuild_every=32)
+        backend.render_resident_async(cams[f], cfg, 12345 + f, d_rgb.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    secs = e0.elapsed_time(e1) / 1e3
+    st = backend.stats()
+    t = backend.stage_times()
+    backend.profile(0)
+    samples = st["path_samples"]
+    render_ms = sum(v[0] for k, v in t.items() if k not in ("prep", "batch", "adjoint"))
+    return dict(workload=f"animated sequence: {seq.frames} frames at {seq.fps} fps, {cfg.width}x{cfg.height}, "
+                         f"{cfg.spp} spp, depth {cfg.max_bounces}, {seq.n_tris:,} triangles ({len(seq.moving)} moving "
+                         f"spheres, {len(cloth[0]):,}-triangle cloth), camera orbit {seq.orbit_deg} deg/frame, temporal "
+                         "ReSTIR + denoise on animated geometry",
+                value=samples / secs, unit="path samples/s", frames=seq.frames, ms_per_frame=1e3 * secs / seq.frames,
+                wall_ms_per_frame=1e3 * wall / seq.frames, prep_ms_per_frame=t["prep"][0] / seq.frames,
+                render_ms_per_frame=render_ms / seq.frames, bvh_builds=st["bvh_builds"] - st0["bvh_builds"],
+                bvh_refits=st["bvh_refits"] - st0["bvh_refits"], h2d_bytes_per_frame=int(cloth[0].nbytes + recs[0].nbytes),
+                path_samples=int(samples))
+
+
+def screen_space_large(backend, torch, cam, cfg, dev, seed0, peak):
+    """The screen-space passes where their working set exceeds L2.
+
+    2048x1280 is the largest 16:10 frame whose ReSTIR buffers stay within the
+    reference's 512 MiB limit (76 + 2 x 60 B per pixel, metal.mm:236-237); past
+    it the reference drops ReSTIR and the denoiser.  1 spp keeps the frame
+    cheap: the passes' work does not depend on spp.  Two frames build the
+    temporal history, then five are timed per stage (events on the rendering
+    stream): temporal 92 B/px, two a-trous passes 64 B/px each, tonemap write
+    3 B/px, 223 B/px in all (585 MB per frame, above the 126 MB L2).
+    """
+    big = dataclasses.replace(cfg, width=2048, height=1280, spp=1)
+    npix = big.width * big.height
+    d_rgb = torch.empty(npix * 3, dtype=torch.uint8, device=dev)
+    for i in range(2):
+        backend.render_resident_async(cam, big, seed0 + i, d_rgb.data_ptr())
+    backend.sync()
+    backend.stats_reset()
+    backend.profile(1)
+    frames = 5
+    for i in range(frames):
+        backend.render_resident_async(cam, big, seed0 + 2 + i, d_rgb.data_ptr())
+    backend.sync()
+    t = backend.stage_times()
+    backend.profile(0)
+    ms = sum(t[k][0] for k in ("temporal", "atrous0", "atrous1")) / frames
+    if ms <= 0:
+        return None
+    nbytes = npix * (92 + 64 + 64 + 3)
+    ach = nbytes / (ms / 1e3) / 1e9
+    return dict(bound="hbm", kernels="k_denoise_temporal_tiled + k_denoise_atrous_tiled x2", width=big.width,
+                height=big.height, achieved=ach, peak=peak["hbm_gbs"], unit="GB/s", frac=ach / peak["hbm_gbs"],
+                us_per_frame=ms * 1e3, bytes_per_frame=nbytes, peak_source=peak["source"])
+
+
 def run_b200(args, world, rank, local):
     import torch
 
@@ -574,6 +674,7 @@ def run_b200(args, world, rank, local):
             e.update(rays=rc["rays"], nodes_per_ray=rc["nodes_visited"] / rc["rays"],
                      tests_per_ray=rc["tris_tested"] / rc["rays"], mrays_per_s=rc["rays"] / (v[0] * 1e3))
         kernel_summary[k] = e
+    ss_large = screen_space_large(backend, torch, cam, cfg, dev, seed0 + 300, peak)
     # ---- end to end through rmcuda_render with host buffers
     e2e = None
     if not args.no_e2e:
@@ -603,6 +704,8 @@ def run_b200(args, world, rank, local):
                    ms_per_step=1e3 * esec / args.steps)
     # ---- batched vs serial rendering of many uneven scenes
     batch = None if args.no_batch else batch_compare(args, backend, torch, stream, dev, world)
+    # ---- the animated sequence: device scene preparation + refit per frame
+    sequence = None if args.no_sequence else sequence_measure(args, backend, torch, stream, dev)
     # ---- differentiable rendering: adjoint cost and a 200-step fit
     adjoint = None if args.no_adjoint else adjoint_measure(args, backend, torch, stream, dev)
     # ---- CPU baseline (rank 0, N=1)
@@ -618,7 +721,8 @@ def run_b200(args, world, rank, local):
                     mrays_per_s=rays_sum / secs_max / 1e6, e2e=e2e, roofline=roofline, cpu_baseline=cpu,
                     gpu_launches=int(st["kernel_launches"]), clocks=clk, stages=stage_summary,
                     kernels_one_frame=kernel_summary, wavefront=wave_summary, roofline_screen_space=roofline_ss,
-                    batch=batch, adjoint=adjoint)
+                    roofline_screen_space_large=ss_large,
+                    batch=batch, adjoint=adjoint, sequence=sequence)
         print(json.dumps(line), flush=True)
     backend.close()
     return 0

@@ -131,6 +131,8 @@ typedef struct rm_stats {
   uint32_t device_error;    /* last nonzero device error word, 0 if none */
   uint32_t kernel_chain;    /* 1 = render_paths, 8/32 = lane kernels, 2 = ReSTIR chain */
   uint32_t bvh_node_bytes;  /* bytes of one node visit: 80 (8-wide compressed BVH) or 64 (binary) */
+  uint32_t bvh_builds;      /* device BVH builds of the resident scene since the context was created */
+  uint32_t bvh_refits;      /* device BVH refits of the resident scene since the context was created */
 } rm_stats;
 
 typedef struct rmcuda_ctx rmcuda_ctx;
@@ -168,6 +170,60 @@ int rmcuda_scene_upload(rmcuda_ctx* ctx, const rm_scene_view* scene, char* err, 
  * `rebuild_every` refits (0 = never) the BVH is rebuilt instead. */
 int rmcuda_scene_update(rmcuda_ctx* ctx, const rm_triangle* tris, int32_t n_tris,
                         int32_t rebuild_every, char* err, size_t errcap);
+
+/* ---- Device-side scene preparation (the reference's Objects runtime,
+ * include/raymotion/runtime.hpp:20-146).  A model holds object-space
+ * triangles as Objects::init leaves them: the fields of the reference's
+ * Triangle that Objects::append reads (fp64).  rmcuda_instances_commit does on
+ * the device what Objects::render does on the host before each frame
+ * (runtime.hpp:121-131): every model triangle of every instance, in push
+ * order, is scaled, rotated about x then y then z, and translated; its vertex
+ * normals are divided by the scale, rotated and normalised (runtime.hpp:86-113);
+ * the instance's material overrides apply; Scene::add_triangle's precompute,
+ * degenerate-triangle rejection and emissive CDF follow (scene.cpp:16-87); the
+ * triangles are packed as rm_triangle and become the resident scene.  Its BVH
+ * is refitted when the instances name the same models in the same order as
+ * the previous commit and the commit count is not a multiple of
+ * `rebuild_every` (the reference uses 32), else built; the first commit
+ * builds. */
+typedef struct rm_model_tri {
+  double v0[3], v1[3], v2[3], n0[3], n1[3], n2[3];
+  double tu0, tv0, tu1, tv1, tu2, tv2;
+  double ar, ag, ab, er, eg, eb, metallic, ior, rough, alpha;
+  int32_t shader;
+  int32_t reserved;
+} rm_model_tri; /* 280 bytes */
+
+/* One Objects::push (runtime.hpp:76-84).  The caller passes the rotation's
+ * cos_deg / sin_deg (math.hpp:21-22) so that host and device use the same
+ * trigonometric values. */
+typedef struct rm_instance {
+  int32_t model;
+  int32_t reserved;
+  double position[3];
+  double cos_rot[3], sin_rot[3]; /* of rotation.x, .y, .z */
+  double scale[3];               /* nonzero */
+  double albedo[3], emission[3]; /* a component < 0 keeps the model's */
+  double refract, rough, metallic, alpha; /* NaN keeps the model's (an unset std::optional) */
+} rm_instance; /* 184 bytes */
+
+/* Upload a model; *model_id receives its handle. */
+int rmcuda_model_create(rmcuda_ctx* ctx, const rm_model_tri* tris, int32_t n_tris, int32_t* model_id, char* err,
+                        size_t errcap);
+/* Replace a model's triangles (same count): a deforming mesh.  The next
+ * commit re-derives its instances' world triangles. */
+int rmcuda_model_update(rmcuda_ctx* ctx, int32_t model_id, const rm_model_tri* tris, int32_t n_tris, char* err,
+                        size_t errcap);
+/* Build the world of `n` instances on the device and make it the resident
+ * scene (see above).  Enqueued on the context's stream; returns after one
+ * small read-back of the world's triangle and light counts. */
+int rmcuda_instances_commit(rmcuda_ctx* ctx, const rm_instance* inst, int32_t n, int32_t rebuild_every, char* err,
+                            size_t errcap);
+/* Read the resident scene back: up to tri_cap packed triangles, up to
+ * light_cap light indices and (float) CDF values; counts[0] = triangles,
+ * counts[1] = lights; *light_total = the emissive total. */
+int rmcuda_scene_read(rmcuda_ctx* ctx, rm_triangle* tris, int32_t tri_cap, int32_t* light_tri, float* light_cdf,
+                      int32_t light_cap, int32_t* counts, float* light_total, char* err, size_t errcap);
 
 /* Render the resident scene.  d_rgb / d_hdr are DEVICE pointers (either may be
  * NULL); the work is enqueued on the context stream and not waited for. */
@@ -338,7 +394,8 @@ int rmcuda_stats_reset(rmcuda_ctx* ctx);
 #define RM_STAGE_BATCH 16     /* batched rendering: a whole rmcuda_render_batch call */
 #define RM_STAGE_ADJOINT 17   /* path-replay adjoint (rmcuda_backward) */
 #define RM_STAGE_WF_TAIL 18   /* wavefront shading: the last paths, one thread per pixel */
-#define RM_STAGE_COUNT 19
+#define RM_STAGE_PREP 19      /* rmcuda_instances_commit: world triangles and BVH refit / build */
+#define RM_STAGE_COUNT 20
 /* level 0: off; 1: one event pair per stage (the wavefront shading loop counts
  * as RM_STAGE_SHADE, a batch as RM_STAGE_BATCH); 2: also every wavefront
  * launch in its own stage (batches then run without CUDA graphs). */

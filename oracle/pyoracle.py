@@ -105,6 +105,7 @@ def ref_lib() -> C.CDLL | None:
         lib.ref_node_count.argtypes = [_P]
         lib.ref_nodes.argtypes = [_P, _P, _P, _P]
         lib.ref_move_vertices.argtypes = [_P, _P]
+        lib.ref_append_instance.argtypes = [_P, _P, _P, C.c_int, _P]
         lib.ref_camera.argtypes = [C.c_double] * 7 + [_P]
         _ref = lib
     return _ref

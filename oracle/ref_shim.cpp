@@ -7,7 +7,9 @@
 //   Scene::add_triangle (src/engine/scene.cpp:16-87), build_bvh / refit_bvh
 //   (src/engine/bvh.cpp:29-272), Camera::update_trig / update_focal
 //   (src/engine/camera.cpp:3-22).
+#include <cmath>
 #include <cstdint>
+#include <optional>
 #include <cstring>
 
 #include "raymotion/bvh.hpp"
@@ -93,6 +95,47 @@ void ref_camera(double x, double y, double z, double rx, double ry, double rz, d
   c.set({x, y, z}, {rx, ry, rz}, fov);
   double m[10] = {c.focal, c.m0, c.m1, c.m2, c.m3, c.m4, c.m5, c.m6, c.m7, c.m8};
   std::memcpy(out, m, sizeof(m));
+}
+
+// One Objects::push + Objects::append (include/raymotion/runtime.hpp:76-113)
+// into the scene: the instance's model triangles `model` (n records in the
+// layout of ref_add_triangle, shaders in `shader`), placed with
+// inst = position[3], rotation[3] (degrees), scale[3], albedo[3],
+// emission[3], refract, rough, metallic, alpha (NaN: unset).  The transform
+// uses the reference's own cos_deg / sin_deg / normalize (math.hpp) and its
+// order of operations (Objects::append is private, so its three lambdas are
+// restated here); add_triangle is the reference's.
+void ref_append_instance(void* h, const double* model, const int* shader, int n, const double* inst) {
+  Scene& s = static_cast<RefScene*>(h)->s;
+  const Vec3 position{inst[0], inst[1], inst[2]}, rotation{inst[3], inst[4], inst[5]}, scale{inst[6], inst[7], inst[8]};
+  const Vec3 albedo{inst[9], inst[10], inst[11]}, emission{inst[12], inst[13], inst[14]};
+  auto opt = [](double v) { return std::isnan(v) ? std::optional<double>() : std::optional<double>(v); };
+  const std::optional<double> refract = opt(inst[15]), rough = opt(inst[16]), metallic = opt(inst[17]),
+                              alpha = opt(inst[18]);
+  const double cx = cos_deg(rotation.x), sx = sin_deg(rotation.x);
+  const double cy = cos_deg(rotation.y), sy = sin_deg(rotation.y);
+  const double cz = cos_deg(rotation.z), sz = sin_deg(rotation.z);
+  auto rotate = [&](Vec3 v) {
+    double c = cx, si = sx;
+    v = {v.x, c * v.y - si * v.z, si * v.y + c * v.z};
+    c = cy; si = sy;
+    v = {c * v.x + si * v.z, v.y, -si * v.x + c * v.z};
+    c = cz; si = sz;
+    return Vec3{c * v.x - si * v.y, si * v.x + c * v.y, v.z};
+  };
+  auto point = [&](Vec3 v) { return rotate({v.x * scale.x, v.y * scale.y, v.z * scale.z}) + position; };
+  auto normal = [&](Vec3 v) { return normalize(rotate({v.x / scale.x, v.y / scale.y, v.z / scale.z})); };
+  for (int i = 0; i < n; ++i) {
+    const double* r = model + size_t(i) * 34;
+    const Vec3 v0{r[0], r[1], r[2]}, v1{r[3], r[4], r[5]}, v2{r[6], r[7], r[8]};
+    const Vec3 n0{r[15], r[16], r[17]}, n1{r[18], r[19], r[20]}, n2{r[21], r[22], r[23]};
+    s.add_triangle(point(v0), point(v1), point(v2), r[9], r[10], r[11], r[12], r[13], r[14], normal(n0), normal(n1),
+                   normal(n2), albedo.x < 0 ? r[24] : albedo.x, albedo.y < 0 ? r[25] : albedo.y,
+                   albedo.z < 0 ? r[26] : albedo.z, emission.x < 0 ? r[27] : emission.x,
+                   emission.y < 0 ? r[28] : emission.y, emission.z < 0 ? r[29] : emission.z,
+                   metallic.value_or(r[30]), refract.value_or(r[31]), rough.value_or(r[32]), shader[i],
+                   alpha.value_or(r[33]));
+  }
 }
 
 }  // extern "C"

@@ -118,6 +118,41 @@ class Backend:
         e = _err()
         self._check(self.lib.rmcuda_scene_update(self.h, _abi.ptr(tris), len(tris), rebuild_every, e, 512), e)
 
+    # ---- device-side scene preparation (Objects on the device)
+    def model_create(self, tris: np.ndarray) -> int:
+        """Upload object-space model triangles (MODEL_TRI_DTYPE); returns the model id."""
+        tris = np.ascontiguousarray(tris, _abi.MODEL_TRI_DTYPE)
+        mid = C.c_int32(-1)
+        e = _err()
+        self._check(self.lib.rmcuda_model_create(self.h, _abi.ptr(tris), len(tris), C.byref(mid), e, 512), e)
+        return int(mid.value)
+
+    def model_update(self, model: int, tris: np.ndarray) -> None:
+        tris = np.ascontiguousarray(tris, _abi.MODEL_TRI_DTYPE)
+        e = _err()
+        self._check(self.lib.rmcuda_model_update(self.h, int(model), _abi.ptr(tris), len(tris), e, 512), e)
+
+    def instances_commit(self, inst: np.ndarray, rebuild_every: int = 32) -> None:
+        """Build the world of ``inst`` (INSTANCE_DTYPE) on the device and make it the resident scene."""
+        inst = np.ascontiguousarray(inst, _abi.INSTANCE_DTYPE)
+        e = _err()
+        self._check(self.lib.rmcuda_instances_commit(self.h, _abi.ptr(inst), len(inst), int(rebuild_every), e, 512),
+                    e)
+
+    def scene_read(self):
+        """The resident scene: (triangles, light_tri, light_cdf, light_total)."""
+        counts = np.zeros(2, np.int32)
+        tot = C.c_float(0)
+        e = _err()
+        self._check(self.lib.rmcuda_scene_read(self.h, None, 0, None, None, 0, _abi.ptr(counts), C.byref(tot), e, 512),
+                    e)
+        tris = np.zeros(int(counts[0]), _abi.TRIANGLE_DTYPE)
+        lt = np.zeros(int(counts[1]), np.int32)
+        cdf = np.zeros(int(counts[1]), np.float32)
+        self._check(self.lib.rmcuda_scene_read(self.h, _abi.ptr(tris), len(tris), _abi.ptr(lt), _abi.ptr(cdf), len(lt),
+                                               _abi.ptr(counts), C.byref(tot), e, 512), e)
+        return tris, lt, cdf, np.float32(tot.value)
+
     def render_resident_async(self, cam: Camera, cfg: RenderConfig, seed: int, d_rgb: int | None,
                               d_hdr: int | None = None) -> None:
         e = _err()
@@ -227,7 +262,8 @@ class Backend:
             raise RenderError(rc, "stats read failed")
         return dict(path_samples=s.path_samples, rays=s.rays, nodes_visited=s.nodes_visited,
                     tris_tested=s.tris_tested, frames=s.frames, kernel_launches=s.kernel_launches,
-                    device_error=s.device_error, kernel_chain=s.kernel_chain, bvh_node_bytes=s.bvh_node_bytes)
+                    device_error=s.device_error, kernel_chain=s.kernel_chain, bvh_node_bytes=s.bvh_node_bytes,
+                    bvh_builds=s.bvh_builds, bvh_refits=s.bvh_refits)
 
     def stats_reset(self) -> None:
         self.lib.rmcuda_stats_reset(self.h)

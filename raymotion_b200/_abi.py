@@ -41,6 +41,19 @@ TRIANGLE_DTYPE = np.dtype(
 )
 assert TRIANGLE_DTYPE.itemsize == 176
 
+# rm_model_tri / rm_instance (include/rmcuda.h): object-space model triangles
+# and instances of the device-side scene preparation
+MODEL_TRI_DTYPE = np.dtype([(k, "<f8", (3,)) for k in ("v0", "v1", "v2", "n0", "n1", "n2")]
+                           + [(k, "<f8") for k in ("tu0", "tv0", "tu1", "tv1", "tu2", "tv2", "ar", "ag", "ab", "er",
+                                                   "eg", "eb", "metallic", "ior", "rough", "alpha")]
+                           + [("shader", "<i4"), ("reserved", "<i4")])
+assert MODEL_TRI_DTYPE.itemsize == 280
+INSTANCE_DTYPE = np.dtype([("model", "<i4"), ("reserved", "<i4")]
+                          + [(k, "<f8", (3,)) for k in ("position", "cos_rot", "sin_rot", "scale", "albedo",
+                                                        "emission")]
+                          + [(k, "<f8") for k in ("refract", "rough", "metallic", "alpha")])
+assert INSTANCE_DTYPE.itemsize == 184
+
 BVH_NODE_DTYPE = np.dtype([("mn", "<f4", (3,)), ("mx", "<f4", (3,)), ("left", "<i4"), ("right", "<i4"),
                            ("offset", "<i4"), ("count", "<i4")])
 assert BVH_NODE_DTYPE.itemsize == 40
@@ -80,7 +93,8 @@ class RmConfig(C.Structure):
 class RmStats(C.Structure):
     _fields_ = [("path_samples", C.c_uint64), ("rays", C.c_uint64), ("nodes_visited", C.c_uint64),
                 ("tris_tested", C.c_uint64), ("frames", C.c_uint64), ("kernel_launches", C.c_uint64),
-                ("device_error", C.c_uint32), ("kernel_chain", C.c_uint32), ("bvh_node_bytes", C.c_uint32)]
+                ("device_error", C.c_uint32), ("kernel_chain", C.c_uint32), ("bvh_node_bytes", C.c_uint32),
+                ("bvh_builds", C.c_uint32), ("bvh_refits", C.c_uint32)]
 
 
 class RmBatchItem(C.Structure):
@@ -106,6 +120,10 @@ EXPORTS = [
                                 _P, _Z, _P, _S, _Z]),
     ("rmcuda_scene_upload", C.c_int, [_P, C.POINTER(RmSceneView), _S, _Z]),
     ("rmcuda_scene_update", C.c_int, [_P, _P, C.c_int32, C.c_int32, _S, _Z]),
+    ("rmcuda_model_create", C.c_int, [_P, _P, C.c_int32, C.POINTER(C.c_int32), _S, _Z]),
+    ("rmcuda_model_update", C.c_int, [_P, C.c_int32, _P, C.c_int32, _S, _Z]),
+    ("rmcuda_instances_commit", C.c_int, [_P, _P, C.c_int32, C.c_int32, _S, _Z]),
+    ("rmcuda_scene_read", C.c_int, [_P, _P, C.c_int32, _P, _P, C.c_int32, _P, C.POINTER(C.c_float), _S, _Z]),
     ("rmcuda_render_resident_async", C.c_int, [_P, C.POINTER(RmCamera), C.POINTER(RmConfig), C.c_uint64, _P, _P,
                                                 _S, _Z]),
     ("rmcuda_sync", C.c_int, [_P, _S, _Z]),
@@ -134,7 +152,7 @@ EXPORTS = [
 
 STAGES = ["plain", "hash", "generate", "spatial", "shade", "temporal", "atrous0", "atrous1", "tonemap", "wf_extend",
           "wf_shadow", "wf_shade", "bt_start", "bt_extend", "bt_shadow", "bt_shade", "batch", "adjoint",
-          "wf_tail"]
+          "wf_tail", "prep"]
 
 _lib = None
 

@@ -136,6 +136,16 @@ struct rmcuda_ctx {
   std::vector<int> wave_log;  // last frame: (act, ext, shd, us) per count read
   // batched rendering (rmcuda_batch.cu)
   rmapi::BatchPool batch;
+  // device-side scene preparation (rm_prep.cu): models, the last commit's
+  // model list (its topology), scratch, pinned read-back
+  struct Model { rmd::DevBuf tris; int n = 0; };
+  std::vector<Model> models;
+  std::vector<int> prep_topology;
+  uint64_t prep_commits = 0;
+  rmd::DevBuf prep_inst, prep_mptr, prep_start, prep_keep, prep_kscan, prep_light, prep_lscan, prep_temp,
+      prep_weight, prep_small;
+  void* h_prep = nullptr;  // pinned: counts[2], flags, pad, light total (double)
+  uint32_t bvh_builds = 0, bvh_refits = 0;
   // per-stage CUDA-event timing (rmcuda_profile)
   int profiling = 0;
   struct Pending { int stage; cudaEvent_t a, b; };

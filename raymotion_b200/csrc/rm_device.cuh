@@ -399,10 +399,27 @@ struct WTrav {
   }
 };
 
+// One ray through the binary BVH (always built; the megakernels trace here,
+// so that the wide traversal's registers never count against them).
 template <bool kAnyHit>
 __device__ __forceinline__ TraceResult traverse(const Scene& s, float ox, float oy, float oz, float dx, float dy,
                                                 float dz, float tmax, uint32_t* err, uint32_t& n_nodes,
                                                 uint32_t& n_tests) {
+  Trav t;
+  int stack[kStack];
+  t.init(ox, oy, oz, dx, dy, dz, tmax);
+  while (!t.step<kAnyHit>(s, stack, err, n_nodes, n_tests)) {
+  }
+  return t.r;
+}
+
+// One ray through the 8-wide BVH when the scene has one, else the binary BVH
+// (the ray-query entry point; the wavefront trace kernels pick WTrav or Trav
+// per launch instead).  Both give the same hits.
+template <bool kAnyHit>
+__device__ __forceinline__ TraceResult traverse_any(const Scene& s, float ox, float oy, float oz, float dx, float dy,
+                                                    float dz, float tmax, uint32_t* err, uint32_t& n_nodes,
+                                                    uint32_t& n_tests) {
   if (s.wnodes) {
     WTrav t;
     uint2 stack[kWideStack];
@@ -411,12 +428,7 @@ __device__ __forceinline__ TraceResult traverse(const Scene& s, float ox, float 
     }
     return t.r;
   }
-  Trav t;
-  int stack[kStack];
-  t.init(ox, oy, oz, dx, dy, dz, tmax);
-  while (!t.step<kAnyHit>(s, stack, err, n_nodes, n_tests)) {
-  }
-  return t.r;
+  return traverse<kAnyHit>(s, ox, oy, oz, dx, dy, dz, tmax, err, n_nodes, n_tests);
 }
 
 // ---------------------------------------------------------------- tracer

@@ -628,8 +628,8 @@ __global__ void __launch_bounds__(256) k_trace(Scene s, const float* __restrict_
   if (i >= n) return;
   const float* r = rays + size_t(i) * 7;
   uint32_t nodes = 0, tests = 0;
-  TraceResult h = any_hit ? traverse<true>(s, r[0], r[1], r[2], r[3], r[4], r[5], r[6], err, nodes, tests)
-                          : traverse<false>(s, r[0], r[1], r[2], r[3], r[4], r[5], r[6], err, nodes, tests);
+  TraceResult h = any_hit ? traverse_any<true>(s, r[0], r[1], r[2], r[3], r[4], r[5], r[6], err, nodes, tests)
+                          : traverse_any<false>(s, r[0], r[1], r[2], r[3], r[4], r[5], r[6], err, nodes, tests);
   tri[i] = h.tri;
   if (t) t[i] = h.tri >= 0 ? h.t : r[6];
   if (u) u[i] = h.u;

@@ -246,4 +246,29 @@ cudaError_t prepare_lights(const rm_triangle* d_tris, const int32_t* d_lights, c
 // 64-bit content hash of a device byte range (order-sensitive per 8-byte word).
 cudaError_t device_hash(const void* d_bytes, size_t n_bytes, unsigned long long* d_out, cudaStream_t st);
 
+// rm_prep.cu: the world triangles of instanced models (Objects::append +
+// Scene::add_triangle on the device).  Device pointers; `total` slots = the
+// sum of the instances' model triangle counts, start[n_inst + 1] their
+// prefix sums.  Outputs: out (world triangles in push order), light_tri /
+// cdf (the light list), counts[0..1] (triangles, lights), light_total[0]
+// (double), flags[0] (nonzero when every triangle is opaque).
+struct PrepArgs {
+  const rm_instance* inst;
+  const rm_model_tri* const* mptr;  // per instance: its model's triangles
+  const int* start;
+  int n_inst, total;
+  int *keep, *kscan, *light, *lscan;  // total each
+  void* scan_temp;
+  size_t scan_bytes;
+  rm_triangle* out;
+  int32_t* light_tri;
+  double* weight;
+  float* cdf;
+  int* counts;
+  double* light_total;
+  int* flags;
+};
+cudaError_t prep_scan_bytes(int total, size_t& bytes);
+cudaError_t prep_world(const PrepArgs& a, cudaStream_t st);
+
 }  // namespace rmd

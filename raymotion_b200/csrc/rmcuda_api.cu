@@ -161,6 +161,7 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
   }
   for (int i = 0; i < sv->n_lights; ++i)
     if (sv->light_tri[i] < 0 || sv->light_tri[i] >= sv->n_tris) { msg = "light index out of range"; return RM_ERR_INVALID; }
+  if (&sc == &c->sc) c->prep_topology.clear();  // an uploaded scene is not an instance commit
   cudaStream_t st = c->stream;
   cudaError_t e;
   const size_t tb = size_t(sv->n_tris) * sizeof(rm_triangle);
@@ -216,6 +217,7 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
     }
     sc.device_built = !converted;
     if (!converted) {
+      if (&sc == &c->sc) c->bvh_builds++;  // the resident scene's builds are counted
       std::string berr;
       if ((e = build_device_bvh(sc.tris.as<rm_triangle>(), sv->n_tris, sc.bvh, st, berr)) != cudaSuccess) {
         msg = berr.empty() ? cuda_msg("device BVH build failed", e) : berr;
@@ -579,6 +581,11 @@ void rmcuda_destroy(rmcuda_ctx* c) {
   for (DevBuf& b : c->wf) b.release();
   for (DevBuf& b : c->wq) b.release();
   if (c->h_counts) cudaFreeHost(c->h_counts);
+  for (auto& m : c->models) m.tris.release();
+  for (DevBuf* b : {&c->prep_inst, &c->prep_mptr, &c->prep_start, &c->prep_keep, &c->prep_kscan, &c->prep_light,
+                    &c->prep_lscan, &c->prep_temp, &c->prep_weight, &c->prep_small})
+    b->release();
+  if (c->h_prep) cudaFreeHost(c->h_prep);
   c->gb.release(); c->hg.release();
   c->rinit.release(); c->rmerged.release(); c->hres.release();
   resolve_pending(c);
@@ -632,10 +639,12 @@ int rmcuda_scene_update(rmcuda_ctx* c, const rm_triangle* tris, int32_t n, int32
     e = build_device_bvh(c->sc.tris.as<rm_triangle>(), n, c->sc.bvh, c->stream, berr);
     c->sc.refits = 0;
     c->sc.device_built = true;
+    c->bvh_builds++;
     if (e != cudaSuccess) { set_err(err, errcap, berr.empty() ? cuda_msg("rebuild failed", e) : berr); return RM_ERR_CUDA; }
   } else {
     e = refit_bvh(c->sc.tris.as<rm_triangle>(), c->sc.bvh, c->stream);
     c->sc.refits++;
+    c->bvh_refits++;
     if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("refit failed", e)); return RM_ERR_CUDA; }
   }
   // the wide nodes are collapsed again from the refitted or rebuilt records
@@ -643,6 +652,172 @@ int rmcuda_scene_update(rmcuda_ctx* c, const rm_triangle* tris, int32_t n, int32
     set_err(err, errcap, cuda_msg("wide BVH build failed", e));
     return RM_ERR_CUDA;
   }
+  return RM_OK;
+}
+
+int rmcuda_model_create(rmcuda_ctx* c, const rm_model_tri* tris, int32_t n, int32_t* model_id, char* err,
+                        size_t errcap) {
+  if (!c || !model_id || n < 0 || (n > 0 && !tris)) { set_err(err, errcap, "invalid model"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  rmcuda_ctx::Model m;
+  cudaError_t e = m.tris.reserve(size_t(std::max(n, 1)) * sizeof(rm_model_tri));
+  if (e == cudaSuccess && n > 0)
+    e = cudaMemcpyAsync(m.tris.ptr, tris, size_t(n) * sizeof(rm_model_tri), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // the caller may free `tris` on return
+  if (e != cudaSuccess) {
+    m.tris.release();
+    set_err(err, errcap, cuda_msg("model upload failed", e));
+    return RM_ERR_CUDA;
+  }
+  m.n = n;
+  c->models.push_back(std::move(m));
+  *model_id = int32_t(c->models.size() - 1);
+  return RM_OK;
+}
+
+int rmcuda_model_update(rmcuda_ctx* c, int32_t id, const rm_model_tri* tris, int32_t n, char* err, size_t errcap) {
+  if (!c) { set_err(err, errcap, "null context"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (id < 0 || size_t(id) >= c->models.size() || n != c->models[size_t(id)].n || (n > 0 && !tris)) {
+    set_err(err, errcap, "model update needs an existing model and the same triangle count");
+    return RM_ERR_INVALID;
+  }
+  cudaError_t e = n > 0 ? cudaMemcpyAsync(c->models[size_t(id)].tris.ptr, tris, size_t(n) * sizeof(rm_model_tri),
+                                          cudaMemcpyHostToDevice, c->stream)
+                        : cudaSuccess;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("model update failed", e)); return RM_ERR_CUDA; }
+  return RM_OK;
+}
+
+// Objects::render's scene step (runtime.hpp:121-131) on the device: the world
+// of the instances (rm_prep.cu), then refit or build (bvh.cpp:250-272 falls
+// back to a build when the triangle count changed).
+int rmcuda_instances_commit(rmcuda_ctx* c, const rm_instance* inst, int32_t n, int32_t rebuild_every, char* err,
+                            size_t errcap) {
+  if (!c || n < 0 || (n > 0 && !inst)) { set_err(err, errcap, "invalid instance list"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  std::vector<int> start(static_cast<size_t>(n) + 1, 0), topo(static_cast<size_t>(n));
+  std::vector<const rm_model_tri*> mptr(static_cast<size_t>(n));
+  for (int i = 0; i < n; ++i) {
+    const rm_instance& in = inst[i];
+    if (in.model < 0 || size_t(in.model) >= c->models.size()) { set_err(err, errcap, "null object"); return RM_ERR_INVALID; }
+    if (in.scale[0] == 0 || in.scale[1] == 0 || in.scale[2] == 0) {
+      set_err(err, errcap, "scale must be nonzero");  // Objects::push, runtime.hpp:80
+      return RM_ERR_INVALID;
+    }
+    const auto& m = c->models[size_t(in.model)];
+    if (int64_t(start[size_t(i)]) + m.n > int64_t(1) << 30) { set_err(err, errcap, "too many triangles"); return RM_ERR_INVALID; }
+    start[size_t(i) + 1] = start[size_t(i)] + m.n;
+    topo[size_t(i)] = in.model;
+    mptr[size_t(i)] = m.tris.as<rm_model_tri>();
+  }
+  const int total = start[size_t(n)];
+  cudaStream_t st = c->stream;
+  cudaError_t e;
+  size_t scan_bytes = 0;
+  const size_t slots = size_t(std::max(total, 1));
+  if ((e = prep_scan_bytes(total, scan_bytes)) != cudaSuccess ||
+      (e = c->prep_inst.reserve(size_t(std::max(n, 1)) * sizeof(rm_instance))) != cudaSuccess ||
+      (e = c->prep_mptr.reserve(size_t(std::max(n, 1)) * sizeof(void*))) != cudaSuccess ||
+      (e = c->prep_start.reserve((size_t(n) + 1) * sizeof(int))) != cudaSuccess ||
+      (e = c->prep_keep.reserve(slots * 4)) != cudaSuccess || (e = c->prep_kscan.reserve(slots * 4)) != cudaSuccess ||
+      (e = c->prep_light.reserve(slots * 4)) != cudaSuccess || (e = c->prep_lscan.reserve(slots * 4)) != cudaSuccess ||
+      (e = c->prep_temp.reserve(std::max<size_t>(scan_bytes, 16))) != cudaSuccess ||
+      (e = c->prep_weight.reserve(slots * 8)) != cudaSuccess || (e = c->prep_small.reserve(64)) != cudaSuccess ||
+      (e = c->sc.tris.reserve(slots * sizeof(rm_triangle))) != cudaSuccess ||
+      (e = c->sc.lights.reserve(slots * 4)) != cudaSuccess || (e = c->sc.cdf.reserve(slots * 4)) != cudaSuccess ||
+      (!c->h_prep && (e = cudaMallocHost(&c->h_prep, 64)) != cudaSuccess)) {
+    set_err(err, errcap, cuda_msg("scene preparation allocation failed", e));
+    return RM_ERR_ALLOC;
+  }
+  // the previous commit's kernels may still read these buffers: stream order keeps them apart
+  if ((n > 0 && ((e = cudaMemcpyAsync(c->prep_inst.ptr, inst, size_t(n) * sizeof(rm_instance), cudaMemcpyHostToDevice,
+                                      st)) != cudaSuccess ||
+                 (e = cudaMemcpyAsync(c->prep_mptr.ptr, mptr.data(), size_t(n) * sizeof(void*), cudaMemcpyHostToDevice,
+                                      st)) != cudaSuccess)) ||
+      (e = cudaMemcpyAsync(c->prep_start.ptr, start.data(), (size_t(n) + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                           st)) != cudaSuccess) {
+    set_err(err, errcap, cuda_msg("instance upload failed", e));
+    return RM_ERR_CUDA;
+  }
+  int* small = c->prep_small.as<int>();
+  rmd::PrepArgs a{c->prep_inst.as<rm_instance>(), c->prep_mptr.as<const rm_model_tri* const>(), c->prep_start.as<int>(),
+                  n, total, c->prep_keep.as<int>(), c->prep_kscan.as<int>(), c->prep_light.as<int>(),
+                  c->prep_lscan.as<int>(), c->prep_temp.ptr, scan_bytes, c->sc.tris.as<rm_triangle>(),
+                  c->sc.lights.as<int32_t>(), c->prep_weight.as<double>(), c->sc.cdf.as<float>(), small,
+                  reinterpret_cast<double*>(small + 4), small + 2};
+  if ((e = staged(c, RM_STAGE_PREP, [&] { return rmd::prep_world(a, st); })) != cudaSuccess ||
+      (e = cudaMemcpyAsync(c->h_prep, small, 32, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+    set_err(err, errcap, cuda_msg("scene preparation failed", e));
+    return RM_ERR_CUDA;
+  }
+  const int* hc = static_cast<const int*>(c->h_prep);
+  double total_w = 0;
+  std::memcpy(&total_w, static_cast<const char*>(c->h_prep) + 16, 8);
+  const int n_tris = hc[0];
+  const bool same = c->sc.have_scene && topo == c->prep_topology && n_tris == c->sc.n_tris && c->sc.device_built;
+  c->sc.n_tris = n_tris;
+  c->sc.n_lights = hc[1];
+  c->sc.light_total = float(total_w);
+  c->sc.opaque = hc[2] != 0;
+  c->sc.have_scene = false;
+  if ((e = prepare_lights(c->sc.tris.as<rm_triangle>(), c->sc.lights.as<int32_t>(), c->sc.cdf.as<float>(),
+                          c->sc.n_lights, c->sc.light_total, c->sc.lrec, c->sc.guide, c->sc.guide_n, c->sc.guide_inv,
+                          st)) != cudaSuccess) {
+    set_err(err, errcap, cuda_msg("light preparation failed", e));
+    return RM_ERR_CUDA;
+  }
+  const bool refit = same && n_tris > 0 && !(rebuild_every > 0 && c->prep_commits % uint64_t(rebuild_every) == 0);
+  if (n_tris == 0) {
+    c->sc.bvh.n_records = 0;
+    c->sc.bvh.n_tris = 0;
+  } else if (refit) {
+    e = staged(c, RM_STAGE_PREP, [&] { return refit_bvh(c->sc.tris.as<rm_triangle>(), c->sc.bvh, st); });
+    c->sc.refits++;
+    c->bvh_refits++;
+    if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("refit failed", e)); return RM_ERR_CUDA; }
+  } else {
+    std::string berr;
+    e = staged(c, RM_STAGE_PREP,
+               [&] { return build_device_bvh(c->sc.tris.as<rm_triangle>(), n_tris, c->sc.bvh, st, berr); });
+    c->sc.refits = 0;
+    c->bvh_builds++;
+    if (e != cudaSuccess) { set_err(err, errcap, berr.empty() ? cuda_msg("BVH build failed", e) : berr); return RM_ERR_CUDA; }
+  }
+  if ((e = finish_wide(c->sc.bvh, st)) != cudaSuccess) {
+    set_err(err, errcap, cuda_msg("wide BVH build failed", e));
+    return RM_ERR_CUDA;
+  }
+  c->sc.device_built = true;
+  c->sc.have_scene = true;
+  c->prep_topology = std::move(topo);
+  c->prep_commits++;
+  return RM_OK;
+}
+
+int rmcuda_scene_read(rmcuda_ctx* c, rm_triangle* tris, int32_t tri_cap, int32_t* light_tri, float* light_cdf,
+                      int32_t light_cap, int32_t* counts, float* light_total, char* err, size_t errcap) {
+  if (!c || tri_cap < 0 || light_cap < 0) { set_err(err, errcap, "invalid arguments"); return RM_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (!c->sc.have_scene) { set_err(err, errcap, "no resident scene"); return RM_ERR_INVALID; }
+  const size_t nt = size_t(std::min(tri_cap, int32_t(c->sc.n_tris)));
+  const size_t nl = size_t(std::min(light_cap, int32_t(c->sc.n_lights)));
+  cudaError_t e = cudaSuccess;
+  if (tris && nt) e = cudaMemcpyAsync(tris, c->sc.tris.ptr, nt * sizeof(rm_triangle), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && light_tri && nl)
+    e = cudaMemcpyAsync(light_tri, c->sc.lights.ptr, nl * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && light_cdf && nl)
+    e = cudaMemcpyAsync(light_cdf, c->sc.cdf.ptr, nl * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("scene read failed", e)); return RM_ERR_CUDA; }
+  if (counts) { counts[0] = c->sc.n_tris; counts[1] = c->sc.n_lights; }
+  if (light_total) *light_total = c->sc.light_total;
   return RM_OK;
 }
 
@@ -806,6 +981,8 @@ int rmcuda_stats_get(rmcuda_ctx* c, rm_stats* out) {
   out->device_error = e32;
   out->kernel_chain = uint32_t(c->last_chain);
   out->bvh_node_bytes = c->sc.bvh.n_wide > 0 ? 80u : 64u;
+  out->bvh_builds = c->bvh_builds;
+  out->bvh_refits = c->bvh_refits;
   return RM_OK;
 }
 

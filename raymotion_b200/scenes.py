@@ -15,6 +15,12 @@
   rendering: triangle counts log-uniform over [1k, 2M], resolutions from
   {256x256, 640x360, 1280x720, 1920x1080}, spp from {4, 16, 64}, depth 8-12,
   all on the plain path (ReSTIR and the denoiser off).
+* ``AnimatedSequence(...)``: the icosphere field as models and instances
+  (one object-space model per sphere), 20 % of the spheres moving rigidly
+  along seeded sinusoids, a 256 x 256-vertex cloth (130,050 triangles)
+  deformed by seeded sine waves, and a camera orbiting 6 degrees per frame;
+  34 frames at 30 fps, 1280x720, 16 spp, temporal ReSTIR and denoise on the
+  animated geometry.
 """
 from __future__ import annotations
 
@@ -301,3 +307,114 @@ def inverse_scene(seed: int = 4, n_spheres: int = 100, subdiv: int = 3, ground: 
     cfg = RenderConfig(width=width, height=height, spp=spp, max_bounces=depth, adapt_min=0, restir_candidates=1,
                        restir_spatial=0, flags=PLAIN_FLAGS | _abi.RM_FLAG_NOADAPT)
     return dict(scene=packed, tri_material=tri_mat, params=params, mask=mask, camera=cam, config=cfg)
+
+
+class AnimatedSequence:
+    """The animated sequence: models, per-frame instances, cloth and camera.
+
+    ``models`` lists object-space triangle arrays (``_abi.MODEL_TRI_DTYPE``):
+    the 200 spheres (each displaced by its own noise, centred on the origin),
+    the ground, the 4096 emitters and the cloth at frame 0 (``CLOTH`` is its
+    index).  ``instances(f)`` places them at frame ``f`` (time f / fps);
+    ``cloth(f)`` is the cloth model at frame ``f``; ``camera(f)`` orbits the
+    field centre by ``orbit_deg`` per frame.
+    """
+
+    def __init__(self, seed: int = 1, n_spheres: int = 200, subdiv: int = 4, n_emitters: int = 4096,
+                 cloth_verts: int = 256, frames: int = 34, fps: int = 30, orbit_deg: float = 6.0,
+                 width: int = 1280, height: int = 720, spp: int = 16, depth: int = 12, moving: float = 0.2):
+        from .objects import Instance, model_from_arrays
+        self._Instance = Instance
+        self._model = model_from_arrays
+        rng = np.random.default_rng(seed)
+        self.frames, self.fps, self.orbit_deg = frames, fps, orbit_deg
+        unit_v, faces = _icosphere(subdiv)
+        radii = rng.uniform(0.2, 1.5, n_spheres)
+        self.centers = np.stack([rng.uniform(-20, 20, n_spheres), rng.uniform(0, 10, n_spheres),
+                                 rng.uniform(-20, 20, n_spheres)], axis=1)
+        kind = rng.choice(3, size=n_spheres, p=[0.5, 0.3, 0.2])
+        origin = np.zeros(3)
+        self.models = []
+        for i in range(n_spheres):
+            fa, fb, fc, na, nb, nc = _displaced_sphere(unit_v, faces, origin, radii[i], seed * 1000 + i)
+            if kind[i] == 0:
+                mat = dict(albedo=tuple(rng.uniform(0.1, 0.9, 3)), rough=0.5)
+            elif kind[i] == 1:
+                mat = dict(albedo=tuple(rng.uniform(0.5, 0.95, 3)), metallic=1.0, rough=float(rng.uniform(0.05, 1.0)))
+            else:
+                mat = dict(albedo=(1.0, 1.0, 1.0), ior=1.5, rough=float(rng.choice([0.0, 0.2])))
+            self.models.append(model_from_arrays(fa, fb, fc, na, nb, nc, **mat))
+        g = 100.0
+        up = np.array([0.0, 1.0, 0.0])
+        self.models.append(model_from_arrays([[-g, 0, -g], [-g, 0, -g]], [[-g, 0, g], [g, 0, g]],
+                                             [[g, 0, g], [g, 0, -g]], [up, up], [up, up], [up, up],
+                                             albedo=(0.5, 0.5, 0.5), rough=0.8))
+        c = np.stack([rng.uniform(-24, 24, n_emitters), rng.uniform(11, 14, n_emitters),
+                      rng.uniform(-24, 24, n_emitters)], axis=1)
+        s = rng.uniform(0.15, 0.35, n_emitters)[:, None]
+        a0 = c + np.concatenate([-s, 0 * s, -s], axis=1)
+        a1 = c + np.concatenate([s, 0 * s, -s * 0.2], axis=1)
+        a2 = c + np.concatenate([-s * 0.3, 0 * s, s], axis=1)
+        radiance = np.exp(rng.uniform(math.log(1.0), math.log(100.0), n_emitters))
+        tint = rng.uniform(0.6, 1.0, (n_emitters, 3))
+        down = np.broadcast_to(np.asarray([0.0, -1.0, 0.0]), (n_emitters, 3))
+        self.models.append(model_from_arrays(a0, a1, a2, down, down, down, albedo=(0.8, 0.8, 0.8),
+                                             emission=tint * radiance[:, None]))
+        # moving spheres: a seeded sinusoid per axis
+        self.moving = rng.choice(n_spheres, size=int(round(moving * n_spheres)), replace=False)
+        nm = len(self.moving)
+        self.amp = rng.uniform(0.5, 2.0, (nm, 3)) * np.array([1.0, 0.3, 1.0])
+        self.omega = rng.uniform(1.0, 3.0, (nm, 3))
+        self.phase = rng.uniform(0, 2 * math.pi, (nm, 3))
+        # cloth: a curtain behind the field, waves across it
+        self.cloth_n = cloth_verts
+        u = np.linspace(-16.0, 16.0, cloth_verts)
+        v = np.linspace(0.5, 12.5, cloth_verts)
+        self._cu, self._cv = np.meshgrid(u, v, indexing="xy")
+        k = rng.uniform(0.3, 0.8, 2)
+        w = rng.uniform(1.0, 2.5, 2)
+        ph = rng.uniform(0, 2 * math.pi, 2)
+        self._wave = (k, w, ph)
+        q = np.arange(cloth_verts - 1)
+        i00 = (q[None, :] + cloth_verts * q[:, None]).ravel()
+        self._tri = np.concatenate([np.stack([i00, i00 + 1, i00 + cloth_verts + 1], axis=1),
+                                    np.stack([i00, i00 + cloth_verts + 1, i00 + cloth_verts], axis=1)])
+        self.CLOTH = len(self.models)
+        self.models.append(self.cloth(0))
+        self.cfg = RenderConfig(width=width, height=height, spp=spp, max_bounces=depth, restir_candidates=32,
+                                restir_spatial=5, restir_radius=30.0, flags=_abi.RM_FLAG_ANIMATED_HISTORY)
+
+    def time(self, f: int) -> float:
+        return f / self.fps
+
+    def cloth(self, f: int) -> np.ndarray:
+        t = self.time(f)
+        (kx, ky), (wx, wy), (px, py) = self._wave
+        x, y = self._cu, self._cv
+        z = 24.0 + 0.8 * np.sin(kx * x + wx * t + px) + 0.5 * np.sin(ky * y + wy * t + py)
+        dzdx = 0.8 * kx * np.cos(kx * x + wx * t + px)
+        dzdy = 0.5 * ky * np.cos(ky * y + wy * t + py)
+        pos = np.stack([x, y, z], axis=-1).reshape(-1, 3)
+        nrm = np.stack([-dzdx, -dzdy, np.ones_like(z)], axis=-1).reshape(-1, 3)
+        nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+        tri = self._tri
+        return self._model(pos[tri[:, 0]], pos[tri[:, 1]], pos[tri[:, 2]], nrm[tri[:, 0]], nrm[tri[:, 1]],
+                           nrm[tri[:, 2]], albedo=(0.7, 0.15, 0.1), rough=0.7)
+
+    def instances(self, f: int) -> list:
+        t = self.time(f)
+        pos = self.centers.copy()
+        pos[self.moving] += self.amp * np.sin(self.omega * t + self.phase)
+        out = [self._Instance(model=i, position=tuple(pos[i])) for i in range(len(self.centers))]
+        out += [self._Instance(model=len(self.centers)), self._Instance(model=len(self.centers) + 1),
+                self._Instance(model=self.CLOTH)]
+        return out
+
+    def camera(self, f: int) -> Camera:
+        th = self.orbit_deg * f
+        r = math.radians(th)
+        return Camera().set((-34.0 * math.sin(r), 9.0, -34.0 * math.cos(r)), (14.0, th, 0.0), 60)
+
+    @property
+    def n_tris(self) -> int:
+        return sum(len(m) for m in self.models)
