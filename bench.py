@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=2)
     ap.add_argument("--no-sequence", action="store_true", help="skip the animated-sequence measurement")
+    ap.add_argument("--screen-space-only", action="store_true",
+                    help="only the 2048x1280 screen-space frames (profiling the denoiser passes)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-rendering measurement")
     ap.add_argument("--fit-iters", type=int, default=200)
     return ap.parse_args()
@@ -550,9 +552,14 @@ def screen_space_large(backend, torch, cam, cfg, dev, seed0, peak):
         return None
     nbytes = npix * (92 + 64 + 64 + 3)
     ach = nbytes / (ms / 1e3) / 1e9
+    passes = {}
+    for k, b in (("temporal", 92), ("atrous0", 64), ("atrous1", 67)):
+        us = t[k][0] / frames * 1e3
+        if us > 0:
+            passes[k] = dict(us=us, bytes_per_px=b, gbs=npix * b / us / 1e3, frac=npix * b / us / 1e3 / peak["hbm_gbs"])
     return dict(bound="hbm", kernels="k_denoise_temporal_tiled + k_denoise_atrous_tiled x2", width=big.width,
                 height=big.height, achieved=ach, peak=peak["hbm_gbs"], unit="GB/s", frac=ach / peak["hbm_gbs"],
-                us_per_frame=ms * 1e3, bytes_per_frame=nbytes, peak_source=peak["source"])
+                us_per_frame=ms * 1e3, bytes_per_frame=nbytes, peak_source=peak["source"], passes=passes)
 
 
 def run_b200(args, world, rank, local):
@@ -573,6 +580,10 @@ def run_b200(args, world, rank, local):
     seed0 = 12345 + 1000 * rank
     # ---- device-resident frames (value)
     backend.upload(scene, use_nodes=False)
+    if args.screen_space_only:
+        print(json.dumps(screen_space_large(backend, torch, cam, cfg, dev, seed0 + 300, measured_peaks())), flush=True)
+        backend.close()
+        return 0
     d_rgb = torch.empty(npix * 3, dtype=torch.uint8, device=dev)
     for i in range(args.warmup):
         backend.render_resident_async(cam, cfg, seed0 + i, d_rgb.data_ptr())

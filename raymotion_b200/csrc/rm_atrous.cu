@@ -7,7 +7,10 @@
 // oracle is a tolerance (1e-4 relative on 99.9 % of pixels), and contraction
 // only shortens the dependency chains.  Per tap the kernel reads four shared
 // memory records (position|kind, normal|luma, colour|albedo.r, albedo.gb);
-// the 5 x 5 footprint's HBM bytes are read once per tile.
+// the 5 x 5 footprint's HBM bytes are read once per tile.  Taps outside the
+// image or on pixels of kind 0 hold a zero normal in the tile, so their weight
+// pow16(max(n.n0, 0)) x exp2(<= 0) is exactly 0 and the reference's explicit
+// skips (bounds, kind) need no test per tap.
 #include <cuda_runtime.h>
 
 #include "rm_device.cuh"
@@ -28,7 +31,8 @@ __device__ __forceinline__ void st3(float* __restrict__ a, uint32_t i, float x, 
   a[size_t(i) * 3] = x; a[size_t(i) * 3 + 1] = y; a[size_t(i) * 3 + 2] = z;
 }
 
-__device__ __forceinline__ float fast_len(float d2) { return d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f; }
+// |d| from d.d: d2 / sqrt(d2), 0 for d2 = 0 (the clamp keeps rsqrt finite)
+__device__ __forceinline__ float fast_len(float d2) { return d2 * rsqrtf(fmaxf(d2, 1e-30f)); }
 
 template <int STEP>
 __global__ void __launch_bounds__(kTX* kTY) k_denoise_atrous_tiled(Params p, GBufSoA gb, const float* __restrict__ in,
@@ -81,15 +85,10 @@ __global__ void __launch_bounds__(kTX* kTY) k_denoise_atrous_tiled(Params p, GBu
     float sx = 0, sy = 0, sz = 0, wsum = 0;
 #pragma unroll
     for (int dy = -2; dy <= 2; ++dy) {
-      const int ny = y + dy * (1 << STEP);
-      if (ny < 0 || ny >= H) continue;
 #pragma unroll
       for (int dx = -2; dx <= 2; ++dx) {
-        const int nx = x + dx * (1 << STEP);
-        if (nx < 0 || nx >= W) continue;
         const int ly = cy + dy * (1 << STEP), lx = cx + dx * (1 << STEP);
         const float4 P = s_pk[ly][lx];
-        if (__float_as_int(P.w) == 0) continue;
         const float4 N = s_nl[ly][lx], C = s_ca[ly][lx];
         const float2 A = s_ag[ly][lx];
         float nd = N.x * N0.x + (N.y * N0.y + N.z * N0.z);
