@@ -522,6 +522,58 @@ def sequence_measure(args, backend, torch, stream, dev):
                 path_samples=int(samples))
 
 
+def _relmse(img, ref):
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 0.01)))
+
+
+def relmse_measure(backend, torch, cam, cfg, dev, seed):
+    """relMSE of single frames against the FP64 16,384-spp references of
+    tests/golden (make_relmse_refs.py: 4096 seeded pixels, the oracle's plain
+    path tracer, same depth and clamp).  The CUDA frames are bit-identical to
+    the oracle's fp32 frames on the same streams (the parity tests), so the CPU
+    arm's relMSE at equal spp is the same.  For the headline workload: the
+    denoised output and the raw ReSTIR radiance (denoiser off), each from a
+    fresh history; for the Cornell box, its plain 16-spp frame (through
+    rmcuda_render, which replaces the resident scene, so this runs last)."""
+    from raymotion_b200.scene import RenderConfig  # noqa: F401  (cfg's type)
+    from raymotion_b200.scenes import cornell_box
+    golden = Path(__file__).resolve().parent / "tests" / "golden"
+    out = {}
+    g = golden / "relmse_icosphere720.npz"
+    if g.exists():
+        ref = np.load(g)
+        pix, r = ref["pixels"], ref["ref"]
+        npix = cfg.width * cfg.height
+        d_rgb = torch.empty(npix * 3, dtype=torch.uint8, device=dev)
+        d_hdr = torch.empty(npix * 3, dtype=torch.float32, device=dev)
+        e = {}
+        A = rb_abi()
+        # switches from the flag bits (RM_FLAG_NO_ENV): the denoiser on, then off
+        for name, flags in (("denoised", cfg.flags | A.RM_FLAG_NO_ENV),
+                            ("restir_raw", cfg.flags | A.RM_FLAG_NO_ENV | A.RM_FLAG_DENOISE_OFF)):
+            backend.reset_history()
+            backend.render_resident_async(cam, dataclasses.replace(cfg, flags=flags), seed, d_rgb.data_ptr(),
+                                          d_hdr.data_ptr())
+            backend.sync()
+            img = d_hdr.cpu().numpy().reshape(-1, 3)[pix].astype(np.float64)
+            e[name] = _relmse(img, r)
+        out["icosphere720"] = dict(pixels=int(len(pix)), ref_spp=int(ref["spp"]), spp=cfg.spp, **e)
+    g = golden / "relmse_cornell.npz"
+    if g.exists():
+        ref = np.load(g)
+        sb, ccam, ccfg = cornell_box(0)
+        _, hdr = backend.render(sb.pack(), ccam, ccfg, seed, hdr=True, use_nodes=False)
+        img = hdr.reshape(-1, 3)[ref["pixels"]].astype(np.float64)
+        out["cornell"] = dict(pixels=int(len(ref["pixels"])), ref_spp=int(ref["spp"]), spp=ccfg.spp,
+                              plain=_relmse(img, ref["ref"]))
+    return out or None
+
+
+def rb_abi():
+    from raymotion_b200 import _abi
+    return _abi
+
+
 def screen_space_large(backend, torch, cam, cfg, dev, seed0, peak):
     """The screen-space passes where their working set exceeds L2.
 
@@ -713,6 +765,8 @@ def run_b200(args, world, rank, local):
         h2d = sum(pinned[k].nbytes for k in pinned)
         e2e = dict(value=es / esec, unit=UNIT, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(npix * 3),
                    ms_per_step=1e3 * esec / args.steps)
+    # ---- relMSE against the FP64 references (before the steps that replace the resident scene)
+    relmse = relmse_measure(backend, torch, cam, cfg, dev, seed0 + 900)
     # ---- batched vs serial rendering of many uneven scenes
     batch = None if args.no_batch else batch_compare(args, backend, torch, stream, dev, world)
     # ---- the animated sequence: device scene preparation + refit per frame
@@ -733,7 +787,7 @@ def run_b200(args, world, rank, local):
                     gpu_launches=int(st["kernel_launches"]), clocks=clk, stages=stage_summary,
                     kernels_one_frame=kernel_summary, wavefront=wave_summary, roofline_screen_space=roofline_ss,
                     roofline_screen_space_large=ss_large,
-                    batch=batch, adjoint=adjoint, sequence=sequence)
+                    batch=batch, adjoint=adjoint, sequence=sequence, relmse=relmse)
         print(json.dumps(line), flush=True)
     backend.close()
     return 0
