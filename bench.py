@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=2)
     ap.add_argument("--no-sequence", action="store_true", help="skip the animated-sequence measurement")
+    ap.add_argument("--no-relmse", action="store_true", help="skip the relMSE frames")
+    ap.add_argument("--no-large", action="store_true", help="skip the 2048x1280 screen-space frames")
     ap.add_argument("--screen-space-only", action="store_true",
                     help="only the 2048x1280 screen-space frames (profiling the denoiser passes)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-rendering measurement")
@@ -737,7 +739,7 @@ def run_b200(args, world, rank, local):
             e.update(rays=rc["rays"], nodes_per_ray=rc["nodes_visited"] / rc["rays"],
                      tests_per_ray=rc["tris_tested"] / rc["rays"], mrays_per_s=rc["rays"] / (v[0] * 1e3))
         kernel_summary[k] = e
-    ss_large = screen_space_large(backend, torch, cam, cfg, dev, seed0 + 300, peak)
+    ss_large = None if args.no_large else screen_space_large(backend, torch, cam, cfg, dev, seed0 + 300, peak)
     # ---- end to end through rmcuda_render with host buffers
     e2e = None
     if not args.no_e2e:
@@ -766,7 +768,7 @@ def run_b200(args, world, rank, local):
         e2e = dict(value=es / esec, unit=UNIT, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(npix * 3),
                    ms_per_step=1e3 * esec / args.steps)
     # ---- relMSE against the FP64 references (before the steps that replace the resident scene)
-    relmse = relmse_measure(backend, torch, cam, cfg, dev, seed0 + 900)
+    relmse = None if args.no_relmse else relmse_measure(backend, torch, cam, cfg, dev, seed0 + 900)
     # ---- batched vs serial rendering of many uneven scenes
     batch = None if args.no_batch else batch_compare(args, backend, torch, stream, dev, world)
     # ---- the animated sequence: device scene preparation + refit per frame
