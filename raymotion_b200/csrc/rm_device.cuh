@@ -300,10 +300,10 @@ __device__ __forceinline__ float dequant(float p, uint32_t q, float scale) {
   return __fmaf_rn(__uint_as_float(0x4B000000u | q) - 8388608.0f, scale, p);
 }
 
-// Byte b of `word` on the grid p + q scale (one byte permute, one add, one fma).
+// Byte b of `word` as a float (exact): 0x4B000000 | q is the float 2^23 + q.
 template <int b>
-__device__ __forceinline__ float dequant_byte(uint32_t word, float p, float scale) {
-  return __fmaf_rn(__uint_as_float(__byte_perm(word, 0x4B000000u, 0x7540u | b)) - 8388608.0f, scale, p);
+__device__ __forceinline__ float byte_float(uint32_t word) {
+  return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7540u | b)) - 8388608.0f;
 }
 
 // Resumable traversal of the wide BVH: init() then step() until it returns
@@ -354,20 +354,41 @@ struct WTrav {
     const float sy = __uint_as_float(((ew >> 8) & 0xFFu) << 23);
     const float sz = __uint_as_float(((ew >> 16) & 0xFFu) << 23);
     // n1: child_base, tri_base, meta 0-3, meta 4-7; n2: qlo_x (8), qlo_y (8);
-    // n3: qlo_z (8), qhi_x (8); n4: qhi_y (8), qhi_z (8)
+    // n3: qlo_z (8), qhi_x (8); n4: qhi_y (8), qhi_z (8).
+    // A child's slab on axis a is t = q s_a i_a + (p_a - o_a) i_a, one fma per
+    // bound from the per-node base (p_a - o_a) i_a and the exact product
+    // s_a i_a (s_a is a power of two).  Its rounding differs from the binary
+    // traversal's (L - o) i, so the near bound's base is lowered and the far
+    // bound's raised by m_a = |i_a| 2^-20 (|p_a - o_a| + 256 s_a + |p_a|),
+    // rounded outward: m_a exceeds the sum of both forms' rounding errors and
+    // of the decoded bound's half ulp, so every box the binary test accepts
+    // is accepted here and the hits stay the binary traversal's.  Which
+    // stored bound is near follows the sign of i_a (the decoded lo <= hi).
+    const float six = sx * ix, siy = sy * iy, siz = sz * iz;
+    const float bx = (n0.x - ox) * ix, by = (n0.y - oy) * iy, bz = (n0.z - oz) * iz;
+    const float mx = fabsf(ix) * 0x1p-20f * (fabsf(n0.x - ox) + 256.0f * sx + fabsf(n0.x));
+    const float my = fabsf(iy) * 0x1p-20f * (fabsf(n0.y - oy) + 256.0f * sy + fabsf(n0.y));
+    const float mz = fabsf(iz) * 0x1p-20f * (fabsf(n0.z - oz) + 256.0f * sz + fabsf(n0.z));
+    const float bnx = __fsub_rd(bx, mx), bfx = __fadd_ru(bx, mx);
+    const float bny = __fsub_rd(by, my), bfy = __fadd_ru(by, my);
+    const float bnz = __fsub_rd(bz, mz), bfz = __fadd_ru(bz, mz);
+    const bool sxp = ix >= 0.0f, syp = iy >= 0.0f, szp = iz >= 0.0f;
+    const uint32_t nx0 = sxp ? n2.x : n3.z, nx1 = sxp ? n2.y : n3.w, fx0 = sxp ? n3.z : n2.x, fx1 = sxp ? n3.w : n2.y;
+    const uint32_t ny0 = syp ? n2.z : n4.x, ny1 = syp ? n2.w : n4.y, fy0 = syp ? n4.x : n2.z, fy1 = syp ? n4.y : n2.w;
+    const uint32_t nz0 = szp ? n3.x : n4.z, nz1 = szp ? n3.y : n4.w, fz0 = szp ? n4.z : n3.x, fz1 = szp ? n4.w : n3.y;
     uint32_t ikeys = 0, tmask = 0;
 #define RM_WIDE_SLOT(J, H, B)                                                                              \
   {                                                                                                        \
     const uint32_t meta = (n1.H >> (8 * B)) & 0xFFu;                                                       \
     if (meta != 0xFFu) {                                                                                   \
-      const float lx = (dequant_byte<B>(J < 4 ? n2.x : n2.y, n0.x, sx) - ox) * ix;                         \
-      const float hx = (dequant_byte<B>(J < 4 ? n3.z : n3.w, n0.x, sx) - ox) * ix;                         \
-      const float ly = (dequant_byte<B>(J < 4 ? n2.z : n2.w, n0.y, sy) - oy) * iy;                         \
-      const float hy = (dequant_byte<B>(J < 4 ? n4.x : n4.y, n0.y, sy) - oy) * iy;                         \
-      const float lz = (dequant_byte<B>(J < 4 ? n3.x : n3.y, n0.z, sz) - oz) * iz;                         \
-      const float hz = (dequant_byte<B>(J < 4 ? n4.z : n4.w, n0.z, sz) - oz) * iz;                         \
-      const float tn = fmaxf(0.0f, fmaxf(fminf(lx, hx), fmaxf(fminf(ly, hy), fminf(lz, hz))));            \
-      const float tf = fminf(r.t, fminf(fmaxf(lx, hx), fminf(fmaxf(ly, hy), fmaxf(lz, hz))));             \
+      const float tnx = __fmaf_rn(byte_float<B>(J < 4 ? nx0 : nx1), six, bnx);                             \
+      const float tny = __fmaf_rn(byte_float<B>(J < 4 ? ny0 : ny1), siy, bny);                             \
+      const float tnz = __fmaf_rn(byte_float<B>(J < 4 ? nz0 : nz1), siz, bnz);                             \
+      const float tfx = __fmaf_rn(byte_float<B>(J < 4 ? fx0 : fx1), six, bfx);                             \
+      const float tfy = __fmaf_rn(byte_float<B>(J < 4 ? fy0 : fy1), siy, bfy);                             \
+      const float tfz = __fmaf_rn(byte_float<B>(J < 4 ? fz0 : fz1), siz, bfz);                             \
+      const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));                                           \
+      const float tf = fminf(fminf(tfx, tfy), fminf(tfz, r.t));                                            \
       if (!(tn > tf * kBoxSlack)) {                                                                        \
         if (meta == 0xFEu) ikeys |= 1u << (uint32_t(J) ^ oct);                                             \
         else tmask |= ((1u << ((meta >> 5) + 1u)) - 1u) << (meta & 31u);                                   \
