@@ -298,6 +298,7 @@ typedef struct rm_batch_tuning {
   int32_t tile_shape;   /* pixels of a chunk: 0 a row segment, 1 a near-square block */
   int32_t grid_scale;   /* persistent grids: resident blocks per SM x this (1..4) */
   int32_t graph_waves;  /* waves per CUDA graph launch (even, 2..64); 0: no graph */
+  int32_t bvh_width;    /* 2: the binary BVH; 8: the 8-wide compressed BVH (collapsed per scene on first use) */
 } rm_batch_tuning;
 
 /* Render many images of (possibly different) scenes, views, resolutions,

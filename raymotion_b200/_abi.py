@@ -104,7 +104,7 @@ class RmBatchItem(C.Structure):
 
 class RmBatchTuning(C.Structure):
     _fields_ = [("pool_chunks", C.c_int32), ("tile_shape", C.c_int32), ("grid_scale", C.c_int32),
-                ("graph_waves", C.c_int32)]
+                ("graph_waves", C.c_int32), ("bvh_width", C.c_int32)]
 
 
 # (name, restype, argtypes) of every symbol declared in include/rmcuda.h

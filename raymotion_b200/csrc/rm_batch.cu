@@ -210,7 +210,17 @@ __global__ void __launch_bounds__(256) k_bt_start(BtBatch b, BtState w, BtQueues
 // rays, pathtrace.metal:119-163 and :536-550; any hit for shadow rays, :164).
 // Finished extension rays are sorted into the shading queue of their surface
 // type.
-template <bool kShadowRays>
+// One ray of a batch job: through the 8-wide BVH (kWide, when the job's scene
+// has one) or the binary BVH; both give the same hit.
+template <bool kAnyHit, bool kWide>
+__device__ __forceinline__ TraceResult bt_traverse(const Scene& s, float ox, float oy, float oz, float dx, float dy,
+                                                   float dz, float tmax, uint32_t* err, uint32_t& nodes,
+                                                   uint32_t& tests) {
+  if (kWide) return traverse_any<kAnyHit>(s, ox, oy, oz, dx, dy, dz, tmax, err, nodes, tests);
+  return traverse<kAnyHit>(s, ox, oy, oz, dx, dy, dz, tmax, err, nodes, tests);
+}
+
+template <bool kShadowRays, bool kWide>
 __global__ void __launch_bounds__(128) k_bt_trace(BtBatch b, BtState w, BtQueues q, unsigned long long* ctr,
                                                   uint32_t* err) {
   const int n = q.counts[kShadowRays ? kBtShd : kBtExt];
@@ -227,14 +237,14 @@ __global__ void __launch_bounds__(128) k_bt_trace(BtBatch b, BtState w, BtQueues
       const Scene& s = J.s;
       if (kShadowRays) {
         const float4 o = w.so[i], d = w.sd[i];
-        const TraceResult r = traverse<true>(s, o.x, o.y, o.z, d.x, d.y, d.z, o.w, err, nodes, tests);
+        const TraceResult r = bt_traverse<true, kWide>(s, o.x, o.y, o.z, d.x, d.y, d.z, o.w, err, nodes, tests);
         ++rays;
         w.occ[i] = r.tri >= 0 ? 1u : 0u;
       } else {
         const float4 o = w.o[i], d = w.d[i];
         TraceResult r;
         if (J.p.opaque) {
-          r = traverse<false>(s, o.x, o.y, o.z, d.x, d.y, d.z, kFar, err, nodes, tests);
+          r = bt_traverse<false, kWide>(s, o.x, o.y, o.z, d.x, d.y, d.z, kFar, err, nodes, tests);
           ++rays;
         } else {
           // stochastic coverage: step through transparent crossings
@@ -246,7 +256,8 @@ __global__ void __launch_bounds__(128) k_bt_trace(BtBatch b, BtState w, BtQueues
           float hx = o.x, hy = o.y, hz = o.z;
           for (int it = 0; it < kMaxAlphaCrossings && traveled < kFar; ++it) {
             const float qx = o.x + d.x * traveled, qy = o.y + d.y * traveled, qz = o.z + d.z * traveled;
-            const TraceResult h = traverse<false>(s, qx, qy, qz, d.x, d.y, d.z, kFar - traveled, err, nodes, tests);
+            const TraceResult h =
+                bt_traverse<false, kWide>(s, qx, qy, qz, d.x, d.y, d.z, kFar - traveled, err, nodes, tests);
             ++rays;
             if (h.tri < 0) break;
             const float opacity = s.tris[h.tri].alpha;
@@ -471,10 +482,15 @@ cudaError_t launch_batch_combine(int lanes, const BtBatch& b, const BtState& w, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_batch_trace(const BtBatch& b, const BtState& w, const BtQueues& q, bool shadow, int grid,
-                               unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
-  if (shadow) k_bt_trace<true><<<grid, 128, 0, st>>>(b, w, q, ctr, err);
-  else k_bt_trace<false><<<grid, 128, 0, st>>>(b, w, q, ctr, err);
+cudaError_t launch_batch_trace(const BtBatch& b, const BtState& w, const BtQueues& q, bool shadow, bool wide,
+                               int grid, unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
+  if (wide) {
+    if (shadow) k_bt_trace<true, true><<<grid, 128, 0, st>>>(b, w, q, ctr, err);
+    else k_bt_trace<false, true><<<grid, 128, 0, st>>>(b, w, q, ctr, err);
+  } else {
+    if (shadow) k_bt_trace<true, false><<<grid, 128, 0, st>>>(b, w, q, ctr, err);
+    else k_bt_trace<false, false><<<grid, 128, 0, st>>>(b, w, q, ctr, err);
+  }
   return cudaGetLastError();
 }
 
@@ -491,7 +507,8 @@ void batch_occupancy(int& aux, int& trace, int& shade) {
   aux = trace = shade = 1;
   int v = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_bt_start, 256, 0) == cudaSuccess && v > 0) aux = v;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_bt_trace<false>, 128, 0) == cudaSuccess && v > 0) trace = v;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_bt_trace<false, false>, 128, 0) == cudaSuccess && v > 0)
+    trace = v;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_bt_shade<0>, 256, 0) == cudaSuccess && v > 0) shade = v;
 }
 

@@ -79,7 +79,7 @@ struct BatchPool {
   DevBuf chunk[3];   // per chunk arrays of BtState
   DevBuf queue[2 * rmd::kBtQueues + 1];  // the queues of two waves + the counts of both
   DevBuf jobs, tile_begin, next_tile;
-  rm_batch_tuning tuning{65536, 0, 1, 8};
+  rm_batch_tuning tuning{65536, 0, 1, 8, 2};
   int chunks = 0;    // pool size the buffers hold, in chunks of 32 lane slots
   int occ[3] = {0, 0, 0};  // resident blocks per SM of the batch kernels
   int* h_counts = nullptr;  // pinned: queue lengths read back between graph launches (2 x kBtCounts)

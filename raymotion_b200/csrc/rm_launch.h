@@ -131,7 +131,7 @@ cudaError_t launch_batch_init(const BtState& w, const BtQueues& q0, int chunks, 
 cudaError_t launch_batch_refill(const BtBatch& b, const BtState& w, const BtQueues& q, int grid, cudaStream_t st);
 cudaError_t launch_batch_start(const BtBatch& b, const BtState& w, const BtQueues& q, const BtQueues& nq, int grid,
                                unsigned long long* ctr, uint32_t* err, cudaStream_t st);
-cudaError_t launch_batch_trace(const BtBatch& b, const BtState& w, const BtQueues& q, bool shadow, int grid,
+cudaError_t launch_batch_trace(const BtBatch& b, const BtState& w, const BtQueues& q, bool shadow, bool wide, int grid,
                                unsigned long long* ctr, uint32_t* err, cudaStream_t st);
 cudaError_t launch_batch_shade(int vk, const BtBatch& b, const BtState& w, const BtQueues& q, const BtQueues& nq,
                                int grid, unsigned long long* ctr, uint32_t* err, cudaStream_t st);

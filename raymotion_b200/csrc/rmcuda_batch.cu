@@ -91,7 +91,8 @@ BtQueues queue_view(const BatchPool& bp, int k) {
 bool valid_tuning(const rm_batch_tuning& t) {
   return t.pool_chunks >= 1 && t.pool_chunks <= (1 << 22) && (t.tile_shape == 0 || t.tile_shape == 1) &&
          t.grid_scale >= 1 && t.grid_scale <= 4 &&
-         (t.graph_waves == 0 || (t.graph_waves >= 2 && t.graph_waves <= 64 && t.graph_waves % 2 == 0));
+         (t.graph_waves == 0 || (t.graph_waves >= 2 && t.graph_waves <= 64 && t.graph_waves % 2 == 0)) &&
+         (t.bvh_width == 2 || t.bvh_width == 8);
 }
 
 // Tile of a chunk: tile_w x tile_h pixels of `lanes` lane slots each.
@@ -112,7 +113,8 @@ struct Prepared {
   uint64_t max_waves = 0;
 };
 
-int prepare(rmcuda_ctx* c, const rm_batch_item* items, int n, int shape, Prepared& out, std::string& msg) {
+int prepare(rmcuda_ctx* c, const rm_batch_item* items, int n, int shape, int width, Prepared& out,
+            std::string& msg) {
   if (n < 0 || (n > 0 && !items)) { msg = "invalid batch"; return RM_ERR_INVALID; }
   std::vector<std::pair<double, int>> order;
   std::vector<BtJob> jobs(static_cast<size_t>(n));
@@ -138,7 +140,19 @@ int prepare(rmcuda_ctx* c, const rm_batch_item* items, int n, int shape, Prepare
     }
     BtJob& J = jobs[size_t(i)];
     std::memset(&J, 0, sizeof(J));
+    // the collapse is a cache of the scene object, built once under the context lock
+    rmd::DevBvh& bvh = const_cast<rmcuda_scene*>(it.scene)->d.bvh;
+    if (width == 8 && bvh.n_wide == 0 && bvh.n_records > 0) {
+      // collapse this scene's binary BVH on first use (none if too deep: the
+      // job then traverses the binary BVH, which gives the same hits)
+      const cudaError_t e = rmd::build_wide(bvh, c->stream);
+      if (e != cudaSuccess) { msg = cuda_msg("wide BVH build failed", e); return RM_ERR_CUDA; }
+    }
     J.s = scene_view(it.scene->d);
+    if (width != 8) {
+      J.s.wnodes = nullptr;
+      J.s.wtgeo = nullptr;
+    }
     J.p = pl.p;
     J.seed = it.seed;
     J.hdr = it.d_hdr;
@@ -176,6 +190,7 @@ int prepare(rmcuda_ctx* c, const rm_batch_item* items, int n, int shape, Prepare
 
 struct Grids {
   int aux, trace, shade;
+  bool wide;  // traverse the 8-wide BVHs
 };
 
 Grids grids(rmcuda_ctx* c, int scale) {
@@ -183,7 +198,7 @@ Grids grids(rmcuda_ctx* c, int scale) {
   if (!occ[0]) batch_occupancy(occ[0], occ[1], occ[2]);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-  return Grids{sms * occ[0] * scale, sms * occ[1] * scale, sms * occ[2] * scale};
+  return Grids{sms * occ[0] * scale, sms * occ[1] * scale, sms * occ[2] * scale, false};
 }
 
 // Kernels of a wave: refill, start, 2 traversals, 4 shades, 3 round sums.
@@ -205,10 +220,10 @@ cudaError_t enqueue_wave(rmcuda_ctx* c, const BtBatch& b, const BtState& w, cons
                 [&] { return launch_batch_start(b, w, Q, N, g.aux, ctr + 4 * RM_STAGE_BT_START, err, st); });
   if (e == cudaSuccess)
     e = staged2(c, RM_STAGE_BT_EXTEND,
-                [&] { return launch_batch_trace(b, w, Q, false, g.trace, ctr + 4 * RM_STAGE_BT_EXTEND, err, st); });
+                [&] { return launch_batch_trace(b, w, Q, false, g.wide, g.trace, ctr + 4 * RM_STAGE_BT_EXTEND, err, st); });
   if (e == cudaSuccess)
     e = staged2(c, RM_STAGE_BT_SHADOW,
-                [&] { return launch_batch_trace(b, w, Q, true, g.trace, ctr + 4 * RM_STAGE_BT_SHADOW, err, st); });
+                [&] { return launch_batch_trace(b, w, Q, true, g.wide, g.trace, ctr + 4 * RM_STAGE_BT_SHADOW, err, st); });
   for (int vk = 0; vk < 4 && e == cudaSuccess; ++vk)
     e = staged2(c, RM_STAGE_BT_SHADE,
                 [&] { return launch_batch_shade(vk, b, w, Q, N, g.shade, ctr + 4 * RM_STAGE_BT_SHADE, err, st); });
@@ -254,7 +269,8 @@ int run_batch(rmcuda_ctx* c, const Prepared& P, const rm_batch_tuning& tune, Win
     return RM_ERR_CUDA;
   }
   c->launches += 1;
-  const Grids g = grids(c, tune.grid_scale);
+  Grids g = grids(c, tune.grid_scale);
+  g.wide = tune.bvh_width == 8;
   // (the legacy default stream cannot be captured)
   const bool use_graph = tune.graph_waves > 0 && c->profiling < 2 && c->stream != nullptr;
   const int per_launch = use_graph ? tune.graph_waves : 8;
@@ -386,7 +402,7 @@ int rmcuda_render_batch(rmcuda_ctx* c, const rm_batch_item* items, int32_t n, ch
   cudaSetDevice(c->device);
   std::string msg;
   Prepared P;
-  int rc = prepare(c, items, n, c->batch.tuning.tile_shape, P, msg);
+  int rc = prepare(c, items, n, c->batch.tuning.tile_shape, c->batch.tuning.bvh_width, P, msg);
   cudaEvent_t a = nullptr, b = nullptr;
   if (rc == RM_OK && c->profiling > 0 && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess)
     cudaEventRecord(a, c->stream);
@@ -422,12 +438,13 @@ int rmcuda_batch_tune(rmcuda_ctx* c, const rm_batch_item* items, int32_t n, rm_b
   const int saved_profiling = c->profiling;
   c->profiling = 0;
   for (int pool : pools) {
+    for (int width : {2, 8}) {
     for (int shape = 0; shape < 2 && rc == RM_OK; ++shape) {
       for (int scale = 1; scale <= 2 && rc == RM_OK; ++scale) {
-        const rm_batch_tuning t{pool, shape, scale, keep.graph_waves > 0 ? keep.graph_waves : 8};
+        const rm_batch_tuning t{pool, shape, scale, keep.graph_waves > 0 ? keep.graph_waves : 8, width};
         c->batch.tuning = t;
         Prepared P;
-        if ((rc = prepare(c, items, n, shape, P, msg)) != RM_OK) break;
+        if ((rc = prepare(c, items, n, shape, width, P, msg)) != RM_OK) break;
         if ((rc = run_batch(c, P, t, &win, msg)) != RM_OK) break;
         float ms = 0.f;
         cudaEventElapsedTime(&ms, win.t0, win.t1);
@@ -436,6 +453,7 @@ int rmcuda_batch_tune(rmcuda_ctx* c, const rm_batch_item* items, int32_t n, rm_b
         const double rate = ms > 0.f ? samples / double(ms) : 0.0;
         if (rate > best_rate) { best_rate = rate; best = t; }
       }
+    }
     }
     if (rc != RM_OK) break;
   }

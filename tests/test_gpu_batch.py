@@ -100,13 +100,14 @@ def _render_batch(backend, images, handles):
 
 
 TUNINGS = [
-    dict(pool_chunks=65536, tile_shape=0, grid_scale=1, graph_waves=8),
-    dict(pool_chunks=5, tile_shape=1, grid_scale=1, graph_waves=2),
-    dict(pool_chunks=37, tile_shape=0, grid_scale=2, graph_waves=0),
+    dict(pool_chunks=65536, tile_shape=0, grid_scale=1, graph_waves=8, bvh_width=2),
+    dict(pool_chunks=5, tile_shape=1, grid_scale=1, graph_waves=2, bvh_width=2),
+    dict(pool_chunks=37, tile_shape=0, grid_scale=2, graph_waves=0, bvh_width=2),
+    dict(pool_chunks=65536, tile_shape=1, grid_scale=1, graph_waves=8, bvh_width=8),
 ]
 
 
-@pytest.mark.parametrize("tuning", TUNINGS, ids=["default", "tiny_pool_graph2", "small_pool_nograph"])
+@pytest.mark.parametrize("tuning", TUNINGS, ids=["default", "tiny_pool_graph2", "small_pool_nograph", "wide_bvh"])
 def test_batch_equals_single_image_renders(backend, batch_case, tuning):
     images, handles, refs = batch_case
     backend.set_batch_tuning(**tuning)
