@@ -320,7 +320,7 @@ def batch_compare(args, backend, torch, stream, dev, world):
         equal_samples=bool(s_samples == b_samples), scene_build_s=build_s, tune_s=tune_s)
 
 
-def adjoint_measure(args, backend, torch, stream, dev):
+def adjoint_measure(args, backend, torch, stream, dev, rank=0, world=1):
     """Differentiable rendering on raymotion_b200.scenes.inverse_scene: 100
     displaced icospheres (subdivision 3) + a 190 x 190-quad ground + 16 quad
     lights = 200,232 triangles, 256 materials, 512 x 512, 32 spp, depth 8.
@@ -334,7 +334,10 @@ def adjoint_measure(args, backend, torch, stream, dev):
     replaying an independent frame each step (an unbiased gradient of the
     expected loss).  Reports the mean normalised parameter error before and
     after, over all fitted parameters and over those of materials the camera
-    sees directly on at least 256 pixels."""
+    sees directly on at least 256 pixels.  With several ranks the fit is data
+    parallel (raymotion_b200.inverse.MaterialFit): each rank renders its own
+    seeds and the gradients are averaged by one all-reduce per step."""
+    from raymotion_b200.inverse import MaterialFit
     import raymotion_b200 as rb
     from raymotion_b200.scene import with_materials
     from raymotion_b200.scenes import INVERSE_HI, INVERSE_LO, inverse_scene
@@ -410,8 +413,7 @@ def adjoint_measure(args, backend, torch, stream, dev):
     gen = torch.Generator(device=dev).manual_seed(4)
     noise = (torch.rand(true.shape, device=dev, generator=gen) * 2 - 1) * 0.3
     start = torch.where(mask, torch.minimum(torch.maximum(true * (1 + noise), lo), hi), true)
-    u = ((start - lo) / (hi - lo)).clone()
-    opt = torch.optim.Adam([u.requires_grad_(True)], lr=1e-2)
+    fit = MaterialFit(start, true, mask, lo, hi, lr=1e-2)
     seen_t = torch.from_numpy(seen).to(dev)[:, None] & mask
 
     def errors(p):
@@ -430,24 +432,19 @@ def adjoint_measure(args, backend, torch, stream, dev):
     f0.record(stream)
     losses = []
     for it in range(args.fit_iters):
-        p = torch.where(mask, lo + (hi - lo) * u.detach().clamp(0, 1), true)
-        set_params(p.cpu().numpy())
-        backend.render_scene_async(h, cam, cfg, 10000 + it, None, img.data_ptr())
+        set_params(fit.params().cpu().numpy())
+        backend.render_scene_async(h, cam, cfg, 10000 + it + 1000003 * rank, None, img.data_ptr())
         dl.copy_((2.0 / img.numel()) * (img - target))
         losses.append(((img - target) ** 2).mean())
         grad.zero_()
-        backend.backward(h, cam, cfg, 20000 + it, dl.data_ptr(), grad.data_ptr())
-        opt.zero_grad()
-        u.grad = torch.where(mask, grad.view(n_mat, 8) * (hi - lo), torch.zeros_like(u))
-        opt.step()
-        with torch.no_grad():
-            u.clamp_(0, 1)
+        backend.backward(h, cam, cfg, 20000 + it + 1000003 * rank, dl.data_ptr(), grad.data_ptr())
+        backend.sync()
+        fit.step(grad)  # with several ranks: the mean gradient (one all-reduce)
     f1.record(stream)
     backend.sync()
     torch.cuda.synchronize()
     fit_s = time.time() - t0
-    p = torch.where(mask, lo + (hi - lo) * u.detach(), true)
-    err1 = errors(p)
+    err1 = errors(fit.params())
     backend.scene_destroy(h)
     loss_curve = [float(x) for x in torch.stack(losses).cpu().numpy()]
     return dict(
@@ -456,7 +453,7 @@ def adjoint_measure(args, backend, torch, stream, dev):
         forward_ms=fwd_ms, adjoint_ms=bwd_ms, adjoint_over_forward=bwd_ms / fwd_ms,
         adjoint_samples_per_call=int(st["adjoint"]["path_samples"] / 5),
         fit=dict(iterations=args.fit_iters, lr=1e-2, optimiser="Adam on normalised parameters",
-                 target_spp=1024, fit_spp=cfg.spp, wall_s=fit_s, gpu_ms=f0.elapsed_time(f1),
+                 target_spp=1024, fit_spp=cfg.spp, ranks=world, wall_s=fit_s, gpu_ms=f0.elapsed_time(f1),
                  param_error_start=err0, param_error_end=err1, materials_seen=int(seen.sum()),
                  loss_first10=float(np.mean(loss_curve[:10])), loss_last10=float(np.mean(loss_curve[-10:]))))
 
@@ -774,7 +771,7 @@ def run_b200(args, world, rank, local):
     # ---- the animated sequence: device scene preparation + refit per frame
     sequence = None if args.no_sequence else sequence_measure(args, backend, torch, stream, dev)
     # ---- differentiable rendering: adjoint cost and a 200-step fit
-    adjoint = None if args.no_adjoint else adjoint_measure(args, backend, torch, stream, dev)
+    adjoint = None if args.no_adjoint else adjoint_measure(args, backend, torch, stream, dev, rank, world)
     # ---- CPU baseline (rank 0, N=1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
