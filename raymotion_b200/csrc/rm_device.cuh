@@ -602,6 +602,62 @@ struct Tracer {
   }
 
   // pathtrace.metal:243-295
+  // The factors of eval_bsdf that do not depend on wi, computed once for a
+  // vertex whose candidate loop evaluates many wi (same expressions, so the
+  // same values as eval_bsdf computes per call).
+  struct BsdfPrep {
+    float cos_o, g1, di, f0r, f0g, f0b, adr, adg, adb;
+  };
+  __device__ static __forceinline__ BsdfPrep prep_bsdf(float wox, float woy, float woz, float nx, float ny, float nz,
+                                                       float alpha2, float metallic, float ar, float ag, float ab) {
+    BsdfPrep q;
+    q.cos_o = wox * nx + (woy * ny + woz * nz);
+    q.g1 = 2.0f * q.cos_o / (q.cos_o + sqrtf(q.cos_o * q.cos_o + alpha2 * (1.0f - q.cos_o * q.cos_o)));
+    q.di = 1.0f - metallic;
+    q.f0r = 0.04f * q.di + ar * metallic;
+    q.f0g = 0.04f * q.di + ag * metallic;
+    q.f0b = 0.04f * q.di + ab * metallic;
+    q.adr = ar * q.di;
+    q.adg = ag * q.di;
+    q.adb = ab * q.di;
+    return q;
+  }
+
+  // eval_bsdf with the wi-independent factors of prep_bsdf.
+  __device__ static __forceinline__ Bsdf eval_bsdf_prep(const BsdfPrep& q, float wix, float wiy, float wiz, float wox,
+                                                        float woy, float woz, float nx, float ny, float nz,
+                                                        float alpha2, float spec_prob) {
+    Bsdf out{0.f, 0.f, 0.f, 0.f};
+    float cos_i = wix * nx + (wiy * ny + wiz * nz);
+    const float cos_o = q.cos_o;
+    if (!(cos_i > 1e-8f && cos_o > 1e-8f)) return out;
+    float hx = wix + wox, hy = wiy + woy, hz = wiz + woz;
+    float hl = sqrtf(hx * hx + hy * hy + hz * hz);
+    if (!(hl > 1e-8f)) return out;
+    float inv = 1.0f / hl;
+    hx *= inv; hy *= inv; hz *= inv;
+    float cos_h = hx * nx + (hy * ny + hz * nz);
+    float vo_h = wox * hx + (woy * hy + woz * hz);
+    if (cos_h < 0.0f) { hx = -hx; hy = -hy; hz = -hz; cos_h = -cos_h; vo_h = -vo_h; }
+    if (!(vo_h > 1e-8f)) return out;
+    float dd = cos_h * cos_h * (alpha2 - 1.0f) + 1.0f;
+    float D = alpha2 / (kPi * dd * dd);
+    float g2 = 2.0f * cos_i / (cos_i + sqrtf(cos_i * cos_i + alpha2 * (1.0f - cos_i * cos_i)));
+    float G = q.g1 * g2;
+    float om = 1.0f - vo_h;
+    om *= om; om *= om; om *= 1.0f - vo_h;
+    float fr = q.f0r + (1.0f - q.f0r) * om, fg = q.f0g + (1.0f - q.f0g) * om, fb = q.f0b + (1.0f - q.f0b) * om;
+    float kdr = q.adr * (1.0f - fr), kdg = q.adg * (1.0f - fg), kdb = q.adb * (1.0f - fb);
+    float base = D * G / (4.0f * cos_i * cos_o);
+    out.r = kdr / kPi + base * fr;
+    out.g = kdg / kPi + base * fg;
+    out.b = kdb / kPi + base * fb;
+    float pdf_d = cos_i / kPi;
+    float pdf_s = D * cos_h / (4.0f * vo_h);
+    out.pdf = (1.0f - spec_prob) * pdf_d + spec_prob * pdf_s;
+    return out;
+  }
+
   __device__ static __forceinline__ Bsdf eval_bsdf(float wix, float wiy, float wiz, float wox, float woy, float woz,
                                                    float nx, float ny, float nz, float alpha2, float metallic,
                                                    float spec_prob, float ar, float ag, float ab) {
@@ -882,6 +938,7 @@ struct Tracer {
     float sumW = 0.0f;
     float sel_lx = 0, sel_ly = 0, sel_lz = 0, sel_Fr = 0, sel_Fg = 0, sel_Fb = 0, sel_phat = 0, sel_epdf = 0;
     bool have = false;
+    const BsdfPrep bp = prep_bsdf(wox, woy, woz, nx, ny, nz, alpha2, metallic, ar, ag, ab);
     for (int j = 0; j < Mc; ++j) {
       float pick = U() * LT;
       const LightRec t = load_light(s, pick_light(pick));
@@ -904,7 +961,7 @@ struct Tracer {
           if (lt_lum < 1e-6f) lt_lum = 1e-6f;
           float q = dist * dist * lt_lum / (lcos * LT);
           if (q > 1e-12f) {
-            Bsdf e = eval_bsdf(dxn, dyn, dzn, wox, woy, woz, nx, ny, nz, alpha2, metallic, spec_prob, ar, ag, ab);
+            Bsdf e = eval_bsdf_prep(bp, dxn, dyn, dzn, wox, woy, woz, nx, ny, nz, alpha2, spec_prob);
             epdf = e.pdf;
             Fr = t.er * e.r * scos * t.alpha;
             Fg = t.eg * e.g * scos * t.alpha;

@@ -181,6 +181,8 @@ __global__ void __launch_bounds__(256) k_restir_generate(Scene s, Params p, uint
         float sel_er = 0, sel_eg = 0, sel_eb = 0, sel_alpha = 1, sel_ph = 0;
         bool have = false;
         const float sox = px + pnx * 0.002f, soy = py + pny * 0.002f, soz = pz + pnz * 0.002f;
+        const Tracer::BsdfPrep bp =
+            Tracer::prep_bsdf(wox, woy, woz, pnx, pny, pnz, alpha2, metallic, hit.ar, hit.ag, hit.ab);
         for (int j = 0; j < Mc; ++j) {
           float pick = pt.U() * p.light_total;
           const LightRec t = load_light(s, pt.pick_light(pick));
@@ -202,8 +204,7 @@ __global__ void __launch_bounds__(256) k_restir_generate(Scene s, Params p, uint
               float ll = lum3(t.er, t.eg, t.eb); if (ll < 1e-6f) ll = 1e-6f;
               float q = dist * dist * ll / (lcos * p.light_total);
               if (q > 1e-12f) {
-                Bsdf e = Tracer::eval_bsdf(dxn, dyn, dzn, wox, woy, woz, pnx, pny, pnz, alpha2, metallic, spec_prob,
-                                           hit.ar, hit.ag, hit.ab);
+                Bsdf e = Tracer::eval_bsdf_prep(bp, dxn, dyn, dzn, wox, woy, woz, pnx, pny, pnz, alpha2, spec_prob);
                 float Fr = t.er * e.r * scos * t.alpha, Fg = t.eg * e.g * scos * t.alpha,
                       Fb = t.eb * e.b * scos * t.alpha;
                 ph = lum3(Fr, Fg, Fb);
