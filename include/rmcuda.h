@@ -133,6 +133,7 @@ typedef struct rm_stats {
   uint32_t bvh_node_bytes;  /* bytes of one node visit: 80 (8-wide compressed BVH) or 64 (binary) */
   uint32_t bvh_builds;      /* device BVH builds of the resident scene since the context was created */
   uint32_t bvh_refits;      /* device BVH refits of the resident scene since the context was created */
+  uint32_t bvh_kept;        /* uploads of the resident scene with unchanged triangles: BVH kept, not rebuilt */
 } rm_stats;
 
 typedef struct rmcuda_ctx rmcuda_ctx;

@@ -263,7 +263,7 @@ class Backend:
         return dict(path_samples=s.path_samples, rays=s.rays, nodes_visited=s.nodes_visited,
                     tris_tested=s.tris_tested, frames=s.frames, kernel_launches=s.kernel_launches,
                     device_error=s.device_error, kernel_chain=s.kernel_chain, bvh_node_bytes=s.bvh_node_bytes,
-                    bvh_builds=s.bvh_builds, bvh_refits=s.bvh_refits)
+                    bvh_builds=s.bvh_builds, bvh_refits=s.bvh_refits, bvh_kept=s.bvh_kept)
 
     def stats_reset(self) -> None:
         self.lib.rmcuda_stats_reset(self.h)

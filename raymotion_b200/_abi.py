@@ -94,7 +94,7 @@ class RmStats(C.Structure):
     _fields_ = [("path_samples", C.c_uint64), ("rays", C.c_uint64), ("nodes_visited", C.c_uint64),
                 ("tris_tested", C.c_uint64), ("frames", C.c_uint64), ("kernel_launches", C.c_uint64),
                 ("device_error", C.c_uint32), ("kernel_chain", C.c_uint32), ("bvh_node_bytes", C.c_uint32),
-                ("bvh_builds", C.c_uint32), ("bvh_refits", C.c_uint32)]
+                ("bvh_builds", C.c_uint32), ("bvh_refits", C.c_uint32), ("bvh_kept", C.c_uint32)]
 
 
 class RmBatchItem(C.Structure):

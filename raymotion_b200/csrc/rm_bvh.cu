@@ -318,6 +318,16 @@ __global__ void k_hash(const unsigned long long* __restrict__ w, size_t n, unsig
   if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
 }
 
+// flag[0] |= 1 where the two word arrays differ.
+__global__ void k_differ(const uint4* __restrict__ a, const uint4* __restrict__ b, size_t n, int* flag) {
+  bool d = false;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    const uint4 x = a[i], y = b[i];
+    d |= (x.x != y.x) | (x.y != y.y) | (x.z != y.z) | (x.w != y.w);
+  }
+  if (__any_sync(0xffffffffu, d) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 __global__ void k_light_records(const rm_triangle* __restrict__ tris, const int32_t* __restrict__ lights, int n,
                                 float4* __restrict__ rec) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -387,6 +397,14 @@ cudaError_t refit_bvh(const rm_triangle* d_tris, DevBvh& bvh, cudaStream_t st) {
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return pack_tgeo(d_tris, bvh, st);
+}
+
+cudaError_t device_differ(const void* a, const void* b, size_t n_bytes, int* d_flag, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(d_flag, 0, sizeof(int), st);
+  if (e != cudaSuccess || n_bytes == 0) return e;
+  if (n_bytes % 16) return cudaErrorInvalidValue;
+  k_differ<<<148 * 4, 256, 0, st>>>(static_cast<const uint4*>(a), static_cast<const uint4*>(b), n_bytes / 16, d_flag);
+  return cudaGetLastError();
 }
 
 cudaError_t device_hash(const void* d_bytes, size_t n_bytes, unsigned long long* d_out, cudaStream_t st) {

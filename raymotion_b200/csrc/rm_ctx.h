@@ -48,6 +48,9 @@ struct ResSet {
 // light-sampling tables and the BVH.
 struct DevScene {
   DevBuf tris, lights, cdf, texels, lrec, guide;
+  DevBuf tris_in;  // staging of an upload compared with `tris` before the BVH is rebuilt
+  uint64_t reuses = 0;  // uploads whose triangles equalled the resident ones (BVH kept)
+  std::string build_key;  // the BVH build settings the resident BVH was built with
   int guide_n = 0;
   float guide_inv = 0.0f;
   DevBvh bvh;
@@ -62,7 +65,7 @@ struct DevScene {
   DevBuf tri_mat, mats;
   int n_materials = 0;
   void release() {
-    for (DevBuf* b : {&tri_mat, &mats, &tris, &lights, &cdf, &texels, &lrec, &guide, &bvh.records, &bvh.parents, &bvh.counters,
+    for (DevBuf* b : {&tri_mat, &mats, &tris, &tris_in, &lights, &cdf, &texels, &lrec, &guide, &bvh.records, &bvh.parents, &bvh.counters,
                       &bvh.order, &bvh.tgeo, &bvh.keys, &bvh.keys_alt, &bvh.vals_alt, &bvh.knodes, &bvh.kbox,
                       &bvh.kcount, &bvh.ranges, &bvh.temp, &bvh.bounds, &bvh.depth, &bvh.wnodes, &bvh.wtgeo,
                       &bvh.wq})

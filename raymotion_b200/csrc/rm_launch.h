@@ -243,6 +243,8 @@ size_t lbvh_box_bytes();
 cudaError_t prepare_lights(const rm_triangle* d_tris, const int32_t* d_lights, const float* d_cdf, int n_lights,
                            float light_total, DevBuf& rec, DevBuf& guide, int& guide_n, float& guide_inv,
                            cudaStream_t st);
+// d_flag[0] = 1 when the two device byte ranges differ, else 0 (n_bytes a multiple of 16).
+cudaError_t device_differ(const void* a, const void* b, size_t n_bytes, int* d_flag, cudaStream_t st);
 // 64-bit content hash of a device byte range (order-sensitive per 8-byte word).
 cudaError_t device_hash(const void* d_bytes, size_t n_bytes, unsigned long long* d_out, cudaStream_t st);
 

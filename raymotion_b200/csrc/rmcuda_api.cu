@@ -171,7 +171,34 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
     msg = cuda_msg("Metal scene buffer allocation failed", e);
     return RM_ERR_ALLOC;
   }
-  if ((tb && (e = cudaMemcpyAsync(sc.tris.ptr, sv->tris, tb, cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+  // The reference re-uploads the scene every frame (metal.mm:171-186).  When a
+  // device-built scene is uploaded again with the same triangle count, the new
+  // triangles go to a staging buffer and are compared with the resident ones
+  // on the device: equal bytes keep the BVH (the build is deterministic, so
+  // it would come out the same), different bytes swap in and rebuild.
+  std::string key;
+  for (const char* k : {"RAYMOTION_CUDA_BVH", "RAYMOTION_CUDA_BVH_LEAF", "RAYMOTION_CUDA_WIDE"}) {
+    const char* v = std::getenv(k);
+    key += v ? v : "-";
+    key += '|';
+  }
+  const bool may_reuse = sc.have_scene && sc.device_built && !sv->nodes && sv->n_tris > 0 &&
+                         sv->n_tris == sc.n_tris && sc.bvh.n_records > 0 && key == sc.build_key;
+  bool reuse = false;
+  if (may_reuse) {
+    int differ = 1;
+    if ((e = sc.tris_in.reserve(tb)) != cudaSuccess || (e = c->hash_out.reserve(8)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(sc.tris_in.ptr, sv->tris, tb, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = device_differ(sc.tris_in.ptr, sc.tris.ptr, tb, c->hash_out.as<int>(), st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&differ, c->hash_out.ptr, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+      msg = cuda_msg("scene upload failed", e);
+      return RM_ERR_CUDA;
+    }
+    reuse = differ == 0;
+    if (!reuse) std::swap(sc.tris, sc.tris_in);
+  }
+  if ((!may_reuse && tb && (e = cudaMemcpyAsync(sc.tris.ptr, sv->tris, tb, cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
       (sv->n_lights &&
        (e = cudaMemcpyAsync(sc.lights.ptr, sv->light_tri, size_t(sv->n_lights) * 4, cudaMemcpyHostToDevice, st)) !=
            cudaSuccess) ||
@@ -191,6 +218,10 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
                           sc.light_total, sc.lrec, sc.guide, sc.guide_n, sc.guide_inv, st)) != cudaSuccess) {
     msg = cuda_msg("light preparation failed", e);
     return RM_ERR_CUDA;
+  }
+  if (reuse) {
+    sc.reuses++;
+    return RM_OK;  // BVH (and wide nodes) of these very triangles kept
   }
   sc.refits = 0;
   sc.have_scene = false;
@@ -232,6 +263,7 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
     msg = cuda_msg("wide BVH build failed", e);
     return RM_ERR_CUDA;
   }
+  sc.build_key = key;
   sc.have_scene = true;
   return RM_OK;
 }
@@ -983,6 +1015,7 @@ int rmcuda_stats_get(rmcuda_ctx* c, rm_stats* out) {
   out->bvh_node_bytes = c->sc.bvh.n_wide > 0 ? 80u : 64u;
   out->bvh_builds = c->bvh_builds;
   out->bvh_refits = c->bvh_refits;
+  out->bvh_kept = uint32_t(c->sc.reuses);
   return RM_OK;
 }
 

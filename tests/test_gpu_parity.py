@@ -174,3 +174,28 @@ def test_wavefront_shading_variants_bit_exact(backend, oracle, candidates, flags
     npix = cfg.width * cfg.height
     assert np.array_equal(backend.debug_read(4, npix), o.debug_read(4, npix))
     assert exact_fraction(g_hdr, o_hdr) == 1.0
+
+
+def test_reupload_of_unchanged_triangles_keeps_the_bvh(backend, oracle, small_field):
+    """rmcuda_render re-uploads the scene every call (metal.mm:171-186); equal
+    triangles keep the device BVH (compared byte for byte on the device),
+    changed ones rebuild it; the images match the oracle either way."""
+    sc, cam, _ = small_field
+    cfg = RenderConfig(width=64, height=40, spp=2, max_bounces=3, adapt_min=0,
+                       flags=_abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_RESTIR_OFF | _abi.RM_FLAG_DENOISE_OFF)
+    backend.render(sc, cam, cfg, 5, use_nodes=False)
+    st0 = backend.stats()
+    a = backend.render(sc, cam, cfg, 5, use_nodes=False)
+    st1 = backend.stats()
+    assert st1["bvh_kept"] == st0["bvh_kept"] + 1 and st1["bvh_builds"] == st0["bvh_builds"]
+    moved = sc.tris.copy()
+    moved["v0"][::7] += np.float32(0.05)
+    v64 = np.concatenate([moved["v0"], moved["v1"], moved["v2"]], axis=1).astype(np.float64)
+    msc = type(sc)(tris=moved, light_tri=sc.light_tri, light_cdf=sc.light_cdf, light_total=sc.light_total,
+                   texels=sc.texels, verts64=v64)
+    b = backend.render(msc, cam, cfg, 5, use_nodes=False)
+    st2 = backend.stats()
+    assert st2["bvh_builds"] == st1["bvh_builds"] + 1 and st2["bvh_kept"] == st1["bvh_kept"]
+    o_rgb, _, _ = oracle.Oracle().render(oracle.with_reference_bvh(msc), cam, cfg, 5)
+    assert np.array_equal(b, o_rgb)
+    assert not np.array_equal(a, b)
