@@ -396,9 +396,11 @@ __global__ void __launch_bounds__(256) k_wf_shade(Scene s, Params p, GBufSoA gb,
 // their order (extension ray, pending shadow ray, shade_path of the vertex
 // type), so the pixel comes out the same, without a launch and a queue round
 // trip per vertex.  ctr: the stage counters of the tail, extension and
-// shadow traversal.
+// shadow traversal.  Three 128-thread blocks per SM (up to 168 registers, few
+// spills): the tail is latency-bound, its path count is capped to one wave of
+// resident blocks, and with four blocks the spills cost more (30 vs 27.5 ms).
 template <int NEE>
-__global__ void __launch_bounds__(128, 4) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
+__global__ void __launch_bounds__(128, 3) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
                                                  float* __restrict__ hdr, uint32_t* __restrict__ dbg,
                                                  unsigned long long* ctr, unsigned long long* ctr_ext,
                                                  unsigned long long* ctr_shd, uint32_t* err) {
