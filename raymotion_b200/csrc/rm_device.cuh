@@ -190,8 +190,49 @@ __device__ __forceinline__ bool test_triangle(const float4* __restrict__ g, floa
 // word), tests that leaf, and pops the next subtree.  The persistent kernels
 // interleave steps of different rays on one thread; traverse() below runs
 // one ray to the end.
+//
+// Box test.  The base test is the reference's slab form: per axis the bounds
+// A = (L - o) * i with two roundings, entry = max(0, max A_near), exit =
+// min(t, min A_far), the box culled when entry > exit (1 + 2^-16).  The
+// traversal evaluates each bound as one fma, B = fma(L, i, c), with the
+// per-ray addend c = -(o i) lowered by m = |o i| 2^-21 for the bound that is
+// near for the sign of i and raised by m for the far one.  m exceeds the
+// rounding of o i and of c, so as real numbers L i + c_near <= (L - o) i <=
+// L i + c_far, and the rounded B_near <= RN((L - o) i) <= B_far.  Each RN
+// differs from A by at most 2^-23 relative, so B_entry <= A_entry (1 + 2^-22)
+// and B_exit >= A_exit (1 - 2^-22) for A_exit >= 0 (a box with A_exit < 0 is
+// culled by the base test), and with the slack 1 + 2^-15 every box the base
+// test accepts is accepted: the hits stay those of the base test.
+constexpr float kFmaBoxSlack = 1.000030517578125f;  // 1 + 2^-15
+
+// three-input min / max of sm_100 (PTX ISA 8.8); like fminf / fmaxf, a NaN
+// operand is ignored
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+  float d;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+
+// The addends of one axis: lo is the near bound for i >= 0, hi for i < 0.
+// If o i overflows (|o| near FLT_MAX / |i|) the axis culls nothing.
+__device__ __forceinline__ void slab_addends(float o, float i, float& c_lo, float& c_hi) {
+  const float oi = o * i;
+  const float m = fabsf(oi) * 0x1p-21f;
+  const float lowered = -oi - m, raised = -oi + m;
+  const bool finite = fabsf(oi) <= 3.4028234663852886e38f;
+  const float inf = __int_as_float(0x7f800000);
+  c_lo = finite ? (i >= 0.0f ? lowered : raised) : (i >= 0.0f ? -inf : inf);
+  c_hi = finite ? (i >= 0.0f ? raised : lowered) : (i >= 0.0f ? inf : -inf);
+}
+
 struct Trav {
   float ox, oy, oz, dx, dy, dz, ix, iy, iz;
+  float cxl, cxh, cyl, cyh, czl, czh;  // slab addends of the lo / hi bound per axis
   TraceResult r;
   int sp, node, leaf_first, leaf_count;
 
@@ -200,6 +241,9 @@ struct Trav {
     ix = 1.0f / (dx == 0.0f ? 1e-30f : dx);
     iy = 1.0f / (dy == 0.0f ? 1e-30f : dy);
     iz = 1.0f / (dz == 0.0f ? 1e-30f : dz);
+    slab_addends(ox, ix, cxl, cxh);
+    slab_addends(oy, iy, cyl, cyh);
+    slab_addends(oz, iz, czl, czh);
     r = TraceResult{tmax, -1, 0.f, 0.f};
     sp = 0;
     node = 0;
@@ -229,19 +273,19 @@ struct Trav {
     const float4 c = __ldg(n + 2);
     const int4 d = __ldg(reinterpret_cast<const int4*>(n + 3));
     // child 0
-    float l0x = (a.x - ox) * ix, h0x = (a.y - ox) * ix;
-    float l0y = (a.z - oy) * iy, h0y = (a.w - oy) * iy;
-    float l0z = (c.x - oz) * iz, h0z = (c.y - oz) * iz;
-    float n0 = fmaxf(0.0f, fmaxf(fminf(l0x, h0x), fmaxf(fminf(l0y, h0y), fminf(l0z, h0z))));
-    float f0 = fminf(r.t, fminf(fmaxf(l0x, h0x), fminf(fmaxf(l0y, h0y), fmaxf(l0z, h0z))));
+    const float l0x = __fmaf_rn(a.x, ix, cxl), h0x = __fmaf_rn(a.y, ix, cxh);
+    const float l0y = __fmaf_rn(a.z, iy, cyl), h0y = __fmaf_rn(a.w, iy, cyh);
+    const float l0z = __fmaf_rn(c.x, iz, czl), h0z = __fmaf_rn(c.y, iz, czh);
+    const float n0 = fmax3(fminf(l0x, h0x), fminf(l0y, h0y), fmaxf(fminf(l0z, h0z), 0.0f));
+    const float f0 = fmin3(fmaxf(l0x, h0x), fmaxf(l0y, h0y), fminf(fmaxf(l0z, h0z), r.t));
     // child 1
-    float l1x = (b.x - ox) * ix, h1x = (b.y - ox) * ix;
-    float l1y = (b.z - oy) * iy, h1y = (b.w - oy) * iy;
-    float l1z = (c.z - oz) * iz, h1z = (c.w - oz) * iz;
-    float n1 = fmaxf(0.0f, fmaxf(fminf(l1x, h1x), fmaxf(fminf(l1y, h1y), fminf(l1z, h1z))));
-    float f1 = fminf(r.t, fminf(fmaxf(l1x, h1x), fminf(fmaxf(l1y, h1y), fmaxf(l1z, h1z))));
-    bool hit0 = d.z >= 0 && !(n0 > f0 * kBoxSlack);
-    bool hit1 = d.w >= 0 && !(n1 > f1 * kBoxSlack);
+    const float l1x = __fmaf_rn(b.x, ix, cxl), h1x = __fmaf_rn(b.y, ix, cxh);
+    const float l1y = __fmaf_rn(b.z, iy, cyl), h1y = __fmaf_rn(b.w, iy, cyh);
+    const float l1z = __fmaf_rn(c.z, iz, czl), h1z = __fmaf_rn(c.w, iz, czh);
+    const float n1 = fmax3(fminf(l1x, h1x), fminf(l1y, h1y), fmaxf(fminf(l1z, h1z), 0.0f));
+    const float f1 = fmin3(fmaxf(l1x, h1x), fmaxf(l1y, h1y), fminf(fmaxf(l1z, h1z), r.t));
+    bool hit0 = d.z >= 0 && !(n0 > f0 * kFmaBoxSlack);
+    bool hit1 = d.w >= 0 && !(n1 > f1 * kFmaBoxSlack);
     // a child record: link d.x/d.y, count d.z/d.w (>0 leaf, 0 internal, <0 empty)
     if (hit0 && hit1) {
       int first = d.x, firstc = d.z, second = d.y, secondc = d.w;
@@ -357,12 +401,12 @@ struct WTrav {
     // n3: qlo_z (8), qhi_x (8); n4: qhi_y (8), qhi_z (8).
     // A child's slab on axis a is t = q s_a i_a + (p_a - o_a) i_a, one fma per
     // bound from the per-node base (p_a - o_a) i_a and the exact product
-    // s_a i_a (s_a is a power of two).  Its rounding differs from the binary
-    // traversal's (L - o) i, so the near bound's base is lowered and the far
+    // s_a i_a (s_a is a power of two).  Its rounding differs from the base
+    // test's (L - o) i (Trav), so the near bound's base is lowered and the far
     // bound's raised by m_a = |i_a| 2^-20 (|p_a - o_a| + 256 s_a + |p_a|),
     // rounded outward: m_a exceeds the sum of both forms' rounding errors and
-    // of the decoded bound's half ulp, so every box the binary test accepts
-    // is accepted here and the hits stay the binary traversal's.  Which
+    // of the decoded bound's half ulp, so every box the base test accepts
+    // is accepted here and the hits stay the base test's.  Which
     // stored bound is near follows the sign of i_a (the decoded lo <= hi).
     const float six = sx * ix, siy = sy * iy, siz = sz * iz;
     const float bx = (n0.x - ox) * ix, by = (n0.y - oy) * iy, bz = (n0.z - oz) * iz;
