@@ -353,11 +353,13 @@ int rmcuda_scene_set_materials(rmcuda_ctx* ctx, rmcuda_scene* scene, const int32
  * same arguments: adds dL/dparams into d_grad (DEVICE, n_materials x
  * RM_MATERIAL_PARAMS floats) given d_dL_dimage (DEVICE, W*H*3 floats, the
  * loss gradient with respect to the linear radiance image).  Sampling is held
- * fixed (random decisions, directions, pdfs, MIS weights, Russian-roulette
+ * fixed (random decisions, directions, pdfs, MIS weights, the light sample
+ * chosen by RIS NEE and its resampling weight, Russian-roulette
  * probabilities); the material-dependent factors of each path are
  * differentiated; each sample is replayed from its random state instead of
- * being stored.  Needs the plain chain with single-candidate NEE and a fixed
- * sample count (adapt_min 0 or RM_FLAG_NOADAPT).  Enqueued, not waited for. */
+ * being stored.  Needs the plain chain (single-candidate or RIS NEE) and a
+ * fixed sample count (adapt_min 0 or RM_FLAG_NOADAPT).  Enqueued, not waited
+ * for. */
 int rmcuda_backward(rmcuda_ctx* ctx, const rmcuda_scene* scene, const rm_camera* cam, const rm_config* cfg,
                     uint64_t seed, const float* d_dL_dimage, float* d_grad, char* err, size_t errcap);
 

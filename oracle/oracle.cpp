@@ -870,7 +870,8 @@ namespace {
 // as the fp32 path made it, and only the material-dependent factors of the
 // path integrand move.  frozen_path() walks the fp32 path exactly as
 // Tracer<float>::pathtrace does (pathtrace.metal:552-728, single-candidate
-// NEE :319-384, dielectric :470-534), taking every decision from it, and
+// NEE :319-384 or RIS NEE :385-469 with the selection and its resampling
+// weight held, dielectric :470-534), taking every decision from it, and
 // evaluates alongside in double the sample's value with the material factors
 // at parameters `prm`: the opaque BSDF value (albedo x texel, alpha2 from the
 // roughness), the emission of hit and sampled lights, and for a dielectric
@@ -1083,8 +1084,91 @@ V3<double> frozen_path(Tracer<float>& pt, const MatTable& mt, V3<float> ro, V3<f
       if (metallic >= 0.999f) spec_prob = 1.0f;
       float cur_sumW = 0;
       uint32_t cur_M = 0;
+      int Mc = P.restir_candidates;
+      if (Mc < 1) Mc = 1;
+      if (Mc > 32) Mc = 32;
+      // direct_lighting with RIS over Mc candidates (pathtrace.metal:385-469):
+      // the selection, its resampling weight W and the MIS weight are held;
+      // the selected light's emission and this surface's BSDF move
+      if (Mc > 1 && P.lights != 0 && LT > 1e-12f) {
+        float r2 = rough;
+        if (r2 < 0.02f) r2 = 0.02f;
+        float al2 = (r2 * r2) * (r2 * r2);
+        float sumW = 0;
+        float sel_lx = 0, sel_ly = 0, sel_lz = 0, sel_phat = 0, sel_epdf = 0, sel_sa = 0;
+        float sel_dx = 0, sel_dy = 0, sel_dz = 0;
+        int sel_tri = -1;
+        bool have = false;
+        for (int j = 0; j < Mc; ++j) {
+          float pick = pt.U() * LT;
+          const int ltri = pt.pick_light(pick);
+          const rm_triangle& t = S.tris[ltri];
+          float lu = pt.U(), lv = pt.U();
+          if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
+          float lw = 1.0f - lu - lv;
+          float qx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x);
+          float qy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y);
+          float qz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z);
+          float ldx = qx - hit.p.x, ldy = qy - hit.p.y, ldz = qz - hit.p.z;
+          float dist = std::sqrt(ldx * ldx + ldy * ldy + ldz * ldz);
+          float w = 0, ph = 0, epdf = 0, sa = 0, dxn = 0, dyn = 0, dzn = 0;
+          if (dist > 0.003f) {
+            float inv = 1.0f / dist;
+            dxn = ldx * inv; dyn = ldy * inv; dzn = ldz * inv;
+            float lcos = -(t.nn.x * dxn + (t.nn.y * dyn + t.nn.z * dzn));
+            float scos = pnx * dxn + (pny * dyn + pnz * dzn);
+            if (lcos > 1e-8f && scos > 1e-8f) {
+              float lt_lum = lum3(t.er, t.eg, t.eb);
+              if (lt_lum < 1e-6f) lt_lum = 1e-6f;
+              float q = dist * dist * lt_lum / (lcos * LT);
+              if (q > 1e-12f) {
+                auto e = Tracer<float>::eval_bsdf(dxn, dyn, dzn, wox, woy, woz, pnx, pny, pnz, al2, metallic,
+                                                  spec_prob, hit.ar, hit.ag, hit.ab);
+                epdf = e.pdf;
+                float Fr = t.er * e.r * scos * t.alpha;
+                float Fg = t.eg * e.g * scos * t.alpha;
+                float Fb = t.eb * e.b * scos * t.alpha;
+                ph = lum3(Fr, Fg, Fb);
+                if (ph > 0.0f) w = ph / q;
+                sa = scos * t.alpha;
+              }
+            }
+          }
+          sumW += w;
+          float r = pt.U();
+          if (w > 0.0f && r * sumW < w) {
+            have = true;
+            sel_lx = qx; sel_ly = qy; sel_lz = qz;
+            sel_phat = ph; sel_epdf = epdf; sel_sa = sa;
+            sel_dx = dxn; sel_dy = dyn; sel_dz = dzn;
+            sel_tri = ltri;
+          }
+        }
+        cur_sumW = sumW;
+        cur_M = uint32_t(Mc);
+        if (have && sumW > 0.0f && sel_phat > 0.0f) {
+          float pdf_ris = float(Mc) * sel_phat / sumW;
+          float wnee = 1.0f;
+          if (!P.nomis && sel_epdf > 1e-20f) wnee = pdf_ris / (pdf_ris + sel_epdf);
+          float vdx = sel_lx - hit.p.x, vdy = sel_ly - hit.p.y, vdz = sel_lz - hit.p.z;
+          float vdist = std::sqrt(vdx * vdx + vdy * vdy + vdz * vdz);
+          if (vdist > 0.003f) {
+            float vinv = 1.0f / vdist;
+            vdx *= vinv; vdy *= vinv; vdz *= vinv;
+            V3<float> so = mk(hit.p.x + pnx * 0.002f, hit.p.y + pny * 0.002f, hit.p.z + pnz * 0.002f);
+            if (!pt.occluded(so, mk(vdx, vdy, vdz), vdist - 0.003f)) {
+              const float W = sumW / (float(Mc) * sel_phat);
+              const double k = double(sel_sa) * double(W) * double(wnee);
+              const V3<double> f = bsdf64(mt, S, hit, sel_dx, sel_dy, sel_dz, wox, woy, woz, pnx, pny, pnz, metallic,
+                                          spec_prob);
+              const double fv[3] = {f.x, f.y, f.z};
+              for (int c = 0; c < 3; ++c) a64[c] += t64[c] * mt.get(S.tris, sel_tri, 4 + c) * fv[c] * k;
+            }
+          }
+        }
+      }
       // direct_lighting, single candidate (pathtrace.metal:319-384)
-      if (P.lights != 0 && LT > 1e-12f) {
+      if (Mc <= 1 && P.lights != 0 && LT > 1e-12f) {
         float r2 = rough;
         if (r2 < 0.02f) r2 = 0.02f;
         float al2 = (r2 * r2) * (r2 * r2);
@@ -1568,8 +1652,8 @@ void orc_detmath(int which, const float* x, float* y0, float* y1, int n) {
 // W*H*3 doubles, the mean over spp samples of each pixel's clamped sample
 // values with material parameters prm (n_materials x 8 doubles) applied
 // through tri_material; every decision comes from the fp32 path of the scene
-// as given.  The frame must have a fixed sample count and single-candidate
-// NEE.  Returns 0, or RM_ERR_INVALID.
+// as given.  The frame must have a fixed sample count and take the plain
+// chain.  Returns 0, or RM_ERR_INVALID.
 int orc_render_frozen(const rm_scene_view* sv, const rm_camera* cam, const rm_config* cfg, uint64_t seed,
                       const int32_t* tri_material, const double* prm, int n_materials, double* out, int nthreads) {
   using namespace orc;
@@ -1585,7 +1669,11 @@ int orc_render_frozen(const rm_scene_view* sv, const rm_camera* cam, const rm_co
     if (!(sv->tris[i].alpha >= 1)) { opaque = false; break; }
   Env env = read_env(cfg->flags);
   Params p = resolve(*cfg, *cam, int(s.nodes.size()), sv->n_lights, sv->light_total, opaque, env);
-  if (p.adapt_min > 0 || p.restir_candidates > 1) return RM_ERR_INVALID;
+  if (p.adapt_min > 0) return RM_ERR_INVALID;
+  // the ReSTIR chain's policy (metal.mm:236-237) would not render the plain frame
+  if (p.restir_spatial > 0 && p.lights > 0 && p.bounces > 0 && p.opaque &&
+      size_t(cfg->width) * size_t(cfg->height) * (76 + 2 * 60) <= size_t(512) * 1024 * 1024)
+    return RM_ERR_INVALID;
   int lanes = 1;
   if (p.spp >= 8) lanes = 8;
   if (p.spp >= 32) lanes = 32;

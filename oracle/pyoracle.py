@@ -240,7 +240,7 @@ def render_frozen(scene: PackedScene, cam: Camera, cfg: RenderConfig, seed: int,
                                         tm.ctypes.data, prm.ctypes.data, len(prm), out.ctypes.data,
                                         threads or nthreads())
     if rc != 0:
-        raise ValueError("frozen evaluation needs a fixed sample count and single-candidate NEE")
+        raise ValueError("frozen evaluation needs a fixed sample count and the plain chain")
     return out
 
 

@@ -4,8 +4,9 @@
 //
 // The differentiated estimator is the frame of render_paths (K1) or the lane
 // kernel (K2) (pathtrace.metal:739-815) with its sampling held fixed: every
-// random decision, sampled direction, pdf, MIS weight and Russian-roulette
-// probability keeps its value at the current parameters, and only the
+// random decision, sampled direction, pdf, MIS weight, light-sample
+// resampling weight (RIS NEE) and Russian-roulette probability keeps its
+// value at the current parameters, and only the
 // factors of the path integrand that depend on the materials are
 // differentiated - the opaque BSDF value (albedo, roughness), the emission of
 // hit and sampled lights, and for a dielectric the Fresnel and (eta_i/eta_t)^2
@@ -289,9 +290,18 @@ __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict_
         float dlr, dlg, dlb, sdist, sox, soy, soz, sdx, sdy, sdz;
         bool has_ray;
         float parts[2];
-        pt.nee_single_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob,
-                               hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray, sox, soy, soz, sdx,
-                               sdy, sdz, sdist, parts);
+        // single-candidate NEE (pathtrace.metal:319-384) or RIS over the
+        // candidates (:385-469), with the same draws; the selection, its
+        // resampling weight W and the MIS weight are held, so the light sample
+        // N_k = Le f k moves only with the light's emission and this BSDF
+        if (p.restir_candidates > 1)
+          pt.direct_lighting_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic,
+                                      spec_prob, hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray, sox,
+                                      soy, soz, sdx, sdy, sdz, sdist, parts);
+        else
+          pt.nee_single_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob,
+                                 hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray, sox, soy, soz, sdx,
+                                 sdy, sdz, sdist, parts);
         if (has_ray && !pt.occluded(sox, soy, soz, sdx, sdy, sdz, sdist)) {
           accr += dlr * thr_r; accg += dlg * thr_g; accb += dlb * thr_b;
           // N_k = Le * f * k: derivative in the light's emission and this surface's BSDF

@@ -959,11 +959,13 @@ struct Tracer {
                                                         float spec_prob, float ar, float ag, float ab, float& o_r,
                                                         float& o_g, float& o_b, float& out_sumW, uint32_t& out_M,
                                                         bool& has_ray, float& sox, float& soy, float& soz,
-                                                        float& sdx, float& sdy, float& sdz, float& sdist) {
+                                                        float& sdx, float& sdy, float& sdz, float& sdist,
+                                                        float* parts = nullptr) {
     o_r = o_g = o_b = 0.0f;
     out_sumW = 0.0f;
     out_M = 0;
     has_ray = false;
+    if (parts) { parts[0] = __int_as_float(0); parts[1] = 0.0f; }
     if (p.lights == 0 || !(p.light_total > 1e-12f)) return;
     int Mc = p.restir_candidates;
     if (Mc < 1) Mc = 1;
@@ -976,16 +978,19 @@ struct Tracer {
     const float LT = p.light_total;
     if (Mc <= 1) {
       nee_single_deferred(px, py, pz, nx, ny, nz, wox, woy, woz, rough, metallic, spec_prob, ar, ag, ab, o_r, o_g,
-                          o_b, out_sumW, out_M, has_ray, sox, soy, soz, sdx, sdy, sdz, sdist);
+                          o_b, out_sumW, out_M, has_ray, sox, soy, soz, sdx, sdy, sdz, sdist, parts);
       return;
     }
     float sumW = 0.0f;
     float sel_lx = 0, sel_ly = 0, sel_lz = 0, sel_Fr = 0, sel_Fg = 0, sel_Fb = 0, sel_phat = 0, sel_epdf = 0;
+    float sel_sa = 0;  // scos * alpha of the selected candidate (for `parts`)
+    int sel_li = 0;
     bool have = false;
     const BsdfPrep bp = prep_bsdf(wox, woy, woz, nx, ny, nz, alpha2, metallic, ar, ag, ab);
     for (int j = 0; j < Mc; ++j) {
       float pick = U() * LT;
-      const LightRec t = load_light(s, pick_light(pick));
+      const int li = pick_light(pick);
+      const LightRec t = load_light(s, li);
       float lu = U(), lv = U();
       if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
       float lw = 1.0f - lu - lv;
@@ -994,7 +999,7 @@ struct Tracer {
       float qz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z);
       float ldx = qx - px, ldy = qy - py, ldz = qz - pz;
       float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
-      float w = 0, ph = 0, epdf = 0, Fr = 0, Fg = 0, Fb = 0;
+      float w = 0, ph = 0, epdf = 0, Fr = 0, Fg = 0, Fb = 0, sa = 0;
       if (dist > 0.003f) {
         float inv = 1.0f / dist;
         float dxn = ldx * inv, dyn = ldy * inv, dzn = ldz * inv;
@@ -1012,6 +1017,7 @@ struct Tracer {
             Fb = t.eb * e.b * scos * t.alpha;
             ph = lum3(Fr, Fg, Fb);
             if (ph > 0.0f) w = ph / q;
+            sa = scos * t.alpha;
           }
         }
       }
@@ -1022,6 +1028,7 @@ struct Tracer {
         sel_lx = qx; sel_ly = qy; sel_lz = qz;
         sel_Fr = Fr; sel_Fg = Fg; sel_Fb = Fb;
         sel_phat = ph; sel_epdf = epdf;
+        sel_sa = sa; sel_li = li;
       }
     }
     out_sumW = sumW;
@@ -1042,6 +1049,8 @@ struct Tracer {
     o_r = sel_Fr * W * wnee;
     o_g = sel_Fg * W * wnee;
     o_b = sel_Fb * W * wnee;
+    // the selected light and the factor k of o = Le * f * k (held by the adjoint)
+    if (parts) { parts[0] = __int_as_float(sel_li); parts[1] = sel_sa * W * wnee; }
   }
 
   __device__ static __forceinline__ float fresnel(float ci_in, float eta_in, float eta_out) {

@@ -84,10 +84,6 @@ int rmcuda_backward(rmcuda_ctx* c, const rmcuda_scene* scene, const rm_camera* c
     set_err(err, errcap, "the adjoint covers the plain chain; the policy picks ReSTIR (set RM_FLAG_RESTIR_OFF)");
     return RM_ERR_INVALID;
   }
-  if (pl.p.restir_candidates > 1) {
-    set_err(err, errcap, "the adjoint needs single-candidate NEE (restir_candidates 1 or RM_FLAG_RESTIR_OFF)");
-    return RM_ERR_INVALID;
-  }
   if (pl.p.adapt_min > 0) {
     set_err(err, errcap, "the adjoint needs a fixed sample count (adapt_min 0 or RM_FLAG_NOADAPT)");
     return RM_ERR_INVALID;

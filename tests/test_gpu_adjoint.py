@@ -19,7 +19,7 @@ drive them.
 import numpy as np
 import pytest
 
-from raymotion_b200 import RenderError
+from raymotion_b200 import RenderError, _abi
 from raymotion_b200.scene import with_materials
 from raymotion_b200.scenes import inverse_scene
 
@@ -77,10 +77,16 @@ def central_difference(loss, prm, m, col):
     return (4.0 * d(H / 2) - d(H)) / 3.0
 
 
-@pytest.mark.parametrize("spp", [4, 8], ids=["one_lane", "eight_lanes"])
-def test_adjoint_matches_fp64_central_differences(backend, oracle, spp):
+@pytest.mark.parametrize("spp,candidates", [(4, 1), (8, 1), (4, 8)], ids=["one_lane", "eight_lanes", "ris_nee"])
+def test_adjoint_matches_fp64_central_differences(backend, oracle, spp, candidates):
+    """ris_nee: the plain chain with RIS over 8 light candidates per vertex;
+    the selection and its resampling weight are held on both sides."""
     torch = _torch()
     d = _scene(oracle, spp)
+    if candidates > 1:
+        c = d["config"]
+        d["config"] = type(c)(**{**c.__dict__, "restir_candidates": candidates, "restir_spatial": 0,
+                                 "flags": c.flags & ~_abi.RM_FLAG_RESTIR_OFF})
     seed = 2024
     sc, cam, cfg, tm = d["scene"], d["camera"], d["config"], d["tri_material"]
     prm = d["params"].astype(np.float64)

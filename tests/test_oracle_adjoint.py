@@ -10,6 +10,7 @@ differences (second differences small next to first differences).
 import numpy as np
 import pytest
 
+from raymotion_b200 import _abi
 from raymotion_b200.scene import with_materials
 from raymotion_b200.scenes import inverse_scene
 
@@ -22,8 +23,17 @@ def small(oracle):
     return d
 
 
-def test_frozen_at_scene_parameters_is_the_fp32_frame(oracle, small):
+def ris_config(cfg, candidates=8):
+    """The plain chain with RIS NEE over `candidates` lights per vertex."""
+    return type(cfg)(**{**cfg.__dict__, "restir_candidates": candidates, "restir_spatial": 0,
+                        "flags": cfg.flags & ~_abi.RM_FLAG_RESTIR_OFF})
+
+
+@pytest.mark.parametrize("nee", ["single", "ris8"])
+def test_frozen_at_scene_parameters_is_the_fp32_frame(oracle, small, nee):
     sc, cam, cfg = small["scene"], small["camera"], small["config"]
+    if nee == "ris8":
+        cfg = ris_config(cfg)
     _, hdr, _ = oracle.Oracle().render(sc, cam, cfg, 99)
     fro = oracle.render_frozen(sc, cam, cfg, 99, small["tri_material"], small["params"].astype(np.float64))
     hdr = hdr.reshape(-1, 3).astype(np.float64)
@@ -35,8 +45,13 @@ def test_frozen_at_scene_parameters_is_the_fp32_frame(oracle, small):
     assert rel.max() < 5e-4
 
 
-def test_frozen_frame_is_linear_in_emission(oracle, small):
+@pytest.mark.parametrize("nee", ["single", "ris8"])
+def test_frozen_frame_is_linear_in_emission(oracle, small, nee):
+    """RIS NEE holds its selection and resampling weight, so its light sample
+    is Le f k with k fixed: still linear in the emission."""
     sc, cam, cfg = small["scene"], small["camera"], small["config"]
+    if nee == "ris8":
+        cfg = ris_config(cfg)
     cfg.clamp = 0.0
     prm = small["params"].astype(np.float64)
     a = oracle.render_frozen(sc, cam, cfg, 5, small["tri_material"], prm)
