@@ -60,6 +60,9 @@ struct DevScene {
   bool have_scene = false;
   int refits = 0;
   bool device_built = false;
+  // the texel count the resident triangles were last checked against by
+  // upload_scene (texture ranges, opacity); -1 after any other write
+  long long validated_texels = -1;
   // per-triangle materials (rmcuda_scene_set_materials): index per triangle,
   // 8 parameters per material
   DevBuf tri_mat, mats;

@@ -51,6 +51,7 @@ int rmcuda_scene_set_materials(rmcuda_ctx* c, rmcuda_scene* scene, const int32_t
   if (e == cudaSuccess) e = cudaMemcpyAsync(sc.mats.ptr, mats, mbytes, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && light_cdf && sc.n_lights > 0)
     e = cudaMemcpyAsync(sc.cdf.ptr, light_cdf, size_t(sc.n_lights) * 4, cudaMemcpyHostToDevice, st);
+  sc.validated_texels = -1;  // the triangles' material fields are rewritten
   if (e == cudaSuccess)
     e = apply_materials(sc.tris.as<rm_triangle>(), sc.tri_mat.as<int32_t>(), sc.mats.as<float>(), sc.n_tris, st);
   if (e == cudaSuccess && light_cdf) sc.light_total = light_total;

@@ -147,21 +147,27 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
     msg = "invalid scene view";
     return RM_ERR_INVALID;
   }
-  bool opaque = true;
-  for (int i = 0; i < sv->n_tris; ++i) {
-    const rm_triangle& t = sv->tris[i];
-    if (!(t.alpha >= 1.0f)) opaque = false;
-    if (t.texture_offset >= 0) {
-      if (t.texture_width <= 0 || t.texture_height <= 0 ||
-          int64_t(t.texture_offset) + int64_t(t.texture_width) * t.texture_height > sv->n_texels) {
-        msg = "triangle texture outside the texel array";
-        return RM_ERR_INVALID;
-      }
-    }
-  }
   for (int i = 0; i < sv->n_lights; ++i)
     if (sv->light_tri[i] < 0 || sv->light_tri[i] >= sv->n_tris) { msg = "light index out of range"; return RM_ERR_INVALID; }
-  if (&sc == &c->sc) c->prep_topology.clear();  // an uploaded scene is not an instance commit
+  // Texture ranges and opacity, from the host triangles (a pass over all of
+  // them); skipped below for triangles equal to resident ones that passed it
+  // against the same texel count.
+  bool opaque = true;
+  auto check_tris = [&]() {
+    opaque = true;
+    for (int i = 0; i < sv->n_tris; ++i) {
+      const rm_triangle& t = sv->tris[i];
+      if (!(t.alpha >= 1.0f)) opaque = false;
+      if (t.texture_offset >= 0) {
+        if (t.texture_width <= 0 || t.texture_height <= 0 ||
+            int64_t(t.texture_offset) + int64_t(t.texture_width) * t.texture_height > sv->n_texels) {
+          msg = "triangle texture outside the texel array";
+          return false;
+        }
+      }
+    }
+    return true;
+  };
   cudaStream_t st = c->stream;
   cudaError_t e;
   const size_t tb = size_t(sv->n_tris) * sizeof(rm_triangle);
@@ -196,8 +202,12 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
       return RM_ERR_CUDA;
     }
     reuse = differ == 0;
-    if (!reuse) std::swap(sc.tris, sc.tris_in);
   }
+  if (reuse && sc.validated_texels == int64_t(sv->n_texels)) opaque = sc.opaque;
+  else if (!check_tris()) return RM_ERR_INVALID;  // the resident scene is untouched
+  if (may_reuse && !reuse) std::swap(sc.tris, sc.tris_in);
+  if (&sc == &c->sc) c->prep_topology.clear();  // an uploaded scene is not an instance commit
+  sc.validated_texels = -1;
   if ((!may_reuse && tb && (e = cudaMemcpyAsync(sc.tris.ptr, sv->tris, tb, cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
       (sv->n_lights &&
        (e = cudaMemcpyAsync(sc.lights.ptr, sv->light_tri, size_t(sv->n_lights) * 4, cudaMemcpyHostToDevice, st)) !=
@@ -214,6 +224,7 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
   sc.n_lights = sv->n_lights;
   sc.light_total = sv->light_total;
   sc.opaque = opaque;
+  sc.validated_texels = sv->n_texels;
   if ((e = prepare_lights(sc.tris.as<rm_triangle>(), sc.lights.as<int32_t>(), sc.cdf.as<float>(), sc.n_lights,
                           sc.light_total, sc.lrec, sc.guide, sc.guide_n, sc.guide_inv, st)) != cudaSuccess) {
     msg = cuda_msg("light preparation failed", e);
@@ -656,6 +667,7 @@ int rmcuda_scene_update(rmcuda_ctx* c, const rm_triangle* tris, int32_t n, int32
     set_err(err, errcap, "scene update needs a resident scene with the same triangle count");
     return RM_ERR_INVALID;
   }
+  c->sc.validated_texels = -1;
   cudaError_t e = cudaMemcpyAsync(c->sc.tris.ptr, tris, size_t(n) * sizeof(rm_triangle), cudaMemcpyHostToDevice, c->stream);
   if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("scene update upload failed", e)); return RM_ERR_CUDA; }
   bool opaque = true;
@@ -751,6 +763,7 @@ int rmcuda_instances_commit(rmcuda_ctx* c, const rm_instance* inst, int32_t n, i
   cudaStream_t st = c->stream;
   cudaError_t e;
   size_t scan_bytes = 0;
+  c->sc.validated_texels = -1;  // the world triangles are rewritten below
   const size_t slots = size_t(std::max(total, 1));
   if ((e = prep_scan_bytes(total, scan_bytes)) != cudaSuccess ||
       (e = c->prep_inst.reserve(size_t(std::max(n, 1)) * sizeof(rm_instance))) != cudaSuccess ||

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from raymotion_b200 import _abi
+from raymotion_b200 import RenderError, _abi
 from raymotion_b200.scene import Camera, RenderConfig
 from raymotion_b200.scenes import cornell_box, icosphere_field
 
@@ -199,3 +199,28 @@ def test_reupload_of_unchanged_triangles_keeps_the_bvh(backend, oracle, small_fi
     o_rgb, _, _ = oracle.Oracle().render(oracle.with_reference_bvh(msc), cam, cfg, 5)
     assert np.array_equal(b, o_rgb)
     assert not np.array_equal(a, b)
+
+
+def test_reupload_checks_textures_against_the_new_texel_array(backend, small_field):
+    """Equal triangles skip the host pass over them only when they were checked
+    against the same texel count: the same textured triangles with a shorter
+    texel array are still rejected, and the resident scene stays usable."""
+    sc, cam, _ = small_field
+    cfg = RenderConfig(width=32, height=20, spp=1, max_bounces=2, adapt_min=0,
+                       flags=_abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_RESTIR_OFF | _abi.RM_FLAG_DENOISE_OFF)
+    tris = sc.tris.copy()
+    tris["texture_offset"][0] = 0
+    tris["texture_width"][0] = 2
+    tris["texture_height"][0] = 2
+
+    def scene(n_texels):
+        return type(sc)(tris=tris, light_tri=sc.light_tri, light_cdf=sc.light_cdf, light_total=sc.light_total,
+                        texels=np.full((n_texels, 3), 0.5, np.float32), verts64=sc.verts64)
+
+    a = backend.render(scene(4), cam, cfg, 3, use_nodes=False)
+    kept = backend.stats()["bvh_kept"]
+    with pytest.raises(RenderError, match="texture outside the texel array"):
+        backend.render(scene(2), cam, cfg, 3, use_nodes=False)
+    b = backend.render(scene(4), cam, cfg, 3, use_nodes=False)
+    assert np.array_equal(a, b)
+    assert backend.stats()["bvh_kept"] >= kept + 1
