@@ -157,6 +157,9 @@ struct Deferred {
 // term that does not depend on it - the emission and light-sample terms and
 // the -(g . acc) halves of the scattering terms g . dlogB_k . (C - acc_k) -
 // and the g . dlogB_k . C halves when the path ends, returning C in C_out.
+// kRis: the frame's NEE takes several candidates (RIS); a separate
+// instantiation keeps the single-candidate walk's registers as they were.
+template <bool kRis>
 __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict__ tri_mat, float ox, float oy,
                                           float oz, float dx, float dy, float dz, int max_bounces, float Cr, float Cg,
                                           float Cb, float gr, float gg, float gb, const GradSink& sink,
@@ -294,7 +297,7 @@ __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict_
         // candidates (:385-469), with the same draws; the selection, its
         // resampling weight W and the MIS weight are held, so the light sample
         // N_k = Le f k moves only with the light's emission and this BSDF
-        if (p.restir_candidates > 1)
+        if (kRis)
           pt.direct_lighting_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic,
                                       spec_prob, hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray, sox,
                                       soy, soz, sdx, sdy, sdz, sdist, parts);
@@ -428,7 +431,7 @@ __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict_
 
 // One pixel lane per thread, the samples of K1 (LANES 1) or of one lane of K2,
 // in the forward kernels' order (pathtrace.metal:749-758, :787-796).
-template <int LANES>
+template <int LANES, bool kRis>
 __global__ void __launch_bounds__(256) k_adjoint(Scene s, Params p, uint64_t seed, const int32_t* __restrict__ tri_mat,
                                                  int n_mat, const float* __restrict__ dLdI, float* __restrict__ grad,
                                                  int use_shared, unsigned long long* ctr, uint32_t* err) {
@@ -471,12 +474,12 @@ __global__ void __launch_bounds__(256) k_adjoint(Scene s, Params p, uint64_t see
         // derivative as if no channel were clamped; a clamped channel (rare)
         // is taken back out by a second walk with -g on that channel
         Deferred dfr;
-        adjoint_path(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, 0.f, 0.f, 0.f, d0, d1, d2, sink, &dfr,
+        adjoint_path<kRis>(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, 0.f, 0.f, 0.f, d0, d1, d2, sink, &dfr,
                      C);
         if (cl && !(C[0] < p.clamp_value && C[1] < p.clamp_value && C[2] < p.clamp_value)) {
           const uint32_t st1 = pt.rng.state;
           pt.rng.state = st0;
-          adjoint_path(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, C[0], C[1], C[2],
+          adjoint_path<kRis>(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, C[0], C[1], C[2],
                        C[0] < p.clamp_value ? 0.f : -d0, C[1] < p.clamp_value ? 0.f : -d1,
                        C[2] < p.clamp_value ? 0.f : -d2, sink, nullptr, nullptr);
           pt.rng.state = st1;
@@ -488,7 +491,7 @@ __global__ void __launch_bounds__(256) k_adjoint(Scene s, Params p, uint64_t see
         const float gr = (cl && !(C[0] < p.clamp_value)) ? 0.0f : d0;
         const float gg = (cl && !(C[1] < p.clamp_value)) ? 0.0f : d1;
         const float gb = (cl && !(C[2] < p.clamp_value)) ? 0.0f : d2;
-        adjoint_path(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, C[0], C[1], C[2], gr, gg, gb, sink,
+        adjoint_path<kRis>(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, C[0], C[1], C[2], gr, gg, gb, sink,
                      nullptr, nullptr);
       }
       ++samples;
@@ -528,9 +531,12 @@ cudaError_t launch_adjoint(int lanes, const Scene& s, const Params& p, uint64_t 
   const size_t threads = size_t(p.width) * size_t(p.height) * size_t(lanes);
   const unsigned grid = unsigned((threads + 255) / 256);
   const size_t sm = use_shared ? shmem : 0;
-  if (lanes == 32) k_adjoint<32><<<grid, 256, sm, st>>>(s, p, seed, tri_mat, n_mat, dLdI, grad, use_shared, ctr, err);
-  else if (lanes == 8) k_adjoint<8><<<grid, 256, sm, st>>>(s, p, seed, tri_mat, n_mat, dLdI, grad, use_shared, ctr, err);
-  else k_adjoint<1><<<grid, 256, sm, st>>>(s, p, seed, tri_mat, n_mat, dLdI, grad, use_shared, ctr, err);
+#define RM_ADJ(L, R) k_adjoint<L, R><<<grid, 256, sm, st>>>(s, p, seed, tri_mat, n_mat, dLdI, grad, use_shared, ctr, err)
+  const bool ris = p.restir_candidates > 1;
+  if (lanes == 32) { if (ris) RM_ADJ(32, true); else RM_ADJ(32, false); }
+  else if (lanes == 8) { if (ris) RM_ADJ(8, true); else RM_ADJ(8, false); }
+  else { if (ris) RM_ADJ(1, true); else RM_ADJ(1, false); }
+#undef RM_ADJ
   return cudaGetLastError();
 }
 
