@@ -357,9 +357,12 @@ int rmcuda_scene_set_materials(rmcuda_ctx* ctx, rmcuda_scene* scene, const int32
  * chosen by RIS NEE and its resampling weight, Russian-roulette
  * probabilities); the material-dependent factors of each path are
  * differentiated; each sample is replayed from its random state instead of
- * being stored.  Needs the plain chain (single-candidate or RIS NEE) and a
- * fixed sample count (adapt_min 0 or RM_FLAG_NOADAPT).  Enqueued, not waited
- * for. */
+ * being stored.  Needs a fixed sample count (adapt_min 0 or RM_FLAG_NOADAPT).
+ * The plain chain (single-candidate or RIS NEE) is replayed from the seed.  On
+ * the ReSTIR chain the frame's G-buffer and merged reservoirs are the
+ * checkpoint: call it after rendering that frame on this context (same
+ * scene, camera, config and seed; the denoiser off), and the reservoirs'
+ * light samples and weights are held.  Enqueued, not waited for. */
 int rmcuda_backward(rmcuda_ctx* ctx, const rmcuda_scene* scene, const rm_camera* cam, const rm_config* cfg,
                     uint64_t seed, const float* d_dL_dimage, float* d_grad, char* err, size_t errcap);
 

@@ -286,7 +286,7 @@ static void k_render_paths(const SceneRef& s, const Params& p, uint64_t seed, in
 
 // K3 restir_generate (pathtrace.metal:817-917)
 static void k_generate(const SceneRef& s, const Params& p, uint64_t seed, int row0, int row1, GBuf* gb,
-                       Reservoir* ri, int nthreads, std::atomic<uint64_t>& rays) {
+                       Reservoir* ri, int nthreads, std::atomic<uint64_t>& rays, int32_t* rl = nullptr) {
   const int W = p.width;
   parallel_for(row1 - row0, nthreads, [&](int ry) {
     uint32_t y = uint32_t(row0 + ry);
@@ -299,6 +299,7 @@ static void k_generate(const SceneRef& s, const Params& p, uint64_t seed, int ro
       Reservoir& r = ri[id];
       g.kind = 0;
       r.valid = 0;
+      if (rl) rl[id] = -1;  // the selected light's triangle (the adjoint's check), or -1
       float sx = float(x) + 1e-12f + (p.resolution - 2e-12f) * pt.U() - float(p.width) * 0.5f;
       float sy = float(p.height) * 0.5f - (float(y) + 1e-12f + (p.resolution - 2e-12f) * pt.U());
       float f2 = p.camera.focal * p.camera.focal;
@@ -335,11 +336,13 @@ static void k_generate(const SceneRef& s, const Params& p, uint64_t seed, int ro
       float px = hit.p.x, py = hit.p.y, pz = hit.p.z;
       float sumWs = 0, sumWu = 0, sel_lx = 0, sel_ly = 0, sel_lz = 0, sel_nx = 0, sel_ny = 0, sel_nz = 0;
       float sel_er = 0, sel_eg = 0, sel_eb = 0, sel_alpha = 1, sel_ph = 0;
+      int sel_tri = -1;
       bool have = false;
       V3<float> so = mk(px + pnx * 0.002f, py + pny * 0.002f, pz + pnz * 0.002f);
       for (int j = 0; j < Mc; ++j) {
         float pick = pt.U() * p.light_total;
-        const rm_triangle& t = s.tris[pt.pick_light(pick)];
+        const int ltri = pt.pick_light(pick);
+        const rm_triangle& t = s.tris[ltri];
         float lu = pt.U(), lv = pt.U();
         if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
         float lw = 1.0f - lu - lv;
@@ -377,6 +380,7 @@ static void k_generate(const SceneRef& s, const Params& p, uint64_t seed, int ro
           sel_lx = qx; sel_ly = qy; sel_lz = qz;
           sel_nx = t.nn.x; sel_ny = t.nn.y; sel_nz = t.nn.z;
           sel_er = t.er; sel_eg = t.eg; sel_eb = t.eb; sel_alpha = t.alpha; sel_ph = ph;
+          sel_tri = ltri;
         }
       }
       if (!have || !(sumWs > 0) || !(sumWu > 0) || !(sel_ph > 0)) continue;
@@ -384,6 +388,7 @@ static void k_generate(const SceneRef& s, const Params& p, uint64_t seed, int ro
       r.lightNormal = {sel_nx, sel_ny, sel_nz};
       r.emission = {sel_er, sel_eg, sel_eb};
       r.alpha = sel_alpha; r.p_hat = sel_ph; r.sumWs = sumWs; r.sumWu = sumWu; r.M = uint32_t(Mc); r.valid = 1;
+      if (rl) rl[id] = sel_tri;
     }
     rays += ctr.rays;
   });
@@ -392,7 +397,8 @@ static void k_generate(const SceneRef& s, const Params& p, uint64_t seed, int ro
 // K4 restir_spatial (pathtrace.metal:919-1054)
 static void k_spatial(const SceneRef& s, const Params& p, uint64_t seed, int row0, int row1, const GBuf* gb,
                       const Reservoir* ri, Reservoir* ro_, const GBuf* hg, const Reservoir* hr, int nthreads,
-                      std::atomic<uint64_t>& rays) {
+                      std::atomic<uint64_t>& rays, const int32_t* ril = nullptr, int32_t* rol = nullptr,
+                      const int32_t* hrl = nullptr) {
   const int W = p.width, H = p.height;
   parallel_for(row1 - row0, nthreads, [&](int ry) {
     uint32_t y = uint32_t(row0 + ry);
@@ -400,6 +406,7 @@ static void k_spatial(const SceneRef& s, const Params& p, uint64_t seed, int row
     for (uint32_t x = 0; x < uint32_t(W); ++x) {
       uint32_t id = y * uint32_t(W) + x;
       ro_[id] = ri[id];
+      if (rol) rol[id] = ril ? ril[id] : -1;  // the selected light's triangle follows the sample
       if (gb[id].kind != 1 || ri[id].valid == 0) continue;
       int S = p.restir_spatial; if (S < 0) S = 0; if (S > 8) S = 8;
       if (S == 0) continue;
@@ -421,6 +428,7 @@ static void k_spatial(const SceneRef& s, const Params& p, uint64_t seed, int row
       float cur_ph = R.p_hat;
       rm_vec3 cur_lp = R.lightPos, cur_ln = R.lightNormal, cur_le = R.emission;
       float cur_alpha = R.alpha;
+      int cur_l = ril ? ril[id] : -1;
       auto eval_at = [&](const rm_vec3& lp, const rm_vec3& ln, const rm_vec3& le, float la, float& ph_out,
                          float& dist_out, V3<float>& dn_out) -> bool {
         float ldx = lp.x - cpos.x, ldy = lp.y - cpos.y, ldz = lp.z - cpos.z;
@@ -463,6 +471,7 @@ static void k_spatial(const SceneRef& s, const Params& p, uint64_t seed, int row
                 float r = pt.U();
                 if (sum_s > 0 && r * sum_s < ws) {
                   cur_lp = hrr.lightPos; cur_ln = hrr.lightNormal; cur_le = hrr.emission; cur_alpha = hrr.alpha; cur_ph = ph;
+                  cur_l = hrl ? hrl[rp.hidx] : -1;
                 }
                 cur_sumWs = sum_s; cur_sumWu = sum_u; cur_M = newM;
               }
@@ -498,12 +507,14 @@ static void k_spatial(const SceneRef& s, const Params& p, uint64_t seed, int row
         uint32_t newM = cur_M + N.M; if (newM > uint32_t(mcap)) newM = uint32_t(mcap);
         if (sum_s > 0 && r * sum_s < w_nbr_s) {
           cur_lp = N.lightPos; cur_ln = N.lightNormal; cur_le = N.emission; cur_alpha = N.alpha; cur_ph = ph_cur;
+          cur_l = ril ? ril[nidx] : -1;
         }
         cur_sumWs = sum_s; cur_sumWu = sum_u; cur_M = newM;
       }
       Reservoir& O = ro_[id];
       O.lightPos = cur_lp; O.lightNormal = cur_ln; O.emission = cur_le; O.alpha = cur_alpha;
       O.p_hat = cur_ph; O.sumWs = cur_sumWs; O.sumWu = cur_sumWu; O.M = cur_M; O.valid = 1;
+      if (rol) rol[id] = cur_l;
     }
     rays += ctr.rays;
   });
@@ -944,7 +955,19 @@ double diel_value(double ior, bool front, int event, double cos_m, bool rough_br
   return v;
 }
 
-V3<double> frozen_path(Tracer<float>& pt, const MatTable& mt, V3<float> ro, V3<float> rd, int max_bounces) {
+// A path continued from a vertex already shaded (the ReSTIR shade's first
+// hit, pathtrace.metal:1135-1255): its throughput (fp32, and in double at the
+// parameters), the BSDF sample that left it and its light-sample sums.
+struct FrozenFrom {
+  float thr[3];
+  double t64[3];
+  float last_pdf, prev_b[3], prev_cos, prev_sumW;
+  uint32_t prev_M;
+  int prev_delta;
+};
+
+V3<double> frozen_path(Tracer<float>& pt, const MatTable& mt, V3<float> ro, V3<float> rd, int max_bounces,
+                       const FrozenFrom* from = nullptr) {
   const SceneRef& S = *pt.s;
   const Params& P = *pt.p;
   float ox = ro.x, oy = ro.y, oz = ro.z, dx = rd.x, dy = rd.y, dz = rd.z;
@@ -954,6 +977,14 @@ V3<double> frozen_path(Tracer<float>& pt, const MatTable& mt, V3<float> ro, V3<f
   float last_pdf = 0, prev_sumW = 0;
   uint32_t prev_M = 0;
   float prev_br = 0, prev_bg = 0, prev_bb = 0, prev_cos = 0;
+  const bool camera = from == nullptr;
+  if (from) {
+    thr_r = from->thr[0]; thr_g = from->thr[1]; thr_b = from->thr[2];
+    for (int c = 0; c < 3; ++c) t64[c] = from->t64[c];
+    last_pdf = from->last_pdf;
+    prev_br = from->prev_b[0]; prev_bg = from->prev_b[1]; prev_bb = from->prev_b[2]; prev_cos = from->prev_cos;
+    prev_sumW = from->prev_sumW; prev_M = from->prev_M; prev_delta = from->prev_delta;
+  }
   const float LT = float(P.light_total);
   for (int b = 0; b < max_bounces; ++b) {
     Hit<float> hit = pt.cast_alpha_ray(mk(ox, oy, oz), mk(dx, dy, dz), 1e30f);
@@ -976,7 +1007,7 @@ V3<double> frozen_path(Tracer<float>& pt, const MatTable& mt, V3<float> ro, V3<f
     if (metallic < 0) metallic = 0;
     if (metallic > 1) metallic = 1;
     float we = 1.0f;
-    if (!(bounce == 0 || prev_delta == 1)) {
+    if (!((camera && bounce == 0) || prev_delta == 1)) {
       float lx = hit.p.x - ox, ly = hit.p.y - oy, lz = hit.p.z - oz;
       float dist2 = lx * lx + ly * ly + lz * lz;
       float dist = std::sqrt(dist2);
@@ -1707,6 +1738,203 @@ int orc_render_frozen(const rm_scene_view* sv, const rm_camera* cam, const rm_co
         }
       }
       double* o = out + (size_t(y) * size_t(W) + size_t(x)) * 3;
+      for (int k = 0; k < 3; ++k) o[k] = sum[k] / double(p.spp);
+    }
+  });
+  return RM_OK;
+}
+
+// Frozen evaluation of a ReSTIR frame (K3, K4, K5; the first frame of a
+// history, denoiser not applied): K3 and K4 run in fp32 at the scene's own
+// materials and their G-buffer and merged reservoirs are held (the adjoint's
+// checkpoint), with each reservoir's light triangle; K5 is replayed from them
+// with its decisions from the fp32 path and the material factors in double at
+// `prm`: a kind-3 pixel's samples are frozen camera paths; a kind-1 pixel's
+// base is the first hit's emission plus the held light sample's Le f cos
+// alpha W w_MIS, and each indirect sample leaves the first hit with the BSDF
+// sample f cos / pdf and goes on as a frozen path (pathtrace.metal:1056-1258).
+// The first hit's triangle comes from K3's primary ray traced again.
+int orc_render_frozen_restir(const rm_scene_view* sv, const rm_camera* cam, const rm_config* cfg, uint64_t seed,
+                             const int32_t* tri_material, const double* prm, int n_materials, double* out,
+                             int nthreads) {
+  using namespace orc;
+  if (cfg->width <= 0 || cfg->height <= 0 || cfg->spp <= 0 || cfg->max_bounces < 0 || n_materials < 0)
+    return RM_ERR_INVALID;
+  SceneRef s;
+  s.tris = sv->tris; s.n_tris = sv->n_tris;
+  s.nodes = to_preorder(sv->nodes, sv->n_nodes);
+  s.indices = sv->bvh_tri; s.lights = sv->light_tri; s.cdf = sv->light_cdf;
+  s.n_lights = sv->n_lights; s.light_total = sv->light_total; s.texels = sv->texels;
+  bool opaque = true;
+  for (int i = 0; i < sv->n_tris; ++i)
+    if (!(sv->tris[i].alpha >= 1)) { opaque = false; break; }
+  Env env = read_env(cfg->flags);
+  Params p = resolve(*cfg, *cam, int(s.nodes.size()), sv->n_lights, sv->light_total, opaque, env);
+  const int W = p.width, H = p.height;
+  const size_t pixels = size_t(W) * size_t(H);
+  if (!(p.restir_spatial > 0 && p.lights > 0 && p.bounces > 0 && p.opaque &&
+        pixels * (sizeof(GBuf) + 2 * sizeof(Reservoir)) <= size_t(512) * 1024 * 1024))
+    return RM_ERR_INVALID;  // the policy renders the plain frame: orc_render_frozen
+  p.hasHistory = 0;
+  std::vector<GBuf> g(pixels), hg(pixels);
+  std::vector<Reservoir> ri(pixels), rmg(pixels), hr(pixels);
+  std::vector<int32_t> ril(pixels, -1), rml(pixels, -1);
+  std::atomic<uint64_t> rays{0};
+  k_generate(s, p, seed, 0, H, g.data(), ri.data(), nthreads, rays, ril.data());
+  k_spatial(s, p, seed, 0, H, g.data(), ri.data(), rmg.data(), hg.data(), hr.data(), nthreads, rays, ril.data(),
+            rml.data(), nullptr);
+  MatTable mt;
+  mt.tri_mat = tri_material;
+  mt.prm = prm;
+  const double cl = p.clamp_value;
+  parallel_for(H, nthreads, [&](int yy) {
+    Counters ctr;
+    const uint32_t y = uint32_t(yy);
+    for (uint32_t x = 0; x < uint32_t(W); ++x) {
+      const uint32_t id = y * uint32_t(W) + x;
+      double* o = out + size_t(id) * 3;
+      o[0] = o[1] = o[2] = 0;
+      const GBuf& gg = g[id];
+      if (gg.kind == 0) continue;
+      Tracer<float> pt{&s, &p, Rng{}, &ctr};
+      pt.rng.seed(seed_shade(seed, id));
+      auto clampd = [&](double* v) {
+        if (cl > 0)
+          for (int c = 0; c < 3; ++c) v[c] = std::fmin(v[c], cl);
+      };
+      const rm_camera& c = p.camera;
+      if (gg.kind == 3) {
+        double sum[3] = {0, 0, 0};
+        for (int si = 0; si < p.spp; ++si) {
+          float sx, sy;
+          pt.jitter(x, y, sx, sy);
+          float focal2 = c.focal * c.focal;
+          float dist = 1.0f / std::sqrt(sx * sx + (sy * sy + focal2));
+          float tx = sx * dist, ty = sy * dist, tz = c.focal * dist;
+          V3<float> rd = mk(tx * c.m0 + (ty * c.m1 + tz * c.m2), tx * c.m3 + (ty * c.m4 + tz * c.m5),
+                            tx * c.m6 + (ty * c.m7 + tz * c.m8));
+          const V3<double> v = frozen_path(pt, mt, mk(c.x, c.y, c.z), rd, p.bounces);
+          double vv[3] = {v.x, v.y, v.z};
+          clampd(vv);
+          for (int k = 0; k < 3; ++k) sum[k] += vv[k];
+        }
+        for (int k = 0; k < 3; ++k) o[k] = sum[k] / double(p.spp);
+        clampd(o);
+        continue;
+      }
+      // kind 1: the first hit's triangle, from K3's primary ray
+      Hit<float> h0;
+      {
+        Tracer<float> p3{&s, &p, Rng{}, &ctr};
+        p3.rng.seed(seed_pixel(seed, x, y));
+        float sx = float(x) + 1e-12f + (p.resolution - 2e-12f) * p3.U() - float(p.width) * 0.5f;
+        float sy = float(p.height) * 0.5f - (float(y) + 1e-12f + (p.resolution - 2e-12f) * p3.U());
+        float f2 = c.focal * c.focal;
+        float dinv = 1.0f / std::sqrt(sx * sx + sy * sy + f2);
+        float tx = sx * dinv, ty = sy * dinv, tz = c.focal * dinv;
+        V3<float> rd = mk(tx * c.m0 + (ty * c.m1 + tz * c.m2), tx * c.m3 + (ty * c.m4 + tz * c.m5),
+                          tx * c.m6 + (ty * c.m7 + tz * c.m8));
+        h0 = p3.cast_alpha_ray(mk(c.x, c.y, c.z), rd, 1e30f);
+      }
+      if (h0.tri < 0) continue;
+      V3<float> gpos = vf<float>(gg.pos), gnor = vf<float>(gg.normal), galb = vf<float>(gg.albedo),
+                gwo = vf<float>(gg.wo);
+      float rough = gg.rough; if (rough < 0) rough = 0; if (rough > 1) rough = 1;
+      float metallic = gg.metallic; if (metallic < 0) metallic = 0; if (metallic > 1) metallic = 1;
+      float r2 = rough; if (r2 < 0.02f) r2 = 0.02f;
+      float alpha2 = (r2 * r2) * (r2 * r2);
+      float spec_prob = 0.05f + 0.95f * metallic; if (spec_prob > 0.98f) spec_prob = 0.98f;
+      if (metallic >= 0.999f) spec_prob = 1.0f;
+      double base[3];
+      for (int k = 0; k < 3; ++k) base[k] = mt.get(s.tris, h0.tri, 4 + k);
+      float m_sumWu = 0;
+      uint32_t m_M = 0;
+      const Reservoir& R = rmg[id];
+      if (R.valid != 0 && R.M > 0 && R.sumWu > 0 && R.sumWs > 0 && R.p_hat > 0) {
+        m_sumWu = R.sumWu; m_M = R.M;
+        float ldx = R.lightPos.x - gpos.x, ldy = R.lightPos.y - gpos.y, ldz = R.lightPos.z - gpos.z;
+        float dist = std::sqrt(ldx * ldx + ldy * ldy + ldz * ldz);
+        if (dist > 0.003f) {
+          float inv = 1.0f / dist;
+          float dxn = ldx * inv, dyn = ldy * inv, dzn = ldz * inv;
+          float lcos = -(R.lightNormal.x * dxn + (R.lightNormal.y * dyn + R.lightNormal.z * dzn));
+          float scos = gnor.x * dxn + (gnor.y * dyn + gnor.z * dzn);
+          if (lcos > 1e-8f && scos > 1e-8f) {
+            auto e = Tracer<float>::eval_bsdf(dxn, dyn, dzn, gwo.x, gwo.y, gwo.z, gnor.x, gnor.y, gnor.z, alpha2,
+                                              metallic, spec_prob, galb.x, galb.y, galb.z);
+            float Fr = R.emission.x * e.r * scos * R.alpha, Fg = R.emission.y * e.g * scos * R.alpha,
+                  Fb = R.emission.z * e.b * scos * R.alpha;
+            float ph = lum3(Fr, Fg, Fb);
+            if (ph > 0 && rml[id] >= 0) {
+              float pdf_ris = float(m_M) * ph / m_sumWu;
+              float wnee = 1.0f;
+              if (!p.nomis && e.pdf > 1e-20f) wnee = pdf_ris / (pdf_ris + e.pdf);
+              float Wt = R.sumWs / (float(m_M) * ph);
+              const double k = double(scos) * double(R.alpha) * double(Wt) * double(wnee);
+              const V3<double> f = bsdf64(mt, s, h0, dxn, dyn, dzn, gwo.x, gwo.y, gwo.z, gnor.x, gnor.y, gnor.z,
+                                          metallic, spec_prob);
+              const double fv[3] = {f.x, f.y, f.z};
+              for (int q = 0; q < 3; ++q) base[q] += mt.get(s.tris, rml[id], 4 + q) * fv[q] * k;
+            }
+          }
+        }
+      }
+      if (p.bounces <= 1) {
+        for (int k = 0; k < 3; ++k) o[k] = base[k];
+        clampd(o);
+        continue;
+      }
+      double sum[3] = {0, 0, 0};
+      for (int si = 0; si < p.spp; ++si) {
+        float nx2 = 0, ny2 = 0, nz2 = 0;
+        int pdelta = 0;
+        bool early = false;
+        if (pt.U() < spec_prob) {
+          float hx, hy, hz;
+          pt.sample_ggx_half(alpha2, gnor.x, gnor.y, gnor.z, hx, hy, hz);
+          float md = gwo.x * hx + (gwo.y * hy + gwo.z * hz);
+          if (!(md > 1e-8f)) early = true;
+          else {
+            nx2 = 2.0f * md * hx - gwo.x; ny2 = 2.0f * md * hy - gwo.y; nz2 = 2.0f * md * hz - gwo.z;
+            pdelta = (rough <= 0.0201f) ? 1 : 0;
+          }
+        } else {
+          pt.sample_cosine(gnor.x, gnor.y, gnor.z, nx2, ny2, nz2);
+          pdelta = 0;
+        }
+        Tracer<float>::Bsdf e0;
+        if (!early) {
+          float ncos = nx2 * gnor.x + (ny2 * gnor.y + nz2 * gnor.z);
+          if (!(ncos > 1e-8f)) early = true;
+          else {
+            float d = 1.0f / std::sqrt(nx2 * nx2 + ny2 * ny2 + nz2 * nz2);
+            nx2 *= d; ny2 *= d; nz2 *= d;
+            e0 = Tracer<float>::eval_bsdf(nx2, ny2, nz2, gwo.x, gwo.y, gwo.z, gnor.x, gnor.y, gnor.z, alpha2,
+                                          metallic, spec_prob, galb.x, galb.y, galb.z);
+            if (!(e0.pdf > 1e-12f)) early = true;
+          }
+        }
+        double v[3] = {base[0], base[1], base[2]};
+        if (!early) {
+          float cos0 = nx2 * gnor.x + (ny2 * gnor.y + nz2 * gnor.z);
+          const V3<double> f0 = bsdf64(mt, s, h0, nx2, ny2, nz2, gwo.x, gwo.y, gwo.z, gnor.x, gnor.y, gnor.z,
+                                       metallic, spec_prob);
+          FrozenFrom ff;
+          ff.thr[0] = e0.r * cos0 / e0.pdf; ff.thr[1] = e0.g * cos0 / e0.pdf; ff.thr[2] = e0.b * cos0 / e0.pdf;
+          ff.t64[0] = f0.x * double(cos0) / double(e0.pdf);
+          ff.t64[1] = f0.y * double(cos0) / double(e0.pdf);
+          ff.t64[2] = f0.z * double(cos0) / double(e0.pdf);
+          ff.last_pdf = e0.pdf;
+          ff.prev_b[0] = e0.r; ff.prev_b[1] = e0.g; ff.prev_b[2] = e0.b; ff.prev_cos = cos0;
+          ff.prev_sumW = m_sumWu; ff.prev_M = m_M; ff.prev_delta = pdelta;
+          const V3<double> a = frozen_path(pt, mt, mk(gpos.x + gnor.x * 0.001f, gpos.y + gnor.y * 0.001f,
+                                                      gpos.z + gnor.z * 0.001f),
+                                           mk(nx2, ny2, nz2), p.bounces - 1, &ff);
+          v[0] += a.x; v[1] += a.y; v[2] += a.z;
+        }
+        clampd(v);
+        for (int k = 0; k < 3; ++k) sum[k] += v[k];
+      }
       for (int k = 0; k < 3; ++k) o[k] = sum[k] / double(p.spp);
     }
   });

@@ -77,6 +77,10 @@ def oracle_lib() -> C.CDLL:
         lib.orc_render_frozen.restype = C.c_int
         lib.orc_render_frozen.argtypes = [C.POINTER(_abi.RmSceneView), C.POINTER(_abi.RmCamera),
                                           C.POINTER(_abi.RmConfig), C.c_uint64, _P, _P, C.c_int, _P, C.c_int]
+        lib.orc_render_frozen_restir.restype = C.c_int
+        lib.orc_render_frozen_restir.argtypes = [C.POINTER(_abi.RmSceneView), C.POINTER(_abi.RmCamera),
+                                                 C.POINTER(_abi.RmConfig), C.c_uint64, _P, _P, C.c_int, _P,
+                                                 C.c_int]
         lib.orc_build_bvh.restype = C.c_int
         lib.orc_build_bvh.argtypes = [_P, C.c_int, C.c_int, _P, _P, _P]
         lib.orc_refit_bvh.argtypes = [_P, C.c_int, _P, _P, _P]
@@ -241,6 +245,24 @@ def render_frozen(scene: PackedScene, cam: Camera, cfg: RenderConfig, seed: int,
                                         threads or nthreads())
     if rc != 0:
         raise ValueError("frozen evaluation needs a fixed sample count and the plain chain")
+    return out
+
+
+def render_frozen_restir(scene: PackedScene, cam: Camera, cfg: RenderConfig, seed: int, tri_material: np.ndarray,
+                         params: np.ndarray, threads: int | None = None) -> np.ndarray:
+    """The ReSTIR frame (first of a history, no denoiser) with K3/K4 run at the
+    scene's own materials and held, and K5 replayed frozen with the material
+    factors in double at ``params``; W*H x 3."""
+    tm = np.ascontiguousarray(tri_material, np.int32)
+    prm = np.ascontiguousarray(params, np.float64)
+    assert len(tm) == scene.n_tris and prm.ndim == 2 and prm.shape[1] == 8
+    out = np.zeros((cfg.width * cfg.height, 3), np.float64)
+    sv = scene.view(True)
+    rc = oracle_lib().orc_render_frozen_restir(C.byref(sv), C.byref(cam.packed()), C.byref(cfg.packed()),
+                                               C.c_uint64(seed), tm.ctypes.data, prm.ctypes.data, len(prm),
+                                               out.ctypes.data, threads or nthreads())
+    if rc != 0:
+        raise ValueError("frozen ReSTIR evaluation needs a configuration the policy renders with ReSTIR")
     return out
 
 

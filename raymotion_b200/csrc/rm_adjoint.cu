@@ -159,11 +159,21 @@ struct Deferred {
 // and the g . dlogB_k . C halves when the path ends, returning C in C_out.
 // kRis: the frame's NEE takes several candidates (RIS); a separate
 // instantiation keeps the single-candidate walk's registers as they were.
+// `from` (null: a camera ray) continues a path from a vertex already shaded
+// (the ReSTIR shade's primary vertex, pathtrace.metal:1135-1255): its
+// throughput, the BSDF sample that left it and its light-sample sums, so that
+// the first vertex's emission takes its MIS weight.
+struct WalkFrom {
+  float thr[3], last_pdf, prev_b[3], prev_cos, prev_sumW;
+  uint32_t prev_M;
+  int prev_delta;
+};
+
 template <bool kRis>
 __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict__ tri_mat, float ox, float oy,
                                           float oz, float dx, float dy, float dz, int max_bounces, float Cr, float Cg,
                                           float Cb, float gr, float gg, float gb, const GradSink& sink,
-                                          Deferred* dfr, float* C_out) {
+                                          Deferred* dfr, float* C_out, const WalkFrom* from = nullptr) {
   if (dfr) dfr->n = 0;
   const Scene& s = pt.s;
   const Params& p = pt.p;
@@ -172,6 +182,13 @@ __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict_
   float last_pdf = 0, prev_sumW = 0;
   uint32_t prev_M = 0;
   float prev_br = 0, prev_bg = 0, prev_bb = 0, prev_cos = 0;
+  const bool camera = from == nullptr;
+  if (from) {
+    thr_r = from->thr[0]; thr_g = from->thr[1]; thr_b = from->thr[2];
+    last_pdf = from->last_pdf;
+    prev_br = from->prev_b[0]; prev_bg = from->prev_b[1]; prev_bb = from->prev_b[2]; prev_cos = from->prev_cos;
+    prev_sumW = from->prev_sumW; prev_M = from->prev_M; prev_delta = from->prev_delta;
+  }
   const float LT = p.light_total;
   for (int b = 0; b < max_bounces; ++b) {
     Hit hit = pt.cast_alpha_ray(ox, oy, oz, dx, dy, dz, kFar);
@@ -196,7 +213,7 @@ __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict_
     if (metallic < 0.0f) metallic = 0.0f;
     if (metallic > 1.0f) metallic = 1.0f;
     float we = 1.0f;  // MIS weight of the emission term (held fixed)
-    if (bounce == 0 || prev_delta == 1) {
+    if ((camera && bounce == 0) || prev_delta == 1) {
       accr += hit.er * thr_r; accg += hit.eg * thr_g; accb += hit.eb * thr_b;
     } else {
       float lx = hit.px - ox, ly = hit.py - oy, lz = hit.pz - oz;
@@ -429,6 +446,55 @@ __device__ __noinline__ void adjoint_path(Tracer& pt, const int32_t* __restrict_
   }
 }
 
+// One sample of a camera path (pathtrace.metal:749-758, the samples of K1, K2
+// and of K5's kind-3 pixels :1070-1084): the jitter draws, then the path's
+// adjoint for the loss gradient (d0, d1, d2) of the sample's clamped value.
+// One walk when the path's vertices fit the deferred list, else a first walk
+// for C (Tracer::sample_sensor) and a second for the derivative.
+template <bool kRis>
+__device__ __forceinline__ void camera_sample_adjoint(Tracer& pt, const int32_t* __restrict__ tri_mat, uint32_t x,
+                                                      uint32_t y, float d0, float d1, float d2,
+                                                      const GradSink& sink) {
+  const Params& p = pt.p;
+  const bool one_walk = p.bounces <= Deferred::kMax;
+  const bool cl = p.clamp_value > 0.0f;
+  float sx, sy;
+  pt.jitter(x, y, sx, sy);
+  const uint32_t st0 = pt.rng.state;
+  const rm_camera& cam = p.camera;
+  const float focal2 = cam.focal * cam.focal;
+  const float dist = 1.0f / sqrtf(sx * sx + (sy * sy + focal2));
+  const float tx = sx * dist, ty = sy * dist, tz = cam.focal * dist;
+  const float dx = tx * cam.m0 + (ty * cam.m1 + tz * cam.m2);
+  const float dy = tx * cam.m3 + (ty * cam.m4 + tz * cam.m5);
+  const float dz = tx * cam.m6 + (ty * cam.m7 + tz * cam.m8);
+  float C[3];
+  if (one_walk) {
+    // derivative as if no channel were clamped; a clamped channel (rare)
+    // is taken back out by a second walk with -g on that channel
+    Deferred dfr;
+    adjoint_path<kRis>(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, 0.f, 0.f, 0.f, d0, d1, d2, sink, &dfr,
+                 C);
+    if (cl && !(C[0] < p.clamp_value && C[1] < p.clamp_value && C[2] < p.clamp_value)) {
+      const uint32_t st1 = pt.rng.state;
+      pt.rng.state = st0;
+      adjoint_path<kRis>(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, C[0], C[1], C[2],
+                   C[0] < p.clamp_value ? 0.f : -d0, C[1] < p.clamp_value ? 0.f : -d1,
+                   C[2] < p.clamp_value ? 0.f : -d2, sink, nullptr, nullptr);
+      pt.rng.state = st1;
+    }
+  } else {
+    pt.sample_sensor(sx, sy, p.bounces, C[0], C[1], C[2]);
+    pt.rng.state = st0;
+    // the sample enters the pixel mean clamped (pathtrace.metal:757)
+    const float gr = (cl && !(C[0] < p.clamp_value)) ? 0.0f : d0;
+    const float gg = (cl && !(C[1] < p.clamp_value)) ? 0.0f : d1;
+    const float gb = (cl && !(C[2] < p.clamp_value)) ? 0.0f : d2;
+    adjoint_path<kRis>(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, C[0], C[1], C[2], gr, gg, gb, sink,
+                 nullptr, nullptr);
+  }
+}
+
 // One pixel lane per thread, the samples of K1 (LANES 1) or of one lane of K2,
 // in the forward kernels' order (pathtrace.metal:749-758, :787-796).
 template <int LANES, bool kRis>
@@ -454,47 +520,230 @@ __global__ void __launch_bounds__(256) k_adjoint(Scene s, Params p, uint64_t see
     const float inv_n = 1.0f / float(p.spp);
     const float d0 = dLdI[size_t(pixel) * 3] * inv_n, d1 = dLdI[size_t(pixel) * 3 + 1] * inv_n,
                 d2 = dLdI[size_t(pixel) * 3 + 2] * inv_n;
-    // one walk per sample when its vertices fit the deferred list, else a
-    // first walk for C (Tracer::pathtrace) and a second for the derivative
-    const bool one_walk = p.bounces <= Deferred::kMax;
-    const bool cl = p.clamp_value > 0.0f;
     for (uint32_t si = lane; si < uint32_t(p.spp); si += LANES) {
-      float sx, sy;
-      pt.jitter(x, y, sx, sy);
-      const uint32_t st0 = pt.rng.state;
-      const rm_camera& cam = p.camera;
-      const float focal2 = cam.focal * cam.focal;
-      const float dist = 1.0f / sqrtf(sx * sx + (sy * sy + focal2));
-      const float tx = sx * dist, ty = sy * dist, tz = cam.focal * dist;
-      const float dx = tx * cam.m0 + (ty * cam.m1 + tz * cam.m2);
-      const float dy = tx * cam.m3 + (ty * cam.m4 + tz * cam.m5);
-      const float dz = tx * cam.m6 + (ty * cam.m7 + tz * cam.m8);
-      float C[3];
-      if (one_walk) {
-        // derivative as if no channel were clamped; a clamped channel (rare)
-        // is taken back out by a second walk with -g on that channel
-        Deferred dfr;
-        adjoint_path<kRis>(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, 0.f, 0.f, 0.f, d0, d1, d2, sink, &dfr,
-                     C);
-        if (cl && !(C[0] < p.clamp_value && C[1] < p.clamp_value && C[2] < p.clamp_value)) {
-          const uint32_t st1 = pt.rng.state;
-          pt.rng.state = st0;
-          adjoint_path<kRis>(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, C[0], C[1], C[2],
-                       C[0] < p.clamp_value ? 0.f : -d0, C[1] < p.clamp_value ? 0.f : -d1,
-                       C[2] < p.clamp_value ? 0.f : -d2, sink, nullptr, nullptr);
-          pt.rng.state = st1;
-        }
-      } else {
-        pt.sample_sensor(sx, sy, p.bounces, C[0], C[1], C[2]);
-        pt.rng.state = st0;
-        // the sample enters the pixel mean clamped (pathtrace.metal:757)
-        const float gr = (cl && !(C[0] < p.clamp_value)) ? 0.0f : d0;
-        const float gg = (cl && !(C[1] < p.clamp_value)) ? 0.0f : d1;
-        const float gb = (cl && !(C[2] < p.clamp_value)) ? 0.0f : d2;
-        adjoint_path<kRis>(pt, tri_mat, cam.x, cam.y, cam.z, dx, dy, dz, p.bounces, C[0], C[1], C[2], gr, gg, gb, sink,
-                     nullptr, nullptr);
-      }
+      camera_sample_adjoint<kRis>(pt, tri_mat, x, y, d0, d1, d2, sink);
       ++samples;
+    }
+  }
+  const unsigned long long tot = __reduce_add_sync(0xffffffffu, samples);
+  if ((threadIdx.x & 31) == 0 && tot) atomicAdd(ctr, tot);
+  if (use_shared) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < n_mat * kMatParams; i += blockDim.x)
+      if (sh[i] != 0.0f) atomicAdd(grad + i, sh[i]);
+  }
+}
+
+// The adjoint of K5, the ReSTIR shade (pathtrace.metal:1056-1258), from the
+// frame's checkpoint: its G-buffer and merged reservoirs (the light sample
+// each kind-1 pixel shades, with its light index) stay as the forward pass
+// left them, and the pixel's K5 draws are replayed.  Kind-3 pixels (a
+// dielectric first hit) are camera paths, as in K1.  A kind-1 pixel's value
+// is the mean over samples of clamp(base + C_s): base = the first hit's
+// emission + the reservoir sample's Le f cos alpha W w_MIS (sample, W and MIS
+// weight held), C_s an indirect path that leaves the first hit with the BSDF
+// sample B_0 = f cos / pdf and goes on as a camera path's vertices do
+// (adjoint_path from the first hit; Russian roulette from its second vertex).
+// d(base) moves with the first hit's emission, albedo and roughness and the
+// sampled light's emission; C_s with its vertices (the walk) and with B_0
+// (dlog B_0 * C_s).  The first hit's material is found by tracing K3's
+// primary ray again (pathtrace.metal:829-840).
+template <bool kRis>
+__global__ void __launch_bounds__(256) k_adjoint_restir(Scene s, Params p, uint64_t seed, GBufSoA gb, ResSoA rm,
+                                                        const int32_t* __restrict__ tri_mat, int n_mat,
+                                                        const float* __restrict__ dLdI, float* __restrict__ grad,
+                                                        int use_shared, unsigned long long* ctr, uint32_t* err) {
+  extern __shared__ float sh[];
+  if (use_shared) {
+    for (int i = threadIdx.x; i < n_mat * kMatParams; i += blockDim.x) sh[i] = 0.0f;
+    __syncthreads();
+  }
+  const GradSink sink{use_shared ? sh : nullptr, grad};
+  const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t npix = uint32_t(p.width) * uint32_t(p.height);
+  uint32_t samples = 0;
+  const float4 PK = id < npix ? gb.pos_kind[id] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const int kind = __float_as_int(PK.w);
+  if (id < npix && kind != 0) {
+    const uint32_t x = id % uint32_t(p.width), y = id / uint32_t(p.width);
+    Tracer pt(s, p, err);
+    pt.rng.seed(seed ^ (uint64_t(id + 1) * 0xBF58476D1CE4E5B9ull) ^ 0x94D049BB133111EBull);
+    const bool cl = p.clamp_value > 0.0f;
+    const float D[3] = {dLdI[size_t(id) * 3], dLdI[size_t(id) * 3 + 1], dLdI[size_t(id) * 3 + 2]};
+    if (kind == 3) {
+      const float inv_n = 1.0f / float(p.spp);
+      for (int si = 0; si < p.spp; ++si) {
+        camera_sample_adjoint<kRis>(pt, tri_mat, x, y, D[0] * inv_n, D[1] * inv_n, D[2] * inv_n, sink);
+        ++samples;
+      }
+    } else {
+      // the first hit's triangle: K3's primary ray (its own random stream)
+      int m0 = -1;
+      float tx0[3] = {1.f, 1.f, 1.f};
+      bool alb0 = false;
+      float dal0 = 0.0f;
+      {
+        Tracer p3(s, p, err);
+        p3.rng.seed(seed_pixel(seed, x, y));
+        float sx = float(x) + 1e-12f + (p.resolution - 2e-12f) * p3.U() - float(p.width) * 0.5f;
+        float sy = float(p.height) * 0.5f - (float(y) + 1e-12f + (p.resolution - 2e-12f) * p3.U());
+        const rm_camera& c = p.camera;
+        float f2 = c.focal * c.focal;
+        float dinv = 1.0f / sqrtf(sx * sx + sy * sy + f2);
+        float tx = sx * dinv, ty = sy * dinv, tz = c.focal * dinv;
+        float rdx = tx * c.m0 + (ty * c.m1 + tz * c.m2);
+        float rdy = tx * c.m3 + (ty * c.m4 + tz * c.m5);
+        float rdz = tx * c.m6 + (ty * c.m7 + tz * c.m8);
+        const Hit h0 = p3.cast_alpha_ray(c.x, c.y, c.z, rdx, rdy, rdz, kFar);
+        if (h0.tri >= 0) {
+          m0 = tri_mat[h0.tri];
+          tx0[0] = h0.txr; tx0[1] = h0.txg; tx0[2] = h0.txb;
+          alb0 = h0.shader != 1;
+          dal0 = dalpha2(h0.rough);
+        }
+      }
+      const float4 NR = gb.nor_rough[id], AM = gb.alb_met[id], WO = gb.wo_ior[id], EM = gb.emi[id];
+      const float gpx = PK.x, gpy = PK.y, gpz = PK.z, gnx = NR.x, gny = NR.y, gnz = NR.z;
+      float rough = NR.w; if (rough < 0.0f) rough = 0.0f; if (rough > 1.0f) rough = 1.0f;
+      float metallic = AM.w; if (metallic < 0.0f) metallic = 0.0f; if (metallic > 1.0f) metallic = 1.0f;
+      float r2 = rough; if (r2 < 0.02f) r2 = 0.02f;
+      const float alpha2 = (r2 * r2) * (r2 * r2);
+      float spec_prob = 0.05f + 0.95f * metallic; if (spec_prob > 0.98f) spec_prob = 0.98f;
+      if (metallic >= 0.999f) spec_prob = 1.0f;
+      // base: emission + the reservoir's light sample (pathtrace.metal:1100-1128)
+      float pd[3] = {0.f, 0.f, 0.f};
+      float pk = 0.0f, pdx = 0.f, pdy = 0.f, pdz = 0.f, ple[3] = {0.f, 0.f, 0.f};
+      int pli = -1;
+      float m_sumWu = 0.0f;
+      uint32_t m_M = 0;
+      const float4 R3 = rm.sumwu_m_valid[id];
+      const float4 R0 = rm.lp_alpha[id], R1 = rm.ln_phat[id], R2 = rm.le_sumws[id];
+      if (__float_as_int(R3.z) != 0 && __float_as_int(R3.y) != 0 && R3.x > 0.0f && R2.w > 0.0f && R1.w > 0.0f) {
+        m_sumWu = R3.x; m_M = uint32_t(__float_as_int(R3.y));
+        const float m_sumWs = R2.w;
+        float ldx = R0.x - gpx, ldy = R0.y - gpy, ldz = R0.z - gpz;
+        float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
+        if (dist > 0.003f) {
+          float inv = 1.0f / dist;
+          float dxn = ldx * inv, dyn = ldy * inv, dzn = ldz * inv;
+          float lcos = -(R1.x * dxn + (R1.y * dyn + R1.z * dzn));
+          float scos = gnx * dxn + (gny * dyn + gnz * dzn);
+          if (lcos > 1e-8f && scos > 1e-8f) {
+            Bsdf e = Tracer::eval_bsdf(dxn, dyn, dzn, WO.x, WO.y, WO.z, gnx, gny, gnz, alpha2, metallic, spec_prob,
+                                       AM.x, AM.y, AM.z);
+            float Fr = R2.x * e.r * scos * R0.w, Fg = R2.y * e.g * scos * R0.w, Fb = R2.z * e.b * scos * R0.w;
+            float ph = lum3(Fr, Fg, Fb);
+            if (ph > 0.0f) {
+              float pdf_ris = float(m_M) * ph / m_sumWu;
+              float wnee = 1.0f;
+              if (!p.nomis && e.pdf > 1e-20f) wnee = pdf_ris / (pdf_ris + e.pdf);
+              float Wt = m_sumWs / (float(m_M) * ph);
+              pd[0] = Fr * Wt * wnee; pd[1] = Fg * Wt * wnee; pd[2] = Fb * Wt * wnee;
+              pk = scos * R0.w * Wt * wnee;
+              pdx = dxn; pdy = dyn; pdz = dzn;
+              ple[0] = R2.x; ple[1] = R2.y; ple[2] = R2.z;
+              pli = __float_as_int(R3.w);
+            }
+          }
+        }
+      }
+      const float base[3] = {EM.x + pd[0], EM.y + pd[1], EM.z + pd[2]};
+      float gbase[3] = {0.f, 0.f, 0.f};  // sum over samples of the gradient reaching `base`
+      if (p.bounces <= 1 || p.spp <= 0) {
+        for (int c = 0; c < 3; ++c) gbase[c] = (cl && !(base[c] < p.clamp_value)) ? 0.0f : D[c];
+      } else {
+        const float inv_n = 1.0f / float(p.spp);
+        const float g[3] = {D[0] * inv_n, D[1] * inv_n, D[2] * inv_n};
+        for (int si = 0; si < p.spp; ++si) {
+          ++samples;
+          float nx2 = 0, ny2 = 0, nz2 = 0;
+          int pdelta = 0;
+          bool early = false;
+          if (pt.U() < spec_prob) {
+            float hx, hy, hz;
+            pt.sample_ggx_half(alpha2, gnx, gny, gnz, hx, hy, hz);
+            float md = WO.x * hx + (WO.y * hy + WO.z * hz);
+            if (!(md > 1e-8f)) early = true;
+            else {
+              nx2 = 2.0f * md * hx - WO.x; ny2 = 2.0f * md * hy - WO.y; nz2 = 2.0f * md * hz - WO.z;
+              pdelta = (rough <= 0.0201f) ? 1 : 0;
+            }
+          } else {
+            pt.sample_cosine(gnx, gny, gnz, nx2, ny2, nz2);
+            pdelta = 0;
+          }
+          Bsdf e0{0.f, 0.f, 0.f, 0.f};
+          if (!early) {
+            float ncos = nx2 * gnx + (ny2 * gny + nz2 * gnz);
+            if (!(ncos > 1e-8f)) early = true;
+            else {
+              float d = 1.0f / sqrtf(nx2 * nx2 + ny2 * ny2 + nz2 * nz2);
+              nx2 *= d; ny2 *= d; nz2 *= d;
+              e0 = Tracer::eval_bsdf(nx2, ny2, nz2, WO.x, WO.y, WO.z, gnx, gny, gnz, alpha2, metallic, spec_prob,
+                                     AM.x, AM.y, AM.z);
+              if (!(e0.pdf > 1e-12f)) early = true;
+            }
+          }
+          if (early) {
+            for (int c = 0; c < 3; ++c) gbase[c] += (cl && !(base[c] < p.clamp_value)) ? 0.0f : g[c];
+            continue;
+          }
+          const float cos0 = nx2 * gnx + (ny2 * gny + nz2 * gnz);
+          WalkFrom wf;
+          wf.thr[0] = e0.r * cos0 / e0.pdf; wf.thr[1] = e0.g * cos0 / e0.pdf; wf.thr[2] = e0.b * cos0 / e0.pdf;
+          wf.last_pdf = e0.pdf;
+          wf.prev_b[0] = e0.r; wf.prev_b[1] = e0.g; wf.prev_b[2] = e0.b; wf.prev_cos = cos0;
+          wf.prev_sumW = m_sumWu; wf.prev_M = m_M; wf.prev_delta = pdelta;
+          const float ox = gpx + gnx * 0.001f, oy = gpy + gny * 0.001f, oz = gpz + gnz * 0.001f;
+          const uint32_t st0 = pt.rng.state;
+          Deferred dfr;
+          float C[3];
+          adjoint_path<kRis>(pt, tri_mat, ox, oy, oz, nx2, ny2, nz2, p.bounces - 1, 0.f, 0.f, 0.f, g[0], g[1], g[2],
+                             sink, &dfr, C, &wf);
+          bool clamped[3];
+          float ge[3];
+          for (int c = 0; c < 3; ++c) {
+            clamped[c] = cl && !(base[c] + C[c] < p.clamp_value);
+            ge[c] = clamped[c] ? 0.0f : g[c];
+            gbase[c] += ge[c];
+          }
+          if (clamped[0] || clamped[1] || clamped[2]) {
+            // the clamped channels' walk terms back out
+            const uint32_t st1 = pt.rng.state;
+            pt.rng.state = st0;
+            adjoint_path<kRis>(pt, tri_mat, ox, oy, oz, nx2, ny2, nz2, p.bounces - 1, C[0], C[1], C[2],
+                               clamped[0] ? -g[0] : 0.f, clamped[1] ? -g[1] : 0.f, clamped[2] ? -g[2] : 0.f, sink,
+                               nullptr, nullptr, &wf);
+            pt.rng.state = st1;
+          }
+          // B_0 = f cos / pdf: dlog B_0 = df / f, times the walk's radiance C
+          const BsdfGrad bg = bsdf_grad(nx2, ny2, nz2, WO.x, WO.y, WO.z, gnx, gny, gnz, alpha2, metallic, AM.x, AM.y,
+                                        AM.z);
+          float drough = 0.0f;
+          for (int c = 0; c < 3; ++c) {
+            if (!(bg.f[c] > 0.0f)) continue;
+            const float w = ge[c] * C[c] / bg.f[c];
+            if (alb0) sink.add(m0, c, w * bg.da[c] * tx0[c]);
+            drough += w * bg.dal2[c];
+          }
+          sink.add(m0, 3, drough * dal0);
+        }
+      }
+      // base terms: the first hit's emission and the held light sample Le f k
+      for (int c = 0; c < 3; ++c) sink.add(m0, 4 + c, gbase[c]);
+      if (pli >= 0 && pk != 0.0f) {
+        const int ml = tri_mat[s.lights[pli]];
+        const BsdfGrad bg = bsdf_grad(pdx, pdy, pdz, WO.x, WO.y, WO.z, gnx, gny, gnz, alpha2, metallic, AM.x, AM.y,
+                                      AM.z);
+        float drough = 0.0f;
+        for (int c = 0; c < 3; ++c) {
+          const float gt = gbase[c] * pk;
+          sink.add(ml, 4 + c, gt * bg.f[c]);
+          if (alb0) sink.add(m0, c, gt * ple[c] * bg.da[c] * tx0[c]);
+          drough += gt * ple[c] * bg.dal2[c];
+        }
+        sink.add(m0, 3, drough * dal0);
+      }
     }
   }
   const unsigned long long tot = __reduce_add_sync(0xffffffffu, samples);
@@ -544,6 +793,21 @@ cudaError_t apply_materials(rm_triangle* tris, const int32_t* tri_mat, const flo
                             cudaStream_t st) {
   if (n_tris <= 0) return cudaSuccess;
   k_apply_materials<<<(n_tris + 255) / 256, 256, 0, st>>>(tris, tri_mat, mats, n_tris);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_restir(const Scene& s, const Params& p, uint64_t seed, const GBufSoA& gb, const ResSoA& rm,
+                                  const int32_t* tri_mat, int n_mat, const float* dLdI, float* grad,
+                                  unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
+  const size_t shmem = size_t(n_mat) * kMatParams * sizeof(float);
+  const int use_shared = shmem <= 32 * 1024 ? 1 : 0;
+  const unsigned grid = unsigned((size_t(p.width) * size_t(p.height) + 255) / 256);
+  const size_t sm = use_shared ? shmem : 0;
+  if (p.restir_candidates > 1)
+    k_adjoint_restir<true><<<grid, 256, sm, st>>>(s, p, seed, gb, rm, tri_mat, n_mat, dLdI, grad, use_shared, ctr, err);
+  else
+    k_adjoint_restir<false><<<grid, 256, sm, st>>>(s, p, seed, gb, rm, tri_mat, n_mat, dLdI, grad, use_shared, ctr,
+                                                   err);
   return cudaGetLastError();
 }
 

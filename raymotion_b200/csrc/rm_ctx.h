@@ -127,6 +127,10 @@ struct rmcuda_ctx {
   uint64_t hist_seed = 0;
   unsigned long long hist_hash = 0;
   bool hist_valid = false, have_hist_bufs = false;
+  // the frame the history buffers hold (the ReSTIR adjoint's checkpoint)
+  const void* hist_scene = nullptr;
+  rm_config hist_cfg{};
+  bool hist_denoised = false;
   // last frame
   int last_chain = 0;
   uint64_t frames = 0;

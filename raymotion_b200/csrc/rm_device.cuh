@@ -101,7 +101,8 @@ struct GBufSoA {
   float4* wo_ior;
   float4* emi;
 };
-// SoA reservoir: lightPos|alpha, lightNormal|p_hat, emission|sumWs, (sumWu, M, valid, 0).
+// SoA reservoir: lightPos|alpha, lightNormal|p_hat, emission|sumWs, (sumWu, M, valid,
+// the selected light index as int bits; 0 for no sample).
 struct ResSoA {
   float4* lp_alpha;
   float4* ln_phat;

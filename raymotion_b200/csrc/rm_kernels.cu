@@ -180,12 +180,14 @@ __global__ void __launch_bounds__(256) k_restir_generate(Scene s, Params p, uint
         float sumWs = 0, sumWu = 0, sel_lx = 0, sel_ly = 0, sel_lz = 0, sel_nx = 0, sel_ny = 0, sel_nz = 0;
         float sel_er = 0, sel_eg = 0, sel_eb = 0, sel_alpha = 1, sel_ph = 0;
         bool have = false;
+        int sel_li = 0;  // light index of the selected sample (kept in the reservoir's free word)
         const float sox = px + pnx * 0.002f, soy = py + pny * 0.002f, soz = pz + pnz * 0.002f;
         const Tracer::BsdfPrep bp =
             Tracer::prep_bsdf(wox, woy, woz, pnx, pny, pnz, alpha2, metallic, hit.ar, hit.ag, hit.ab);
         for (int j = 0; j < Mc; ++j) {
           float pick = pt.U() * p.light_total;
-          const LightRec t = load_light(s, pt.pick_light(pick));
+          const int li = pt.pick_light(pick);
+          const LightRec t = load_light(s, li);
           float lu = pt.U(), lv = pt.U();
           if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
           float lw = 1.0f - lu - lv;
@@ -223,13 +225,14 @@ __global__ void __launch_bounds__(256) k_restir_generate(Scene s, Params p, uint
             sel_lx = qx; sel_ly = qy; sel_lz = qz;
             sel_nx = t.nn.x; sel_ny = t.nn.y; sel_nz = t.nn.z;
             sel_er = t.er; sel_eg = t.eg; sel_eb = t.eb; sel_alpha = t.alpha; sel_ph = ph;
+            sel_li = li;
           }
         }
         if (have && sumWs > 0.0f && sumWu > 0.0f && sel_ph > 0.0f) {
           ri.lp_alpha[id] = make_float4(sel_lx, sel_ly, sel_lz, sel_alpha);
           ri.ln_phat[id] = make_float4(sel_nx, sel_ny, sel_nz, sel_ph);
           ri.le_sumws[id] = make_float4(sel_er, sel_eg, sel_eb, sumWs);
-          ri.sumwu_m_valid[id] = make_float4(sumWu, __int_as_float(Mc), __int_as_float(1), 0.f);
+          ri.sumwu_m_valid[id] = make_float4(sumWu, __int_as_float(Mc), __int_as_float(1), __int_as_float(sel_li));
         }
       }
     }
@@ -283,6 +286,7 @@ __global__ void __launch_bounds__(256) k_restir_spatial(Scene s, Params p, uint6
       float cur_sumWs = R2.w, cur_sumWu = R3.x;
       uint32_t cur_M = uint32_t(__float_as_int(R3.y));
       float4 cur0 = R0, cur1 = R1, cur2 = R2;  // lp|alpha, ln|p_hat, le|(sumWs)
+      float cur_li = R3.w;                     // the sample's light index (bits)
       const float sox = cpx + cnx * 0.002f, soy = cpy + cny * 0.002f, soz = cpz + cnz * 0.002f;
       // target p_hat of a light sample at this pixel; false if it fails a test
       auto eval_at = [&](const float4& lpa, const float4& ln, const float4& le, float& ph, float& dist, float& dxn,
@@ -325,7 +329,9 @@ __global__ void __launch_bounds__(256) k_restir_spatial(Scene s, Params p, uint6
               float sum_s = cur_sumWs + ws, sum_u = cur_sumWu + wu;
               uint32_t newM = cur_M + hM; if (newM > uint32_t(mcap)) newM = uint32_t(mcap);
               float r = pt.U();
-              if (sum_s > 0.0f && r * sum_s < ws) { cur0 = H0; cur1 = make_float4(H1.x, H1.y, H1.z, ph); cur2 = H2; }
+              if (sum_s > 0.0f && r * sum_s < ws) {
+                cur0 = H0; cur1 = make_float4(H1.x, H1.y, H1.z, ph); cur2 = H2; cur_li = H3.w;
+              }
               cur_sumWs = sum_s; cur_sumWu = sum_u; cur_M = newM;
             }
           }
@@ -358,13 +364,15 @@ __global__ void __launch_bounds__(256) k_restir_spatial(Scene s, Params p, uint6
         if (!(sum_u > 0.0f) || !(sum_s >= 0.0f)) continue;
         float r = pt.U();
         uint32_t newM = cur_M + nbr_M; if (newM > uint32_t(mcap)) newM = uint32_t(mcap);
-        if (sum_s > 0.0f && r * sum_s < w_nbr_s) { cur0 = N0; cur1 = make_float4(N1.x, N1.y, N1.z, ph_cur); cur2 = N2; }
+        if (sum_s > 0.0f && r * sum_s < w_nbr_s) {
+          cur0 = N0; cur1 = make_float4(N1.x, N1.y, N1.z, ph_cur); cur2 = N2; cur_li = N3.w;
+        }
         cur_sumWs = sum_s; cur_sumWu = sum_u; cur_M = newM;
       }
       ro.lp_alpha[id] = cur0;
       ro.ln_phat[id] = cur1;
       ro.le_sumws[id] = make_float4(cur2.x, cur2.y, cur2.z, cur_sumWs);
-      ro.sumwu_m_valid[id] = make_float4(cur_sumWu, __int_as_float(int(cur_M)), __int_as_float(1), 0.f);
+      ro.sumwu_m_valid[id] = make_float4(cur_sumWu, __int_as_float(int(cur_M)), __int_as_float(1), cur_li);
       rays = pt.rays; nodes = pt.nodes; tests = pt.tests;
     }
   }

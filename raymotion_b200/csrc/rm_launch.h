@@ -146,6 +146,11 @@ void batch_occupancy(int& aux, int& trace, int& shade);
 cudaError_t launch_adjoint(int lanes, const Scene& s, const Params& p, uint64_t seed, const int32_t* tri_mat,
                            int n_mat, const float* dLdI, float* grad, unsigned long long* ctr, uint32_t* err,
                            cudaStream_t st);
+// The adjoint of the ReSTIR shade from the frame's G-buffer and merged
+// reservoirs (one thread per pixel).
+cudaError_t launch_adjoint_restir(const Scene& s, const Params& p, uint64_t seed, const GBufSoA& gb, const ResSoA& rm,
+                                  const int32_t* tri_mat, int n_mat, const float* dLdI, float* grad,
+                                  unsigned long long* ctr, uint32_t* err, cudaStream_t st);
 // Write per-material parameters (8 floats each) into the triangles with tri_mat >= 0.
 cudaError_t apply_materials(rm_triangle* tris, const int32_t* tri_mat, const float* mats, int n_tris,
                             cudaStream_t st);

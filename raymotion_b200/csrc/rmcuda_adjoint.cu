@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <string>
 
 #include "rm_ctx.h"
@@ -82,8 +83,33 @@ int rmcuda_backward(rmcuda_ctx* c, const rmcuda_scene* scene, const rm_camera* c
   if (sc.n_materials <= 0) { set_err(err, errcap, "scene has no materials (rmcuda_scene_set_materials)"); return RM_ERR_INVALID; }
   Plan pl = make_plan(sc, *cam, *cfg);
   if (pl.use_spatial) {
-    set_err(err, errcap, "the adjoint covers the plain chain; the policy picks ReSTIR (set RM_FLAG_RESTIR_OFF)");
-    return RM_ERR_INVALID;
+    // the ReSTIR chain: K5 replayed from the checkpoint the frame left in the
+    // history slots (its G-buffer and merged reservoirs)
+    if (pl.denoise) {
+      set_err(err, errcap, "the adjoint of the ReSTIR chain needs the denoiser off (RM_FLAG_DENOISE_OFF)");
+      return RM_ERR_INVALID;
+    }
+    if (pl.p.bounces - 1 > 24) {
+      set_err(err, errcap, "the adjoint of the ReSTIR chain takes at most 25 bounces");
+      return RM_ERR_INVALID;
+    }
+    if (!c->hist_valid || !c->have_hist_bufs || c->hist_scene != static_cast<const void*>(&sc) ||
+        c->hist_seed != seed || c->hist_denoised || std::memcmp(&c->hist_cam, cam, sizeof(rm_camera)) != 0 ||
+        std::memcmp(&c->hist_cfg, cfg, sizeof(rm_config)) != 0) {
+      set_err(err, errcap,
+              "the adjoint of the ReSTIR chain replays the last frame rendered on this context: render it first "
+              "with the same scene, camera, config and seed");
+      return RM_ERR_INVALID;
+    }
+    pl.p.hasHistory = 0;
+    cudaError_t e = staged(c, RM_STAGE_ADJOINT, [&] {
+      return launch_adjoint_restir(scene_view(sc), pl.p, seed, c->hg.view(), c->hres.view(), sc.tri_mat.as<int32_t>(),
+                                   sc.n_materials, d_dL_dimage, d_grad,
+                                   c->ctr.as<unsigned long long>() + 4 * RM_STAGE_ADJOINT, c->err.as<uint32_t>(),
+                                   c->stream);
+    });
+    if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("adjoint launch failed", e)); return RM_ERR_CUDA; }
+    return RM_OK;
   }
   if (pl.p.adapt_min > 0) {
     set_err(err, errcap, "the adjoint needs a fixed sample count (adapt_min 0 or RM_FLAG_NOADAPT)");

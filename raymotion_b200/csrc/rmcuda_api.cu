@@ -555,6 +555,7 @@ int enqueue_frame(rmcuda_ctx* c, DevScene& sc, const rm_camera& cam, const rm_co
     c->hist_w = cfg.width; c->hist_h = cfg.height;
     c->hist_seed = seed; c->hist_hash = h;
     c->hist_valid = true;
+    c->hist_scene = &sc; c->hist_cfg = cfg; c->hist_denoised = pl.denoise;
   }
   c->last_w = cfg.width;
   c->last_h = cfg.height;

@@ -282,3 +282,60 @@ def test_gradients_converge_to_a_high_spp_reference_gradient(backend, oracle):
         assert r["rms"][1024] < top, report
         assert r["mean4"] < 3.0 * r["rms"][64], report
     assert report["ior"]["median"][1024] < 0.5 * report["ior"]["median"][4], report
+
+
+def test_restir_frame_adjoint_matches_fp64_central_differences(backend, oracle):
+    """The ReSTIR chain (K3 4 candidates with visibility, K4 2 neighbours, K5;
+    first frame, denoiser off): the adjoint replays K5 from the checkpoint the
+    frame left (its G-buffer and merged reservoirs); the oracle runs K3/K4 in
+    fp32 and evaluates K5 frozen in double.  Same acceptance as the plain
+    frame's check."""
+    torch = _torch()
+    d = _scene(oracle, 4)
+    c = d["config"]
+    cfg = type(c)(**{**c.__dict__, "restir_candidates": 4, "restir_spatial": 2, "restir_radius": 6.0,
+                     "flags": (c.flags & ~_abi.RM_FLAG_RESTIR_OFF) | _abi.RM_FLAG_DENOISE_OFF})
+    d["config"] = cfg
+    seed = 515
+    sc, cam, tm = d["scene"], d["camera"], d["tri_material"]
+    prm = d["params"].astype(np.float64)
+    h = backend.scene_create(sc)
+    try:
+        _set(backend, h, d, d["params"])
+        backend.reset_history()
+        img = _render(backend, h, d, seed)  # the frame whose G-buffer and reservoirs are the checkpoint
+        assert backend.stats()["kernel_chain"] == 2
+        T = (img.cpu().numpy() * np.float32(0.75) + np.float32(0.01)).reshape(-1, 3).astype(np.float64)
+        i64 = oracle.render_frozen_restir(sc, cam, cfg, seed, tm, prm)
+        assert np.allclose(i64, img.cpu().numpy().reshape(-1, 3), rtol=1e-3, atol=1e-5)
+        dl = torch.from_numpy(((2.0 / i64.size) * (i64 - T)).astype(np.float32).ravel()).cuda()
+        g = _grad(backend, h, d, seed, dl)
+        # the checkpoint must be this frame's
+        with pytest.raises(RenderError, match="replays the last frame"):
+            _grad(backend, h, d, seed + 1, dl)
+    finally:
+        backend.scene_destroy(h)
+
+    def loss(q):
+        return np.mean((oracle.render_frozen_restir(sc, cam, cfg, seed, tm, q) - T) ** 2)
+
+    rng = np.random.default_rng(1)
+    checks = []
+    for col in range(8):
+        cand = np.nonzero(d["mask"][:, col])[0]
+        top = cand[np.argsort(-np.abs(g[cand, col]))][:3]
+        extra = rng.choice(cand, 1)
+        for m in sorted(set(top.tolist()) | set(extra.tolist())):
+            checks.append((m, col, central_difference(loss, prm, m, col), float(g[m, col])))
+    significant = 0
+    for col in range(8):
+        rows = [ch for ch in checks if ch[1] == col]
+        big = max(abs(ch[2]) for ch in rows)
+        assert big > 0, f"param {col}: no gradient"
+        for (m, _, f, a) in rows:
+            if abs(f) >= 1e-2 * big:
+                significant += 1
+                assert abs(a - f) <= 1e-3 * abs(f), f"material {m} param {col}: adjoint {a} vs FD {f}"
+            else:
+                assert abs(a - f) <= 1e-5 * big, f"material {m} param {col}: adjoint {a} vs FD {f}"
+    assert significant >= 12

@@ -224,3 +224,30 @@ def test_reupload_checks_textures_against_the_new_texel_array(backend, small_fie
     b = backend.render(scene(4), cam, cfg, 3, use_nodes=False)
     assert np.array_equal(a, b)
     assert backend.stats()["bvh_kept"] >= kept + 1
+
+
+def test_failed_call_drops_temporal_history(backend, small_field):
+    """The reference's CacheGuard (metal.mm:105-108): a call that fails
+    invalidates the temporal history, so the next ReSTIR frame renders as a
+    first frame.  The failure is made on the host (a light index out of
+    range), after which the scene is uploaded again unchanged."""
+    sc, cam, _ = small_field
+    cfg = _restir_cfg(_abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_DENOISE_OFF)
+    bad = type(sc)(tris=sc.tris, light_tri=np.full_like(sc.light_tri, len(sc.tris) + 5), light_cdf=sc.light_cdf,
+                   light_total=sc.light_total, texels=sc.texels, verts64=sc.verts64)
+
+    def frames(fail_between):
+        backend.reset_history()
+        backend.render(sc, cam, cfg, 41, use_nodes=False)
+        if fail_between:
+            with pytest.raises(RenderError, match="light index out of range"):
+                backend.render(bad, cam, cfg, 42, use_nodes=False)
+        _, hdr = backend.render(sc, cam, cfg, 43, hdr=True, use_nodes=False)
+        return hdr
+
+    with_history = frames(False)
+    after_failure = frames(True)
+    backend.reset_history()
+    _, first = backend.render(sc, cam, cfg, 43, hdr=True, use_nodes=False)
+    assert np.array_equal(after_failure.view(np.uint32), first.view(np.uint32))
+    assert not np.array_equal(with_history.view(np.uint32), first.view(np.uint32))

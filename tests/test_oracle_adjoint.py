@@ -88,3 +88,37 @@ def test_with_materials_matches_builder_light_table(small):
     assert again.light_total == d["scene"].light_total
     for name in ("ar", "rough", "er", "ior"):
         assert np.array_equal(again.tris[name], d["scene"].tris[name])
+
+
+def restir_config(cfg, spp=4):
+    """The ReSTIR chain (first frame, denoiser off) on the same scene."""
+    return type(cfg)(**{**cfg.__dict__, "spp": spp, "restir_candidates": 4, "restir_spatial": 2,
+                        "restir_radius": 6.0,
+                        "flags": (cfg.flags & ~_abi.RM_FLAG_RESTIR_OFF) | _abi.RM_FLAG_DENOISE_OFF})
+
+
+def test_frozen_restir_frame_at_scene_parameters_is_the_fp32_frame(oracle, small):
+    sc, cam = small["scene"], small["camera"]
+    cfg = restir_config(small["config"])
+    o = oracle.Oracle()
+    _, hdr, st = o.render(sc, cam, cfg, 77)
+    assert st["chain"] == 2
+    fro = oracle.render_frozen_restir(sc, cam, cfg, 77, small["tri_material"], small["params"].astype(np.float64))
+    hdr = hdr.reshape(-1, 3).astype(np.float64)
+    assert hdr.max() > 0.05
+    rel = np.abs(fro - hdr) / (np.abs(hdr) + 1e-7)
+    assert np.median(rel) < 1e-6
+    assert rel.max() < 5e-4
+
+
+def test_frozen_restir_frame_is_linear_in_emission(oracle, small):
+    sc, cam = small["scene"], small["camera"]
+    cfg = restir_config(small["config"])
+    cfg.clamp = 0.0
+    prm = small["params"].astype(np.float64)
+    a = oracle.render_frozen_restir(sc, cam, cfg, 5, small["tri_material"], prm)
+    prm2 = prm.copy()
+    prm2[:, 4:7] *= 2.0
+    b = oracle.render_frozen_restir(sc, cam, cfg, 5, small["tri_material"], prm2)
+    assert np.allclose(b, 2.0 * a, rtol=1e-12, atol=1e-15)
+    assert np.abs(a).max() > 0
