@@ -1744,8 +1744,58 @@ int orc_render_frozen(const rm_scene_view* sv, const rm_camera* cam, const rm_co
   return RM_OK;
 }
 
-// Frozen evaluation of a ReSTIR frame (K3, K4, K5; the first frame of a
-// history, denoiser not applied): K3 and K4 run in fp32 at the scene's own
+// K7 (pathtrace.metal:1315-1354) in double on a held G-buffer: the denoiser of
+// the frozen frame, the colour it filters in double (the first frame's K6 is
+// the identity).
+static void atrous64(const Params& p, const GBuf* gb, const double* in, double* out, int step, int nthreads) {
+  const int W = p.width, H = p.height;
+  const int stride = 1 << step;
+  auto lum = [](const double* c) { return 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2]; };
+  parallel_for(H, nthreads, [&](int yi) {
+    for (int x = 0; x < W; ++x) {
+      const size_t id = size_t(yi) * size_t(W) + size_t(x);
+      const GBuf& g0 = gb[id];
+      double* o = out + id * 3;
+      if (g0.kind == 0) { o[0] = o[1] = o[2] = 0; continue; }
+      const double* c0 = in + id * 3;
+      const double l0 = lum(c0);
+      const double dcx = double(g0.pos.x) - p.camera.x, dcy = double(g0.pos.y) - p.camera.y,
+                   dcz = double(g0.pos.z) - p.camera.z;
+      const double dc = std::sqrt(dcx * dcx + dcy * dcy + dcz * dcz);
+      double sum[3] = {0, 0, 0}, wsum = 0;
+      for (int dy = -2; dy <= 2; ++dy)
+        for (int dx = -2; dx <= 2; ++dx) {
+          const int nx = x + dx * stride, ny = yi + dy * stride;
+          if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;
+          const size_t n = size_t(ny) * size_t(W) + size_t(nx);
+          const GBuf& g = gb[n];
+          if (g.kind == 0) continue;
+          const double* c = in + n * 3;
+          double nd = double(g.normal.x) * g0.normal.x + double(g.normal.y) * g0.normal.y +
+                      double(g.normal.z) * g0.normal.z;
+          double wn = std::max(nd, 0.0);
+          wn *= wn; wn *= wn; wn *= wn; wn *= wn;
+          const double ex = double(g.pos.x) - g0.pos.x, ey = double(g.pos.y) - g0.pos.y,
+                       ez = double(g.pos.z) - g0.pos.z;
+          const double wz = std::exp(-std::sqrt(ex * ex + ey * ey + ez * ez) / (0.1 * dc + 1e-4));
+          const double wl = std::exp(-std::fabs(lum(c) - l0) / (0.3 * std::max(l0, 0.5) + 1e-3));
+          const double ax = double(g.albedo.x) - g0.albedo.x, ay = double(g.albedo.y) - g0.albedo.y,
+                       az = double(g.albedo.z) - g0.albedo.z;
+          const double wa = std::exp(-std::sqrt(ax * ax + ay * ay + az * az) / 0.25);
+          const double w = wn * wz * wl * wa;
+          for (int k = 0; k < 3; ++k) sum[k] += w * c[k];
+          wsum += w;
+        }
+      if (wsum > 1e-12)
+        for (int k = 0; k < 3; ++k) o[k] = sum[k] / wsum;
+      else
+        for (int k = 0; k < 3; ++k) o[k] = c0[k];
+    }
+  });
+}
+
+// Frozen evaluation of a ReSTIR frame (K3, K4, K5 and the denoiser; the first
+// frame of a history): K3 and K4 run in fp32 at the scene's own
 // materials and their G-buffer and merged reservoirs are held (the adjoint's
 // checkpoint), with each reservoir's light triangle; K5 is replayed from them
 // with its decisions from the fp32 path and the material factors in double at
@@ -1753,7 +1803,9 @@ int orc_render_frozen(const rm_scene_view* sv, const rm_camera* cam, const rm_co
 // base is the first hit's emission plus the held light sample's Le f cos
 // alpha W w_MIS, and each indirect sample leaves the first hit with the BSDF
 // sample f cos / pdf and goes on as a frozen path (pathtrace.metal:1056-1258).
-// The first hit's triangle comes from K3's primary ray traced again.
+// The first hit's triangle comes from K3's primary ray traced again.  Unless
+// the frame's denoiser is off, the two a-trous passes then run in double on
+// the held G-buffer (K6 is the identity on a first frame).
 int orc_render_frozen_restir(const rm_scene_view* sv, const rm_camera* cam, const rm_config* cfg, uint64_t seed,
                              const int32_t* tri_material, const double* prm, int n_materials, double* out,
                              int nthreads) {
@@ -1938,6 +1990,13 @@ int orc_render_frozen_restir(const rm_scene_view* sv, const rm_camera* cam, cons
       for (int k = 0; k < 3; ++k) o[k] = sum[k] / double(p.spp);
     }
   });
+  if (!env.denoise_off) {
+    // the frame's denoiser on the frozen HDR: K6 is the identity on a first
+    // frame, then the two a-trous passes in double on the held G-buffer
+    std::vector<double> tmp(pixels * 3);
+    atrous64(p, g.data(), out, tmp.data(), 0, nthreads);
+    atrous64(p, g.data(), tmp.data(), out, 1, nthreads);
+  }
   return RM_OK;
 }
 

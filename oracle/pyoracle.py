@@ -250,9 +250,10 @@ def render_frozen(scene: PackedScene, cam: Camera, cfg: RenderConfig, seed: int,
 
 def render_frozen_restir(scene: PackedScene, cam: Camera, cfg: RenderConfig, seed: int, tri_material: np.ndarray,
                          params: np.ndarray, threads: int | None = None) -> np.ndarray:
-    """The ReSTIR frame (first of a history, no denoiser) with K3/K4 run at the
-    scene's own materials and held, and K5 replayed frozen with the material
-    factors in double at ``params``; W*H x 3."""
+    """The ReSTIR frame (first of a history) with K3/K4 run at the scene's own
+    materials and held, K5 replayed frozen with the material factors in double
+    at ``params``, and the denoiser (unless the config turns it off) in double
+    on the held G-buffer; W*H x 3."""
     tm = np.ascontiguousarray(tri_material, np.int32)
     prm = np.ascontiguousarray(params, np.float64)
     assert len(tm) == scene.n_tris and prm.ndim == 2 and prm.shape[1] == 8

@@ -131,6 +131,9 @@ struct rmcuda_ctx {
   const void* hist_scene = nullptr;
   rm_config hist_cfg{};
   bool hist_denoised = false;
+  bool hist_had_history = false;  // the frame's temporal passes used the history before it
+  rm_camera hist_prev_cam{};       // and this camera for reprojection
+  rmd::DevBuf adj_scratch;         // the denoiser backward's intermediate images
   // last frame
   int last_chain = 0;
   uint64_t frames = 0;

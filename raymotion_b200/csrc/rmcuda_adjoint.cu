@@ -85,26 +85,46 @@ int rmcuda_backward(rmcuda_ctx* c, const rmcuda_scene* scene, const rm_camera* c
   if (pl.use_spatial) {
     // the ReSTIR chain: K5 replayed from the checkpoint the frame left in the
     // history slots (its G-buffer and merged reservoirs)
-    if (pl.denoise) {
-      set_err(err, errcap, "the adjoint of the ReSTIR chain needs the denoiser off (RM_FLAG_DENOISE_OFF)");
-      return RM_ERR_INVALID;
-    }
     if (pl.p.bounces - 1 > 24) {
       set_err(err, errcap, "the adjoint of the ReSTIR chain takes at most 25 bounces");
       return RM_ERR_INVALID;
     }
     if (!c->hist_valid || !c->have_hist_bufs || c->hist_scene != static_cast<const void*>(&sc) ||
-        c->hist_seed != seed || c->hist_denoised || std::memcmp(&c->hist_cam, cam, sizeof(rm_camera)) != 0 ||
+        c->hist_seed != seed || c->hist_denoised != pl.denoise ||
+        std::memcmp(&c->hist_cam, cam, sizeof(rm_camera)) != 0 ||
         std::memcmp(&c->hist_cfg, cfg, sizeof(rm_config)) != 0) {
       set_err(err, errcap,
               "the adjoint of the ReSTIR chain replays the last frame rendered on this context: render it first "
               "with the same scene, camera, config and seed");
       return RM_ERR_INVALID;
     }
+    const float* dl_hdr = d_dL_dimage;
+    cudaError_t e = cudaSuccess;
+    if (pl.denoise) {
+      // through the denoiser first: its inputs are the frame's shaded HDR, its
+      // G-buffer and the history it blended (the previous final colour and
+      // G-buffer, in the slots the frame's swap left them in)
+      const size_t npix = size_t(cfg->width) * size_t(cfg->height);
+      if ((e = c->adj_scratch.reserve(npix * 17 * sizeof(float))) != cudaSuccess) {
+        set_err(err, errcap, cuda_msg("adjoint buffer allocation failed", e));
+        return RM_ERR_ALLOC;
+      }
+      Params dp = pl.p;
+      dp.hasHistory = c->hist_had_history ? 1 : 0;
+      dp.prevCamera = c->hist_prev_cam;
+      float* scratch = c->adj_scratch.as<float>();
+      float* g_hdr = scratch + npix * 14;
+      e = staged(c, RM_STAGE_ADJOINT, [&] {
+        return launch_denoise_backward(dp, c->hg.view(), c->gb.view(), c->hdr.as<float>(), c->tmp_a.as<float>(),
+                                       d_dL_dimage, scratch, g_hdr, c->stream);
+      });
+      if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("denoiser adjoint launch failed", e)); return RM_ERR_CUDA; }
+      dl_hdr = g_hdr;
+    }
     pl.p.hasHistory = 0;
-    cudaError_t e = staged(c, RM_STAGE_ADJOINT, [&] {
+    e = staged(c, RM_STAGE_ADJOINT, [&] {
       return launch_adjoint_restir(scene_view(sc), pl.p, seed, c->hg.view(), c->hres.view(), sc.tri_mat.as<int32_t>(),
-                                   sc.n_materials, d_dL_dimage, d_grad,
+                                   sc.n_materials, dl_hdr, d_grad,
                                    c->ctr.as<unsigned long long>() + 4 * RM_STAGE_ADJOINT, c->err.as<uint32_t>(),
                                    c->stream);
     });

@@ -556,6 +556,7 @@ int enqueue_frame(rmcuda_ctx* c, DevScene& sc, const rm_camera& cam, const rm_co
     c->hist_seed = seed; c->hist_hash = h;
     c->hist_valid = true;
     c->hist_scene = &sc; c->hist_cfg = cfg; c->hist_denoised = pl.denoise;
+    c->hist_had_history = p.hasHistory != 0; c->hist_prev_cam = p.prevCamera;
   }
   c->last_w = cfg.width;
   c->last_h = cfg.height;
@@ -620,7 +621,8 @@ void rmcuda_destroy(rmcuda_ctx* c) {
   cudaStreamSynchronize(c->stream);
   c->sc.release();
   c->batch.release();
-  for (DevBuf* b : {&c->hdr, &c->tmp_a, &c->tmp_b, &c->hist_col, &c->rgb, &c->dbg, &c->hash_out, &c->ctr, &c->err})
+  for (DevBuf* b : {&c->hdr, &c->tmp_a, &c->tmp_b, &c->hist_col, &c->rgb, &c->dbg, &c->hash_out, &c->ctr, &c->err,
+                    &c->adj_scratch})
     b->release();
   for (DevBuf& b : c->wf) b.release();
   for (DevBuf& b : c->wq) b.release();

@@ -90,16 +90,17 @@ def test_with_materials_matches_builder_light_table(small):
         assert np.array_equal(again.tris[name], d["scene"].tris[name])
 
 
-def restir_config(cfg, spp=4):
-    """The ReSTIR chain (first frame, denoiser off) on the same scene."""
+def restir_config(cfg, spp=4, denoise=False):
+    """The ReSTIR chain (first frame) on the same scene."""
+    flags = cfg.flags & ~_abi.RM_FLAG_RESTIR_OFF & ~_abi.RM_FLAG_DENOISE_OFF
     return type(cfg)(**{**cfg.__dict__, "spp": spp, "restir_candidates": 4, "restir_spatial": 2,
-                        "restir_radius": 6.0,
-                        "flags": (cfg.flags & ~_abi.RM_FLAG_RESTIR_OFF) | _abi.RM_FLAG_DENOISE_OFF})
+                        "restir_radius": 6.0, "flags": flags | (0 if denoise else _abi.RM_FLAG_DENOISE_OFF)})
 
 
-def test_frozen_restir_frame_at_scene_parameters_is_the_fp32_frame(oracle, small):
+@pytest.mark.parametrize("denoise", [False, True], ids=["raw", "denoised"])
+def test_frozen_restir_frame_at_scene_parameters_is_the_fp32_frame(oracle, small, denoise):
     sc, cam = small["scene"], small["camera"]
-    cfg = restir_config(small["config"])
+    cfg = restir_config(small["config"], denoise=denoise)
     o = oracle.Oracle()
     _, hdr, st = o.render(sc, cam, cfg, 77)
     assert st["chain"] == 2
@@ -107,8 +108,14 @@ def test_frozen_restir_frame_at_scene_parameters_is_the_fp32_frame(oracle, small
     hdr = hdr.reshape(-1, 3).astype(np.float64)
     assert hdr.max() > 0.05
     rel = np.abs(fro - hdr) / (np.abs(hdr) + 1e-7)
-    assert np.median(rel) < 1e-6
-    assert rel.max() < 5e-4
+    if not denoise:
+        assert np.median(rel) < 1e-6
+        assert rel.max() < 5e-4
+    else:
+        # the a-trous weights in double against the fp32 pass: luma differences
+        # in the exponents carry fp32 rounding (as the CUDA filter's 1e-4)
+        assert np.median(rel) < 1e-5
+        assert np.quantile(rel, 0.999) < 5e-4 and rel.max() < 2e-3
 
 
 def test_frozen_restir_frame_is_linear_in_emission(oracle, small):
