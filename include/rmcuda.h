@@ -359,10 +359,12 @@ int rmcuda_scene_set_materials(rmcuda_ctx* ctx, rmcuda_scene* scene, const int32
  * differentiated; each sample is replayed from its random state instead of
  * being stored.  Needs a fixed sample count (adapt_min 0 or RM_FLAG_NOADAPT).
  * The plain chain (single-candidate or RIS NEE) is replayed from the seed.  On
- * the ReSTIR chain the frame's G-buffer and merged reservoirs are the
- * checkpoint: call it after rendering that frame on this context (same
- * scene, camera, config and seed; the denoiser off), and the reservoirs'
- * light samples and weights are held.  Enqueued, not waited for. */
+ * the ReSTIR chain the frame's G-buffer, merged reservoirs and denoiser
+ * inputs are the checkpoint: call it after rendering that frame on this
+ * context (same scene, camera, config and seed); the reservoirs' light
+ * samples and weights and the denoiser's G-buffers and history are held, and
+ * d_dL_dimage is the gradient with respect to the frame's final (denoised when
+ * the denoiser is on) linear image.  Enqueued, not waited for. */
 int rmcuda_backward(rmcuda_ctx* ctx, const rmcuda_scene* scene, const rm_camera* cam, const rm_config* cfg,
                     uint64_t seed, const float* d_dL_dimage, float* d_grad, char* err, size_t errcap);
 
