@@ -1794,6 +1794,49 @@ static void atrous64(const Params& p, const GBuf* gb, const double* in, double* 
   });
 }
 
+// K6 (pathtrace.metal:1263-1314) in double on held G-buffers and a held
+// history colour: the blend of the frozen colour with the reprojected,
+// neighbourhood-clamped history.
+static void temporal64(const Params& p, const GBuf* gb, const GBuf* hg, const double* cur, const float* hc,
+                       double* out, int nthreads) {
+  const int W = p.width, H = p.height;
+  parallel_for(H, nthreads, [&](int yi) {
+    for (int x = 0; x < W; ++x) {
+      const size_t id = size_t(yi) * size_t(W) + size_t(x);
+      const double* c = cur + id * 3;
+      double* o = out + id * 3;
+      for (int k = 0; k < 3; ++k) o[k] = c[k];
+      if (p.hasHistory == 0 || gb[id].kind != 1) continue;
+      double mn[3] = {c[0], c[1], c[2]}, mx[3] = {c[0], c[1], c[2]};
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int nx = x + dx, ny = yi + dy;
+          if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;
+          const size_t n = size_t(ny) * size_t(W) + size_t(nx);
+          for (int k = 0; k < 3; ++k) {
+            mn[k] = std::min(mn[k], cur[n * 3 + size_t(k)]);
+            mx[k] = std::max(mx[k], cur[n * 3 + size_t(k)]);
+          }
+        }
+      const GBuf& g = gb[id];
+      const Reproj rp = reproject(p, g.pos.x, g.pos.y, g.pos.z);
+      if (!(rp.ok && hg[rp.hidx].kind == 1)) continue;
+      const GBuf& h = hg[rp.hidx];
+      float ddx = g.pos.x - h.pos.x, ddy = g.pos.y - h.pos.y, ddz = g.pos.z - h.pos.z;
+      float dd = std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+      float dcx = g.pos.x - p.camera.x, dcy = g.pos.y - p.camera.y, dcz = g.pos.z - p.camera.z;
+      float dc = std::sqrt(dcx * dcx + dcy * dcy + dcz * dcz);
+      if (!(dd < 0.02f * dc + 1e-3f &&
+            (g.normal.x * h.normal.x + (g.normal.y * h.normal.y + g.normal.z * h.normal.z)) > 0.9f))
+        continue;
+      for (int k = 0; k < 3; ++k) {
+        const double hv = std::min(std::max(double(hc[size_t(rp.hidx) * 3 + size_t(k)]), mn[k]), mx[k]);
+        o[k] = hv + (c[k] - hv) * 0.2;
+      }
+    }
+  });
+}
+
 // Frozen evaluation of a ReSTIR frame (K3, K4, K5 and the denoiser; the first
 // frame of a history): K3 and K4 run in fp32 at the scene's own
 // materials and their G-buffer and merged reservoirs are held (the adjoint's
@@ -1804,11 +1847,14 @@ static void atrous64(const Params& p, const GBuf* gb, const double* in, double* 
 // alpha W w_MIS, and each indirect sample leaves the first hit with the BSDF
 // sample f cos / pdf and goes on as a frozen path (pathtrace.metal:1056-1258).
 // The first hit's triangle comes from K3's primary ray traced again.  Unless
-// the frame's denoiser is off, the two a-trous passes then run in double on
-// the held G-buffer (K6 is the identity on a first frame).
+// the frame's denoiser is off, K6 and the two a-trous passes then run in
+// double on the held G-buffers and history colour.  With prev_cam, the frame
+// is the second of a history: the first (prev_cam, prev_seed) is rendered in
+// fp32 as the CUDA path renders it and supplies the history G-buffer,
+// reservoirs (with their light indices) and final colour.
 int orc_render_frozen_restir(const rm_scene_view* sv, const rm_camera* cam, const rm_config* cfg, uint64_t seed,
                              const int32_t* tri_material, const double* prm, int n_materials, double* out,
-                             int nthreads) {
+                             int nthreads, const rm_camera* prev_cam, uint64_t prev_seed) {
   using namespace orc;
   if (cfg->width <= 0 || cfg->height <= 0 || cfg->spp <= 0 || cfg->max_bounces < 0 || n_materials < 0)
     return RM_ERR_INVALID;
@@ -1830,11 +1876,36 @@ int orc_render_frozen_restir(const rm_scene_view* sv, const rm_camera* cam, cons
   p.hasHistory = 0;
   std::vector<GBuf> g(pixels), hg(pixels);
   std::vector<Reservoir> ri(pixels), rmg(pixels), hr(pixels);
-  std::vector<int32_t> ril(pixels, -1), rml(pixels, -1);
+  std::vector<int32_t> ril(pixels, -1), rml(pixels, -1), hrl(pixels, -1);
+  std::vector<float> hcol(pixels * 3, 0.0f);
   std::atomic<uint64_t> rays{0};
+  if (prev_cam) {
+    // the history frame, in fp32 as rendered (its light indices tracked): the
+    // held G-buffer, reservoirs and final colour the frame reuses
+    Params p1 = resolve(*cfg, *prev_cam, int(s.nodes.size()), sv->n_lights, sv->light_total, opaque, env);
+    p1.hasHistory = 0;
+    std::vector<GBuf> g0(pixels);
+    std::vector<Reservoir> r0(pixels), hr0(pixels);
+    std::vector<int32_t> l0(pixels, -1);
+    std::vector<float> h1(pixels * 3), t1(pixels * 3);
+    std::atomic<uint64_t> smp{0};
+    k_generate(s, p1, prev_seed, 0, H, hg.data(), r0.data(), nthreads, rays, l0.data());
+    k_spatial(s, p1, prev_seed, 0, H, hg.data(), r0.data(), hr.data(), g0.data(), hr0.data(), nthreads, rays,
+              l0.data(), hrl.data(), nullptr);
+    k_shade(s, p1, prev_seed, 0, H, hg.data(), hr.data(), h1.data(), nullptr, nthreads, smp, rays);
+    if (!env.denoise_off) {
+      k_temporal(p1, hg.data(), g0.data(), h1.data(), hcol.data(), t1.data(), nthreads);
+      k_atrous(p1, hg.data(), t1.data(), h1.data(), 0, nthreads);
+      k_atrous(p1, hg.data(), h1.data(), hcol.data(), 1, nthreads);
+    } else {
+      hcol = h1;
+    }
+    p.hasHistory = 1;
+    p.prevCamera = *prev_cam;
+  }
   k_generate(s, p, seed, 0, H, g.data(), ri.data(), nthreads, rays, ril.data());
   k_spatial(s, p, seed, 0, H, g.data(), ri.data(), rmg.data(), hg.data(), hr.data(), nthreads, rays, ril.data(),
-            rml.data(), nullptr);
+            rml.data(), hrl.data());
   MatTable mt;
   mt.tri_mat = tri_material;
   mt.prm = prm;
@@ -1991,10 +2062,12 @@ int orc_render_frozen_restir(const rm_scene_view* sv, const rm_camera* cam, cons
     }
   });
   if (!env.denoise_off) {
-    // the frame's denoiser on the frozen HDR: K6 is the identity on a first
-    // frame, then the two a-trous passes in double on the held G-buffer
+    // the frame's denoiser on the frozen HDR, in double on the held G-buffers
+    // and history colour
     std::vector<double> tmp(pixels * 3);
-    atrous64(p, g.data(), out, tmp.data(), 0, nthreads);
+    temporal64(p, g.data(), hg.data(), out, hcol.data(), tmp.data(), nthreads);
+    atrous64(p, g.data(), tmp.data(), out, 0, nthreads);
+    for (size_t i = 0; i < pixels * 3; ++i) tmp[i] = out[i];
     atrous64(p, g.data(), tmp.data(), out, 1, nthreads);
   }
   return RM_OK;

@@ -80,7 +80,7 @@ def oracle_lib() -> C.CDLL:
         lib.orc_render_frozen_restir.restype = C.c_int
         lib.orc_render_frozen_restir.argtypes = [C.POINTER(_abi.RmSceneView), C.POINTER(_abi.RmCamera),
                                                  C.POINTER(_abi.RmConfig), C.c_uint64, _P, _P, C.c_int, _P,
-                                                 C.c_int]
+                                                 C.c_int, C.POINTER(_abi.RmCamera), C.c_uint64]
         lib.orc_build_bvh.restype = C.c_int
         lib.orc_build_bvh.argtypes = [_P, C.c_int, C.c_int, _P, _P, _P]
         lib.orc_refit_bvh.argtypes = [_P, C.c_int, _P, _P, _P]
@@ -249,19 +249,23 @@ def render_frozen(scene: PackedScene, cam: Camera, cfg: RenderConfig, seed: int,
 
 
 def render_frozen_restir(scene: PackedScene, cam: Camera, cfg: RenderConfig, seed: int, tri_material: np.ndarray,
-                         params: np.ndarray, threads: int | None = None) -> np.ndarray:
-    """The ReSTIR frame (first of a history) with K3/K4 run at the scene's own
-    materials and held, K5 replayed frozen with the material factors in double
-    at ``params``, and the denoiser (unless the config turns it off) in double
-    on the held G-buffer; W*H x 3."""
+                         params: np.ndarray, threads: int | None = None, prev: tuple[Camera, int] | None = None
+                         ) -> np.ndarray:
+    """The ReSTIR frame with K3/K4 run at the scene's own materials and held,
+    K5 replayed frozen with the material factors in double at ``params``, and
+    the denoiser (unless the config turns it off) in double on the held
+    G-buffers; W*H x 3.  ``prev`` = (camera, seed) of the frame before it (its
+    history, rendered in fp32), else the first frame of a history."""
     tm = np.ascontiguousarray(tri_material, np.int32)
     prm = np.ascontiguousarray(params, np.float64)
     assert len(tm) == scene.n_tris and prm.ndim == 2 and prm.shape[1] == 8
     out = np.zeros((cfg.width * cfg.height, 3), np.float64)
     sv = scene.view(True)
+    pcam = C.byref(prev[0].packed()) if prev else None
     rc = oracle_lib().orc_render_frozen_restir(C.byref(sv), C.byref(cam.packed()), C.byref(cfg.packed()),
                                                C.c_uint64(seed), tm.ctypes.data, prm.ctypes.data, len(prm),
-                                               out.ctypes.data, threads or nthreads())
+                                               out.ctypes.data, threads or nthreads(), pcam,
+                                               C.c_uint64(prev[1] if prev else 0))
     if rc != 0:
         raise ValueError("frozen ReSTIR evaluation needs a configuration the policy renders with ReSTIR")
     return out

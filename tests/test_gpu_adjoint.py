@@ -284,13 +284,16 @@ def test_gradients_converge_to_a_high_spp_reference_gradient(backend, oracle):
     assert report["ior"]["median"][1024] < 0.5 * report["ior"]["median"][4], report
 
 
-@pytest.mark.parametrize("denoise", [False, True], ids=["raw", "denoised"])
-def test_restir_frame_adjoint_matches_fp64_central_differences(backend, oracle, denoise):
+@pytest.mark.parametrize("denoise,second", [(False, False), (True, False), (True, True)],
+                         ids=["raw", "denoised", "denoised_with_history"])
+def test_restir_frame_adjoint_matches_fp64_central_differences(backend, oracle, denoise, second):
     """The ReSTIR chain (K3 4 candidates with visibility, K4 2 neighbours, K5,
     and the denoiser when on; first frame): the adjoint takes the loss
     gradient back through the denoiser (G-buffer held) and replays K5 from the
     checkpoint the frame left (its G-buffer and merged reservoirs); the oracle
     runs K3/K4 in fp32 and evaluates K5 frozen and the denoiser in double.
+    with_history: the frame is the second of a history (temporal reservoir
+    reuse and the temporal blend; the oracle renders the first in fp32).
     Same acceptance as the plain frame's check."""
     torch = _torch()
     d = _scene(oracle, 4)
@@ -306,10 +309,14 @@ def test_restir_frame_adjoint_matches_fp64_central_differences(backend, oracle, 
     try:
         _set(backend, h, d, d["params"])
         backend.reset_history()
+        prev = None
+        if second:
+            _render(backend, h, d, seed - 7)
+            prev = (cam, seed - 7)
         img = _render(backend, h, d, seed)  # the frame whose G-buffer and reservoirs are the checkpoint
         assert backend.stats()["kernel_chain"] == 2
         T = (img.cpu().numpy() * np.float32(0.75) + np.float32(0.01)).reshape(-1, 3).astype(np.float64)
-        i64 = oracle.render_frozen_restir(sc, cam, cfg, seed, tm, prm)
+        i64 = oracle.render_frozen_restir(sc, cam, cfg, seed, tm, prm, prev=prev)
         assert np.allclose(i64, img.cpu().numpy().reshape(-1, 3), rtol=2e-3, atol=1e-5)
         dl = torch.from_numpy(((2.0 / i64.size) * (i64 - T)).astype(np.float32).ravel()).cuda()
         g = _grad(backend, h, d, seed, dl)
@@ -320,7 +327,7 @@ def test_restir_frame_adjoint_matches_fp64_central_differences(backend, oracle, 
         backend.scene_destroy(h)
 
     def loss(q):
-        return np.mean((oracle.render_frozen_restir(sc, cam, cfg, seed, tm, q) - T) ** 2)
+        return np.mean((oracle.render_frozen_restir(sc, cam, cfg, seed, tm, q, prev=prev) - T) ** 2)
 
     rng = np.random.default_rng(1)
     checks = []

@@ -129,3 +129,23 @@ def test_frozen_restir_frame_is_linear_in_emission(oracle, small):
     b = oracle.render_frozen_restir(sc, cam, cfg, 5, small["tri_material"], prm2)
     assert np.allclose(b, 2.0 * a, rtol=1e-12, atol=1e-15)
     assert np.abs(a).max() > 0
+
+
+@pytest.mark.parametrize("denoise", [False, True], ids=["raw", "denoised"])
+def test_frozen_restir_second_frame_is_the_fp32_frame(oracle, small, denoise):
+    """A frame with temporal history: the frozen evaluation renders the first
+    frame in fp32 for its history and reproduces the oracle's second frame."""
+    sc, cam = small["scene"], small["camera"]
+    cfg = restir_config(small["config"], denoise=denoise)
+    o = oracle.Oracle()
+    o.render(sc, cam, cfg, 90)
+    _, hdr, st = o.render(sc, cam, cfg, 91)
+    assert st["chain"] == 2
+    fro = oracle.render_frozen_restir(sc, cam, cfg, 91, small["tri_material"], small["params"].astype(np.float64),
+                                      prev=(cam, 90))
+    first = oracle.render_frozen_restir(sc, cam, cfg, 91, small["tri_material"], small["params"].astype(np.float64))
+    hdr = hdr.reshape(-1, 3).astype(np.float64)
+    rel = np.abs(fro - hdr) / (np.abs(hdr) + 1e-7)
+    assert np.median(rel) < 1e-5
+    assert np.quantile(rel, 0.999) < 5e-4 and rel.max() < 2e-3
+    assert not np.allclose(first, hdr, rtol=1e-3)  # the history mattered
