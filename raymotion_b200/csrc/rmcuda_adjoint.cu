@@ -27,6 +27,8 @@ int rmcuda_scene_set_materials(rmcuda_ctx* c, rmcuda_scene* scene, const int32_t
   cudaSetDevice(c->device);
   DevScene& sc = scene->d;
   if (!sc.have_scene) { set_err(err, errcap, "no scene"); return RM_ERR_INVALID; }
+  // a frame rendered with the old materials is no longer the ReSTIR adjoint's checkpoint
+  if (c->hist_scene == static_cast<const void*>(&sc)) c->hist_scene = nullptr;
   if (!tri_material && (sc.n_materials == 0 || sc.n_materials != n_materials)) {
     set_err(err, errcap, "the first call needs tri_material, and later calls the same material count");
     return RM_ERR_INVALID;

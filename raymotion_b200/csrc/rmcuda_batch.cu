@@ -374,6 +374,9 @@ void rmcuda_scene_destroy(rmcuda_ctx* c, rmcuda_scene* s) {
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    // a checkpoint of this scene's last frame must not match a later scene
+    // allocated at the same address
+    if (c->hist_scene == static_cast<const void*>(&s->d)) c->hist_scene = nullptr;
   }
   s->d.release();
   delete s;

@@ -320,9 +320,13 @@ def test_restir_frame_adjoint_matches_fp64_central_differences(backend, oracle, 
         assert np.allclose(i64, img.cpu().numpy().reshape(-1, 3), rtol=2e-3, atol=1e-5)
         dl = torch.from_numpy(((2.0 / i64.size) * (i64 - T)).astype(np.float32).ravel()).cuda()
         g = _grad(backend, h, d, seed, dl)
-        # the checkpoint must be this frame's
+        # the checkpoint must be this frame's, with the materials it was rendered with
         with pytest.raises(RenderError, match="replays the last frame"):
             _grad(backend, h, d, seed + 1, dl)
+        if not second:
+            _set(backend, h, d, d["params"])
+            with pytest.raises(RenderError, match="replays the last frame"):
+                _grad(backend, h, d, seed, dl)
     finally:
         backend.scene_destroy(h)
 
