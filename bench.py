@@ -382,25 +382,29 @@ def adjoint_measure(args, backend, torch, stream, dev, rank=0, world=1):
     st = backend.stage_counters()
     # the ReSTIR chain on the same scene: each adjoint replays the frame just
     # rendered (its G-buffer and reservoirs are the checkpoint)
-    cfg_r = rb.RenderConfig(**{k: getattr(cfg, k) for k in cfg.__dataclass_fields__})
-    cfg_r.restir_candidates, cfg_r.restir_spatial, cfg_r.restir_radius = 32, 5, 30.0
-    cfg_r.flags = (cfg.flags & ~rb._abi.RM_FLAG_RESTIR_OFF) | rb._abi.RM_FLAG_DENOISE_OFF
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    r_fwd = r_bwd = 0.0
-    for i in range(5):
-        ev[0].record(stream)
-        backend.render_scene_async(h, cam, cfg_r, 300 + i, None, img.data_ptr())
-        ev[1].record(stream)
-        backend.backward(h, cam, cfg_r, 300 + i, dl.data_ptr(), grad.data_ptr())
-        ev[2].record(stream)
-        backend.sync()
-        torch.cuda.synchronize()
-        if i >= 2:
-            r_fwd += ev[0].elapsed_time(ev[1]) / 3
-            r_bwd += ev[1].elapsed_time(ev[2]) / 3
     restir = dict(workload="the same scene and 32 spp on the ReSTIR chain (32 candidates, 5 neighbours, radius 30 "
-                           "px, temporal), denoiser off; the adjoint replays K5 from the frame's G-buffer and "
-                           "reservoirs", forward_ms=r_fwd, adjoint_ms=r_bwd, adjoint_over_forward=r_bwd / r_fwd)
+                           "px, temporal); the adjoint replays K5 from the frame's G-buffer and reservoirs, and "
+                           "transposes the denoiser when it is on")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    for name, denoise in (("denoiser_off", False), ("denoised", True)):
+        cfg_r = rb.RenderConfig(**{k: getattr(cfg, k) for k in cfg.__dataclass_fields__})
+        cfg_r.restir_candidates, cfg_r.restir_spatial, cfg_r.restir_radius = 32, 5, 30.0
+        cfg_r.flags = cfg.flags & ~rb._abi.RM_FLAG_RESTIR_OFF & ~rb._abi.RM_FLAG_DENOISE_OFF
+        if not denoise:
+            cfg_r.flags |= rb._abi.RM_FLAG_DENOISE_OFF
+        r_fwd = r_bwd = 0.0
+        for i in range(5):
+            ev[0].record(stream)
+            backend.render_scene_async(h, cam, cfg_r, 300 + i, None, img.data_ptr())
+            ev[1].record(stream)
+            backend.backward(h, cam, cfg_r, 300 + i, dl.data_ptr(), grad.data_ptr())
+            ev[2].record(stream)
+            backend.sync()
+            torch.cuda.synchronize()
+            if i >= 2:
+                r_fwd += ev[0].elapsed_time(ev[1]) / 3
+                r_bwd += ev[1].elapsed_time(ev[2]) / 3
+        restir[name] = dict(forward_ms=r_fwd, adjoint_ms=r_bwd, adjoint_over_forward=r_bwd / r_fwd)
     # which materials the camera sees: primary hits of the pixel centres
     backend.upload(sc, use_nodes=False)
     ys, xs = np.mgrid[0:cfg.height, 0:cfg.width]
