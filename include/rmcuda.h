@@ -263,6 +263,20 @@ int rmcuda_trace_noalloc(const rm_triangle* d_tris, int32_t n_tris, const float*
                          int32_t any_hit, int32_t* d_tri, float* d_t, float* d_u, float* d_v,
                          void* cuda_stream, char* err, size_t errcap);
 
+/* ---- Preview frame channel (include/raymotion/preview.hpp:8-27).  A frame
+ * goes out as the line "RAY1 <w> <h> <frame> <bytes>\n" and its RGB8 bytes,
+ * row-major, top row first.  rmcuda_preview_frame writes a host image;
+ * rmcuda_preview_last writes the last frame rendered on the context straight
+ * from its device RGB8 image (read back through a pinned buffer).  With
+ * grant_fd >= 0 the call then reads one byte from it (the reference reads
+ * stdin): RM_PREVIEW_DONE when that descriptor is at end of file, the
+ * reference's RenderComplete.  A failed write returns RM_ERR_INVALID with
+ * "preview channel closed". */
+#define RM_PREVIEW_DONE 7
+int rmcuda_preview_frame(int32_t fd, const uint8_t* rgb, int32_t width, int32_t height, int32_t frame,
+                         int32_t grant_fd, char* err, size_t errcap);
+int rmcuda_preview_last(rmcuda_ctx* ctx, int32_t fd, int32_t frame, int32_t grant_fd, char* err, size_t errcap);
+
 /* ---- Scene objects and batched rendering.  No counterpart in the reference,
  * which renders one scene per call (metal.mm:95-414). */
 typedef struct rmcuda_scene rmcuda_scene;

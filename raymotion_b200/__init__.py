@@ -252,6 +252,16 @@ class Backend:
         self._check(self.lib.rmcuda_backward(self.h, handle, C.byref(cam.packed()), C.byref(cfg.packed()),
                                              C.c_uint64(seed & 0xFFFFFFFFFFFFFFFF), d_dl_dimage, d_grad, e, 512), e)
 
+    def preview_last(self, fd: int, frame: int, grant_fd: int = -1) -> bool:
+        """Write the last frame to the preview channel `fd` (RAY1 framing); with
+        grant_fd, wait for one byte there.  False when grant_fd is at end of file."""
+        e = _err()
+        rc = self.lib.rmcuda_preview_last(self.h, fd, frame, grant_fd, e, 512)
+        if rc == _abi.RM_PREVIEW_DONE:
+            return False
+        self._check(rc, e)
+        return True
+
     def reset_history(self) -> None:
         self.lib.rmcuda_reset_history(self.h)
 
@@ -316,3 +326,19 @@ def render_image_metal(scene: PackedScene, cam: Camera, cfg: RenderConfig, seed:
         return True, _default.render(scene, cam, cfg, seed), ""
     except RenderError as ex:
         return False, np.zeros(0, np.uint8), str(ex)
+
+
+def preview_frame(fd: int, rgb: np.ndarray, width: int, height: int, frame: int, grant_fd: int = -1) -> bool:
+    """Write a host RGB8 image to the preview channel `fd` ("RAY1 w h frame
+    bytes" line, then the bytes; include/raymotion/preview.hpp:17-23).  With
+    grant_fd, wait for one byte there; False when it is at end of file."""
+    buf = np.ascontiguousarray(rgb, np.uint8)
+    assert buf.size == width * height * 3
+    lib = _abi.load_library()
+    e = _err()
+    rc = lib.rmcuda_preview_frame(fd, _abi.ptr(buf), width, height, frame, grant_fd, e, 512)
+    if rc == _abi.RM_PREVIEW_DONE:
+        return False
+    if rc != _abi.RM_OK:
+        raise RenderError(rc, e.value.decode())
+    return True

@@ -21,6 +21,7 @@ RM_ERR_CUDA = 3
 RM_ERR_ALLOC = 4
 RM_ERR_BVH = 5
 RM_ERR_DEVICE = 6
+RM_PREVIEW_DONE = 7  # the preview grant descriptor reached end of file
 
 RM_FLAG_NO_ENV = 0x1
 RM_FLAG_NOADAPT = 0x2
@@ -124,6 +125,8 @@ EXPORTS = [
     ("rmcuda_model_update", C.c_int, [_P, C.c_int32, _P, C.c_int32, _S, _Z]),
     ("rmcuda_instances_commit", C.c_int, [_P, _P, C.c_int32, C.c_int32, _S, _Z]),
     ("rmcuda_scene_read", C.c_int, [_P, _P, C.c_int32, _P, _P, C.c_int32, _P, C.POINTER(C.c_float), _S, _Z]),
+    ("rmcuda_preview_frame", C.c_int, [C.c_int32, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _S, _Z]),
+    ("rmcuda_preview_last", C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _S, _Z]),
     ("rmcuda_render_resident_async", C.c_int, [_P, C.POINTER(RmCamera), C.POINTER(RmConfig), C.c_uint64, _P, _P,
                                                 _S, _Z]),
     ("rmcuda_sync", C.c_int, [_P, _S, _Z]),

@@ -134,6 +134,8 @@ struct rmcuda_ctx {
   bool hist_had_history = false;  // the frame's temporal passes used the history before it
   rm_camera hist_prev_cam{};       // and this camera for reprojection
   rmd::DevBuf adj_scratch;         // the denoiser backward's intermediate images
+  uint8_t* h_preview = nullptr;    // pinned RGB8 read-back of rmcuda_preview_last
+  size_t h_preview_cap = 0;
   // last frame
   int last_chain = 0;
   uint64_t frames = 0;

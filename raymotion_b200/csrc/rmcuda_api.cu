@@ -14,7 +14,10 @@
 //    kernels on one stream, then one device-to-host copy of the RGB8 image.
 #include <cuda_runtime.h>
 
+#include <unistd.h>
+
 #include <algorithm>
+#include <cerrno>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -632,6 +635,7 @@ void rmcuda_destroy(rmcuda_ctx* c) {
                     &c->prep_lscan, &c->prep_temp, &c->prep_weight, &c->prep_small})
     b->release();
   if (c->h_prep) cudaFreeHost(c->h_prep);
+  if (c->h_preview) cudaFreeHost(c->h_preview);
   c->gb.release(); c->hg.release();
   c->rinit.release(); c->rmerged.release(); c->hres.release();
   resolve_pending(c);
@@ -927,6 +931,68 @@ int rmcuda_render(rmcuda_ctx* c, const rm_scene_view* sv, const rm_camera* cam, 
     set_err(err, errcap, msg);
   }
   return rc;
+}
+
+// include/raymotion/preview.hpp:17-23: the frame line, the bytes, then one
+// byte granted for the next frame (end of file: rendering is complete)
+int rmcuda_preview_frame(int32_t fd, const uint8_t* rgb, int32_t width, int32_t height, int32_t frame,
+                         int32_t grant_fd, char* err, size_t errcap) {
+  if (fd < 0 || !rgb || width <= 0 || height <= 0) { set_err(err, errcap, "invalid preview frame"); return RM_ERR_INVALID; }
+  const size_t bytes = size_t(width) * size_t(height) * 3;
+  char head[96];
+  const int n = std::snprintf(head, sizeof(head), "RAY1 %d %d %d %zu\n", width, height, frame, bytes);
+  auto write_all = [fd](const void* data, size_t len) {
+    const char* q = static_cast<const char*>(data);
+    while (len > 0) {
+      const ssize_t k = ::write(fd, q, len);
+      if (k < 0 && errno == EINTR) continue;
+      if (k <= 0) return false;
+      q += k;
+      len -= size_t(k);
+    }
+    return true;
+  };
+  if (n <= 0 || !write_all(head, size_t(n)) || !write_all(rgb, bytes)) {
+    set_err(err, errcap, "preview channel closed");
+    return RM_ERR_INVALID;
+  }
+  if (grant_fd >= 0) {
+    char b;
+    ssize_t k;
+    do k = ::read(grant_fd, &b, 1);
+    while (k < 0 && errno == EINTR);
+    if (k <= 0) return RM_PREVIEW_DONE;
+  }
+  return RM_OK;
+}
+
+int rmcuda_preview_last(rmcuda_ctx* c, int32_t fd, int32_t frame, int32_t grant_fd, char* err, size_t errcap) {
+  if (!c) { set_err(err, errcap, "null argument"); return RM_ERR_INVALID; }
+  {
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    if (c->frames == 0 || !c->last_final || c->last_w <= 0 || c->last_h <= 0) {
+      set_err(err, errcap, "no frame rendered");
+      return RM_ERR_INVALID;
+    }
+    const size_t npix = size_t(c->last_w) * size_t(c->last_h);
+    cudaError_t e = c->rgb.reserve(npix * 3);
+    if (e == cudaSuccess && c->h_preview_cap < npix * 3) {
+      if (c->h_preview) cudaFreeHost(c->h_preview);
+      c->h_preview = nullptr;
+      c->h_preview_cap = 0;
+      if ((e = cudaMallocHost(reinterpret_cast<void**>(&c->h_preview), npix * 3)) == cudaSuccess)
+        c->h_preview_cap = npix * 3;
+    }
+    // the device tonemap of the last linear image (pathtrace.metal:1355-1363)
+    if (e == cudaSuccess) e = launch_tonemap(c->last_final, c->rgb.as<uint8_t>(), uint32_t(npix), c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c->h_preview, c->rgb.ptr, npix * 3, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("preview read-back failed", e)); return RM_ERR_CUDA; }
+    // written under the context's lock: the pinned image is the context's
+    return rmcuda_preview_frame(fd, c->h_preview, c->last_w, c->last_h, frame, grant_fd, err, errcap);
+  }
 }
 
 int rmcuda_trace(rmcuda_ctx* c, const float* d_rays, int32_t n, int32_t any_hit, int32_t* d_tri, float* d_t,

@@ -57,3 +57,32 @@ def test_render_image_metal_validates_first():
     from raymotion_b200.scene import Camera, RenderConfig, SceneBuilder
     ok, rgb, err = rb.render_image_metal(SceneBuilder().pack(), Camera(), RenderConfig(width=0), 1)
     assert not ok and err == "Invalid Metal render dimensions or sample count"
+
+
+def test_preview_channel_framing():
+    """rmcuda_preview_frame (no GPU): the frame line and bytes of the
+    reference's preview channel, then one granted byte per frame; end of file
+    on the grant descriptor ends the preview, a closed channel is an error."""
+    import os
+
+    import numpy as np
+
+    import raymotion_b200 as rb
+    rgb = (np.arange(4 * 3 * 3) % 256).astype(np.uint8)
+    r, w = os.pipe()
+    gr, gw = os.pipe()
+    os.write(gw, b"x")
+    assert rb.preview_frame(w, rgb, 4, 3, 7, gr)
+    os.close(w)
+    data = os.read(r, 1 << 16)
+    head, body = data.split(b"\n", 1)
+    assert head == b"RAY1 4 3 7 36" and body == rgb.tobytes()
+    os.close(gw)  # no further grant: the preview is complete
+    r2, w2 = os.pipe()
+    assert not rb.preview_frame(w2, rgb, 4, 3, 8, gr)
+    os.close(r2)
+    os.close(gr)
+    with pytest.raises(rb.RenderError, match="preview channel closed"):
+        rb.preview_frame(w2, rgb, 4, 3, 9)
+    os.close(w2)
+    os.close(r)

@@ -82,3 +82,38 @@ def test_caller_bvh_validation(backend, oracle):
     with pytest.raises(rb.RenderError) as ex:
         backend.render(sc, cam, cfg, 1)
     assert ex.value.code == rb._abi.RM_ERR_BVH
+
+
+def test_preview_last_sends_the_frame_rendered(backend, oracle):
+    """rmcuda_preview_last: the last frame's RGB8, tonemapped on the device from
+    its final linear image, through the reference's preview framing."""
+    import os
+
+    from raymotion_b200.scenes import cornell_box
+    sb, cam, cfg = cornell_box(0)
+    sc = sb.pack()
+    rgb = backend.render(sc, cam, cfg, 12345, use_nodes=False)
+    import threading
+
+    r, w = os.pipe()
+    gr, gw = os.pipe()
+    os.write(gw, b"g")
+    chunks = []
+
+    def drain():  # the frame is larger than a pipe's buffer
+        while True:
+            b = os.read(r, 1 << 20)
+            if not b:
+                break
+            chunks.append(b)
+
+    t = threading.Thread(target=drain)
+    t.start()
+    assert backend.preview_last(w, 3, gr)
+    os.close(w)
+    t.join(timeout=30)
+    head, body = b"".join(chunks).split(b"\n", 1)
+    assert head == f"RAY1 {cfg.width} {cfg.height} 3 {cfg.width * cfg.height * 3}".encode()
+    assert body == rgb.tobytes()
+    for fd in (r, gr, gw):
+        os.close(fd)
