@@ -1744,10 +1744,11 @@ int orc_render_frozen(const rm_scene_view* sv, const rm_camera* cam, const rm_co
   return RM_OK;
 }
 
-// K7 (pathtrace.metal:1315-1354) in double on a held G-buffer: the denoiser of
-// the frozen frame, the colour it filters in double (the first frame's K6 is
-// the identity).
-static void atrous64(const Params& p, const GBuf* gb, const double* in, double* out, int step, int nthreads) {
+// K7 (pathtrace.metal:1315-1354) in double on a held G-buffer geometry: the
+// denoiser of the frozen frame, with the colour it filters and the albedo of
+// its weights (each pixel's first-hit albedo at the parameters) in double.
+static void atrous64(const Params& p, const GBuf* gb, const double* alb, const double* in, double* out, int step,
+                     int nthreads) {
   const int W = p.width, H = p.height;
   const int stride = 1 << step;
   auto lum = [](const double* c) { return 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2]; };
@@ -1779,8 +1780,8 @@ static void atrous64(const Params& p, const GBuf* gb, const double* in, double* 
                        ez = double(g.pos.z) - g0.pos.z;
           const double wz = std::exp(-std::sqrt(ex * ex + ey * ey + ez * ez) / (0.1 * dc + 1e-4));
           const double wl = std::exp(-std::fabs(lum(c) - l0) / (0.3 * std::max(l0, 0.5) + 1e-3));
-          const double ax = double(g.albedo.x) - g0.albedo.x, ay = double(g.albedo.y) - g0.albedo.y,
-                       az = double(g.albedo.z) - g0.albedo.z;
+          const double ax = alb[n * 3] - alb[id * 3], ay = alb[n * 3 + 1] - alb[id * 3 + 1],
+                       az = alb[n * 3 + 2] - alb[id * 3 + 2];
           const double wa = std::exp(-std::sqrt(ax * ax + ay * ay + az * az) / 0.25);
           const double w = wn * wz * wl * wa;
           for (int k = 0; k < 3; ++k) sum[k] += w * c[k];
@@ -1909,6 +1910,7 @@ int orc_render_frozen_restir(const rm_scene_view* sv, const rm_camera* cam, cons
   MatTable mt;
   mt.tri_mat = tri_material;
   mt.prm = prm;
+  std::vector<double> alb64(pixels * 3, 0.0);
   const double cl = p.clamp_value;
   parallel_for(H, nthreads, [&](int yy) {
     Counters ctr;
@@ -1926,6 +1928,27 @@ int orc_render_frozen_restir(const rm_scene_view* sv, const rm_camera* cam, cons
           for (int c = 0; c < 3; ++c) v[c] = std::fmin(v[c], cl);
       };
       const rm_camera& c = p.camera;
+      // the first hit's triangle, from K3's primary ray
+      Hit<float> h0;
+      {
+        Tracer<float> p3{&s, &p, Rng{}, &ctr};
+        p3.rng.seed(seed_pixel(seed, x, y));
+        float sx = float(x) + 1e-12f + (p.resolution - 2e-12f) * p3.U() - float(p.width) * 0.5f;
+        float sy = float(p.height) * 0.5f - (float(y) + 1e-12f + (p.resolution - 2e-12f) * p3.U());
+        float f2 = c.focal * c.focal;
+        float dinv = 1.0f / std::sqrt(sx * sx + sy * sy + f2);
+        float tx = sx * dinv, ty = sy * dinv, tz = c.focal * dinv;
+        V3<float> rd = mk(tx * c.m0 + (ty * c.m1 + tz * c.m2), tx * c.m3 + (ty * c.m4 + tz * c.m5),
+                          tx * c.m6 + (ty * c.m7 + tz * c.m8));
+        h0 = p3.cast_alpha_ray(mk(c.x, c.y, c.z), rd, 1e30f);
+      }
+      if (h0.tri < 0) continue;
+      // the G-buffer albedo at the parameters (the denoiser's weights)
+      {
+        const double tx[3] = {double(h0.txr), double(h0.txg), double(h0.txb)};
+        const double own[3] = {double(h0.ar), double(h0.ag), double(h0.ab)};
+        for (int k = 0; k < 3; ++k) alb64[size_t(id) * 3 + k] = h0.shader == 1 ? own[k] : mt.get(s.tris, h0.tri, k) * tx[k];
+      }
       if (gg.kind == 3) {
         double sum[3] = {0, 0, 0};
         for (int si = 0; si < p.spp; ++si) {
@@ -1945,21 +1968,6 @@ int orc_render_frozen_restir(const rm_scene_view* sv, const rm_camera* cam, cons
         clampd(o);
         continue;
       }
-      // kind 1: the first hit's triangle, from K3's primary ray
-      Hit<float> h0;
-      {
-        Tracer<float> p3{&s, &p, Rng{}, &ctr};
-        p3.rng.seed(seed_pixel(seed, x, y));
-        float sx = float(x) + 1e-12f + (p.resolution - 2e-12f) * p3.U() - float(p.width) * 0.5f;
-        float sy = float(p.height) * 0.5f - (float(y) + 1e-12f + (p.resolution - 2e-12f) * p3.U());
-        float f2 = c.focal * c.focal;
-        float dinv = 1.0f / std::sqrt(sx * sx + sy * sy + f2);
-        float tx = sx * dinv, ty = sy * dinv, tz = c.focal * dinv;
-        V3<float> rd = mk(tx * c.m0 + (ty * c.m1 + tz * c.m2), tx * c.m3 + (ty * c.m4 + tz * c.m5),
-                          tx * c.m6 + (ty * c.m7 + tz * c.m8));
-        h0 = p3.cast_alpha_ray(mk(c.x, c.y, c.z), rd, 1e30f);
-      }
-      if (h0.tri < 0) continue;
       V3<float> gpos = vf<float>(gg.pos), gnor = vf<float>(gg.normal), galb = vf<float>(gg.albedo),
                 gwo = vf<float>(gg.wo);
       float rough = gg.rough; if (rough < 0) rough = 0; if (rough > 1) rough = 1;
@@ -2066,9 +2074,9 @@ int orc_render_frozen_restir(const rm_scene_view* sv, const rm_camera* cam, cons
     // and history colour
     std::vector<double> tmp(pixels * 3);
     temporal64(p, g.data(), hg.data(), out, hcol.data(), tmp.data(), nthreads);
-    atrous64(p, g.data(), tmp.data(), out, 0, nthreads);
+    atrous64(p, g.data(), alb64.data(), tmp.data(), out, 0, nthreads);
     for (size_t i = 0; i < pixels * 3; ++i) tmp[i] = out[i];
-    atrous64(p, g.data(), tmp.data(), out, 1, nthreads);
+    atrous64(p, g.data(), alb64.data(), tmp.data(), out, 1, nthreads);
   }
   return RM_OK;
 }

@@ -551,7 +551,8 @@ __global__ void __launch_bounds__(256) k_adjoint(Scene s, Params p, uint64_t see
 template <bool kRis>
 __global__ void __launch_bounds__(256) k_adjoint_restir(Scene s, Params p, uint64_t seed, GBufSoA gb, ResSoA rm,
                                                         const int32_t* __restrict__ tri_mat, int n_mat,
-                                                        const float* __restrict__ dLdI, float* __restrict__ grad,
+                                                        const float* __restrict__ dLdI,
+                                                        const float* __restrict__ dLdalb, float* __restrict__ grad,
                                                         int use_shared, unsigned long long* ctr, uint32_t* err) {
   extern __shared__ float sh[];
   if (use_shared) {
@@ -570,6 +571,35 @@ __global__ void __launch_bounds__(256) k_adjoint_restir(Scene s, Params p, uint6
     pt.rng.seed(seed ^ (uint64_t(id + 1) * 0xBF58476D1CE4E5B9ull) ^ 0x94D049BB133111EBull);
     const bool cl = p.clamp_value > 0.0f;
     const float D[3] = {dLdI[size_t(id) * 3], dLdI[size_t(id) * 3 + 1], dLdI[size_t(id) * 3 + 2]};
+    // the first hit's triangle: K3's primary ray (its own random stream)
+    int m0 = -1;
+    float tx0[3] = {1.f, 1.f, 1.f};
+    bool alb0 = false;
+    float dal0 = 0.0f;
+    if (kind == 1 || dLdalb) {
+      Tracer p3(s, p, err);
+      p3.rng.seed(seed_pixel(seed, x, y));
+      float sx = float(x) + 1e-12f + (p.resolution - 2e-12f) * p3.U() - float(p.width) * 0.5f;
+      float sy = float(p.height) * 0.5f - (float(y) + 1e-12f + (p.resolution - 2e-12f) * p3.U());
+      const rm_camera& c = p.camera;
+      float f2 = c.focal * c.focal;
+      float dinv = 1.0f / sqrtf(sx * sx + sy * sy + f2);
+      float tx = sx * dinv, ty = sy * dinv, tz = c.focal * dinv;
+      float rdx = tx * c.m0 + (ty * c.m1 + tz * c.m2);
+      float rdy = tx * c.m3 + (ty * c.m4 + tz * c.m5);
+      float rdz = tx * c.m6 + (ty * c.m7 + tz * c.m8);
+      const Hit h0 = p3.cast_alpha_ray(c.x, c.y, c.z, rdx, rdy, rdz, kFar);
+      if (h0.tri >= 0) {
+        m0 = tri_mat[h0.tri];
+        tx0[0] = h0.txr; tx0[1] = h0.txg; tx0[2] = h0.txb;
+        alb0 = h0.shader != 1;
+        dal0 = dalpha2(h0.rough);
+      }
+    }
+    // the denoiser's weights through this pixel's G-buffer albedo (the first
+    // hit's albedo times its texel)
+    if (dLdalb && alb0)
+      for (int k = 0; k < 3; ++k) sink.add(m0, k, dLdalb[size_t(id) * 3 + k] * tx0[k]);
     if (kind == 3) {
       const float inv_n = 1.0f / float(p.spp);
       for (int si = 0; si < p.spp; ++si) {
@@ -577,31 +607,6 @@ __global__ void __launch_bounds__(256) k_adjoint_restir(Scene s, Params p, uint6
         ++samples;
       }
     } else {
-      // the first hit's triangle: K3's primary ray (its own random stream)
-      int m0 = -1;
-      float tx0[3] = {1.f, 1.f, 1.f};
-      bool alb0 = false;
-      float dal0 = 0.0f;
-      {
-        Tracer p3(s, p, err);
-        p3.rng.seed(seed_pixel(seed, x, y));
-        float sx = float(x) + 1e-12f + (p.resolution - 2e-12f) * p3.U() - float(p.width) * 0.5f;
-        float sy = float(p.height) * 0.5f - (float(y) + 1e-12f + (p.resolution - 2e-12f) * p3.U());
-        const rm_camera& c = p.camera;
-        float f2 = c.focal * c.focal;
-        float dinv = 1.0f / sqrtf(sx * sx + sy * sy + f2);
-        float tx = sx * dinv, ty = sy * dinv, tz = c.focal * dinv;
-        float rdx = tx * c.m0 + (ty * c.m1 + tz * c.m2);
-        float rdy = tx * c.m3 + (ty * c.m4 + tz * c.m5);
-        float rdz = tx * c.m6 + (ty * c.m7 + tz * c.m8);
-        const Hit h0 = p3.cast_alpha_ray(c.x, c.y, c.z, rdx, rdy, rdz, kFar);
-        if (h0.tri >= 0) {
-          m0 = tri_mat[h0.tri];
-          tx0[0] = h0.txr; tx0[1] = h0.txg; tx0[2] = h0.txb;
-          alb0 = h0.shader != 1;
-          dal0 = dalpha2(h0.rough);
-        }
-      }
       const float4 NR = gb.nor_rough[id], AM = gb.alb_met[id], WO = gb.wo_ior[id], EM = gb.emi[id];
       const float gpx = PK.x, gpy = PK.y, gpz = PK.z, gnx = NR.x, gny = NR.y, gnz = NR.z;
       float rough = NR.w; if (rough < 0.0f) rough = 0.0f; if (rough > 1.0f) rough = 1.0f;
@@ -797,17 +802,18 @@ cudaError_t apply_materials(rm_triangle* tris, const int32_t* tri_mat, const flo
 }
 
 cudaError_t launch_adjoint_restir(const Scene& s, const Params& p, uint64_t seed, const GBufSoA& gb, const ResSoA& rm,
-                                  const int32_t* tri_mat, int n_mat, const float* dLdI, float* grad,
-                                  unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
+                                  const int32_t* tri_mat, int n_mat, const float* dLdI, const float* dLdalb,
+                                  float* grad, unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
   const size_t shmem = size_t(n_mat) * kMatParams * sizeof(float);
   const int use_shared = shmem <= 32 * 1024 ? 1 : 0;
   const unsigned grid = unsigned((size_t(p.width) * size_t(p.height) + 255) / 256);
   const size_t sm = use_shared ? shmem : 0;
   if (p.restir_candidates > 1)
-    k_adjoint_restir<true><<<grid, 256, sm, st>>>(s, p, seed, gb, rm, tri_mat, n_mat, dLdI, grad, use_shared, ctr, err);
+    k_adjoint_restir<true><<<grid, 256, sm, st>>>(s, p, seed, gb, rm, tri_mat, n_mat, dLdI, dLdalb, grad, use_shared,
+                                                  ctr, err);
   else
-    k_adjoint_restir<false><<<grid, 256, sm, st>>>(s, p, seed, gb, rm, tri_mat, n_mat, dLdI, grad, use_shared, ctr,
-                                                   err);
+    k_adjoint_restir<false><<<grid, 256, sm, st>>>(s, p, seed, gb, rm, tri_mat, n_mat, dLdI, dLdalb, grad,
+                                                   use_shared, ctr, err);
   return cudaGetLastError();
 }
 

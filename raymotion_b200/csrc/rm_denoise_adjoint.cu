@@ -1,9 +1,10 @@
 // rm_denoise_adjoint.cu - the denoiser's backward pass (pathtrace.metal:
 // 1263-1354): the transpose of the temporal blend and of the two a-trous
-// passes as functions of the colour they filter, the G-buffers and the
-// history colour held (the frame's checkpoint).  It turns dL/d(denoised image)
-// into dL/d(the ReSTIR shade's HDR image), which the path-replay adjoint then
-// takes.
+// passes as functions of the colour they filter and of the G-buffer albedo in
+// their weights, the G-buffer geometry and the history colour held (the
+// frame's checkpoint).  It turns dL/d(denoised image) into dL/d(the ReSTIR
+// shade's HDR image) and dL/d(G-buffer albedo), which the path-replay adjoint
+// then takes.
 //
 // An a-trous pass is out_i = sum_j w_ij c_j / W_i, W_i = sum_j w_ij (out_i = c_i
 // when W_i <= 1e-12; 0 on kind-0 pixels), with
@@ -12,9 +13,14 @@
 // so besides the linear term w_ij / W_i each colour moves the weights through
 // its luma:  dL/dw_ij = g_i . (c_j - out_i) / W_i,  dw_ij/dl_j = -w_ij sgn(l_j -
 // l_i) / t_i,  dw_ij/dl_i = w_ij (sgn(l_j - l_i) / t_i + |l_j - l_i| t_i' / t_i^2).
-// The forward pass is recomputed here with the library's exp and sqrt (the
-// oracle's exact form; the frame's own a-trous kernel uses exp2 / rsqrt
-// approximations within 1e-4), keeping out_i and W_i for the backward.
+// The weights also move with the G-buffer albedo of both pixels (the first
+// hit's material albedo times its texel): dw_ij/da_j = -w_ij u_ij / 0.25 and
+// dw_ij/da_i = w_ij u_ij / 0.25, u_ij the unit vector of a_j - a_i; those
+// gradients go to the materials through the path-replay adjoint, which knows
+// each pixel's first hit.  The forward pass is recomputed here with the
+// library's exp and sqrt (the oracle's exact form; the frame's own a-trous
+// kernel uses exp2 / rsqrt approximations within 1e-4), keeping out_i and W_i
+// for the backward.
 #include <cuda_runtime.h>
 
 #include "rm_device.cuh"
@@ -40,6 +46,16 @@ __device__ __forceinline__ float atrous_w(const GBufSoA& gb, uint32_t i, uint32_
   const float ax = Aj.x - Ai.x, ay = Aj.y - Ai.y, az = Aj.z - Ai.z;
   const float wa = expf(-sqrtf(ax * ax + ay * ay + az * az) / 0.25f);
   return wn * wz * wl * wa;
+}
+
+// (a_j - a_i) / (0.25 |a_j - a_i|), zero for equal albedos: dlog wa_ij / da_i
+__device__ __forceinline__ float3 alb_dir(const GBufSoA& gb, uint32_t i, uint32_t j) {
+  const float4 Ai = gb.alb_met[i], Aj = gb.alb_met[j];
+  const float ax = Aj.x - Ai.x, ay = Aj.y - Ai.y, az = Aj.z - Ai.z;
+  const float l = sqrtf(ax * ax + ay * ay + az * az);
+  if (!(l > 0.0f)) return make_float3(0.f, 0.f, 0.f);
+  const float k = 1.0f / (0.25f * l);
+  return make_float3(ax * k, ay * k, az * k);
 }
 
 __device__ __forceinline__ float cam_dist(const Params& p, const float4& P) {
@@ -90,12 +106,12 @@ __global__ void __launch_bounds__(256) k_atrous_fwd(Params p, GBufSoA gb, const 
 __global__ void __launch_bounds__(256) k_atrous_bwd(Params p, GBufSoA gb, const float* __restrict__ in,
                                                     const float* __restrict__ out, const float* __restrict__ wsum,
                                                     const float* __restrict__ g_out, float* __restrict__ g_in,
-                                                    int step) {
+                                                    float* __restrict__ g_alb, int step) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t npix = uint32_t(p.width) * uint32_t(p.height);
   if (j >= npix) return;
   const int x = int(j % uint32_t(p.width)), y = int(j / uint32_t(p.width));
-  float gj[3] = {0.f, 0.f, 0.f};
+  float gj[3] = {0.f, 0.f, 0.f}, ga[3] = {0.f, 0.f, 0.f};
   const float4 Pj = gb.pos_kind[j];
   const int stride = 1 << step;
   const float cj[3] = {in[size_t(j) * 3], in[size_t(j) * 3 + 1], in[size_t(j) * 3 + 2]};
@@ -127,6 +143,9 @@ __global__ void __launch_bounds__(256) k_atrous_bwd(Params p, GBufSoA gb, const 
         }
         const float sg = lj > li ? 1.0f : (lj < li ? -1.0f : 0.0f);
         dl_j += dw * (-w * sg / ti);
+        // j's albedo in wa_ij: dlog wa_ij / da_j = -(a_j - a_i) / (0.25 |.|)
+        const float3 u = alb_dir(gb, i, j);
+        ga[0] -= dw * w * u.x; ga[1] -= dw * w * u.y; ga[2] -= dw * w * u.z;
       }
     // j as the centre: its luma in |l_k - l_j| and in t_j
     const float Wj = wsum[j];
@@ -148,11 +167,17 @@ __global__ void __launch_bounds__(256) k_atrous_bwd(Params p, GBufSoA gb, const 
           const float d = ln - lj;
           const float sg = d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f);
           dl_j += dw * w * (sg / tj + fabsf(d) * dtj / (tj * tj));
+          // j's albedo as the centre: dlog wa_jn / da_j = (a_n - a_j) / (0.25 |.|)
+          const float3 u = alb_dir(gb, j, n);
+          ga[0] += dw * w * u.x; ga[1] += dw * w * u.y; ga[2] += dw * w * u.z;
         }
     }
     gj[0] += dl_j * 0.2126f; gj[1] += dl_j * 0.7152f; gj[2] += dl_j * 0.0722f;
   }
-  for (int k = 0; k < 3; ++k) g_in[size_t(j) * 3 + k] = gj[k];
+  for (int k = 0; k < 3; ++k) {
+    g_in[size_t(j) * 3 + k] = gj[k];
+    g_alb[size_t(j) * 3 + k] += ga[k];
+  }
 }
 
 // backward temporal pass: o = h' + (c - h') 0.2 with h' = clamp(h, mn, mx)
@@ -222,7 +247,7 @@ __global__ void __launch_bounds__(256) k_temporal_bwd(Params p, GBufSoA gb, GBuf
 
 cudaError_t launch_denoise_backward(const Params& p, const GBufSoA& gb, const GBufSoA& hg, const float* hdr,
                                     const float* hist_col, const float* dLdout, float* scratch, float* dLdhdr,
-                                    cudaStream_t st) {
+                                    float* dLdalb, cudaStream_t st) {
   const size_t npix = size_t(p.width) * size_t(p.height);
   const unsigned g = unsigned((npix + 255) / 256);
   // scratch: T, A0, A1, G1 (3 floats per pixel each), W0, W1 (1 each)
@@ -234,10 +259,11 @@ cudaError_t launch_denoise_backward(const Params& p, const GBufSoA& gb, const GB
   float* W1 = W0 + npix;
   cudaError_t e = launch_denoise_stage(0, p, gb, hg, hdr, hist_col, T, nullptr, st);  // the frame's own temporal pass
   if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(dLdalb, 0, npix * 3 * sizeof(float), st)) != cudaSuccess) return e;
   k_atrous_fwd<<<g, 256, 0, st>>>(p, gb, T, A0, W0, 0);
   k_atrous_fwd<<<g, 256, 0, st>>>(p, gb, A0, A1, W1, 1);
-  k_atrous_bwd<<<g, 256, 0, st>>>(p, gb, A0, A1, W1, dLdout, G, 1);   // dL/dA0
-  k_atrous_bwd<<<g, 256, 0, st>>>(p, gb, T, A0, W0, G, A1, 0);        // dL/dT (into A1)
+  k_atrous_bwd<<<g, 256, 0, st>>>(p, gb, A0, A1, W1, dLdout, G, dLdalb, 1);   // dL/dA0
+  k_atrous_bwd<<<g, 256, 0, st>>>(p, gb, T, A0, W0, G, A1, dLdalb, 0);        // dL/dT (into A1)
   if ((e = cudaMemsetAsync(dLdhdr, 0, npix * 3 * sizeof(float), st)) != cudaSuccess) return e;
   k_temporal_bwd<<<g, 256, 0, st>>>(p, gb, hg, hdr, hist_col, A1, dLdhdr);
   return cudaGetLastError();

@@ -149,13 +149,14 @@ cudaError_t launch_adjoint(int lanes, const Scene& s, const Params& p, uint64_t 
 // The adjoint of the ReSTIR shade from the frame's G-buffer and merged
 // reservoirs (one thread per pixel).
 cudaError_t launch_adjoint_restir(const Scene& s, const Params& p, uint64_t seed, const GBufSoA& gb, const ResSoA& rm,
-                                  const int32_t* tri_mat, int n_mat, const float* dLdI, float* grad,
-                                  unsigned long long* ctr, uint32_t* err, cudaStream_t st);
-// rm_denoise_adjoint.cu: dL/d(ReSTIR shade HDR) from dL/d(denoised image), the
-// G-buffers and history colour of the frame held; scratch holds 14 floats per pixel.
+                                  const int32_t* tri_mat, int n_mat, const float* dLdI, const float* dLdalb,
+                                  float* grad, unsigned long long* ctr, uint32_t* err, cudaStream_t st);
+// rm_denoise_adjoint.cu: dL/d(ReSTIR shade HDR) and dL/d(G-buffer albedo) from
+// dL/d(denoised image), the G-buffer geometry and history colour of the frame
+// held; scratch holds 14 floats per pixel.
 cudaError_t launch_denoise_backward(const Params& p, const GBufSoA& gb, const GBufSoA& hg, const float* hdr,
                                     const float* hist_col, const float* dLdout, float* scratch, float* dLdhdr,
-                                    cudaStream_t st);
+                                    float* dLdalb, cudaStream_t st);
 // Write per-material parameters (8 floats each) into the triangles with tri_mat >= 0.
 cudaError_t apply_materials(rm_triangle* tris, const int32_t* tri_mat, const float* mats, int n_tris,
                             cudaStream_t st);

@@ -101,13 +101,14 @@ int rmcuda_backward(rmcuda_ctx* c, const rmcuda_scene* scene, const rm_camera* c
       return RM_ERR_INVALID;
     }
     const float* dl_hdr = d_dL_dimage;
+    const float* dl_alb = nullptr;  // dL/d(G-buffer albedo), through the denoiser's weights
     cudaError_t e = cudaSuccess;
     if (pl.denoise) {
       // through the denoiser first: its inputs are the frame's shaded HDR, its
       // G-buffer and the history it blended (the previous final colour and
       // G-buffer, in the slots the frame's swap left them in)
       const size_t npix = size_t(cfg->width) * size_t(cfg->height);
-      if ((e = c->adj_scratch.reserve(npix * 17 * sizeof(float))) != cudaSuccess) {
+      if ((e = c->adj_scratch.reserve(npix * 20 * sizeof(float))) != cudaSuccess) {
         set_err(err, errcap, cuda_msg("adjoint buffer allocation failed", e));
         return RM_ERR_ALLOC;
       }
@@ -116,17 +117,19 @@ int rmcuda_backward(rmcuda_ctx* c, const rmcuda_scene* scene, const rm_camera* c
       dp.prevCamera = c->hist_prev_cam;
       float* scratch = c->adj_scratch.as<float>();
       float* g_hdr = scratch + npix * 14;
+      float* g_alb = scratch + npix * 17;
       e = staged(c, RM_STAGE_ADJOINT, [&] {
         return launch_denoise_backward(dp, c->hg.view(), c->gb.view(), c->hdr.as<float>(), c->tmp_a.as<float>(),
-                                       d_dL_dimage, scratch, g_hdr, c->stream);
+                                       d_dL_dimage, scratch, g_hdr, g_alb, c->stream);
       });
       if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("denoiser adjoint launch failed", e)); return RM_ERR_CUDA; }
       dl_hdr = g_hdr;
+      dl_alb = g_alb;
     }
     pl.p.hasHistory = 0;
     e = staged(c, RM_STAGE_ADJOINT, [&] {
       return launch_adjoint_restir(scene_view(sc), pl.p, seed, c->hg.view(), c->hres.view(), sc.tri_mat.as<int32_t>(),
-                                   sc.n_materials, dl_hdr, d_grad,
+                                   sc.n_materials, dl_hdr, dl_alb, d_grad,
                                    c->ctr.as<unsigned long long>() + 4 * RM_STAGE_ADJOINT, c->err.as<uint32_t>(),
                                    c->stream);
     });
