@@ -251,3 +251,28 @@ def test_failed_call_drops_temporal_history(backend, small_field):
     _, first = backend.render(sc, cam, cfg, 43, hdr=True, use_nodes=False)
     assert np.array_equal(after_failure.view(np.uint32), first.view(np.uint32))
     assert not np.array_equal(with_history.view(np.uint32), first.view(np.uint32))
+
+
+@pytest.mark.parametrize("shading", ["wavefront", "megakernel"])
+def test_restir_chain_on_a_textured_scene_matches_oracle(backend, oracle, shading, monkeypatch):
+    """The ReSTIR chain (generate, temporal + spatial reuse, shade, denoiser
+    off) on the known-answer scene with its 2x2 texture on walls, metal and
+    both dielectrics (nearest sampling with wrap, pathtrace.metal:178-185):
+    bit-exact radiance over two frames, the second with temporal history."""
+    from . import kat_scenes as K
+    if shading == "megakernel":
+        monkeypatch.setenv("RAYMOTION_CUDA_MEGAKERNEL", "1")
+    cam, _ = K.metal_config()
+    cfg = RenderConfig(width=96, height=64, spp=8, max_bounces=6, adapt_min=0, restir_candidates=8,
+                       restir_spatial=3, restir_radius=8.0, flags=_abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_DENOISE_OFF)
+    sc = K.metal_scene().pack()
+    assert (sc.tris["texture_offset"] >= 0).any()
+    oracle.with_reference_bvh(sc, 2)
+    o = oracle.Oracle()
+    backend.reset_history()
+    for seed in (5, 6):
+        _, o_hdr, o_st = o.render(sc, cam, cfg, seed)
+        _, g_hdr = backend.render(sc, cam, cfg, seed, hdr=True)
+        assert o_st["chain"] == 2 and backend.stats()["kernel_chain"] == 2
+        assert o_hdr.max() > 0
+        assert exact_fraction(g_hdr, o_hdr) == 1.0
