@@ -64,7 +64,7 @@ def _grad(backend, h, d, seed, dl):
     return g.cpu().numpy().reshape(-1, 8)
 
 
-def central_difference(loss, prm, m, col):
+def central_difference(loss, prm, m, col, h0=H):
     """Central differences at H and H/2, Richardson-extrapolated: the plain
     H-difference carries an H^2 error of up to a few percent on the peaks of
     glossy lobes and near a dielectric's critical angle, where the frame's
@@ -74,7 +74,7 @@ def central_difference(loss, prm, m, col):
         qp[m, col] += h
         qm[m, col] -= h
         return (loss(qp) - loss(qm)) / (2 * h)
-    return (4.0 * d(H / 2) - d(H)) / 3.0
+    return (4.0 * d(h0 / 2) - d(h0)) / 3.0
 
 
 @pytest.mark.parametrize("spp,candidates", [(4, 1), (8, 1), (4, 8)], ids=["one_lane", "eight_lanes", "ris_nee"])
@@ -359,10 +359,11 @@ def test_adjoint_on_a_textured_scene_matches_fp64_central_differences(backend, o
     """The known-answer scene with its 2x2 texture on walls, metal and both
     dielectrics, one material per quad: the albedo derivative carries the
     texel (the G-buffer and BSDF albedo are albedo x texel).  Plain chain,
-    single-candidate NEE; every material's albedo, the opaque quads'
-    roughness, the light's emission and the dielectrics' IOR against FP64
-    central differences.  (The rough dielectric quad, a single open sheet, has
-    a roughness derivative 7 % off its central difference, not explained yet.)"""
+    single-candidate NEE; every material's albedo and roughness, the light's
+    emission and the dielectrics' IOR against FP64 central differences with a
+    step of 1e-5: the loss's third derivative in the rough dielectric quad's
+    roughness is large enough that steps of 1e-3 and 5e-4 (Richardson) are 7 %
+    off, while the differences at 1e-4 ... 1e-6 agree to seven digits."""
     from raymotion_b200.scenes import PLAIN_FLAGS
 
     from . import kat_scenes as K
@@ -377,11 +378,7 @@ def test_adjoint_on_a_textured_scene_matches_fp64_central_differences(backend, o
     n_mat = int(tm.max()) + 1
     params = np.stack([t[k][::2] for k in ("ar", "ag", "ab", "rough", "er", "eg", "eb", "ior")], 1).astype(np.float32)
     mask = np.zeros((n_mat, 8), bool)
-    mask[:, 0:3] = True
-    # roughness of the opaque quads; the thin rough dielectric quad's
-    # roughness derivative is an open item (see above), the closed
-    # dielectrics of the inverse scenes check it
-    mask[params[:, 7] <= 1.0001, 3] = True
+    mask[:, 0:4] = True
     mask[params[:, 4:7].max(1) > 0, 4:7] = True
     mask[params[:, 7] > 1.0001, 7] = True
     d = dict(scene=sc, tri_material=tm, params=params, camera=cam, config=cfg)
@@ -401,7 +398,7 @@ def test_adjoint_on_a_textured_scene_matches_fp64_central_differences(backend, o
     def loss(q):
         return np.mean((oracle.render_frozen(sc, cam, cfg, seed, tm, q) - T) ** 2)
 
-    fd = {(m, col): central_difference(loss, prm, m, col) for m, col in zip(*np.nonzero(mask))}
+    fd = {(m, col): central_difference(loss, prm, m, col, 1e-5) for m, col in zip(*np.nonzero(mask))}
     significant = 0
     for cols in ([0, 1, 2], [3], [4, 5, 6], [7]):
         rows = [(k, f) for k, f in fd.items() if k[1] in cols]
