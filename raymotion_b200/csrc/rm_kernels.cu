@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(256) k_render_paths(Scene s, Params p, uint64_
 __device__ __forceinline__ int gkind(const GBufSoA& g, uint32_t i) { return __float_as_int(g.pos_kind[i].w); }
 
 // K3 restir_generate (pathtrace.metal:817-917)
-__global__ void __launch_bounds__(256) k_restir_generate(Scene s, Params p, uint64_t seed, GBufSoA gb, ResSoA ri,
+__global__ void __launch_bounds__(128, 8) k_restir_generate(Scene s, Params p, uint64_t seed, GBufSoA gb, ResSoA ri,
                                                          unsigned long long* ctr, uint32_t* err) {
   const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t npix = uint32_t(p.width) * uint32_t(p.height);
@@ -664,7 +664,7 @@ cudaError_t launch_restir_stage(int stage, const Scene& s, const Params& p, uint
                                 uint32_t* dbg, unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
   const uint64_t npix = uint64_t(p.width) * uint64_t(p.height);
   const unsigned g = blocks_for(npix, 256);
-  if (stage == 0) k_restir_generate<<<g, 256, 0, st>>>(s, p, seed, gb, ri, ctr, err);
+  if (stage == 0) k_restir_generate<<<blocks_for(npix, 128), 128, 0, st>>>(s, p, seed, gb, ri, ctr, err);
   else if (stage == 1) k_restir_spatial<<<g, 256, 0, st>>>(s, p, seed, gb, ri, rm, hg, hr, ctr, err);
   else k_restir_shade<<<g, 256, 0, st>>>(s, p, seed, gb, rm, hdr, dbg, ctr, err);
   return cudaGetLastError();
