@@ -495,9 +495,11 @@ cudaError_t build_lbvh(const rm_triangle* d_tris, int n, int leaf_max, DevBvh& b
 cudaError_t build_lbvh_into(const rm_triangle* d_tris, int n, int leaf_max, const LbvhScratch& w, DevBvhView& out,
                             cudaStream_t st, std::string& err) {
   out.n_records = 0;
+  // The error word lives in scratch shared by every call: clear it before any
+  // early return, or an empty scene would report the last call's overflow.
+  RM_TRY(cudaMemsetAsync(w.err_word, 0, sizeof(uint32_t), st));
   if (n <= 0) return cudaSuccess;
   leaf_max = std::max(1, std::min(leaf_max, kMaxLeaf));
-  RM_TRY(cudaMemsetAsync(w.err_word, 0, sizeof(uint32_t), st));
   if (n <= leaf_max) {
     k_single_leaf<<<1, 1, 0, st>>>(d_tris, n, w.records, w.parents, w.order);
     RM_TRY(cudaGetLastError());
