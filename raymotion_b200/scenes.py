@@ -79,7 +79,9 @@ def cornell_box(seed: int = 0):
           normal=(0, -1, 0), albedo=(0.78, 0.78, 0.78), emission=(17, 12, 4))
     cj = rng.uniform(-0.05, 0.05, size=3)
     cam = Camera().set((cj[0], 1.0 + cj[1], -2.2 + cj[2]), (0, 0, 0), 106)
-    cfg = RenderConfig(width=320, height=180, spp=16, max_bounces=8, restir_candidates=1, restir_spatial=0)
+    # config 0 as stated: NEE + MIS, Russian roulette off (the reference always applies it; RM_FLAG_NO_RR)
+    cfg = RenderConfig(width=320, height=180, spp=16, max_bounces=8, restir_candidates=1, restir_spatial=0,
+                       flags=_abi.RM_FLAG_NO_RR)
     return sb, cam, cfg
 
 
