@@ -33,20 +33,31 @@ def build_oracle() -> Path:
     return ORACLE_SO
 
 
-def build_ref(ref_root: str = "/root/reference") -> Path | None:
+def reference_root() -> Path | None:
+    """The reference checkout that oracle/Makefile.ref reads (the environment
+    variable RAYMOTION_REFERENCE overrides the recipe's default), or None when
+    it is absent, as on a machine without the checkout."""
+    r = subprocess.run(["make", "-s", "-f", str(HERE / "Makefile.ref"), "print-ref"], capture_output=True, text=True)
+    root = r.stdout.strip() if r.returncode == 0 else ""
+    return Path(root) if root and Path(root, "src/engine/bvh.cpp").exists() else None
+
+
+def build_ref(ref_root: str | None = None) -> Path | None:
     """Compile libref.so from the reference checkout when it is present."""
-    if not Path(ref_root, "src/engine/bvh.cpp").exists():
+    root = Path(ref_root) if ref_root else reference_root()
+    if root is None or not Path(root, "src/engine/bvh.cpp").exists():
         return REF_SO if REF_SO.exists() else None
-    subprocess.run(["make", "-s", "-f", str(HERE / "Makefile.ref"), f"REF={ref_root}"], check=True)
+    subprocess.run(["make", "-s", "-f", str(HERE / "Makefile.ref"), f"REF={root}"], check=True)
     return REF_SO
 
 
-def build_dropin(ref_root: str = "/root/reference") -> bool:
+def build_dropin(ref_root: str | None = None) -> bool:
     """Build the reference's own test_metal / test_alpha against librmcuda.so
     (the drop-in check) when the reference checkout is present."""
-    if not Path(ref_root, "tests/test_metal.cpp").exists():
+    root = Path(ref_root) if ref_root else reference_root()
+    if root is None or not Path(root, "tests/test_metal.cpp").exists():
         return False
-    subprocess.run(["make", "-s", "-f", str(HERE / "Makefile.ref"), f"REF={ref_root}", "dropin"], check=True)
+    subprocess.run(["make", "-s", "-f", str(HERE / "Makefile.ref"), f"REF={root}", "dropin"], check=True)
     return True
 
 
