@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-step-seconds", type=float, default=None,
+                    help="--impl reference: CPU seconds per step (default: about a minute over all steps)")
     ap.add_argument("--no-breakdown", action="store_true", help="skip the per-kernel timing frame")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-serial measurement")
     ap.add_argument("--batch-scenes", type=int, default=64)
@@ -167,6 +169,22 @@ def ncu_traffic(kernel: str) -> float | None:
         return None
 
 
+def rank_launch_command(argv: list[str], n: int, port: int) -> list[str]:
+    """torch.distributed.run over n local ranks, rendezvous on 127.0.0.1, running
+    this file with the same arguments (one process per GPU)."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+            "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *argv]
+
+
+def launch_ranks(args, argv: list[str]) -> int:
+    """bench.py --gpus N started without a launcher: start the N ranks here."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    return subprocess.run(rank_launch_command(argv, args.gpus, port)).returncode
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -223,7 +241,7 @@ def run_reference(args, world, rank):
     if rank != 0:
         return 0
     scene, cam, cfg, desc = workload(args.workload)
-    per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    per_step = args.ref_step_seconds or max(2.0, 60.0 / max(1, args.steps + args.warmup))
     _, _, threads, rows, _ = cpu_band(scene, cam, cfg, per_step)
     for _ in range(args.warmup):
         cpu_band(scene, cam, cfg, per_step, rows_hint=rows)
@@ -259,7 +277,13 @@ def batch_compare(args, backend, torch, stream, dev, world):
     images bit for bit (checked), so their relMSE is equal."""
     from raymotion_b200 import BatchItem
     from raymotion_b200.scenes import batch_workload, sized_field
-    specs = batch_workload(seed=3, n_scenes=args.batch_scenes)
+    from raymotion_b200.shard import rank_items
+    all_specs = batch_workload(seed=3, n_scenes=args.batch_scenes)
+    # with several ranks each renders a disjoint, cost-balanced subset of the
+    # images (no data-path collective); one rank renders them all
+    rank = int(os.environ.get("RANK", "0")) if world > 1 else 0
+    mine = rank_items(all_specs, rank, world)
+    specs = [all_specs[i] for i in mine]
     t0 = time.time()
     items, hdrs, handles = [], [], []
     for sp in specs:
@@ -305,18 +329,23 @@ def batch_compare(args, backend, torch, stream, dev, world):
     identical = all(torch.equal(h.view(torch.int32), r.view(torch.int32)) for (_, h), r in zip(hdrs, ref))
     s_sec, s_samples = timed(serial)
     b_sec, b_samples = timed(batched)
+    s_own, = allreduce([float(sum(r[1].numel() for r in hdrs))], "sum", world, dev)  # every image rendered once
+    identical, = allreduce([1.0 if identical else 0.0], "sum", world, dev)
     log = backend.batch_log()
     for h in handles:
         backend.scene_destroy(h)
     return dict(
-        workload=f"{len(specs)} seeded icosphere-field scenes, triangles log-uniform in [1k, 2M], resolutions "
+        workload=f"{len(all_specs)} seeded icosphere-field scenes, triangles log-uniform in [1k, 2M], resolutions "
                  "{256x256, 640x360, 1280x720, 1920x1080}, spp {4, 16, 64}, depth 8-12, plain path",
-        triangles=int(sum(sp["n_tris"] for sp in specs)), pixels=int(sum(sp["width"] * sp["height"] for sp in specs)),
+        triangles=int(sum(sp["n_tris"] for sp in all_specs)),
+        pixels=int(sum(sp["width"] * sp["height"] for sp in all_specs)),
+        sharding=dict(ranks=world, images_per_rank=len(mine), rank0_images=mine if rank == 0 else None,
+                      pixels_rendered=int(s_own / 3), collective="none (timings and counts reduced only)"),
         steps=args.batch_steps, path_samples_per_step=int(b_samples / args.batch_steps),
         serial=dict(value=s_samples / s_sec, unit=UNIT, ms_per_step=1e3 * s_sec / args.batch_steps),
         batched=dict(value=b_samples / b_sec, unit=UNIT, ms_per_step=1e3 * b_sec / args.batch_steps,
                      tuning=tuning, progress_checks=int(len(log))),
-        speedup=(b_samples / b_sec) / (s_samples / s_sec), identical_images=bool(identical),
+        speedup=(b_samples / b_sec) / (s_samples / s_sec), identical_images=bool(identical == world),
         equal_samples=bool(s_samples == b_samples), scene_build_s=build_s, tune_s=tune_s)
 
 
@@ -507,12 +536,16 @@ def sequence_measure(args, backend, torch, stream, dev):
         r["model"] = np.asarray(ids, np.int32)[r["model"]]
     npix = cfg.width * cfg.height
     d_rgb = torch.empty(npix * 3, dtype=torch.uint8, device=dev)
-    # warm-up: the first frames of the sequence, once
+    # warm-up: the first frames of the sequence rendered once, then commits up
+    # to the next multiple of 32, so that the timed frames follow the
+    # reference's schedule from frame 0 (runtime.hpp:124-125: a build whenever
+    # geometry_updates % 32 == 0): build, 31 refits, build, refit
     backend.reset_history()
-    for f in range(2):
-        backend.model_update(ids[seq.CLOTH], cloth[f])
-        backend.instances_commit(recs[f], rebuild_every=32)
-        backend.render_resident_async(cams[f], cfg, 12345 + f, d_rgb.data_ptr())
+    for f in range(32):
+        backend.model_update(ids[seq.CLOTH], cloth[f % seq.frames])
+        backend.instances_commit(recs[f % seq.frames], rebuild_every=32)
+        if f < 2:
+            backend.render_resident_async(cams[f], cfg, 12345 + f, d_rgb.data_ptr())
     backend.sync()
     backend.reset_history()
     backend.stats_reset()
@@ -719,6 +752,11 @@ def run_b200(args, world, rank, local):
     dom = max(kernel_stages, key=lambda k: kernel_stages[k][0])
     ms_total, launches = kern_t[dom]
     c = kern_c[dom]
+    # one launch per wave traverses extension and shadow rays (k_wf_trace2):
+    # its time is the extension stage's, its shadow rays' counters sit apart
+    merged_trace = kern_t["wf_extend"][1] > 0 and kern_t["wf_shadow"][1] == 0
+    if dom == "wf_extend" and merged_trace:
+        c = {k: kern_c["wf_extend"][k] + kern_c["wf_shadow"][k] for k in c}
     if dom == "shade" and not c["nodes_visited"] and kern_c["wf_extend"]["nodes_visited"]:
         # without the per-launch breakdown the wavefront loop is timed as one
         # stage; its traversal counters sit with its traversal kernels
@@ -731,12 +769,17 @@ def run_b200(args, world, rank, local):
     achieved = alg_bytes / avg_s / 1e9 if avg_s > 0 else 0.0
     kernel_names = dict(plain="k_render_paths", shade="k_restir_shade", generate="k_restir_generate",
                         spatial="k_restir_spatial", temporal="k_denoise_temporal", atrous0="k_denoise_atrous",
-                        atrous1="k_denoise_atrous", hash="k_hash", tonemap="k_tonemap", wf_extend="k_wf_extend",
+                        atrous1="k_denoise_atrous", hash="k_hash", tonemap="k_tonemap",
+                        wf_extend="k_wf_trace2" if merged_trace else "k_wf_extend",
                         wf_shadow="k_wf_shadow", wf_shade="k_wf_shade", wf_tail="k_wf_tail",
                         **{"wavefront shading loop": "k_wf_init + k_wf_trace + k_wf_shade (one stage)"})
     roofline = dict(bound="hbm", kernel=kernel_names.get(dom, dom), achieved=achieved, peak=peak["hbm_gbs"],
                     unit="GB/s", frac=achieved / peak["hbm_gbs"], traffic=ncu_traffic(kernel_names.get(dom, dom)),
                     peak_source=peak["source"],
+                    mrays_per_s=c["rays"] / (ms_total * 1e3) if ms_total > 0 else None,
+                    limiter=("traversal: latency and divergence of incoherent rays, fed from L1/L2 (DRAM a few per "
+                             "cent busy); the HBM fraction is the rate at which node and triangle records are "
+                             "fetched" if c["nodes_visited"] else "hbm"),
                     note=f"achieved = ({node_bytes} B x BVH nodes fetched + 48 B x triangle tests) per launch / "
                          "average launch time; most of these bytes hit L1/L2")
     # screen-space passes (temporal 92 B/px, two a-trous 64 B/px each, fused tonemap write 3 B/px):
@@ -760,6 +803,12 @@ def run_b200(args, world, rank, local):
         if rc.get("rays"):
             e.update(rays=rc["rays"], nodes_per_ray=rc["nodes_visited"] / rc["rays"],
                      tests_per_ray=rc["tris_tested"] / rc["rays"], mrays_per_s=rc["rays"] / (v[0] * 1e3))
+        if k == "wf_extend" and merged_trace:
+            # extension and shadow rays of one launch per wave
+            rs = kern_c["wf_shadow"]
+            e.update(kernel="k_wf_trace2 (extension + shadow rays)", shadow_rays=rs["rays"],
+                     shadow_nodes_per_ray=rs["nodes_visited"] / max(rs["rays"], 1),
+                     mrays_per_s_both=(rc["rays"] + rs["rays"]) / (v[0] * 1e3))
         kernel_summary[k] = e
     ss_large = None if args.no_large else screen_space_large(backend, torch, cam, cfg, dev, seed0 + 300, peak)
     # ---- end to end through rmcuda_render with host buffers
@@ -819,6 +868,12 @@ def run_b200(args, world, rank, local):
 
 def main():
     args = parse()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        return launch_ranks(args, sys.argv[1:])
+    if int(os.environ.get("WORLD_SIZE", "1")) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={os.environ.get('WORLD_SIZE')} ranks were started",
+              file=sys.stderr)
+        return 2
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":
