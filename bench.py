@@ -330,6 +330,18 @@ def batch_compare(args, backend, torch, stream, dev, world):
     s_sec, s_samples = timed(serial)
     b_sec, b_samples = timed(batched)
     s_own, = allreduce([float(sum(r[1].numel() for r in hdrs))], "sum", world, dev)  # every image rendered once
+    # per-scene relMSE against the FP64 references (the batched images; the
+    # serial ones are identical, checked above)
+    rel = []
+    g = ROOT / "tests" / "golden" / "relmse_batch.npz"
+    if g.exists() and len(all_specs) == 64:
+        ref = np.load(g)
+        for k, gi in enumerate(mine):
+            sel = ref["scene"] == gi
+            img = hdrs[k][1].cpu().numpy().reshape(-1, 3)[ref["pixels"][sel]].astype(np.float64)
+            rel.append(_relmse(img, ref["ref"][sel]))
+    rel_sum, rel_n, rel_max = allreduce([float(sum(rel)), float(len(rel))], "sum", world, dev) + \
+        allreduce([max(rel) if rel else 0.0], "max", world, dev)
     identical, = allreduce([1.0 if identical else 0.0], "sum", world, dev)
     log = backend.batch_log()
     for h in handles:
@@ -346,6 +358,9 @@ def batch_compare(args, backend, torch, stream, dev, world):
         batched=dict(value=b_samples / b_sec, unit=UNIT, ms_per_step=1e3 * b_sec / args.batch_steps,
                      tuning=tuning, progress_checks=int(len(log))),
         speedup=(b_samples / b_sec) / (s_samples / s_sec), identical_images=bool(identical == world),
+        relmse=dict(scenes=int(rel_n), pixels_per_scene=256, ref_spp=8192, mean=rel_sum / rel_n, max=rel_max,
+                    rank0_per_scene=[round(x, 5) for x in rel] if rank == 0 else None,
+                    note="batched = serial per scene (identical images)") if rel_n else None,
         equal_samples=bool(s_samples == b_samples), scene_build_s=build_s, tune_s=tune_s)
 
 
@@ -469,6 +484,11 @@ def adjoint_measure(args, backend, torch, stream, dev, rank=0, world=1):
     start = torch.where(mask, torch.minimum(torch.maximum(true * (1 + noise), lo), hi), true)
     fit = MaterialFit(start, true, mask, lo, hi, lr=1e-2)
     seen_t = torch.from_numpy(seen).to(dev)[:, None] & mask
+    # metallic materials (their roughness shapes the whole lobe; a dielectric-free
+    # non-metal's roughness only shapes its 4 % specular part)
+    metal = np.zeros(n_mat, bool)
+    np.logical_or.at(metal, tm, sc.tris["metallic"] > 0.5)
+    metal_t = torch.from_numpy(metal).to(dev)
 
     def errors(p):
         e = (p - true).abs() / (hi - lo)
@@ -477,6 +497,11 @@ def adjoint_measure(args, backend, torch, stream, dev, rank=0, world=1):
                            ("ior", slice(7, 8))):
             mk = mask[:, cols]
             out[name] = e[:, cols][mk].mean().item() if mk.any() else None
+            ms = mk & seen_t[:, cols]
+            out[name + "_seen"] = e[:, cols][ms].mean().item() if ms.any() else None
+        for name, sel in (("rough_seen_metal", metal_t), ("rough_seen_nonmetal", ~metal_t)):
+            ms = mask[:, 3] & seen_t[:, 3] & sel
+            out[name] = e[:, 3][ms].mean().item() if ms.any() else None
         return out
 
     err0 = errors(start)
@@ -499,6 +524,20 @@ def adjoint_measure(args, backend, torch, stream, dev, rank=0, world=1):
     torch.cuda.synchronize()
     fit_s = time.time() - t0
     err1 = errors(fit.params())
+    # image-space recovery: the start and fitted materials rendered at the
+    # target's 1024 spp (another seed), relMSE against the target
+    img_rel = {}
+    for name, prm in (("start", start), ("fitted", fit.params())):
+        set_params(prm.cpu().numpy())
+        backend.render_scene_async(h, cam, cfg_t, 2, None, img.data_ptr())
+        backend.sync()
+        a = img.cpu().numpy().astype(np.float64)
+        b = target.cpu().numpy().astype(np.float64)
+        img_rel[name] = _relmse(a, b)
+    set_params(d["params"])
+    backend.render_scene_async(h, cam, cfg_t, 2, None, img.data_ptr())
+    backend.sync()
+    img_rel["true_other_seed"] = _relmse(img.cpu().numpy().astype(np.float64), target.cpu().numpy().astype(np.float64))
     backend.scene_destroy(h)
     loss_curve = [float(x) for x in torch.stack(losses).cpu().numpy()]
     return dict(
@@ -509,6 +548,7 @@ def adjoint_measure(args, backend, torch, stream, dev, rank=0, world=1):
         fit=dict(iterations=args.fit_iters, lr=1e-2, optimiser="Adam on normalised parameters",
                  target_spp=1024, fit_spp=cfg.spp, ranks=world, wall_s=fit_s, gpu_ms=f0.elapsed_time(f1),
                  param_error_start=err0, param_error_end=err1, materials_seen=int(seen.sum()),
+                 relmse_1024spp_vs_target=img_rel,
                  loss_first10=float(np.mean(loss_curve[:10])), loss_last10=float(np.mean(loss_curve[-10:]))))
 
 
@@ -536,6 +576,7 @@ def sequence_measure(args, backend, torch, stream, dev):
         r["model"] = np.asarray(ids, np.int32)[r["model"]]
     npix = cfg.width * cfg.height
     d_rgb = torch.empty(npix * 3, dtype=torch.uint8, device=dev)
+    d_hdr = torch.empty(npix * 3, dtype=torch.float32, device=dev)  # the last frame's radiance (relMSE)
     # warm-up: the first frames of the sequence rendered once, then commits up
     # to the next multiple of 32, so that the timed frames follow the
     # reference's schedule from frame 0 (runtime.hpp:124-125: a build whenever
@@ -558,7 +599,8 @@ def sequence_measure(args, backend, torch, stream, dev):
     for f in range(seq.frames):
         backend.model_update(ids[seq.CLOTH], cloth[f])
         backend.instances_commit(recs[f], rebuild_every=32)
-        backend.render_resident_async(cams[f], cfg, 12345 + f, d_rgb.data_ptr())
+        last = f == seq.frames - 1
+        backend.render_resident_async(cams[f], cfg, 12345 + f, d_rgb.data_ptr(), d_hdr.data_ptr() if last else None)
     e1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
@@ -568,6 +610,13 @@ def sequence_measure(args, backend, torch, stream, dev):
     backend.profile(0)
     samples = st["path_samples"]
     render_ms = sum(v[0] for k, v in t.items() if k not in ("prep", "batch", "adjoint"))
+    relmse = None
+    g = ROOT / "tests" / "golden" / "relmse_sequence33.npz"
+    if g.exists() and seq.frames == 34:
+        ref = np.load(g)
+        img = d_hdr.cpu().numpy().reshape(-1, 3)[ref["pixels"]].astype(np.float64)
+        relmse = dict(frame=33, pixels=int(len(ref["pixels"])), ref_spp=int(ref["spp"]), spp=cfg.spp,
+                      denoised=_relmse(img, ref["ref"]))
     return dict(workload=f"animated sequence: {seq.frames} frames at {seq.fps} fps, {cfg.width}x{cfg.height}, "
                          f"{cfg.spp} spp, depth {cfg.max_bounces}, {seq.n_tris:,} triangles ({len(seq.moving)} moving "
                          f"spheres, {len(cloth[0]):,}-triangle cloth), camera orbit {seq.orbit_deg} deg/frame, temporal "
@@ -576,7 +625,7 @@ def sequence_measure(args, backend, torch, stream, dev):
                 wall_ms_per_frame=1e3 * wall / seq.frames, prep_ms_per_frame=t["prep"][0] / seq.frames,
                 render_ms_per_frame=render_ms / seq.frames, bvh_builds=st["bvh_builds"] - st0["bvh_builds"],
                 bvh_refits=st["bvh_refits"] - st0["bvh_refits"], h2d_bytes_per_frame=int(cloth[0].nbytes + recs[0].nbytes),
-                path_samples=int(samples))
+                path_samples=int(samples), relmse=relmse)
 
 
 def _relmse(img, ref):
