@@ -407,7 +407,8 @@ int rmcuda_stats_reset(rmcuda_ctx* ctx);
 #define RM_STAGE_ATROUS0 6   /* a-trous stride 1 */
 #define RM_STAGE_ATROUS1 7   /* a-trous stride 2 + tonemap */
 #define RM_STAGE_TONEMAP 8   /* tonemap alone (denoiser off) */
-#define RM_STAGE_WF_EXTEND 9 /* wavefront shading: closest-hit traversal waves */
+#define RM_STAGE_WF_EXTEND 9 /* wavefront shading: traversal waves (extension rays, and the shadow rays
+                                 when one launch traverses both; their counters stay in WF_SHADOW) */
 #define RM_STAGE_WF_SHADOW 10 /* wavefront shading: shadow-ray traversal waves */
 #define RM_STAGE_WF_SHADE 11 /* wavefront shading: shading waves (incl. the first) */
 #define RM_STAGE_BT_START 12  /* batched rendering: tile refill + sample starts */
@@ -416,7 +417,7 @@ int rmcuda_stats_reset(rmcuda_ctx* ctx);
 #define RM_STAGE_BT_SHADE 15  /* batched rendering: shading */
 #define RM_STAGE_BATCH 16     /* batched rendering: a whole rmcuda_render_batch call */
 #define RM_STAGE_ADJOINT 17   /* path-replay adjoint (rmcuda_backward) */
-#define RM_STAGE_WF_TAIL 18   /* wavefront shading: the last paths, one thread per pixel */
+#define RM_STAGE_WF_TAIL 18   /* wavefront shading: the last paths (with their traversals' counters) */
 #define RM_STAGE_PREP 19      /* rmcuda_instances_commit: world triangles and BVH refit / build */
 #define RM_STAGE_COUNT 20
 /* level 0: off; 1: one event pair per stage (the wavefront shading loop counts

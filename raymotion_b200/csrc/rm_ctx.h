@@ -63,6 +63,16 @@ struct DevScene {
   // the texel count the resident triangles were last checked against by
   // upload_scene (texture ranges, opacity); -1 after any other write
   long long validated_texels = -1;
+  // host copies of the last upload's light list, CDF, light total and texels,
+  // and whether that upload's triangles equalled the resident ones: what a
+  // speculative frame (rmcuda_render) needs to know the next upload's small
+  // arrays unchanged without sending them
+  std::vector<int32_t> h_lights;
+  std::vector<float> h_cdf;
+  std::vector<rm_vec3> h_texels;
+  float h_light_total = 0;
+  bool h_valid = false;
+  bool last_upload_equal = false;
   // per-triangle materials (rmcuda_scene_set_materials): index per triangle,
   // 8 parameters per material
   DevBuf tri_mat, mats;
@@ -121,6 +131,14 @@ struct rmcuda_ctx {
   rmapi::ResSet rinit, rmerged, hres;
   rmd::DevBuf hdr, tmp_a, tmp_b, hist_col, rgb, dbg, hash_out;
   rmd::DevBuf ctr, err;
+  // speculative frames of rmcuda_render: the copy stream that uploads and
+  // compares the triangles while the frame renders, its pinned result, a copy
+  // of the counters to restore, and the configuration of the last frame
+  cudaStream_t copy_stream = nullptr;
+  rmd::DevBuf differ, ctr_save;
+  int* h_differ = nullptr;
+  rm_config last_cfg{};
+  bool have_last_cfg = false;
   // temporal history (metal.mm:35-40)
   rm_camera hist_cam{};
   int hist_w = 0, hist_h = 0;

@@ -125,6 +125,20 @@ struct Rng {
   }
 };
 
+// The state k draws after `state`: the generator's step s -> a s + c (mod
+// 2^32) composed k times, by squaring (k < 2^8).
+__device__ __forceinline__ uint32_t rng_jump(uint32_t state, uint32_t k) {
+  uint32_t a = 747796405u, c = 2891336453u, A = 1u, C = 0u;
+#pragma unroll
+  for (int bit = 0; bit < 8; ++bit) {
+    if (k & 1u) { A = A * a; C = C * a + c; }
+    c = c * a + c;
+    a = a * a;
+    k >>= 1;
+  }
+  return A * state + C;
+}
+
 __device__ __forceinline__ uint64_t seed_pixel(uint64_t seed, uint32_t x, uint32_t y) {
   return seed ^ (uint64_t(y + 1) * 0x9E3779B97F4A7C15ull) ^ (uint64_t(x + 1) * 0xBF58476D1CE4E5B9ull);
 }
@@ -311,13 +325,20 @@ struct Trav {
   template <bool kAnyHit>
   __device__ __forceinline__ bool step(const Scene& s, int* stack, uint32_t* err, uint32_t& n_nodes,
                                        uint32_t& n_tests) {
+    return step_rt(s, stack, err, n_nodes, n_tests, kAnyHit);
+  }
+
+  // step() with the any-hit rule as a run-time flag: lanes of one warp that
+  // trace closest-hit and any-hit rays then run the same instructions.
+  __device__ __forceinline__ bool step_rt(const Scene& s, int* stack, uint32_t* err, uint32_t& n_nodes,
+                                          uint32_t& n_tests, bool any_hit) {
     if (s.n_nodes == 0) return true;
     while (node >= 0 && leaf_count == 0)
       if (visit(s, stack, err, n_nodes)) return true;
     // leaf: Moller-Trumbore, pathtrace.metal:150-158
     n_tests += uint32_t(leaf_count);
     for (int k = 0; k < leaf_count; ++k)
-      if (test_triangle(s.tgeo + size_t(leaf_first + k) * 3, ox, oy, oz, dx, dy, dz, r) && kAnyHit) return true;
+      if (test_triangle(s.tgeo + size_t(leaf_first + k) * 3, ox, oy, oz, dx, dy, dz, r) && any_hit) return true;
     leaf_count = 0;
     return pop(stack);
   }
@@ -475,6 +496,19 @@ __device__ __forceinline__ TraceResult traverse(const Scene& s, float ox, float 
   int stack[kStack];
   t.init(ox, oy, oz, dx, dy, dz, tmax);
   while (!t.step<kAnyHit>(s, stack, err, n_nodes, n_tests)) {
+  }
+  return t.r;
+}
+
+// traverse() with the any-hit rule as a run-time flag (one instruction stream
+// for the closest-hit and any-hit rays of a warp).
+__device__ __forceinline__ TraceResult traverse_rt(const Scene& s, float ox, float oy, float oz, float dx, float dy,
+                                                   float dz, float tmax, bool any_hit, uint32_t* err,
+                                                   uint32_t& n_nodes, uint32_t& n_tests) {
+  Trav t;
+  int stack[kStack];
+  t.init(ox, oy, oz, dx, dy, dz, tmax);
+  while (!t.step_rt(s, stack, err, n_nodes, n_tests, any_hit)) {
   }
   return t.r;
 }
@@ -1052,6 +1086,117 @@ struct Tracer {
     o_b = sel_Fb * W * wnee;
     // the selected light and the factor k of o = Le * f * k (held by the adjoint)
     if (parts) { parts[0] = __int_as_float(sel_li); parts[1] = sel_sa * W * wnee; }
+  }
+
+  // direct_lighting_deferred with its Mc candidates spread over the lanes of
+  // the calling warp (pathtrace.metal:385-469).  Every lane of the warp calls
+  // it with the same arguments and the same random state, and every lane
+  // returns the same results.  A candidate takes exactly four draws (light
+  // pick, two barycentrics, the reservoir's acceptance draw), so lane j
+  // starts at draw 4j of the stream: a jump of the generator's state.  Each
+  // lane evaluates its candidate with the loop body's arithmetic, and every
+  // lane then forms the reservoir's running sum and acceptance tests in
+  // candidate order from the lanes' weights, as the loop does: the selection,
+  // the sums and the state after the last draw are bit-identical.
+  __device__ void direct_lighting_deferred_warp(float px, float py, float pz, float nx, float ny, float nz, float wox,
+                                                float woy, float woz, float rough, float metallic, float spec_prob,
+                                                float ar, float ag, float ab, float& o_r, float& o_g, float& o_b,
+                                                float& out_sumW, uint32_t& out_M, bool& has_ray, float& sox,
+                                                float& soy, float& soz, float& sdx, float& sdy, float& sdz,
+                                                float& sdist) {
+    o_r = o_g = o_b = 0.0f;
+    out_sumW = 0.0f;
+    out_M = 0;
+    has_ray = false;
+    if (p.lights == 0 || !(p.light_total > 1e-12f)) return;
+    int Mc = p.restir_candidates;
+    if (Mc < 1) Mc = 1;
+    if (Mc > 32) Mc = 32;
+    if (Mc <= 1) {
+      nee_single_deferred(px, py, pz, nx, ny, nz, wox, woy, woz, rough, metallic, spec_prob, ar, ag, ab, o_r, o_g,
+                          o_b, out_sumW, out_M, has_ray, sox, soy, soz, sdx, sdy, sdz, sdist);
+      return;
+    }
+    float r2 = rough;
+    if (r2 < 0.0f) r2 = 0.0f;
+    if (r2 > 1.0f) r2 = 1.0f;
+    if (r2 < 0.02f) r2 = 0.02f;
+    float alpha2 = (r2 * r2) * (r2 * r2);
+    const float LT = p.light_total;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t s0 = rng.state;
+    float w = 0, ph = 0, epdf = 0, Fr = 0, Fg = 0, Fb = 0, qx = 0, qy = 0, qz = 0, racc = 0;
+    if (int(lane) < Mc) {
+      Rng lr;
+      lr.state = rng_jump(s0, 4u * lane);
+      const BsdfPrep bp = prep_bsdf(wox, woy, woz, nx, ny, nz, alpha2, metallic, ar, ag, ab);
+      float pick = lr.uniform01() * LT;
+      const int li = pick_light(pick);
+      const LightRec t = load_light(s, li);
+      float lu = lr.uniform01(), lv = lr.uniform01();
+      if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
+      float lw = 1.0f - lu - lv;
+      qx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x);
+      qy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y);
+      qz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z);
+      float ldx = qx - px, ldy = qy - py, ldz = qz - pz;
+      float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
+      if (dist > 0.003f) {
+        float inv = 1.0f / dist;
+        float dxn = ldx * inv, dyn = ldy * inv, dzn = ldz * inv;
+        float lcos = -(t.nn.x * dxn + (t.nn.y * dyn + t.nn.z * dzn));
+        float scos = nx * dxn + (ny * dyn + nz * dzn);
+        if (lcos > 1e-8f && scos > 1e-8f) {
+          float lt_lum = lum3(t.er, t.eg, t.eb);
+          if (lt_lum < 1e-6f) lt_lum = 1e-6f;
+          float q = dist * dist * lt_lum / (lcos * LT);
+          if (q > 1e-12f) {
+            Bsdf e = eval_bsdf_prep(bp, dxn, dyn, dzn, wox, woy, woz, nx, ny, nz, alpha2, spec_prob);
+            epdf = e.pdf;
+            Fr = t.er * e.r * scos * t.alpha;
+            Fg = t.eg * e.g * scos * t.alpha;
+            Fb = t.eb * e.b * scos * t.alpha;
+            ph = lum3(Fr, Fg, Fb);
+            if (ph > 0.0f) w = ph / q;
+          }
+        }
+      }
+      racc = lr.uniform01();
+    }
+    rng.state = rng_jump(s0, 4u * uint32_t(Mc));
+    // the reservoir in candidate order, on every lane
+    float sumW = 0.0f;
+    int sel = -1;
+    for (int j = 0; j < Mc; ++j) {
+      const float wj = __shfl_sync(0xffffffffu, w, j);
+      const float rj = __shfl_sync(0xffffffffu, racc, j);
+      sumW += wj;
+      if (wj > 0.0f && rj * sumW < wj) sel = j;
+    }
+    out_sumW = sumW;
+    out_M = uint32_t(Mc);
+    if (sel < 0) return;
+    const float sel_lx = __shfl_sync(0xffffffffu, qx, sel), sel_ly = __shfl_sync(0xffffffffu, qy, sel),
+                sel_lz = __shfl_sync(0xffffffffu, qz, sel);
+    const float sel_Fr = __shfl_sync(0xffffffffu, Fr, sel), sel_Fg = __shfl_sync(0xffffffffu, Fg, sel),
+                sel_Fb = __shfl_sync(0xffffffffu, Fb, sel);
+    const float sel_phat = __shfl_sync(0xffffffffu, ph, sel), sel_epdf = __shfl_sync(0xffffffffu, epdf, sel);
+    if (!(sumW > 0.0f) || !(sel_phat > 0.0f)) return;
+    float pdf_ris = float(Mc) * sel_phat / sumW;
+    float wnee = 1.0f;
+    if (!p.nomis && sel_epdf > 1e-20f) wnee = pdf_ris / (pdf_ris + sel_epdf);
+    float vdx = sel_lx - px, vdy = sel_ly - py, vdz = sel_lz - pz;
+    float vdist = sqrtf(vdx * vdx + vdy * vdy + vdz * vdz);
+    if (!(vdist > 0.003f)) return;
+    float vinv = 1.0f / vdist;
+    vdx *= vinv; vdy *= vinv; vdz *= vinv;
+    has_ray = true;
+    sox = px + nx * 0.002f; soy = py + ny * 0.002f; soz = pz + nz * 0.002f;
+    sdx = vdx; sdy = vdy; sdz = vdz; sdist = vdist - 0.003f;
+    float W = sumW / (float(Mc) * sel_phat);
+    o_r = sel_Fr * W * wnee;
+    o_g = sel_Fg * W * wnee;
+    o_b = sel_Fb * W * wnee;
   }
 
   __device__ static __forceinline__ float fresnel(float ci_in, float eta_in, float eta_out) {

@@ -311,6 +311,47 @@ __global__ void __launch_bounds__(128) k_wf_trace(Scene s, WfState w, WfQueues q
   warp_add(ctr + 3, tests);
 }
 
+// Both traversals of a wave in one launch (binary BVH): thread i < n_ext
+// takes extension ray i (closest hit), the next n_shd threads the shadow rays
+// (any hit), with the any-hit rule as a per-thread flag so that the two kinds
+// run one instruction stream.  Each launch's time is set by its slowest rays
+// while most of the GPU idles; in one launch the shadow rays fill that time.
+// ctr_ext / ctr_shd: the counters of each kind.
+__global__ void __launch_bounds__(128) k_wf_trace2(Scene s, WfState w, WfQueues q, unsigned long long* ctr_ext,
+                                                   unsigned long long* ctr_shd, uint32_t* err) {
+  const int n_ext = q.counts[kCntExt], n_shd = q.counts[kCntShd];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t nodes = 0, tests = 0;
+  int cls = -1;
+  int id = 0;
+  const bool shadow = i >= n_ext;
+  const bool live = i < n_ext + n_shd;
+  if (live) {
+    id = shadow ? q.shd[i - n_ext] : q.ext[i];
+    const float4 o = shadow ? w.so[id] : w.o[id];
+    const float4 d = shadow ? w.sd[id] : w.d[id];
+    const TraceResult r = traverse_rt(s, o.x, o.y, o.z, d.x, d.y, d.z, shadow ? o.w : kFar, shadow, err, nodes,
+                                      tests);
+    if (shadow) {
+      w.occ[id] = r.tri >= 0 ? 1u : 0u;
+    } else {
+      w.hit[id] = make_float4(r.t, r.u, r.v, __int_as_float(r.tri));
+      cls = 2;
+      if (r.tri >= 0) cls = __ldg(&s.tris[r.tri].ior) > 1.0001f ? 1 : 0;
+    }
+  }
+  append(q.qa, q.counts + kCntA, cls == 0, id);
+  append(q.qb, q.counts + kCntB, cls == 1, id);
+  append(q.qc, q.counts + kCntC, cls == 2, id);
+  __syncwarp();
+  warp_add(ctr_ext + 1, live && !shadow ? 1u : 0u);
+  warp_add(ctr_ext + 2, shadow ? 0u : nodes);
+  warp_add(ctr_ext + 3, shadow ? 0u : tests);
+  warp_add(ctr_shd + 1, live && shadow ? 1u : 0u);
+  warp_add(ctr_shd + 2, shadow ? nodes : 0u);
+  warp_add(ctr_shd + 3, shadow ? tests : 0u);
+}
+
 // One path of a shading queue: fold in its shadow ray, shade the vertex its
 // extension ray found (VK 0 opaque, 1 dielectric) or end it (VK 2), finish and
 // restart samples; ext / shd / fin tell which queues of the next wave take it.
@@ -391,14 +432,119 @@ __global__ void __launch_bounds__(256) k_wf_shade(Scene s, Params p, GBufSoA gb,
   warp_add(ctr + 0, samples);
 }
 
-// The end of the wavefront loop, once few paths remain: one thread per
-// unfinished pixel runs its path to the end with the steps of the waves, in
-// their order (extension ray, pending shadow ray, shade_path of the vertex
-// type), so the pixel comes out the same, without a launch and a queue round
-// trip per vertex.  ctr: the stage counters of the tail, extension and
-// shadow traversal.  Three 128-thread blocks per SM (up to 168 registers, few
-// spills): the tail is latency-bound, its path count is capped to one wave of
-// resident blocks, and with four blocks the spills cost more (30 vs 27.5 ms).
+// The three shading queues of a wave in one launch: block b serves queue
+// b % 3 (0 opaque hits, 1 dielectric hits, 2 no vertex), so a block's
+// warps take one branch as in k_wf_shade while the three queues' work
+// overlaps instead of running in three launches one after another.
+template <int NEE>
+__global__ void __launch_bounds__(256) k_wf_shade3(Scene s, Params p, GBufSoA gb, WfState w, WfQueues cq,
+                                                   WfQueues nq, float* __restrict__ hdr, uint32_t* __restrict__ dbg,
+                                                   unsigned long long* ctr, uint32_t* err) {
+  const int vk = int(blockIdx.x % 3u);
+  const int i = int(blockIdx.x / 3u) * 256 + int(threadIdx.x);
+  const int count = cq.counts[vk == 0 ? kCntA : (vk == 1 ? kCntB : kCntC)];
+  const int* queue = vk == 0 ? cq.qa : (vk == 1 ? cq.qb : cq.qc);
+  bool ext = false, shd = false, fin = false;
+  int id = 0;
+  uint32_t samples = 0;
+  if (i < count) {
+    id = queue[i];
+    if (vk == 0) shade_path<0, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+    else if (vk == 1) shade_path<1, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+    else shade_path<2, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+  }
+  append(nq.ext, nq.counts + kCntExt, ext, id);
+  append(nq.shd, nq.counts + kCntShd, shd, id);
+  append(nq.qc, nq.counts + kCntC, fin, id);
+  warp_add(ctr + 0, samples);
+}
+
+// One vertex step of a tail pixel, one thread per pixel: its extension ray,
+// its pending shadow ray and shade_path of the vertex type, in the waves'
+// order.  Returns true while the pixel has work left (ext: its next step
+// starts with an extension ray).  cnt: extension rays, nodes, tests; shadow
+// rays, nodes, tests.
+template <int NEE>
+__device__ __forceinline__ bool tail_step(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w, int id,
+                                          bool& ext, float* __restrict__ hdr, uint32_t* __restrict__ dbg,
+                                          uint32_t* err, uint32_t& samples, uint32_t* cnt) {
+  int vk = 2;
+  if (ext) {
+    const float4 o = w.o[id];
+    const float4 d = w.d[id];
+    const TraceResult r = traverse<false>(s, o.x, o.y, o.z, d.x, d.y, d.z, kFar, err, cnt[1], cnt[2]);
+    ++cnt[0];
+    w.hit[id] = make_float4(r.t, r.u, r.v, __int_as_float(r.tri));
+    if (r.tri >= 0) vk = __ldg(&s.tris[r.tri].ior) > 1.0001f ? 1 : 0;
+  }
+  if (w.u[id].y & kShadow) {
+    const float4 o = w.so[id];
+    const float4 d = w.sd[id];
+    const TraceResult r = traverse<true>(s, o.x, o.y, o.z, d.x, d.y, d.z, o.w, err, cnt[4], cnt[5]);
+    ++cnt[3];
+    w.occ[id] = r.tri >= 0 ? 1u : 0u;
+  }
+  bool shd = false, fin = false;
+  ext = false;
+  if (vk == 0) shade_path<0, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+  else if (vk == 1) shade_path<1, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+  else shade_path<2, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
+  return ext || fin;
+}
+
+// A tail pixel run to its end by the whole warp (opaque scenes).  Every lane
+// runs the same steps on the same path, so each lane holds the same state:
+// the shading is executed redundantly, except that the RIS candidates of a
+// vertex are evaluated one per lane (shade_path NEE variant 3), and the
+// extension ray (lanes 0-15) and the pending shadow ray (lanes 16-31) are
+// traversed at the same time, by one instruction stream with the any-hit rule
+// as a flag.  The results are the thread-per-pixel steps' bit for bit.
+__device__ __noinline__ void tail_pixel_warp(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w,
+                                             int id, bool ext, float* __restrict__ hdr, uint32_t* __restrict__ dbg,
+                                             uint32_t* err, uint32_t& samples, uint32_t* cnt) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const bool shadow_half = lane >= 16u;
+  for (;;) {
+    const bool pending_shadow = (w.u[id].y & kShadow) != 0;
+    const bool mine = shadow_half ? pending_shadow : ext;
+    uint32_t nodes = 0, tests = 0;
+    int tri = -1;
+    if (mine) {
+      const float4 o = shadow_half ? w.so[id] : w.o[id];
+      const float4 d = shadow_half ? w.sd[id] : w.d[id];
+      const TraceResult r = traverse_rt(s, o.x, o.y, o.z, d.x, d.y, d.z, shadow_half ? o.w : kFar, shadow_half, err,
+                                        nodes, tests);
+      tri = r.tri;
+      if (lane == 0u) w.hit[id] = make_float4(r.t, r.u, r.v, __int_as_float(r.tri));
+      if (lane == 16u) w.occ[id] = r.tri >= 0 ? 1u : 0u;
+    }
+    if (lane == 0u && ext) { ++cnt[0]; cnt[1] += nodes; cnt[2] += tests; }
+    if (lane == 16u && pending_shadow) { ++cnt[3]; cnt[4] += nodes; cnt[5] += tests; }
+    const int ext_tri = __shfl_sync(0xffffffffu, tri, 0);
+    int vk = 2;
+    if (ext && ext_tri >= 0) vk = __ldg(&s.tris[ext_tri].ior) > 1.0001f ? 1 : 0;
+    __syncwarp();  // the hit and occlusion words above are visible to every lane
+    bool shd = false, fin = false;
+    uint32_t n = 0;
+    ext = false;
+    if (vk == 0) shade_path<0, 3>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, n);
+    else if (vk == 1) shade_path<1, 3>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, n);
+    else shade_path<2, 3>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, n);
+    if (lane == 0u) samples += n;
+    __syncwarp();  // every lane's copy of the path state is stored before the next step loads it
+    if (!ext && !fin) return;  // the pixel is written
+  }
+}
+
+// The end of the wavefront loop, once few paths remain: each thread takes an
+// unfinished pixel and runs it to the end with the waves' steps, in their
+// order (extension ray, pending shadow ray, shade_path of the vertex type), so
+// the pixel comes out the same, without a launch and a queue round trip per
+// vertex.  When one pixel is left in a warp (its last, longest chains) the
+// whole warp takes it over (tail_pixel_warp, opaque scenes).  ctr: the stage
+// counter of the tail's samples; ctr_ext / ctr_shd: its traversals'.  Three
+// 128-thread blocks per SM (up to 168 registers, few spills): the tail is
+// latency-bound and its path count is capped to one wave of resident blocks.
 template <int NEE>
 __global__ void __launch_bounds__(128, 3) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
                                                  float* __restrict__ hdr, uint32_t* __restrict__ dbg,
@@ -406,43 +552,35 @@ __global__ void __launch_bounds__(128, 3) k_wf_tail(Scene s, Params p, GBufSoA g
                                                  unsigned long long* ctr_shd, uint32_t* err) {
   const int n_ext = q.counts[kCntExt], n_c = q.counts[kCntC];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t samples = 0, rays_e = 0, nodes_e = 0, tests_e = 0, rays_s = 0, nodes_s = 0, tests_s = 0;
-  if (i < n_ext + n_c) {
-    const int id = i < n_ext ? q.ext[i] : q.qc[i - n_ext];
-    bool ext = i < n_ext;
-    for (;;) {
-      int vk = 2;
-      if (ext) {
-        const float4 o = w.o[id];
-        const float4 d = w.d[id];
-        const TraceResult r = traverse<false>(s, o.x, o.y, o.z, d.x, d.y, d.z, kFar, err, nodes_e, tests_e);
-        ++rays_e;
-        w.hit[id] = make_float4(r.t, r.u, r.v, __int_as_float(r.tri));
-        if (r.tri >= 0) vk = __ldg(&s.tris[r.tri].ior) > 1.0001f ? 1 : 0;
-      }
-      if (w.u[id].y & kShadow) {
-        const float4 o = w.so[id];
-        const float4 d = w.sd[id];
-        const TraceResult r = traverse<true>(s, o.x, o.y, o.z, d.x, d.y, d.z, o.w, err, nodes_s, tests_s);
-        ++rays_s;
-        w.occ[id] = r.tri >= 0 ? 1u : 0u;
-      }
-      bool shd = false, fin = false;
-      ext = false;
-      if (vk == 0) shade_path<0, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
-      else if (vk == 1) shade_path<1, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
-      else shade_path<2, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
-      if (!ext && !fin) break;  // the pixel is written
+  uint32_t samples = 0;
+  uint32_t cnt[6] = {0, 0, 0, 0, 0, 0};
+  bool active = i < n_ext + n_c;
+  int id = 0;
+  bool ext = false;
+  if (active) {
+    id = i < n_ext ? q.ext[i] : q.qc[i - n_ext];
+    ext = i < n_ext;
+  }
+  for (;;) {
+    const unsigned am = __ballot_sync(0xffffffffu, active);
+    if (!am) break;
+    if (NEE == 2 && __popc(am) == 1) {
+      const int leader = __ffs(am) - 1;
+      const int pid = __shfl_sync(0xffffffffu, id, leader);
+      const bool pext = __shfl_sync(0xffffffffu, ext ? 1 : 0, leader) != 0;
+      tail_pixel_warp(s, p, gb, w, pid, pext, hdr, dbg, err, samples, cnt);
+      break;
     }
+    if (active) active = tail_step<NEE>(s, p, gb, w, id, ext, hdr, dbg, err, samples, cnt);
   }
   __syncwarp();
   warp_add(ctr + 0, samples);
-  warp_add(ctr_ext + 1, rays_e);
-  warp_add(ctr_ext + 2, nodes_e);
-  warp_add(ctr_ext + 3, tests_e);
-  warp_add(ctr_shd + 1, rays_s);
-  warp_add(ctr_shd + 2, nodes_s);
-  warp_add(ctr_shd + 3, tests_s);
+  warp_add(ctr_ext + 1, cnt[0]);
+  warp_add(ctr_ext + 2, cnt[1]);
+  warp_add(ctr_ext + 3, cnt[2]);
+  warp_add(ctr_shd + 1, cnt[3]);
+  warp_add(ctr_shd + 2, cnt[4]);
+  warp_add(ctr_shd + 3, cnt[5]);
 }
 
 }  // namespace
@@ -471,6 +609,24 @@ cudaError_t launch_wavefront_trace(const Scene& s, const WfState& w, const WfQue
   }
   if (shadow) return trace_grid<true, Trav, int, kStack>(s, w, q, bound, ctr, err, st);
   return trace_grid<false, Trav, int, kStack>(s, w, q, bound, ctr, err, st);
+}
+
+cudaError_t launch_wavefront_trace2(const Scene& s, const WfState& w, const WfQueues& q, int bound,
+                                    unsigned long long* ctr_ext, unsigned long long* ctr_shd, uint32_t* err,
+                                    cudaStream_t st) {
+  if (bound <= 0) return cudaSuccess;
+  k_wf_trace2<<<unsigned((2 * bound + 127) / 128), 128, 0, st>>>(s, w, q, ctr_ext, ctr_shd, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wavefront_shade3(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w,
+                                    const WfQueues& cq, int bound, const WfQueues& nq, float* hdr, uint32_t* dbg,
+                                    unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
+  if (bound <= 0) return cudaSuccess;
+  const unsigned g = unsigned(3 * ((bound + 255) / 256));
+  if (p.opaque) k_wf_shade3<2><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+  else k_wf_shade3<1><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+  return cudaGetLastError();
 }
 
 int wavefront_tail_capacity(bool opaque) {

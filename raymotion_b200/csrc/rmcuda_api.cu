@@ -24,6 +24,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -228,6 +229,14 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
   sc.light_total = sv->light_total;
   sc.opaque = opaque;
   sc.validated_texels = sv->n_texels;
+  if (&sc == &c->sc) {
+    sc.h_lights.assign(sv->light_tri, sv->light_tri + sv->n_lights);
+    sc.h_cdf.assign(sv->light_cdf, sv->light_cdf + sv->n_lights);
+    sc.h_texels.assign(sv->texels, sv->texels + sv->n_texels);
+    sc.h_light_total = sv->light_total;
+    sc.h_valid = true;
+    sc.last_upload_equal = reuse;
+  }
   if ((e = prepare_lights(sc.tris.as<rm_triangle>(), sc.lights.as<int32_t>(), sc.cdf.as<float>(), sc.n_lights,
                           sc.light_total, sc.lrec, sc.guide, sc.guide_n, sc.guide_inv, st)) != cudaSuccess) {
     msg = cuda_msg("light preparation failed", e);
@@ -386,6 +395,11 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
   // device.
   const int kBatch = 4;
   const uint64_t max_waves = uint64_t(p.spp) * uint64_t(p.bounces + 2) * 4 + 64;
+  // One launch per wave for the traversals and one for the shading queues
+  // (each launch's slowest warps then overlap the others' work);
+  // RAYMOTION_CUDA_SPLIT_WAVES=1 launches each traversal and queue alone.
+  const char* split_env = std::getenv("RAYMOTION_CUDA_SPLIT_WAVES");
+  const bool merged = !(split_env && split_env[0] == '1');
   std::chrono::steady_clock::time_point t0;
   int tail = 0;
   for (uint64_t wave = 0;;) {
@@ -407,9 +421,10 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
     if (bound == 0) break;
     if (bound <= tail) {
       e = staged2(c, RM_STAGE_WF_TAIL, [&] {
+        // the tail's traversals are counted with the tail (both kinds in its slot)
         return launch_wavefront_tail(s, p, c->gb.view(), w, q[cur], bound, c->hdr.as<float>(), c->dbg.as<uint32_t>(),
-                                     ctr + 4 * RM_STAGE_WF_SHADE, ctr + 4 * RM_STAGE_WF_EXTEND,
-                                     ctr + 4 * RM_STAGE_WF_SHADOW, err, st);
+                                     ctr + 4 * RM_STAGE_WF_SHADE, ctr + 4 * RM_STAGE_WF_TAIL,
+                                     ctr + 4 * RM_STAGE_WF_TAIL, err, st);
       });
       if (e == cudaSuccess) e = cudaStreamSynchronize(st);
       if (e != cudaSuccess) { msg = cuda_msg("wavefront tail failed", e); return e; }
@@ -422,19 +437,35 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
       c->waves++;
       const WfQueues& Q = q[cur];
       const WfQueues& N = q[cur ^ 1];
-      e = staged2(c, RM_STAGE_WF_EXTEND, [&] {
-        return launch_wavefront_trace(s, w, Q, bound, false, ctr + 4 * RM_STAGE_WF_EXTEND, err, st);
-      });
-      if (e == cudaSuccess)
-        e = staged2(c, RM_STAGE_WF_SHADOW, [&] {
-          return launch_wavefront_trace(s, w, Q, bound, true, ctr + 4 * RM_STAGE_WF_SHADOW, err, st);
+      if (merged && !s.wnodes) {
+        // both traversals in one launch (timed as the extension stage)
+        e = staged2(c, RM_STAGE_WF_EXTEND, [&] {
+          return launch_wavefront_trace2(s, w, Q, bound, ctr + 4 * RM_STAGE_WF_EXTEND, ctr + 4 * RM_STAGE_WF_SHADOW,
+                                         err, st);
         });
+      } else {
+        e = staged2(c, RM_STAGE_WF_EXTEND, [&] {
+          return launch_wavefront_trace(s, w, Q, bound, false, ctr + 4 * RM_STAGE_WF_EXTEND, err, st);
+        });
+        if (e == cudaSuccess)
+          e = staged2(c, RM_STAGE_WF_SHADOW, [&] {
+            return launch_wavefront_trace(s, w, Q, bound, true, ctr + 4 * RM_STAGE_WF_SHADOW, err, st);
+          });
+      }
       if (e == cudaSuccess) e = cudaMemsetAsync(N.counts, 0, kCntSlots * sizeof(int), st);
-      for (int vk = 0; vk < 3 && e == cudaSuccess; ++vk)
-        e = staged2(c, RM_STAGE_WF_SHADE, [&] {
-          return launch_wavefront_shade(vk, s, p, c->gb.view(), w, Q, bound, N, c->hdr.as<float>(),
-                                        c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, st);
-        });
+      if (merged) {
+        if (e == cudaSuccess)
+          e = staged2(c, RM_STAGE_WF_SHADE, [&] {
+            return launch_wavefront_shade3(s, p, c->gb.view(), w, Q, bound, N, c->hdr.as<float>(),
+                                           c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, st);
+          });
+      } else {
+        for (int vk = 0; vk < 3 && e == cudaSuccess; ++vk)
+          e = staged2(c, RM_STAGE_WF_SHADE, [&] {
+            return launch_wavefront_shade(vk, s, p, c->gb.view(), w, Q, bound, N, c->hdr.as<float>(),
+                                          c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, st);
+          });
+      }
       if (e != cudaSuccess) { msg = cuda_msg("wavefront launch failed", e); return e; }
       cur ^= 1;
     }
@@ -625,8 +656,10 @@ void rmcuda_destroy(rmcuda_ctx* c) {
   c->sc.release();
   c->batch.release();
   for (DevBuf* b : {&c->hdr, &c->tmp_a, &c->tmp_b, &c->hist_col, &c->rgb, &c->dbg, &c->hash_out, &c->ctr, &c->err,
-                    &c->adj_scratch})
+                    &c->adj_scratch, &c->differ, &c->ctr_save})
     b->release();
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->h_differ) cudaFreeHost(c->h_differ);
   for (DevBuf& b : c->wf) b.release();
   for (DevBuf& b : c->wq) b.release();
   if (c->h_counts) cudaFreeHost(c->h_counts);
@@ -899,6 +932,145 @@ int rmcuda_sync(rmcuda_ctx* c, char* err, size_t errcap) {
   return rc;
 }
 
+}  // extern "C"
+
+namespace {
+
+// What a frame changes on the host side of the context, and the buffers its
+// history swap exchanges: enough to undo a speculative frame.
+struct FrameSnap {
+  rmapi::GBufSet gb, hg;
+  rmapi::ResSet rmerged, hres;
+  rmd::DevBuf tmp_a, hist_col;
+  rm_camera hist_cam, hist_prev_cam;
+  int hist_w, hist_h, last_chain, last_w, last_h;
+  uint64_t hist_seed, frames, launches, waves;
+  unsigned long long hist_hash;
+  bool hist_valid, have_hist_bufs, hist_denoised, hist_had_history;
+  const void* hist_scene;
+  rm_config hist_cfg;
+  float* last_final;
+  size_t pending;
+  std::vector<int> wave_log;
+};
+
+FrameSnap take_snap(rmcuda_ctx* c) {
+  return FrameSnap{c->gb, c->hg, c->rmerged, c->hres, c->tmp_a, c->hist_col, c->hist_cam, c->hist_prev_cam,
+                   c->hist_w, c->hist_h, c->last_chain, c->last_w, c->last_h, c->hist_seed, c->frames, c->launches,
+                   c->waves, c->hist_hash, c->hist_valid, c->have_hist_bufs, c->hist_denoised, c->hist_had_history,
+                   c->hist_scene, c->hist_cfg, c->last_final, c->pending.size(), c->wave_log};
+}
+
+void restore_snap(rmcuda_ctx* c, const FrameSnap& s) {
+  c->gb = s.gb; c->hg = s.hg; c->rmerged = s.rmerged; c->hres = s.hres; c->tmp_a = s.tmp_a; c->hist_col = s.hist_col;
+  c->hist_cam = s.hist_cam; c->hist_prev_cam = s.hist_prev_cam; c->hist_w = s.hist_w; c->hist_h = s.hist_h;
+  c->last_chain = s.last_chain; c->last_w = s.last_w; c->last_h = s.last_h; c->hist_seed = s.hist_seed;
+  c->frames = s.frames; c->launches = s.launches; c->waves = s.waves; c->hist_hash = s.hist_hash;
+  c->hist_valid = s.hist_valid; c->have_hist_bufs = s.have_hist_bufs; c->hist_denoised = s.hist_denoised;
+  c->hist_had_history = s.hist_had_history; c->hist_scene = s.hist_scene; c->hist_cfg = s.hist_cfg;
+  c->last_final = s.last_final;
+  for (size_t i = s.pending; i < c->pending.size(); ++i) {
+    cudaEventDestroy(c->pending[i].a);
+    cudaEventDestroy(c->pending[i].b);
+  }
+  c->pending.resize(s.pending);
+  c->wave_log = s.wave_log;
+}
+
+// A re-upload of the resident scene is rendered speculatively when nothing but
+// its triangles could have changed since the last frame: the same device-built
+// BVH settings and triangle count, light list, CDF, light total and texels
+// equal to the host copies of the last upload (the small arrays are compared
+// on the host and not sent), triangles that equalled the resident ones on the
+// last upload, and the same configuration as the last frame (so that no frame
+// buffer is reallocated and the frame can be undone by restoring the host
+// state).  RAYMOTION_CUDA_SPECULATE=0 turns it off.
+bool may_speculate(rmcuda_ctx* c, const rm_scene_view* sv, const rm_config& cfg) {
+  const char* v = std::getenv("RAYMOTION_CUDA_SPECULATE");
+  if (v && v[0] == '0') return false;
+  const rmapi::DevScene& sc = c->sc;
+  if (!sv || !sv->tris || !sc.have_scene || !sc.device_built || sv->nodes || sv->n_tris <= 0 ||
+      sv->n_tris != sc.n_tris || sc.bvh.n_records <= 0 || !sc.h_valid || !sc.last_upload_equal ||
+      sc.validated_texels != int64_t(sv->n_texels) || !c->have_last_cfg ||
+      std::memcmp(&c->last_cfg, &cfg, sizeof(cfg)) != 0)
+    return false;
+  std::string key;
+  for (const char* k : {"RAYMOTION_CUDA_BVH", "RAYMOTION_CUDA_BVH_LEAF", "RAYMOTION_CUDA_WIDE"}) {
+    const char* e = std::getenv(k);
+    key += e ? e : "-";
+    key += '|';
+  }
+  if (key != sc.build_key) return false;
+  if (sv->n_lights < 0 || sv->n_texels < 0 || size_t(sv->n_lights) != sc.h_lights.size() ||
+      size_t(sv->n_texels) != sc.h_texels.size())
+    return false;
+  if (std::memcmp(&sv->light_total, &sc.h_light_total, sizeof(float)) != 0) return false;
+  if (sv->n_lights && (!sv->light_tri || !sv->light_cdf ||
+                       std::memcmp(sv->light_tri, sc.h_lights.data(), size_t(sv->n_lights) * 4) != 0 ||
+                       std::memcmp(sv->light_cdf, sc.h_cdf.data(), size_t(sv->n_lights) * 4) != 0))
+    return false;
+  if (sv->n_texels && (!sv->texels ||
+                       std::memcmp(sv->texels, sc.h_texels.data(), size_t(sv->n_texels) * sizeof(rm_vec3)) != 0))
+    return false;
+  return true;
+}
+
+// The speculative frame: the triangles go to the staging buffer on the copy
+// stream (from a helper thread, so that a pageable host array does not hold
+// up the launches) and are compared with the resident ones there, while the
+// frame renders the resident scene.  Equal bytes: the frame stands (true).
+// Different bytes, or any failure: the frame is undone (history, counters,
+// host state) and false is returned, and the caller renders the upload the
+// ordinary way.
+bool speculative_frame(rmcuda_ctx* c, const rm_scene_view* sv, const rm_camera& cam, const rm_config& cfg,
+                       uint64_t seed) {
+  rmapi::DevScene& sc = c->sc;
+  const size_t tb = size_t(sv->n_tris) * sizeof(rm_triangle);
+  if (!c->copy_stream && cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    c->copy_stream = nullptr;
+    return false;
+  }
+  if (!c->h_differ && cudaMallocHost(reinterpret_cast<void**>(&c->h_differ), sizeof(int)) != cudaSuccess) {
+    c->h_differ = nullptr;
+    return false;
+  }
+  if (sc.tris_in.reserve(tb) != cudaSuccess || c->differ.reserve(16) != cudaSuccess ||
+      c->ctr_save.reserve(RM_STAGE_COUNT * 32) != cudaSuccess)
+    return false;
+  if (cudaMemcpyAsync(c->ctr_save.ptr, c->ctr.ptr, RM_STAGE_COUNT * 32, cudaMemcpyDeviceToDevice, c->stream) !=
+      cudaSuccess)
+    return false;
+  const FrameSnap snap = take_snap(c);
+  *c->h_differ = 1;
+  cudaError_t ce = cudaSuccess;
+  std::thread copier([&] {
+    ce = cudaSetDevice(c->device);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(sc.tris_in.ptr, sv->tris, tb, cudaMemcpyHostToDevice, c->copy_stream);
+    if (ce == cudaSuccess) ce = rmd::device_differ(sc.tris_in.ptr, sc.tris.ptr, tb, c->differ.as<int>(), c->copy_stream);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(c->h_differ, c->differ.ptr, sizeof(int), cudaMemcpyDeviceToHost, c->copy_stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(c->copy_stream);
+  });
+  std::string msg;
+  const int rc = rmapi::enqueue_frame(c, sc, cam, cfg, seed, c->rgb.as<uint8_t>(), msg);
+  copier.join();
+  if (rc == RM_OK && ce == cudaSuccess && *c->h_differ == 0) {
+    sc.reuses++;
+    return true;
+  }
+  // undo: the frame's work is discarded once it has finished
+  cudaStreamSynchronize(c->stream);
+  cudaGetLastError();
+  restore_snap(c, snap);
+  cudaMemcpyAsync(c->ctr.ptr, c->ctr_save.ptr, RM_STAGE_COUNT * 32, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemsetAsync(c->err.ptr, 0, 4, c->stream);
+  return false;
+}
+
+}  // namespace
+
+extern "C" {
+
 int rmcuda_render(rmcuda_ctx* c, const rm_scene_view* sv, const rm_camera* cam, const rm_config* cfg, uint64_t seed,
                   uint8_t* rgb, size_t rgb_cap, float* hdr, char* err, size_t errcap) {
   if (!cfg || cfg->width <= 0 || cfg->height <= 0 || cfg->spp <= 0 || cfg->max_bounces < 0 ||
@@ -912,12 +1084,19 @@ int rmcuda_render(rmcuda_ctx* c, const rm_scene_view* sv, const rm_camera* cam, 
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   std::string msg;
-  int rc = upload_scene(c, c->sc, sv, msg);
-  if (rc == RM_OK) {
-    cudaError_t e = c->rgb.reserve(npix * 3);
-    if (e != cudaSuccess) { msg = cuda_msg("Metal image buffer allocation failed", e); rc = RM_ERR_ALLOC; }
+  int rc = RM_OK;
+  // an unchanged re-upload (the reference re-uploads every frame,
+  // metal.mm:171-186) renders while its triangles are sent and compared
+  const bool done = c->rgb.cap >= npix * 3 && may_speculate(c, sv, *cfg) && speculative_frame(c, sv, *cam, *cfg, seed);
+  if (!done) {
+    rc = upload_scene(c, c->sc, sv, msg);
+    if (rc == RM_OK) {
+      cudaError_t e = c->rgb.reserve(npix * 3);
+      if (e != cudaSuccess) { msg = cuda_msg("Metal image buffer allocation failed", e); rc = RM_ERR_ALLOC; }
+    }
+    if (rc == RM_OK) rc = enqueue_frame(c, c->sc, *cam, *cfg, seed, c->rgb.as<uint8_t>(), msg);
   }
-  if (rc == RM_OK) rc = enqueue_frame(c, c->sc, *cam, *cfg, seed, c->rgb.as<uint8_t>(), msg);
+  if (rc == RM_OK) { c->last_cfg = *cfg; c->have_last_cfg = true; }
   if (rc == RM_OK) {
     cudaError_t e = cudaSuccess;
     if (rgb) e = cudaMemcpyAsync(rgb, c->rgb.ptr, npix * 3, cudaMemcpyDeviceToHost, c->stream);

@@ -110,10 +110,12 @@ def _restir_cfg(flags=0):
 
 
 @pytest.mark.parametrize("shading", ["wavefront", "wavefront-no-tail", "wavefront-all-tail", "wavefront-wide",
-                                     "megakernel"])
+                                     "wavefront-split", "megakernel"])
 def test_restir_chain_matches_oracle(backend, oracle, small_field, shading, monkeypatch):
     if shading == "megakernel":
         monkeypatch.setenv("RAYMOTION_CUDA_MEGAKERNEL", "1")
+    if shading == "wavefront-split":  # each traversal and shading queue in a launch of its own
+        monkeypatch.setenv("RAYMOTION_CUDA_SPLIT_WAVES", "1")
     if shading == "wavefront-wide":
         monkeypatch.setenv("RAYMOTION_CUDA_WIDE", "1")  # every traversal on the 8-wide BVH
     # the wavefront loop hands its last paths to one tail launch; "no-tail"
@@ -276,3 +278,41 @@ def test_restir_chain_on_a_textured_scene_matches_oracle(backend, oracle, shadin
         assert o_st["chain"] == 2 and backend.stats()["kernel_chain"] == 2
         assert o_hdr.max() > 0
         assert exact_fraction(g_hdr, o_hdr) == 1.0
+
+
+def test_speculative_reupload_frames_equal_plain_frames(backend, small_field, monkeypatch):
+    """rmcuda_render renders an unchanged re-upload while the triangles are
+    sent and compared on a second stream; when they differ, the speculative
+    frame is undone (temporal history, counters) and the upload rendered the
+    ordinary way.  A ReSTIR sequence over static, then moved, then static
+    triangles gives the same radiance, sample counts and BVH builds with
+    speculation on and off."""
+    sc, cam, _ = small_field
+    cfg = _restir_cfg(_abi.RM_FLAG_NO_ENV)
+    moved = sc.tris.copy()
+    moved["v0"][::5] += np.float32(0.03)
+    v64 = np.concatenate([moved["v0"], moved["v1"], moved["v2"]], axis=1).astype(np.float64)
+    msc = type(sc)(tris=moved, light_tri=sc.light_tri, light_cdf=sc.light_cdf, light_total=sc.light_total,
+                   texels=sc.texels, verts64=v64)
+    tiny = type(sc)(tris=sc.tris[:3], light_tri=sc.light_tri[:0], light_cdf=sc.light_cdf[:0], light_total=0.0,
+                    texels=sc.texels, verts64=sc.verts64[:3])
+    frames = [sc, sc, sc, msc, msc, msc, sc, sc]
+
+    def run(speculate):
+        monkeypatch.setenv("RAYMOTION_CUDA_SPECULATE", "1" if speculate else "0")
+        backend.upload(tiny, use_nodes=False)  # another resident scene first
+        backend.reset_history()
+        backend.stats_reset()
+        st0 = backend.stats()
+        out = []
+        for k, s in enumerate(frames):
+            _, hdr = backend.render(s, cam, cfg, 70 + k, hdr=True, use_nodes=False)
+            st = backend.stats()
+            out.append((hdr.copy(), st["path_samples"], st["bvh_builds"] - st0["bvh_builds"]))
+        return out
+
+    on, off = run(True), run(False)
+    for k, ((h1, s1, b1), (h0, s0, b0)) in enumerate(zip(on, off)):
+        assert np.array_equal(h1.view(np.uint32), h0.view(np.uint32)), k
+        assert s1 == s0 and b1 == b0, (k, s1, s0, b1, b0)
+    assert on[-1][2] == 3  # built for the first frame, the moved triangles and their return
