@@ -7,6 +7,7 @@ G-buffer (76 B) and reservoir (60 B) records used by the debug reads.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -168,7 +169,10 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    default = LIB_PATH
+    if os.environ.get("RAYMOTION_CUDA_CHECKED") == "1":
+        default = LIB_PATH.with_name("librmcuda_checked.so")  # device-side bounds checks (build.py checked)
+    p = Path(path) if path else default
     if not p.exists():
         raise OSError(f"{p} is missing; run raymotion_b200.build.build() first")
     lib = C.CDLL(str(p))

@@ -21,6 +21,11 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "librmcuda.so"
+# The checked build: the same sources with RMCUDA_CHECKED defined (device-side
+# bounds checks that set an error bit and skip the access, see rm_device.cuh);
+# loaded instead of LIB when RAYMOTION_CUDA_CHECKED=1.
+BUILD_CHECKED = PKG / "_build_checked"
+LIB_CHECKED = PKG / "librmcuda_checked.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + [
@@ -56,16 +61,18 @@ def _stale(obj: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps if d.exists())
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
-    """Compile every source and link ``librmcuda.so``; returns its path."""
+def build(verbose: bool = False, ptxas_info: bool = False, checked: bool = False) -> Path:
+    """Compile every source and link ``librmcuda.so`` (``checked``: the bounds-checked
+    ``librmcuda_checked.so``); returns its path."""
     nvcc = _nvcc()
-    BUILD.mkdir(exist_ok=True)
+    build_dir, lib = (BUILD_CHECKED, LIB_CHECKED) if checked else (BUILD, LIB)
+    build_dir.mkdir(exist_ok=True)
     headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((ROOT / "include").rglob("*.h*"))
     jobs = []
     objs = []
     for src in CU_SOURCES + CXX_SOURCES:
         s = CSRC / src
-        o = BUILD / (src + ".o")
+        o = build_dir / (src + ".o")
         objs.append(o)
         if _stale(o, [s] + headers) or ptxas_info:
             extra = ["-Xptxas", "-v"] if (ptxas_info and src.endswith(".cu")) else []
@@ -73,18 +80,20 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
             flags = [f for f in NVFLAGS if not (src in FMA_SOURCES and f == "-fmad=false")]
             if src in FMA_SOURCES:
                 flags.append("-fmad=true")
+            if checked:
+                flags.append("-DRMCUDA_CHECKED")
             jobs.append([nvcc, *flags, *extra, *lang, "-c", str(s), "-o", str(o)])
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         for cmd, fut in [(c, ex.submit(_run, c)) for c in jobs]:
             fut.result()
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
-    if jobs or not LIB.exists():
-        tmp = LIB.with_suffix(".so.tmp")
+    if jobs or not lib.exists():
+        tmp = lib.with_suffix(".so.tmp")
         _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"])
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(verbose=True, ptxas_info="--ptxas" in sys.argv))
+    print(build(verbose=True, ptxas_info="--ptxas" in sys.argv, checked="--checked" in sys.argv))

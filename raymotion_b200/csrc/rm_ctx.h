@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <mutex>
 #include <string>
@@ -63,6 +64,7 @@ struct DevScene {
   // the texel count the resident triangles were last checked against by
   // upload_scene (texture ranges, opacity); -1 after any other write
   long long validated_texels = -1;
+  long long n_texels = 0;  // texels of the last upload
   // host copies of the last upload's light list, CDF, light total and texels,
   // and whether that upload's triangles equalled the resident ones: what a
   // speculative frame (rmcuda_render) needs to know the next upload's small
@@ -195,8 +197,22 @@ extern const char* const kInvalidDims;
 void set_err(char* err, size_t cap, const std::string& m);
 std::string cuda_msg(const char* what, cudaError_t e);
 
+// A named NVTX range over a host scope (API calls, frame stages): profilers
+// (ncu --nvtx, Nsight) attribute the kernels launched inside it to that name.
+// Without a tool attached, a push and a pop cost a few nanoseconds.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+// NVTX names of the RM_STAGE_* stages
+const char* stage_name(int stage);
+
 // Launch through `fn`, bracketed by events on the context stream when profiling.
 template <class Fn> cudaError_t staged(rmcuda_ctx* c, int stage, Fn&& fn) {
+  NvtxRange range(stage_name(stage));
   cudaEvent_t a = nullptr, b = nullptr;
   if (c->profiling > 0 && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess)
     cudaEventRecord(a, c->stream);

@@ -38,6 +38,28 @@ constexpr uint64_t kSpatialSeedXor = 0x1B54A35A6F31B458ull;  // low 64 bits of p
 // device error word bits
 constexpr uint32_t kErrStack = 1u;
 constexpr uint32_t kErrAlpha = 2u;
+constexpr uint32_t kErrBounds = 4u;
+
+// The checked build (RMCUDA_CHECKED defined; raymotion_b200/build.py
+// `checked`, librmcuda_checked.so): every index read from a device structure
+// (a BVH node or leaf range, a hit's triangle, a light, a texel, a queue
+// entry) is compared with its array before the access; a bad one sets
+// kErrBounds in the error word and the access is skipped (a node as an empty
+// subtree, a leaf or hit as a miss, a light as the first light, a texel as
+// white, a queue entry as no work).  The call then fails with RM_ERR_DEVICE
+// instead of reading out of bounds; valid inputs give the same results as
+// the unchecked build.
+#ifdef RMCUDA_CHECKED
+constexpr bool kChecked = true;
+#else
+constexpr bool kChecked = false;
+#endif
+
+__device__ __forceinline__ bool bad_index(long long i, long long n, uint32_t* err) {
+  if (!kChecked || (i >= 0 && i < n)) return false;
+  if (err) atomicOr(err, kErrBounds);
+  return true;
+}
 
 struct Scene {
   const rm_triangle* __restrict__ tris;
@@ -61,6 +83,8 @@ struct Scene {
   // 5 x float4 per node, and the triangle records (as tgeo) in its leaf order
   const float4* __restrict__ wnodes = nullptr;
   const float4* __restrict__ wtgeo = nullptr;
+  int n_tris = 0;          // triangles (and triangle records)
+  long long n_texels = 0;  // texels
 };
 
 // One emissive triangle as light sampling reads it (the fields of
@@ -281,6 +305,7 @@ struct Trav {
   // hit child (pushing the farther one), else to the next pending subtree.
   // True when nothing is left (or the stack overflowed, flagged in err).
   __device__ __forceinline__ bool visit(const Scene& s, int* stack, uint32_t* err, uint32_t& n_nodes) {
+    if (bad_index(node, s.n_nodes, err)) return pop(stack);
     ++n_nodes;
     const float4* n = s.nodes + size_t(node) * 4;
     const float4 a = __ldg(n + 0);
@@ -336,6 +361,8 @@ struct Trav {
     while (node >= 0 && leaf_count == 0)
       if (visit(s, stack, err, n_nodes)) return true;
     // leaf: Moller-Trumbore, pathtrace.metal:150-158
+    if (kChecked && (bad_index(leaf_first, s.n_tris, err) || bad_index(leaf_first + leaf_count - 1, s.n_tris, err)))
+      leaf_count = 0;
     n_tests += uint32_t(leaf_count);
     for (int k = 0; k < leaf_count; ++k)
       if (test_triangle(s.tgeo + size_t(leaf_first + k) * 3, ox, oy, oz, dx, dy, dz, r) && any_hit) return true;
@@ -479,6 +506,7 @@ struct WTrav {
       do {
         const uint32_t i = __ffs(tmask) - 1;
         tmask &= tmask - 1u;
+        if (bad_index((long long)n1.y + i, s.n_tris, err)) continue;
         if (test_triangle(tg + size_t(i) * 3, ox, oy, oz, dx, dy, dz, r) && kAnyHit) return true;
       } while (tmask);
     }
@@ -580,6 +608,7 @@ struct Tracer {
     h.t = tr.t; h.tri = tr.tri; h.u = tr.u; h.v = tr.v;
     h.px = ox + dx * h.t; h.py = oy + dy * h.t; h.pz = oz + dz * h.t;
     h.shader = 0;
+    if (h.tri >= 0 && bad_index(h.tri, s.n_tris, err)) h.tri = -1;
     if (h.tri >= 0) {
       const rm_triangle& t = s.tris[h.tri];
       float w = 1.0f - (h.u + h.v);
@@ -597,7 +626,8 @@ struct Tracer {
         tv = fminf(tv - floorf(tv), 0.99999994f);
         int x = min(int(tu * float(t.texture_width)), t.texture_width - 1);
         int y = t.texture_height - 1 - min(int(tv * float(t.texture_height)), t.texture_height - 1);
-        const rm_vec3 c = s.texels[size_t(t.texture_offset) + size_t(y) * size_t(t.texture_width) + size_t(x)];
+        const size_t ti = size_t(t.texture_offset) + size_t(y) * size_t(t.texture_width) + size_t(x);
+        const rm_vec3 c = bad_index((long long)ti, s.n_texels, err) ? rm_vec3{1.0f, 1.0f, 1.0f} : s.texels[ti];
         h.ar *= c.x; h.ag *= c.y; h.ab *= c.z;
         h.txr = c.x; h.txg = c.y; h.txb = c.z;
       }
@@ -791,6 +821,7 @@ struct Tracer {
       int mid = (lo + hi) / 2;
       if (__ldg(s.cdf + mid) >= pick) hi = mid; else lo = mid + 1;
     }
+    if (bad_index(lo, p.lights, err)) lo = 0;
     return lo;
   }
 

@@ -129,6 +129,7 @@ extern "C" int rmcuda_trace_noalloc(const rm_triangle* d_tris, int32_t n_tris, c
   s.tgeo = bvh.tgeo;
   s.nodes = bvh.records;
   s.n_nodes = n_tris > 0 ? bvh.n_records : 0;
+  s.n_tris = n_tris;
   e = rmd::launch_trace(s, d_rays, n_rays, any_hit, d_tri, d_t, d_u, d_v, w.err_word, st);
   uint32_t word = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&word, w.err_word, sizeof(word), cudaMemcpyDeviceToHost, st);

@@ -449,6 +449,9 @@ __global__ void __launch_bounds__(256) k_wf_shade3(Scene s, Params p, GBufSoA gb
   uint32_t samples = 0;
   if (i < count) {
     id = queue[i];
+    if (bad_index(id, (long long)p.width * p.height, err)) id = -1;
+  }
+  if (id >= 0 && i < count) {
     if (vk == 0) shade_path<0, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
     else if (vk == 1) shade_path<1, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
     else shade_path<2, NEE>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, samples);
@@ -560,6 +563,7 @@ __global__ void __launch_bounds__(128, 3) k_wf_tail(Scene s, Params p, GBufSoA g
   if (active) {
     id = i < n_ext ? q.ext[i] : q.qc[i - n_ext];
     ext = i < n_ext;
+    if (bad_index(id, (long long)p.width * p.height, err)) active = false;
   }
   for (;;) {
     const unsigned am = __ballot_sync(0xffffffffu, active);

@@ -109,6 +109,15 @@ Env read_env(uint32_t flags) {
 
 namespace rmapi {
 
+const char* stage_name(int stage) {
+  static const char* const names[RM_STAGE_COUNT] = {
+      "rm plain paths", "rm scene hash", "rm restir generate", "rm restir spatial", "rm restir shade",
+      "rm denoise temporal", "rm denoise atrous 1", "rm denoise atrous 2", "rm tonemap", "rm wavefront traversal",
+      "rm wavefront shadow", "rm wavefront shade", "rm batch start", "rm batch extend", "rm batch shadow",
+      "rm batch shade", "rm batch", "rm adjoint", "rm wavefront tail", "rm scene preparation"};
+  return stage >= 0 && stage < RM_STAGE_COUNT ? names[stage] : "rm stage";
+}
+
 void resolve_pending(rmcuda_ctx* c) {
   for (auto& pe : c->pending) {
     float ms = 0.f;
@@ -137,6 +146,8 @@ Scene scene_view(const DevScene& sc) {
   s.guide = sc.guide.as<int32_t>();
   s.guide_n = sc.guide_n;
   s.guide_inv = sc.guide_inv;
+  s.n_tris = sc.n_tris;
+  s.n_texels = sc.n_texels;
   if (sc.n_tris > 0 && sc.bvh.n_wide > 0) {
     s.wnodes = sc.bvh.wnodes.as<float4>();
     s.wtgeo = sc.bvh.wtgeo.as<float4>();
@@ -146,6 +157,7 @@ Scene scene_view(const DevScene& sc) {
 
 // Validate and upload one scene; build or convert its BVH.
 int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::string& msg) {
+  NvtxRange range("rm scene upload");
   if (!sv || sv->n_tris < 0 || sv->n_lights < 0 || sv->n_texels < 0 || (sv->n_tris > 0 && !sv->tris) ||
       (sv->n_lights > 0 && (!sv->light_tri || !sv->light_cdf)) || (sv->n_texels > 0 && !sv->texels)) {
     msg = "invalid scene view";
@@ -229,6 +241,7 @@ int upload_scene(rmcuda_ctx* c, DevScene& sc, const rm_scene_view* sv, std::stri
   sc.light_total = sv->light_total;
   sc.opaque = opaque;
   sc.validated_texels = sv->n_texels;
+  sc.n_texels = sv->n_texels;
   if (&sc == &c->sc) {
     sc.h_lights.assign(sv->light_tri, sv->light_tri + sv->n_lights);
     sc.h_cdf.assign(sv->light_cdf, sv->light_cdf + sv->n_lights);
@@ -362,6 +375,7 @@ static int tail_paths(int first_bound, bool opaque) {
 }
 
 cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, uint64_t seed, std::string& msg) {
+  NvtxRange range("rm wavefront shading loop");
   const size_t npix = size_t(p.width) * size_t(p.height);
   cudaStream_t st = c->stream;
   cudaError_t e = ensure_wavefront(c, npix);
@@ -420,6 +434,7 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
                                            int(std::chrono::duration_cast<std::chrono::microseconds>(now - t0).count())});
     if (bound == 0) break;
     if (bound <= tail) {
+      NvtxRange tail_range(stage_name(RM_STAGE_WF_TAIL));
       e = staged2(c, RM_STAGE_WF_TAIL, [&] {
         // the tail's traversals are counted with the tail (both kinds in its slot)
         return launch_wavefront_tail(s, p, c->gb.view(), w, q[cur], bound, c->hdr.as<float>(), c->dbg.as<uint32_t>(),
@@ -493,6 +508,7 @@ cudaError_t ensure_frame(rmcuda_ctx* c, size_t npix, bool restir) {
 // image; the final linear radiance stays in c->last_final.
 int enqueue_frame(rmcuda_ctx* c, DevScene& sc, const rm_camera& cam, const rm_config& cfg, uint64_t seed, uint8_t* d_rgb,
                   std::string& msg) {
+  NvtxRange range("rm frame");
   if (cfg.width <= 0 || cfg.height <= 0 || cfg.spp <= 0 || cfg.max_bounces < 0 ||
       size_t(cfg.width) * size_t(cfg.height) > 100000000) {
     msg = kInvalidDims;
@@ -605,7 +621,9 @@ int check_device_error(rmcuda_ctx* c, std::string& msg) {
   if (e != cudaSuccess) { msg = cuda_msg("Metal command buffer failed", e); return RM_ERR_CUDA; }
   if (dev_err) {
     cudaMemsetAsync(c->err.ptr, 0, 4, c->stream);
-    msg = "device error word " + std::to_string(dev_err) + " (traversal stack or loop bound exceeded)";
+    msg = "device error word " + std::to_string(dev_err) +
+          " (1: traversal stack exceeded, 2: transparent crossings exceeded, 4: index out of bounds in the checked "
+          "build)";
     return RM_ERR_DEVICE;
   }
   return RM_OK;
@@ -1024,6 +1042,7 @@ bool may_speculate(rmcuda_ctx* c, const rm_scene_view* sv, const rm_config& cfg)
 // ordinary way.
 bool speculative_frame(rmcuda_ctx* c, const rm_scene_view* sv, const rm_camera& cam, const rm_config& cfg,
                        uint64_t seed) {
+  NvtxRange range("rm speculative frame");
   rmapi::DevScene& sc = c->sc;
   const size_t tb = size_t(sv->n_tris) * sizeof(rm_triangle);
   if (!c->copy_stream && cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -1083,6 +1102,7 @@ int rmcuda_render(rmcuda_ctx* c, const rm_scene_view* sv, const rm_camera* cam, 
   if (rgb && rgb_cap < npix * 3) { set_err(err, errcap, "rgb buffer too small"); return RM_ERR_INVALID; }
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
+  NvtxRange range("rmcuda_render");
   std::string msg;
   int rc = RM_OK;
   // an unchanged re-upload (the reference re-uploads every frame,

@@ -32,6 +32,27 @@ def test_every_declared_symbol_is_exported(lib):
         assert n in bound, f"{n} lacks a ctypes binding"
 
 
+def test_checked_build_exports_the_same_symbols():
+    """librmcuda_checked.so (device-side bounds checks, RMCUDA_CHECKED) loads
+    and exports every declared symbol, and RAYMOTION_CUDA_CHECKED=1 selects it."""
+    import os
+    import subprocess
+    import sys
+    from raymotion_b200 import build
+    if not build.LIB_CHECKED.exists():
+        build.build(checked=True)
+    lib = _abi.load_library(build.LIB_CHECKED)
+    for n in _declared():
+        assert hasattr(lib, n), n
+    code = ("import raymotion_b200._abi as a; a.load_library(); "
+            "print([l for l in open('/proc/self/maps') if 'librmcuda' in l][0].split()[-1])")
+    env = dict(os.environ, RAYMOTION_CUDA_CHECKED="1")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, cwd=str(build.ROOT),
+                       timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip().splitlines()[-1].endswith("librmcuda_checked.so")
+
+
 def test_record_sizes_match_reference_abi():
     # metal_types.h sizes, asserted in metal.mm:13-17
     assert _abi.TRIANGLE_DTYPE.itemsize == 176
