@@ -39,6 +39,7 @@ constexpr uint64_t kSpatialSeedXor = 0x1B54A35A6F31B458ull;  // low 64 bits of p
 constexpr uint32_t kErrStack = 1u;
 constexpr uint32_t kErrAlpha = 2u;
 constexpr uint32_t kErrBounds = 4u;
+constexpr uint32_t kErrSteps = 8u;  // a loop ran past its bound on the steps a pixel can take
 
 // The checked build (RMCUDA_CHECKED defined; raymotion_b200/build.py
 // `checked`, librmcuda_checked.so): every index read from a device structure
@@ -55,9 +56,13 @@ constexpr bool kChecked = true;
 constexpr bool kChecked = false;
 #endif
 
-__device__ __forceinline__ bool bad_index(long long i, long long n, uint32_t* err) {
+// Which check fired is recorded as bit 8 + site of the error word.
+enum CheckSite : uint32_t {
+  kSiteNode = 0, kSiteLeaf, kSiteWideLeaf, kSiteHit, kSiteTexel, kSiteLight, kSiteQueue, kSiteTailQueue, kSiteVertex
+};
+__device__ __forceinline__ bool bad_index(long long i, long long n, uint32_t* err, uint32_t site) {
   if (!kChecked || (i >= 0 && i < n)) return false;
-  if (err) atomicOr(err, kErrBounds);
+  if (err) atomicOr(err, kErrBounds | (1u << (8u + site)));
   return true;
 }
 
@@ -305,7 +310,7 @@ struct Trav {
   // hit child (pushing the farther one), else to the next pending subtree.
   // True when nothing is left (or the stack overflowed, flagged in err).
   __device__ __forceinline__ bool visit(const Scene& s, int* stack, uint32_t* err, uint32_t& n_nodes) {
-    if (bad_index(node, s.n_nodes, err)) return pop(stack);
+    if (bad_index(node, s.n_nodes, err, kSiteNode)) return pop(stack);
     ++n_nodes;
     const float4* n = s.nodes + size_t(node) * 4;
     const float4 a = __ldg(n + 0);
@@ -361,7 +366,8 @@ struct Trav {
     while (node >= 0 && leaf_count == 0)
       if (visit(s, stack, err, n_nodes)) return true;
     // leaf: Moller-Trumbore, pathtrace.metal:150-158
-    if (kChecked && (bad_index(leaf_first, s.n_tris, err) || bad_index(leaf_first + leaf_count - 1, s.n_tris, err)))
+    if (kChecked && (bad_index(leaf_first, s.n_tris, err, kSiteLeaf) ||
+                     bad_index(leaf_first + leaf_count - 1, s.n_tris, err, kSiteLeaf)))
       leaf_count = 0;
     n_tests += uint32_t(leaf_count);
     for (int k = 0; k < leaf_count; ++k)
@@ -506,7 +512,7 @@ struct WTrav {
       do {
         const uint32_t i = __ffs(tmask) - 1;
         tmask &= tmask - 1u;
-        if (bad_index((long long)n1.y + i, s.n_tris, err)) continue;
+        if (bad_index((long long)n1.y + i, s.n_tris, err, kSiteWideLeaf)) continue;
         if (test_triangle(tg + size_t(i) * 3, ox, oy, oz, dx, dy, dz, r) && kAnyHit) return true;
       } while (tmask);
     }
@@ -566,6 +572,9 @@ struct Tracer {
   Rng rng;
   uint32_t rays, nodes, tests;
   uint32_t* err;
+  // lanes that share this path in direct_lighting_deferred_warp: an aligned
+  // group of 8, 16 or 32 lanes of the warp
+  uint32_t group = 32;
 
   __device__ __forceinline__ Tracer(const Scene& s_, const Params& p_, uint32_t* e)
       : s(s_), p(p_), rays(0), nodes(0), tests(0), err(e) {}
@@ -608,7 +617,7 @@ struct Tracer {
     h.t = tr.t; h.tri = tr.tri; h.u = tr.u; h.v = tr.v;
     h.px = ox + dx * h.t; h.py = oy + dy * h.t; h.pz = oz + dz * h.t;
     h.shader = 0;
-    if (h.tri >= 0 && bad_index(h.tri, s.n_tris, err)) h.tri = -1;
+    if (h.tri >= 0 && bad_index(h.tri, s.n_tris, err, kSiteHit)) h.tri = -1;
     if (h.tri >= 0) {
       const rm_triangle& t = s.tris[h.tri];
       float w = 1.0f - (h.u + h.v);
@@ -627,7 +636,7 @@ struct Tracer {
         int x = min(int(tu * float(t.texture_width)), t.texture_width - 1);
         int y = t.texture_height - 1 - min(int(tv * float(t.texture_height)), t.texture_height - 1);
         const size_t ti = size_t(t.texture_offset) + size_t(y) * size_t(t.texture_width) + size_t(x);
-        const rm_vec3 c = bad_index((long long)ti, s.n_texels, err) ? rm_vec3{1.0f, 1.0f, 1.0f} : s.texels[ti];
+        const rm_vec3 c = bad_index((long long)ti, s.n_texels, err, kSiteTexel) ? rm_vec3{1.0f, 1.0f, 1.0f} : s.texels[ti];
         h.ar *= c.x; h.ag *= c.y; h.ab *= c.z;
         h.txr = c.x; h.txg = c.y; h.txb = c.z;
       }
@@ -821,7 +830,7 @@ struct Tracer {
       int mid = (lo + hi) / 2;
       if (__ldg(s.cdf + mid) >= pick) hi = mid; else lo = mid + 1;
     }
-    if (bad_index(lo, p.lights, err)) lo = 0;
+    if (bad_index(lo, p.lights, err, kSiteLight)) lo = 0;
     return lo;
   }
 
@@ -1120,15 +1129,16 @@ struct Tracer {
   }
 
   // direct_lighting_deferred with its Mc candidates spread over the lanes of
-  // the calling warp (pathtrace.metal:385-469).  Every lane of the warp calls
-  // it with the same arguments and the same random state, and every lane
-  // returns the same results.  A candidate takes exactly four draws (light
-  // pick, two barycentrics, the reservoir's acceptance draw), so lane j
-  // starts at draw 4j of the stream: a jump of the generator's state.  Each
-  // lane evaluates its candidate with the loop body's arithmetic, and every
-  // lane then forms the reservoir's running sum and acceptance tests in
-  // candidate order from the lanes' weights, as the loop does: the selection,
-  // the sums and the state after the last draw are bit-identical.
+  // the calling lane group (pathtrace.metal:385-469): `group` aligned lanes
+  // (8, 16 or 32) call it with the same arguments and the same random state,
+  // and each returns the same results.  A candidate takes exactly four draws
+  // (light pick, two barycentrics, the reservoir's acceptance draw), so
+  // candidate j starts at draw 4j of the stream: a jump of the generator's
+  // state.  In round r, lane l of the group evaluates candidate r*group + l
+  // with the loop body's arithmetic; then every lane runs the reservoir's
+  // running sum and acceptance tests over that round's candidates in order,
+  // as the loop does: the selection, the sums and the state after the last
+  // draw are bit-identical.
   __device__ void direct_lighting_deferred_warp(float px, float py, float pz, float nx, float ny, float nz, float wox,
                                                 float woy, float woz, float rough, float metallic, float spec_prob,
                                                 float ar, float ag, float ab, float& o_r, float& o_g, float& o_b,
@@ -1154,65 +1164,76 @@ struct Tracer {
     if (r2 < 0.02f) r2 = 0.02f;
     float alpha2 = (r2 * r2) * (r2 * r2);
     const float LT = p.light_total;
+    const int G = int(group);
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gl = lane & uint32_t(G - 1);
+    const uint32_t gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane - gl));
     const uint32_t s0 = rng.state;
-    float w = 0, ph = 0, epdf = 0, Fr = 0, Fg = 0, Fb = 0, qx = 0, qy = 0, qz = 0, racc = 0;
-    if (int(lane) < Mc) {
-      Rng lr;
-      lr.state = rng_jump(s0, 4u * lane);
-      const BsdfPrep bp = prep_bsdf(wox, woy, woz, nx, ny, nz, alpha2, metallic, ar, ag, ab);
-      float pick = lr.uniform01() * LT;
-      const int li = pick_light(pick);
-      const LightRec t = load_light(s, li);
-      float lu = lr.uniform01(), lv = lr.uniform01();
-      if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
-      float lw = 1.0f - lu - lv;
-      qx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x);
-      qy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y);
-      qz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z);
-      float ldx = qx - px, ldy = qy - py, ldz = qz - pz;
-      float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
-      if (dist > 0.003f) {
-        float inv = 1.0f / dist;
-        float dxn = ldx * inv, dyn = ldy * inv, dzn = ldz * inv;
-        float lcos = -(t.nn.x * dxn + (t.nn.y * dyn + t.nn.z * dzn));
-        float scos = nx * dxn + (ny * dyn + nz * dzn);
-        if (lcos > 1e-8f && scos > 1e-8f) {
-          float lt_lum = lum3(t.er, t.eg, t.eb);
-          if (lt_lum < 1e-6f) lt_lum = 1e-6f;
-          float q = dist * dist * lt_lum / (lcos * LT);
-          if (q > 1e-12f) {
-            Bsdf e = eval_bsdf_prep(bp, dxn, dyn, dzn, wox, woy, woz, nx, ny, nz, alpha2, spec_prob);
-            epdf = e.pdf;
-            Fr = t.er * e.r * scos * t.alpha;
-            Fg = t.eg * e.g * scos * t.alpha;
-            Fb = t.eb * e.b * scos * t.alpha;
-            ph = lum3(Fr, Fg, Fb);
-            if (ph > 0.0f) w = ph / q;
+    const BsdfPrep bp = prep_bsdf(wox, woy, woz, nx, ny, nz, alpha2, metallic, ar, ag, ab);
+    float sumW = 0.0f;
+    bool have = false;
+    float sel_lx = 0, sel_ly = 0, sel_lz = 0, sel_Fr = 0, sel_Fg = 0, sel_Fb = 0, sel_phat = 0, sel_epdf = 0;
+    for (int base = 0; base < Mc; base += G) {
+      const int j = base + int(gl);
+      float w = 0, ph = 0, epdf = 0, Fr = 0, Fg = 0, Fb = 0, qx = 0, qy = 0, qz = 0, racc = 0;
+      if (j < Mc) {
+        Rng lr;
+        lr.state = rng_jump(s0, 4u * uint32_t(j));
+        float pick = lr.uniform01() * LT;
+        const int li = pick_light(pick);
+        const LightRec t = load_light(s, li);
+        float lu = lr.uniform01(), lv = lr.uniform01();
+        if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
+        float lw = 1.0f - lu - lv;
+        qx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x);
+        qy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y);
+        qz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z);
+        float ldx = qx - px, ldy = qy - py, ldz = qz - pz;
+        float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
+        if (dist > 0.003f) {
+          float inv = 1.0f / dist;
+          float dxn = ldx * inv, dyn = ldy * inv, dzn = ldz * inv;
+          float lcos = -(t.nn.x * dxn + (t.nn.y * dyn + t.nn.z * dzn));
+          float scos = nx * dxn + (ny * dyn + nz * dzn);
+          if (lcos > 1e-8f && scos > 1e-8f) {
+            float lt_lum = lum3(t.er, t.eg, t.eb);
+            if (lt_lum < 1e-6f) lt_lum = 1e-6f;
+            float q = dist * dist * lt_lum / (lcos * LT);
+            if (q > 1e-12f) {
+              Bsdf e = eval_bsdf_prep(bp, dxn, dyn, dzn, wox, woy, woz, nx, ny, nz, alpha2, spec_prob);
+              epdf = e.pdf;
+              Fr = t.er * e.r * scos * t.alpha;
+              Fg = t.eg * e.g * scos * t.alpha;
+              Fb = t.eb * e.b * scos * t.alpha;
+              ph = lum3(Fr, Fg, Fb);
+              if (ph > 0.0f) w = ph / q;
+            }
           }
         }
+        racc = lr.uniform01();
       }
-      racc = lr.uniform01();
+      // this round's candidates in order, on every lane of the group
+      const int n_round = min(G, Mc - base);
+      int selk = -1;
+      for (int k = 0; k < n_round; ++k) {
+        const float wk = __shfl_sync(gmask, w, k, G);
+        const float rk = __shfl_sync(gmask, racc, k, G);
+        sumW += wk;
+        if (wk > 0.0f && rk * sumW < wk) selk = k;
+      }
+      if (selk >= 0) {
+        have = true;
+        sel_lx = __shfl_sync(gmask, qx, selk, G); sel_ly = __shfl_sync(gmask, qy, selk, G);
+        sel_lz = __shfl_sync(gmask, qz, selk, G);
+        sel_Fr = __shfl_sync(gmask, Fr, selk, G); sel_Fg = __shfl_sync(gmask, Fg, selk, G);
+        sel_Fb = __shfl_sync(gmask, Fb, selk, G);
+        sel_phat = __shfl_sync(gmask, ph, selk, G); sel_epdf = __shfl_sync(gmask, epdf, selk, G);
+      }
     }
     rng.state = rng_jump(s0, 4u * uint32_t(Mc));
-    // the reservoir in candidate order, on every lane
-    float sumW = 0.0f;
-    int sel = -1;
-    for (int j = 0; j < Mc; ++j) {
-      const float wj = __shfl_sync(0xffffffffu, w, j);
-      const float rj = __shfl_sync(0xffffffffu, racc, j);
-      sumW += wj;
-      if (wj > 0.0f && rj * sumW < wj) sel = j;
-    }
     out_sumW = sumW;
     out_M = uint32_t(Mc);
-    if (sel < 0) return;
-    const float sel_lx = __shfl_sync(0xffffffffu, qx, sel), sel_ly = __shfl_sync(0xffffffffu, qy, sel),
-                sel_lz = __shfl_sync(0xffffffffu, qz, sel);
-    const float sel_Fr = __shfl_sync(0xffffffffu, Fr, sel), sel_Fg = __shfl_sync(0xffffffffu, Fg, sel),
-                sel_Fb = __shfl_sync(0xffffffffu, Fb, sel);
-    const float sel_phat = __shfl_sync(0xffffffffu, ph, sel), sel_epdf = __shfl_sync(0xffffffffu, epdf, sel);
-    if (!(sumW > 0.0f) || !(sel_phat > 0.0f)) return;
+    if (!have || !(sumW > 0.0f) || !(sel_phat > 0.0f)) return;
     float pdf_ris = float(Mc) * sel_phat / sumW;
     float wnee = 1.0f;
     if (!p.nomis && sel_epdf > 1e-20f) wnee = pdf_ris / (pdf_ris + sel_epdf);

@@ -65,6 +65,8 @@ __device__ __forceinline__ void clamp3(const Params& p, float& r, float& g, floa
 template <int MAT, int NEE = 1>
 __device__ bool vertex(Tracer& pt, const Params& p, PathRegs& r, const Hit& hit, bool& has_shadow, float4& so,
                        float4& sd, float4& c) {
+  // the checked build: a hit whose triangle failed its check ends the path
+  if (kChecked && bad_index(hit.tri, pt.s.n_tris, pt.err, kSiteVertex)) return false;
   const bool ind = (r.meta & kInd) != 0;
   float pnx = hit.nix, pny = hit.niy, pnz = hit.niz;
   float geom = hit.ngx * pnx + (hit.ngy * pny + hit.ngz * pnz);

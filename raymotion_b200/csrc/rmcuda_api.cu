@@ -622,8 +622,10 @@ int check_device_error(rmcuda_ctx* c, std::string& msg) {
   if (dev_err) {
     cudaMemsetAsync(c->err.ptr, 0, 4, c->stream);
     msg = "device error word " + std::to_string(dev_err) +
-          " (1: traversal stack exceeded, 2: transparent crossings exceeded, 4: index out of bounds in the checked "
-          "build)";
+          " (1: traversal stack exceeded, 2: transparent crossings exceeded, 8: a pixel's step bound exceeded, "
+          "4: index out of bounds in the checked "
+          "build, with bit 8 + n for the check that fired: 0 BVH node, 1 leaf range, 2 wide leaf, 3 hit triangle, "
+          "4 texel, 5 light, 6 shading queue, 7 tail queue, 8 vertex triangle)";
     return RM_ERR_DEVICE;
   }
   return RM_OK;
@@ -1256,7 +1258,9 @@ int rmcuda_debug_read(rmcuda_ctx* c, int32_t which, void* host, size_t cap, char
   if (which == 3 || which == 4) {
     const size_t bytes = npix * (which == 3 ? 12 : 8);
     if (cap < bytes) { set_err(err, errcap, "buffer too small"); return RM_ERR_INVALID; }
-    const void* src = which == 3 ? static_cast<const void*>(c->last_final) : c->dbg.ptr;
+    // 3: the shaded radiance before the denoiser (the final image is the
+    // frame's hdr output); the denoiser reads it without writing it
+    const void* src = which == 3 ? static_cast<const void*>(c->last_final ? c->hdr.ptr : nullptr) : c->dbg.ptr;
     if (!src) { set_err(err, errcap, "no frame rendered"); return RM_ERR_INVALID; }
     e = cudaMemcpy(host, src, bytes, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) { set_err(err, errcap, cuda_msg("read failed", e)); return RM_ERR_CUDA; }
