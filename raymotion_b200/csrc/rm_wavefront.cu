@@ -579,6 +579,11 @@ __global__ void __launch_bounds__(128, 3) k_wf_tail(Scene s, Params p, GBufSoA g
   // pixel has at most spp x (depth + 2) vertices left: past that, flag and stop
   const uint32_t max_steps = uint32_t(p.spp) * uint32_t(p.bounces + 2) * 4u + 64u;
   for (uint32_t step = 0;; ++step) {
+    // A pixel changes hands between steps (its own lane, then a lane group,
+    // then another group): the previous step's stores of its path state must
+    // be ordered before the next owner's loads, and the ballot and shuffles
+    // below are not memory barriers.
+    __syncwarp();
     const unsigned am = __ballot_sync(0xffffffffu, active);
     if (!am) break;
     if (step > max_steps) {
