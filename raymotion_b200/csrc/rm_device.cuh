@@ -154,20 +154,6 @@ struct Rng {
   }
 };
 
-// The state k draws after `state`: the generator's step s -> a s + c (mod
-// 2^32) composed k times, by squaring (k < 2^8).
-__device__ __forceinline__ uint32_t rng_jump(uint32_t state, uint32_t k) {
-  uint32_t a = 747796405u, c = 2891336453u, A = 1u, C = 0u;
-#pragma unroll
-  for (int bit = 0; bit < 8; ++bit) {
-    if (k & 1u) { A = A * a; C = C * a + c; }
-    c = c * a + c;
-    a = a * a;
-    k >>= 1;
-  }
-  return A * state + C;
-}
-
 __device__ __forceinline__ uint64_t seed_pixel(uint64_t seed, uint32_t x, uint32_t y) {
   return seed ^ (uint64_t(y + 1) * 0x9E3779B97F4A7C15ull) ^ (uint64_t(x + 1) * 0xBF58476D1CE4E5B9ull);
 }
@@ -572,9 +558,6 @@ struct Tracer {
   Rng rng;
   uint32_t rays, nodes, tests;
   uint32_t* err;
-  // lanes that share this path in direct_lighting_deferred_warp: an aligned
-  // group of 8, 16 or 32 lanes of the warp
-  uint32_t group = 32;
 
   __device__ __forceinline__ Tracer(const Scene& s_, const Params& p_, uint32_t* e)
       : s(s_), p(p_), rays(0), nodes(0), tests(0), err(e) {}
@@ -1126,129 +1109,6 @@ struct Tracer {
     o_b = sel_Fb * W * wnee;
     // the selected light and the factor k of o = Le * f * k (held by the adjoint)
     if (parts) { parts[0] = __int_as_float(sel_li); parts[1] = sel_sa * W * wnee; }
-  }
-
-  // direct_lighting_deferred with its Mc candidates spread over the lanes of
-  // the calling lane group (pathtrace.metal:385-469): `group` aligned lanes
-  // (8, 16 or 32) call it with the same arguments and the same random state,
-  // and each returns the same results.  A candidate takes exactly four draws
-  // (light pick, two barycentrics, the reservoir's acceptance draw), so
-  // candidate j starts at draw 4j of the stream: a jump of the generator's
-  // state.  In round r, lane l of the group evaluates candidate r*group + l
-  // with the loop body's arithmetic; then every lane runs the reservoir's
-  // running sum and acceptance tests over that round's candidates in order,
-  // as the loop does: the selection, the sums and the state after the last
-  // draw are bit-identical.
-  __device__ void direct_lighting_deferred_warp(float px, float py, float pz, float nx, float ny, float nz, float wox,
-                                                float woy, float woz, float rough, float metallic, float spec_prob,
-                                                float ar, float ag, float ab, float& o_r, float& o_g, float& o_b,
-                                                float& out_sumW, uint32_t& out_M, bool& has_ray, float& sox,
-                                                float& soy, float& soz, float& sdx, float& sdy, float& sdz,
-                                                float& sdist) {
-    o_r = o_g = o_b = 0.0f;
-    out_sumW = 0.0f;
-    out_M = 0;
-    has_ray = false;
-    if (p.lights == 0 || !(p.light_total > 1e-12f)) return;
-    int Mc = p.restir_candidates;
-    if (Mc < 1) Mc = 1;
-    if (Mc > 32) Mc = 32;
-    if (Mc <= 1) {
-      nee_single_deferred(px, py, pz, nx, ny, nz, wox, woy, woz, rough, metallic, spec_prob, ar, ag, ab, o_r, o_g,
-                          o_b, out_sumW, out_M, has_ray, sox, soy, soz, sdx, sdy, sdz, sdist);
-      return;
-    }
-    float r2 = rough;
-    if (r2 < 0.0f) r2 = 0.0f;
-    if (r2 > 1.0f) r2 = 1.0f;
-    if (r2 < 0.02f) r2 = 0.02f;
-    float alpha2 = (r2 * r2) * (r2 * r2);
-    const float LT = p.light_total;
-    const int G = int(group);
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t gl = lane & uint32_t(G - 1);
-    const uint32_t gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane - gl));
-    const uint32_t s0 = rng.state;
-    const BsdfPrep bp = prep_bsdf(wox, woy, woz, nx, ny, nz, alpha2, metallic, ar, ag, ab);
-    float sumW = 0.0f;
-    bool have = false;
-    float sel_lx = 0, sel_ly = 0, sel_lz = 0, sel_Fr = 0, sel_Fg = 0, sel_Fb = 0, sel_phat = 0, sel_epdf = 0;
-    for (int base = 0; base < Mc; base += G) {
-      const int j = base + int(gl);
-      float w = 0, ph = 0, epdf = 0, Fr = 0, Fg = 0, Fb = 0, qx = 0, qy = 0, qz = 0, racc = 0;
-      if (j < Mc) {
-        Rng lr;
-        lr.state = rng_jump(s0, 4u * uint32_t(j));
-        float pick = lr.uniform01() * LT;
-        const int li = pick_light(pick);
-        const LightRec t = load_light(s, li);
-        float lu = lr.uniform01(), lv = lr.uniform01();
-        if (lu + lv > 1.0f) { lu = 1.0f - lu; lv = 1.0f - lv; }
-        float lw = 1.0f - lu - lv;
-        qx = lw * t.v0.x + (lu * t.v1.x + lv * t.v2.x);
-        qy = lw * t.v0.y + (lu * t.v1.y + lv * t.v2.y);
-        qz = lw * t.v0.z + (lu * t.v1.z + lv * t.v2.z);
-        float ldx = qx - px, ldy = qy - py, ldz = qz - pz;
-        float dist = sqrtf(ldx * ldx + ldy * ldy + ldz * ldz);
-        if (dist > 0.003f) {
-          float inv = 1.0f / dist;
-          float dxn = ldx * inv, dyn = ldy * inv, dzn = ldz * inv;
-          float lcos = -(t.nn.x * dxn + (t.nn.y * dyn + t.nn.z * dzn));
-          float scos = nx * dxn + (ny * dyn + nz * dzn);
-          if (lcos > 1e-8f && scos > 1e-8f) {
-            float lt_lum = lum3(t.er, t.eg, t.eb);
-            if (lt_lum < 1e-6f) lt_lum = 1e-6f;
-            float q = dist * dist * lt_lum / (lcos * LT);
-            if (q > 1e-12f) {
-              Bsdf e = eval_bsdf_prep(bp, dxn, dyn, dzn, wox, woy, woz, nx, ny, nz, alpha2, spec_prob);
-              epdf = e.pdf;
-              Fr = t.er * e.r * scos * t.alpha;
-              Fg = t.eg * e.g * scos * t.alpha;
-              Fb = t.eb * e.b * scos * t.alpha;
-              ph = lum3(Fr, Fg, Fb);
-              if (ph > 0.0f) w = ph / q;
-            }
-          }
-        }
-        racc = lr.uniform01();
-      }
-      // this round's candidates in order, on every lane of the group
-      const int n_round = min(G, Mc - base);
-      int selk = -1;
-      for (int k = 0; k < n_round; ++k) {
-        const float wk = __shfl_sync(gmask, w, k, G);
-        const float rk = __shfl_sync(gmask, racc, k, G);
-        sumW += wk;
-        if (wk > 0.0f && rk * sumW < wk) selk = k;
-      }
-      if (selk >= 0) {
-        have = true;
-        sel_lx = __shfl_sync(gmask, qx, selk, G); sel_ly = __shfl_sync(gmask, qy, selk, G);
-        sel_lz = __shfl_sync(gmask, qz, selk, G);
-        sel_Fr = __shfl_sync(gmask, Fr, selk, G); sel_Fg = __shfl_sync(gmask, Fg, selk, G);
-        sel_Fb = __shfl_sync(gmask, Fb, selk, G);
-        sel_phat = __shfl_sync(gmask, ph, selk, G); sel_epdf = __shfl_sync(gmask, epdf, selk, G);
-      }
-    }
-    rng.state = rng_jump(s0, 4u * uint32_t(Mc));
-    out_sumW = sumW;
-    out_M = uint32_t(Mc);
-    if (!have || !(sumW > 0.0f) || !(sel_phat > 0.0f)) return;
-    float pdf_ris = float(Mc) * sel_phat / sumW;
-    float wnee = 1.0f;
-    if (!p.nomis && sel_epdf > 1e-20f) wnee = pdf_ris / (pdf_ris + sel_epdf);
-    float vdx = sel_lx - px, vdy = sel_ly - py, vdz = sel_lz - pz;
-    float vdist = sqrtf(vdx * vdx + vdy * vdy + vdz * vdz);
-    if (!(vdist > 0.003f)) return;
-    float vinv = 1.0f / vdist;
-    vdx *= vinv; vdy *= vinv; vdz *= vinv;
-    has_ray = true;
-    sox = px + nx * 0.002f; soy = py + ny * 0.002f; soz = pz + nz * 0.002f;
-    sdx = vdx; sdy = vdy; sdz = vdz; sdist = vdist - 0.003f;
-    float W = sumW / (float(Mc) * sel_phat);
-    o_r = sel_Fr * W * wnee;
-    o_g = sel_Fg * W * wnee;
-    o_b = sel_Fb * W * wnee;
   }
 
   __device__ static __forceinline__ float fresnel(float ci_in, float eta_in, float eta_out) {

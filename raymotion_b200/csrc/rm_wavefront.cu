@@ -359,11 +359,9 @@ __global__ void __launch_bounds__(128) k_wf_trace2(Scene s, WfState w, WfQueues 
 template <int VK, int NEE>
 __device__ __forceinline__ void shade_path(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w, int id,
                                            float* __restrict__ hdr, uint32_t* __restrict__ dbg, uint32_t* err,
-                                           bool& ext, bool& shd, bool& fin, uint32_t& samples,
-                                           uint32_t group = 32) {
+                                           bool& ext, bool& shd, bool& fin, uint32_t& samples) {
   const uint32_t x = uint32_t(id) % uint32_t(p.width), y = uint32_t(id) / uint32_t(p.width);
   Tracer pt(s, p, err);
-  pt.group = group;  // NEE variant 3: the lanes that share this path
   PathRegs r;
   uint32_t n;
   float sr, sg, sb;
@@ -497,66 +495,14 @@ __device__ __forceinline__ bool tail_step(const Scene& s, const Params& p, const
   return ext || fin;
 }
 
-// One vertex step of a tail pixel by an aligned group of G lanes (8, 16 or
-// 32; opaque scenes).  Every lane of the group runs the same step on the same
-// path, so each holds the same state: the shading is executed redundantly,
-// except that the RIS candidates of the vertex are spread over the group's
-// lanes (shade_path NEE variant 3), and the extension ray (the group's first
-// half) and the pending shadow ray (its second half) are traversed at the
-// same time, by one instruction stream with the any-hit rule as a flag.  The
-// results are the thread-per-pixel step's bit for bit.  Returns, on every
-// lane of the group, bit 0: the pixel has work left, bit 1: its next step
-// starts with an extension ray.
-__device__ __noinline__ uint32_t tail_group_step(const Scene& s, const Params& p, const GBufSoA& gb,
-                                                 const WfState& w, int id, bool ext, uint32_t G,
-                                                 float* __restrict__ hdr, uint32_t* __restrict__ dbg, uint32_t* err,
-                                                 uint32_t& samples, uint32_t* cnt) {
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t gl = lane & (G - 1u);
-  const uint32_t gmask = G == 32u ? 0xffffffffu : (((1u << G) - 1u) << (lane - gl));
-  const uint32_t half = G / 2u;
-  const bool shadow_half = gl >= half;
-  const bool pending_shadow = (w.u[id].y & kShadow) != 0;
-  const bool mine = shadow_half ? pending_shadow : ext;
-  uint32_t nodes = 0, tests = 0;
-  int tri = -1;
-  if (mine) {
-    const float4 o = shadow_half ? w.so[id] : w.o[id];
-    const float4 d = shadow_half ? w.sd[id] : w.d[id];
-    const TraceResult r = traverse_rt(s, o.x, o.y, o.z, d.x, d.y, d.z, shadow_half ? o.w : kFar, shadow_half, err,
-                                      nodes, tests);
-    tri = r.tri;
-    if (gl == 0u) w.hit[id] = make_float4(r.t, r.u, r.v, __int_as_float(r.tri));
-    if (gl == half) w.occ[id] = r.tri >= 0 ? 1u : 0u;
-  }
-  if (gl == 0u && ext) { ++cnt[0]; cnt[1] += nodes; cnt[2] += tests; }
-  if (gl == half && pending_shadow) { ++cnt[3]; cnt[4] += nodes; cnt[5] += tests; }
-  const int ext_tri = __shfl_sync(gmask, tri, 0, int(G));
-  int vk = 2;
-  if (ext && ext_tri >= 0) vk = __ldg(&s.tris[ext_tri].ior) > 1.0001f ? 1 : 0;
-  __syncwarp(gmask);  // the hit and occlusion words above are visible to every lane of the group
-  bool shd = false, fin = false;
-  uint32_t n = 0;
-  ext = false;
-  if (vk == 0) shade_path<0, 3>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, n, G);
-  else if (vk == 1) shade_path<1, 3>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, n, G);
-  else shade_path<2, 3>(s, p, gb, w, id, hdr, dbg, err, ext, shd, fin, n, G);
-  if (gl == 0u) samples += n;
-  __syncwarp(gmask);  // every lane's copy of the path state is stored before the next step loads it
-  return ((ext || fin) ? 1u : 0u) | (ext ? 2u : 0u);
-}
-
 // The end of the wavefront loop, once few paths remain: each thread takes an
 // unfinished pixel and runs it to the end with the waves' steps, in their
 // order (extension ray, pending shadow ray, shade_path of the vertex type), so
 // the pixel comes out the same, without a launch and a queue round trip per
-// vertex.  When at most four pixels are left in a warp (its last, longest
-// chains), they are shared out to groups of 8, 16 or 32 lanes, one group per
-// pixel, regrouped after every vertex step (tail_group_step, opaque scenes).
-// ctr: the stage
-// counter of the tail's samples; ctr_ext / ctr_shd: its traversals'.  Three
-// 128-thread blocks per SM (up to 168 registers, few spills): the tail is
-// latency-bound and its path count is capped to one wave of resident blocks.
+// vertex.  ctr: the stage counter of the tail's samples; ctr_ext / ctr_shd:
+// its traversals'.  Three 128-thread blocks per SM (up to 168 registers, few
+// spills): the tail is latency-bound and its path count is capped to one wave
+// of resident blocks.
 template <int NEE>
 __global__ void __launch_bounds__(128, 3) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
                                                  float* __restrict__ hdr, uint32_t* __restrict__ dbg,
@@ -564,7 +510,6 @@ __global__ void __launch_bounds__(128, 3) k_wf_tail(Scene s, Params p, GBufSoA g
                                                  unsigned long long* ctr_shd, uint32_t* err) {
   const int n_ext = q.counts[kCntExt], n_c = q.counts[kCntC];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t lane = threadIdx.x & 31u;
   uint32_t samples = 0;
   uint32_t cnt[6] = {0, 0, 0, 0, 0, 0};
   bool active = i < n_ext + n_c;
@@ -575,40 +520,15 @@ __global__ void __launch_bounds__(128, 3) k_wf_tail(Scene s, Params p, GBufSoA g
     ext = i < n_ext;
     if (bad_index(id, (long long)p.width * p.height, err, kSiteTailQueue)) active = false;
   }
-  // each pass of the loop advances every active pixel by one vertex, and a
-  // pixel has at most spp x (depth + 2) vertices left: past that, flag and stop
+  // each pass of the loop advances the pixel by one vertex, and a pixel has
+  // at most spp x (depth + 2) vertices left: past that, flag and stop
   const uint32_t max_steps = uint32_t(p.spp) * uint32_t(p.bounces + 2) * 4u + 64u;
-  for (uint32_t step = 0;; ++step) {
-    // A pixel changes hands between steps (its own lane, then a lane group,
-    // then another group): the previous step's stores of its path state must
-    // be ordered before the next owner's loads, and the ballot and shuffles
-    // below are not memory barriers.
-    __syncwarp();
-    const unsigned am = __ballot_sync(0xffffffffu, active);
-    if (!am) break;
+  for (uint32_t step = 0; active; ++step) {
     if (step > max_steps) {
-      if (lane == 0u) atomicOr(err, kErrSteps);
+      atomicOr(err, kErrSteps);
       break;
     }
-    const int k_left = __popc(am);
-    if (NEE == 2 && k_left <= 4) {
-      // group g (of G lanes) takes the pixel of the g-th active lane
-      const uint32_t G = k_left == 1 ? 32u : (k_left == 2 ? 16u : 8u);
-      const int g = int(lane / G);
-      unsigned m = am;
-      for (int k = 0; k < g && m; ++k) m &= m - 1u;
-      const int owner = m ? __ffs(m) - 1 : 0;
-      const int pid = __shfl_sync(0xffffffffu, id, owner);
-      const bool pext = __shfl_sync(0xffffffffu, ext ? 1 : 0, owner) != 0;
-      uint32_t res = 0;
-      if (g < k_left) res = tail_group_step(s, p, gb, w, pid, pext, G, hdr, dbg, err, samples, cnt);
-      // each active lane reads its pixel's outcome from its group's first lane
-      const int rank = __popc(am & ((1u << lane) - 1u));
-      const uint32_t mine = __shfl_sync(0xffffffffu, res, (rank & 3) * int(G));
-      if (active) { active = (mine & 1u) != 0; ext = (mine & 2u) != 0; }
-      continue;
-    }
-    if (active) active = tail_step<NEE>(s, p, gb, w, id, ext, hdr, dbg, err, samples, cnt);
+    active = tail_step<NEE>(s, p, gb, w, id, ext, hdr, dbg, err, samples, cnt);
   }
   __syncwarp();
   warp_add(ctr + 0, samples);

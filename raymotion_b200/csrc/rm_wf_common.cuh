@@ -59,9 +59,7 @@ __device__ __forceinline__ void clamp3(const Params& p, float& r, float& g, floa
 // MAT 0: opaque surface, 1: dielectric (hit.ior > 1.0001).  NEE 0: the scene
 // is opaque and NEE takes one candidate (the single-candidate branch inlined);
 // 1: any scene and candidate count; 2: an opaque scene, any candidate count
-// (without the in-place shadow test of partially transparent scenes); 3: as 2,
-// with the whole warp on one path (every lane calls with the same path) and
-// the RIS candidates spread over its lanes.
+// (without the in-place shadow test of partially transparent scenes).
 template <int MAT, int NEE = 1>
 __device__ bool vertex(Tracer& pt, const Params& p, PathRegs& r, const Hit& hit, bool& has_shadow, float4& so,
                        float4& sd, float4& c) {
@@ -147,10 +145,6 @@ __device__ bool vertex(Tracer& pt, const Params& p, PathRegs& r, const Hit& hit,
         pt.nee_single_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob,
                                hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray, sox, soy, soz, sdx,
                                sdy, sdz, sdist);
-      else if (NEE == 3)
-        pt.direct_lighting_deferred_warp(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic,
-                                         spec_prob, hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray,
-                                         sox, soy, soz, sdx, sdy, sdz, sdist);
       else
         pt.direct_lighting_deferred(hit.px, hit.py, hit.pz, pnx, pny, pnz, wox, woy, woz, rough, metallic, spec_prob,
                                   hit.ar, hit.ag, hit.ab, dlr, dlg, dlb, cur_sumW, cur_M, has_ray, sox, soy, soz,

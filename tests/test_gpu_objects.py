@@ -29,7 +29,12 @@ def _check_world(backend, models, instances):
     return ps
 
 
-def test_commit_equals_host_world_and_follows_the_refit_policy(backend):
+def test_commit_equals_host_world_and_follows_the_refit_policy():
+    """On a context of its own: the commit count that sets the rebuild
+    schedule runs over the context's lifetime, as the reference's
+    geometry_updates does over its Objects' (runtime.hpp:124-126)."""
+    import raymotion_b200 as rb
+    backend = rb.Backend(0)
     rng = np.random.default_rng(21)
     models = [_model(1, 300), _model(2, 200, emissive=True), _model(3, 150, emissive=True)]
     ids = [backend.model_create(m) for m in models]
@@ -65,6 +70,7 @@ def test_commit_equals_host_world_and_follows_the_refit_policy(backend):
     models2 = [models[0], bent, models[2]]
     backend.instances_commit(dev(instances[:-1]), rebuild_every=0)
     _check_world(backend, models2, instances[:-1])
+    backend.close()
 
 
 def test_rendering_a_committed_world_equals_the_uploaded_world(backend):
