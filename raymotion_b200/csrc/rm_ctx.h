@@ -164,8 +164,12 @@ struct rmcuda_ctx {
   int last_w = 0, last_h = 0;
   // wavefront shading state (rm_wavefront.cu)
   rmd::DevBuf wf[14];
-  rmd::DevBuf wq[11];
-  int* h_counts = nullptr;  // pinned: the current wave's queue lengths
+  // queues of the two halves of a frame (rows of even / odd index), two wave
+  // sets each (5 arrays per set), then their counts; the second half's stream
+  rmd::DevBuf wq[21];
+  int* h_counts = nullptr;  // pinned: the current wave's queue lengths, per half
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   size_t wf_cap = 0;
   uint64_t waves = 0;
   std::vector<int> wave_log;  // last frame: (act, ext, shd, us) per count read
@@ -222,6 +226,21 @@ template <class Fn> cudaError_t staged(rmcuda_ctx* c, int stage, Fn&& fn) {
     c->pending.push_back({stage, a, b});
   }
   c->launches += 1;
+  return e;
+}
+
+// As staged2(), on another stream of the context.
+template <class Fn> cudaError_t staged2_on(rmcuda_ctx* c, int stage, cudaStream_t st, Fn&& fn) {
+  c->launches += 1;
+  if (c->profiling < 2) return fn();
+  NvtxRange range(stage_name(stage));
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess) cudaEventRecord(a, st);
+  cudaError_t e = fn();
+  if (a && b) {
+    cudaEventRecord(b, st);
+    c->pending.push_back({stage, a, b});
+  }
   return e;
 }
 

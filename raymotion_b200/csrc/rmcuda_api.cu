@@ -349,11 +349,11 @@ cudaError_t ensure_wavefront(rmcuda_ctx* c, size_t npix) {
   cudaError_t e;
   for (int i = 0; i < 14; ++i)
     if ((e = c->wf[i].reserve(npix * (i < 12 ? sizeof(float4) : sizeof(uint32_t)))) != cudaSuccess) return e;
-  for (int i = 0; i < 10; ++i)
+  for (int i = 0; i < 20; ++i)
     if ((e = c->wq[i].reserve(npix * sizeof(int))) != cudaSuccess) return e;
-  if ((e = c->wq[10].reserve(2 * kCntSlots * sizeof(int))) != cudaSuccess) return e;
+  if ((e = c->wq[20].reserve(4 * kCntSlots * sizeof(int))) != cudaSuccess) return e;
   if (!c->h_counts &&
-      (e = cudaMallocHost(reinterpret_cast<void**>(&c->h_counts), kCntSlots * sizeof(int))) != cudaSuccess)
+      (e = cudaMallocHost(reinterpret_cast<void**>(&c->h_counts), 2 * kCntSlots * sizeof(int))) != cudaSuccess)
     return e;
   c->wf_cap = npix;
   return cudaSuccess;
@@ -377,114 +377,172 @@ static int tail_paths(int first_bound, bool opaque) {
 cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, uint64_t seed, std::string& msg) {
   NvtxRange range("rm wavefront shading loop");
   const size_t npix = size_t(p.width) * size_t(p.height);
-  cudaStream_t st = c->stream;
   cudaError_t e = ensure_wavefront(c, npix);
   if (e != cudaSuccess) { msg = cuda_msg("wavefront allocation failed", e); return e; }
   WfState w{c->wf[0].as<uint4>(), c->wf[1].as<float4>(), c->wf[2].as<float4>(), c->wf[3].as<float4>(),
             c->wf[4].as<float4>(), c->wf[5].as<float4>(), c->wf[6].as<float4>(), c->wf[7].as<float4>(),
             c->wf[8].as<float4>(), c->wf[9].as<float4>(), c->wf[10].as<float4>(), c->wf[11].as<float4>(),
             c->wf[12].as<uint32_t>(), c->wf[13].as<uint32_t>()};
-  int* counts = c->wq[10].as<int>();
-  WfQueues q[2];
-  for (int k = 0; k < 2; ++k)
-    q[k] = WfQueues{c->wq[5 * k + 0].as<int>(), c->wq[5 * k + 1].as<int>(), c->wq[5 * k + 2].as<int>(),
-                    c->wq[5 * k + 3].as<int>(), c->wq[5 * k + 4].as<int>(), counts + kCntSlots * k};
-  unsigned long long* ctr = c->ctr.as<unsigned long long>();
-  uint32_t* err = c->err.as<uint32_t>();
-  if ((e = cudaMemsetAsync(counts, 0, 2 * kCntSlots * sizeof(int), st)) != cudaSuccess) {
-    msg = cuda_msg("memset", e);
-    return e;
-  }
-  e = staged2(c, RM_STAGE_WF_SHADE, [&] {
-    return launch_wavefront_init(s, p, seed, c->gb.view(), c->rmerged.view(), w, q[0], c->hdr.as<float>(),
-                                 c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, st);
-  });
-  if (e != cudaSuccess) { msg = cuda_msg("wavefront init failed", e); return e; }
-  int cur = 0;
-  c->wave_log.clear();
-  // Every unfinished pixel has its path either in the extension queue or (if it
-  // only waits for a shadow ray) in queue c, and the number of unfinished
-  // pixels only shrinks: ext + c read every kBatch waves bounds all queues of
-  // the next waves, which size their grids; kernels read exact lengths on the
-  // device.
-  const int kBatch = 4;
-  const uint64_t max_waves = uint64_t(p.spp) * uint64_t(p.bounces + 2) * 4 + 64;
   // One launch per wave for the traversals and one for the shading queues
   // (each launch's slowest warps then overlap the others' work);
   // RAYMOTION_CUDA_SPLIT_WAVES=1 launches each traversal and queue alone.
   const char* split_env = std::getenv("RAYMOTION_CUDA_SPLIT_WAVES");
   const bool merged = !(split_env && split_env[0] == '1');
+  // The frame's pixels in two halves (even and odd rows) with their own queues,
+  // waves and tail, on two streams: every launch ends with its slowest warps
+  // while the GPU idles, and the other half's launches fill that time.  A
+  // pixel's steps are the same either way.  RAYMOTION_CUDA_STREAMS=1: one.
+  const char* streams_env = std::getenv("RAYMOTION_CUDA_STREAMS");
+  bool two = merged && !(streams_env && streams_env[0] == '1') && p.height > 1;
+  if (two && !c->side_stream) {
+    if (cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      two = false;
+    }
+  }
+  const int halves = two ? 2 : 1;
+  cudaStream_t sts[2] = {c->stream, two ? c->side_stream : c->stream};
+  // on an early return (an error), the second half's queued work finishes
+  // before the next frame can reuse the path state
+  struct SideSync {
+    cudaStream_t st;
+    ~SideSync() { if (st) cudaStreamSynchronize(st); }
+  } side_sync{two ? c->side_stream : nullptr};
+  int* counts = c->wq[20].as<int>();
+  WfQueues q[2][2];
+  for (int h = 0; h < 2; ++h)
+    for (int k = 0; k < 2; ++k) {
+      DevBuf* b = c->wq + 10 * h + 5 * k;
+      q[h][k] = WfQueues{b[0].as<int>(), b[1].as<int>(), b[2].as<int>(), b[3].as<int>(), b[4].as<int>(),
+                         counts + kCntSlots * (2 * h + k)};
+    }
+  unsigned long long* ctr = c->ctr.as<unsigned long long>();
+  uint32_t* err = c->err.as<uint32_t>();
+  if ((e = cudaMemsetAsync(counts, 0, 4 * kCntSlots * sizeof(int), c->stream)) != cudaSuccess) {
+    msg = cuda_msg("memset", e);
+    return e;
+  }
+  e = staged2(c, RM_STAGE_WF_SHADE, [&] {
+    return launch_wavefront_init(s, p, seed, c->gb.view(), c->rmerged.view(), w, q[0][0], q[halves - 1][0],
+                                 c->hdr.as<float>(), c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err,
+                                 c->stream);
+  });
+  if (e != cudaSuccess) { msg = cuda_msg("wavefront init failed", e); return e; }
+  if (two && ((e = cudaEventRecord(c->ev_fork, c->stream)) != cudaSuccess ||
+              (e = cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0)) != cudaSuccess)) {
+    msg = cuda_msg("stream fork failed", e);
+    return e;
+  }
+  c->wave_log.clear();
+  // Every unfinished pixel of a half has its path either in the half's
+  // extension queue or (if it only waits for a shadow ray) in its queue c,
+  // and the number of unfinished pixels only shrinks: ext + c read every
+  // kBatch waves bounds all queues of the half's next waves, which size their
+  // grids; kernels read exact lengths on the device.
+  const int kBatch = 4;
+  const uint64_t max_waves = uint64_t(p.spp) * uint64_t(p.bounces + 2) * 4 + 64;
+  int cur[2] = {0, 0};
+  bool done[2] = {false, halves < 2};
+  int bound[2] = {0, 0};
   std::chrono::steady_clock::time_point t0;
   int tail = 0;
-  for (uint64_t wave = 0;;) {
+  for (uint64_t wave = 0;; wave += kBatch) {
     if (wave > max_waves) { msg = "wavefront did not drain"; return cudaErrorLaunchFailure; }
-    if ((e = cudaMemcpyAsync(c->h_counts, counts + kCntSlots * cur, kCntSlots * sizeof(int), cudaMemcpyDeviceToHost,
-                             st)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
-      msg = cuda_msg("wavefront count read failed", e);
-      return e;
+    for (int h = 0; h < 2; ++h)
+      if (!done[h] && (e = cudaMemcpyAsync(c->h_counts + kCntSlots * h, q[h][cur[h]].counts, kCntSlots * sizeof(int),
+                                           cudaMemcpyDeviceToHost, sts[h])) != cudaSuccess) {
+        msg = cuda_msg("wavefront count read failed", e);
+        return e;
+      }
+    for (int h = 0; h < 2; ++h)
+      if (!done[h] && (e = cudaStreamSynchronize(sts[h])) != cudaSuccess) {
+        msg = cuda_msg("wavefront count read failed", e);
+        return e;
+      }
+    int b_all = 0, ext_all = 0, shd_all = 0;
+    for (int h = 0; h < 2; ++h) {
+      if (done[h]) continue;
+      const int* hc = c->h_counts + kCntSlots * h;
+      bound[h] = hc[kCntExt] + hc[kCntC];
+      b_all += bound[h]; ext_all += hc[kCntExt]; shd_all += hc[kCntShd];
     }
-    const int bound = c->h_counts[kCntExt] + c->h_counts[kCntC];
     const auto now = std::chrono::steady_clock::now();
     if (wave == 0) {
       t0 = now;
-      tail = tail_paths(bound, p.opaque != 0);
+      tail = tail_paths(b_all, p.opaque != 0) / halves;
     }
-    c->wave_log.insert(c->wave_log.end(), {bound, c->h_counts[kCntExt], c->h_counts[kCntShd],
+    c->wave_log.insert(c->wave_log.end(), {b_all, ext_all, shd_all,
                                            int(std::chrono::duration_cast<std::chrono::microseconds>(now - t0).count())});
-    if (bound == 0) break;
-    if (bound <= tail) {
-      NvtxRange tail_range(stage_name(RM_STAGE_WF_TAIL));
-      e = staged2(c, RM_STAGE_WF_TAIL, [&] {
-        // the tail's traversals are counted with the tail (both kinds in its slot)
-        return launch_wavefront_tail(s, p, c->gb.view(), w, q[cur], bound, c->hdr.as<float>(), c->dbg.as<uint32_t>(),
-                                     ctr + 4 * RM_STAGE_WF_SHADE, ctr + 4 * RM_STAGE_WF_TAIL,
-                                     ctr + 4 * RM_STAGE_WF_TAIL, err, st);
-      });
-      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-      if (e != cudaSuccess) { msg = cuda_msg("wavefront tail failed", e); return e; }
-      // the end of the tail, as a last record with empty queues
-      c->wave_log.insert(c->wave_log.end(), {0, 0, 0, int(std::chrono::duration_cast<std::chrono::microseconds>(
-                                                              std::chrono::steady_clock::now() - t0).count())});
-      break;
+    for (int h = 0; h < 2; ++h) {
+      if (done[h]) continue;
+      if (bound[h] == 0) { done[h] = true; continue; }
+      if (bound[h] <= tail) {
+        NvtxRange tail_range(stage_name(RM_STAGE_WF_TAIL));
+        e = staged2_on(c, RM_STAGE_WF_TAIL, sts[h], [&] {
+          // the tail's traversals are counted with the tail (both kinds in its slot)
+          return launch_wavefront_tail(s, p, c->gb.view(), w, q[h][cur[h]], bound[h], c->hdr.as<float>(),
+                                       c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, ctr + 4 * RM_STAGE_WF_TAIL,
+                                       ctr + 4 * RM_STAGE_WF_TAIL, err, sts[h]);
+        });
+        if (e != cudaSuccess) { msg = cuda_msg("wavefront tail failed", e); return e; }
+        done[h] = true;
+      }
     }
-    for (int k = 0; k < kBatch; ++k, ++wave) {
+    if (done[0] && done[1]) break;
+    for (int k = 0; k < kBatch; ++k) {
       c->waves++;
-      const WfQueues& Q = q[cur];
-      const WfQueues& N = q[cur ^ 1];
-      if (merged && !s.wnodes) {
-        // both traversals in one launch (timed as the extension stage)
-        e = staged2(c, RM_STAGE_WF_EXTEND, [&] {
-          return launch_wavefront_trace2(s, w, Q, bound, ctr + 4 * RM_STAGE_WF_EXTEND, ctr + 4 * RM_STAGE_WF_SHADOW,
-                                         err, st);
-        });
-      } else {
-        e = staged2(c, RM_STAGE_WF_EXTEND, [&] {
-          return launch_wavefront_trace(s, w, Q, bound, false, ctr + 4 * RM_STAGE_WF_EXTEND, err, st);
-        });
-        if (e == cudaSuccess)
-          e = staged2(c, RM_STAGE_WF_SHADOW, [&] {
-            return launch_wavefront_trace(s, w, Q, bound, true, ctr + 4 * RM_STAGE_WF_SHADOW, err, st);
+      for (int h = 0; h < 2; ++h) {
+        if (done[h]) continue;
+        const WfQueues& Q = q[h][cur[h]];
+        const WfQueues& N = q[h][cur[h] ^ 1];
+        const cudaStream_t st = sts[h];
+        const int bd = bound[h];
+        if (merged && !s.wnodes) {
+          // both traversals in one launch (timed as the extension stage)
+          e = staged2_on(c, RM_STAGE_WF_EXTEND, st, [&] {
+            return launch_wavefront_trace2(s, w, Q, bd, ctr + 4 * RM_STAGE_WF_EXTEND, ctr + 4 * RM_STAGE_WF_SHADOW,
+                                           err, st);
           });
+        } else {
+          e = staged2_on(c, RM_STAGE_WF_EXTEND, st, [&] {
+            return launch_wavefront_trace(s, w, Q, bd, false, ctr + 4 * RM_STAGE_WF_EXTEND, err, st);
+          });
+          if (e == cudaSuccess)
+            e = staged2_on(c, RM_STAGE_WF_SHADOW, st, [&] {
+              return launch_wavefront_trace(s, w, Q, bd, true, ctr + 4 * RM_STAGE_WF_SHADOW, err, st);
+            });
+        }
+        if (e == cudaSuccess) e = cudaMemsetAsync(N.counts, 0, kCntSlots * sizeof(int), st);
+        if (merged) {
+          if (e == cudaSuccess)
+            e = staged2_on(c, RM_STAGE_WF_SHADE, st, [&] {
+              return launch_wavefront_shade3(s, p, c->gb.view(), w, Q, bd, N, c->hdr.as<float>(),
+                                             c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, st);
+            });
+        } else {
+          for (int vk = 0; vk < 3 && e == cudaSuccess; ++vk)
+            e = staged2_on(c, RM_STAGE_WF_SHADE, st, [&] {
+              return launch_wavefront_shade(vk, s, p, c->gb.view(), w, Q, bd, N, c->hdr.as<float>(),
+                                            c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, st);
+            });
+        }
+        if (e != cudaSuccess) { msg = cuda_msg("wavefront launch failed", e); return e; }
+        cur[h] ^= 1;
       }
-      if (e == cudaSuccess) e = cudaMemsetAsync(N.counts, 0, kCntSlots * sizeof(int), st);
-      if (merged) {
-        if (e == cudaSuccess)
-          e = staged2(c, RM_STAGE_WF_SHADE, [&] {
-            return launch_wavefront_shade3(s, p, c->gb.view(), w, Q, bound, N, c->hdr.as<float>(),
-                                           c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, st);
-          });
-      } else {
-        for (int vk = 0; vk < 3 && e == cudaSuccess; ++vk)
-          e = staged2(c, RM_STAGE_WF_SHADE, [&] {
-            return launch_wavefront_shade(vk, s, p, c->gb.view(), w, Q, bound, N, c->hdr.as<float>(),
-                                          c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, st);
-          });
-      }
-      if (e != cudaSuccess) { msg = cuda_msg("wavefront launch failed", e); return e; }
-      cur ^= 1;
     }
   }
+  // join: the frame's later stages on the context stream wait for both halves
+  if (two && ((e = cudaEventRecord(c->ev_join, c->side_stream)) != cudaSuccess ||
+              (e = cudaStreamWaitEvent(c->stream, c->ev_join, 0)) != cudaSuccess)) {
+    msg = cuda_msg("stream join failed", e);
+    return e;
+  }
+  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) { msg = cuda_msg("wavefront tail failed", e); return e; }
+  // the end of the loop (the tails included), as a last record with empty queues
+  c->wave_log.insert(c->wave_log.end(), {0, 0, 0, int(std::chrono::duration_cast<std::chrono::microseconds>(
+                                                          std::chrono::steady_clock::now() - t0).count())});
   return cudaSuccess;
 }
 
@@ -679,6 +737,9 @@ void rmcuda_destroy(rmcuda_ctx* c) {
                     &c->adj_scratch, &c->differ, &c->ctr_save})
     b->release();
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->side_stream) cudaStreamDestroy(c->side_stream);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->h_differ) cudaFreeHost(c->h_differ);
   for (DevBuf& b : c->wf) b.release();
   for (DevBuf& b : c->wq) b.release();

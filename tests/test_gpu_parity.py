@@ -110,12 +110,14 @@ def _restir_cfg(flags=0):
 
 
 @pytest.mark.parametrize("shading", ["wavefront", "wavefront-no-tail", "wavefront-all-tail", "wavefront-wide",
-                                     "wavefront-split", "megakernel"])
+                                     "wavefront-split", "wavefront-one-stream", "megakernel"])
 def test_restir_chain_matches_oracle(backend, oracle, small_field, shading, monkeypatch):
     if shading == "megakernel":
         monkeypatch.setenv("RAYMOTION_CUDA_MEGAKERNEL", "1")
     if shading == "wavefront-split":  # each traversal and shading queue in a launch of its own
         monkeypatch.setenv("RAYMOTION_CUDA_SPLIT_WAVES", "1")
+    if shading == "wavefront-one-stream":  # both halves of the frame's pixels on one stream
+        monkeypatch.setenv("RAYMOTION_CUDA_STREAMS", "1")
     if shading == "wavefront-wide":
         monkeypatch.setenv("RAYMOTION_CUDA_WIDE", "1")  # every traversal on the 8-wide BVH
     # the wavefront loop hands its last paths to one tail launch; "no-tail"
