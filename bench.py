@@ -773,12 +773,20 @@ def run_b200(args, world, rank, local):
     secs_max, = allreduce([secs], "max", world, dev)
     samples_sum, rays_sum = allreduce([float(st["path_samples"]), float(st["rays"])], "sum", world, dev)
     value = samples_sum / secs_max
-    # ---- per-kernel breakdown on one more (untimed) frame: every launch event-timed
+    # ---- per-kernel breakdown on one more (untimed) frame: every launch
+    # event-timed, with the wavefront as one part so that launches do not
+    # overlap (the timed frames run its parts on several streams)
     backend.stats_reset()
     backend.profile(2)
+    parts_env = os.environ.get("RAYMOTION_CUDA_STREAMS")
+    os.environ["RAYMOTION_CUDA_STREAMS"] = "1"
     if not args.no_breakdown:
         backend.render_resident_async(cam, cfg, seed0 + args.warmup + args.steps, d_rgb.data_ptr())
     backend.sync()
+    if parts_env is None:
+        del os.environ["RAYMOTION_CUDA_STREAMS"]
+    else:
+        os.environ["RAYMOTION_CUDA_STREAMS"] = parts_env
     kern_t = backend.stage_times()
     kern_c = backend.stage_counters()
     kern_st = backend.stats()
@@ -906,6 +914,9 @@ def run_b200(args, world, rank, local):
                     vs_baseline=None, dtype="f32", data="synthetic (seeded procedural scene)",
                     config=dict(desc, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
                     mrays_per_s=rays_sum / secs_max / 1e6, e2e=e2e, roofline=roofline, cpu_baseline=cpu,
+                    kernel_attribution="kernels_one_frame and roofline: one more frame with every launch "
+                                       "event-timed and the wavefront as one part (no overlapping launches); "
+                                       "the timed frames run the wavefront's parts on their own streams",
                     gpu_launches=int(st["kernel_launches"]), clocks=clk, stages=stage_summary,
                     kernels_one_frame=kernel_summary, wavefront=wave_summary, roofline_screen_space=roofline_ss,
                     roofline_screen_space_large=ss_large,

@@ -164,12 +164,12 @@ struct rmcuda_ctx {
   int last_w = 0, last_h = 0;
   // wavefront shading state (rm_wavefront.cu)
   rmd::DevBuf wf[14];
-  // queues of the two halves of a frame (rows of even / odd index), two wave
-  // sets each (5 arrays per set), then their counts; the second half's stream
-  rmd::DevBuf wq[21];
-  int* h_counts = nullptr;  // pinned: the current wave's queue lengths, per half
-  cudaStream_t side_stream = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // queues of the parts of a frame (rows y mod parts), two wave sets each (5
+  // arrays per set), then their counts; the streams of the parts after the first
+  rmd::DevBuf wq[10 * rmd::kWfParts + 1];
+  int* h_counts = nullptr;  // pinned: the current wave's queue lengths, per part
+  cudaStream_t side_stream[rmd::kWfParts - 1] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[rmd::kWfParts - 1] = {};
   size_t wf_cap = 0;
   uint64_t waves = 0;
   std::vector<int> wave_log;  // last frame: (act, ext, shd, us) per count read

@@ -51,9 +51,16 @@ struct WfQueues {
   int* qc;
   int* counts;  // kCntSlots ints
 };
-// The first wave: odd rows' pixels queue their rays in q1, the others in q.
+// The frame's pixels in up to kWfParts parts by row (row y in part y mod
+// parts), each with its own queues.
+constexpr int kWfParts = 4;
+struct WfParts {
+  WfQueues q[kWfParts];
+  int parts;
+};
+// The first wave: each pixel queues its first ray in its part's queue.
 cudaError_t launch_wavefront_init(const Scene& s, const Params& p, uint64_t seed, const GBufSoA& gb, const ResSoA& rm,
-                                  const WfState& w, const WfQueues& q, const WfQueues& q1, float* hdr, uint32_t* dbg,
+                                  const WfState& w, const WfParts& parts, float* hdr, uint32_t* dbg,
                                   unsigned long long* ctr, uint32_t* err, cudaStream_t st);
 cudaError_t launch_wavefront_trace(const Scene& s, const WfState& w, const WfQueues& q, int bound, bool shadow,
                                    unsigned long long* ctr, uint32_t* err, cudaStream_t st);

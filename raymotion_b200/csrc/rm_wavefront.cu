@@ -188,14 +188,14 @@ __device__ __forceinline__ void write_pixel(const Params& p, uint32_t id, bool i
 
 // Wave 0: per pixel, the kind-1 primary direct light (pathtrace.metal:1097-1128)
 // and the first samples.
-// Pixels of odd rows queue their first rays in q1, the others in q (the two
-// halves of a frame that run on two streams; q1 == q for one).
+// A pixel of row y queues its first ray in part y mod parts (the parts of a
+// frame that run on their own streams).
 __global__ void __launch_bounds__(256) k_wf_init(Scene s, Params p, uint64_t seed, GBufSoA gb, ResSoA rm,
-                                                 WfState w, WfQueues q, WfQueues q1, float* __restrict__ hdr,
+                                                 WfState w, WfParts parts, float* __restrict__ hdr,
                                                  uint32_t* __restrict__ dbg, unsigned long long* ctr, uint32_t* err) {
   const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t npix = uint32_t(p.width) * uint32_t(p.height);
-  const bool odd_row = id < npix && ((id / uint32_t(p.width)) & 1u) != 0;
+  const int part = id < npix ? int((id / uint32_t(p.width)) % uint32_t(parts.parts)) : 0;
   bool push = false, ext = false;
   uint32_t samples = 0;
   if (id < npix) {
@@ -266,8 +266,7 @@ __global__ void __launch_bounds__(256) k_wf_init(Scene s, Params p, uint64_t see
     }
   }
   (void)push;
-  append(q.ext, q.counts + kCntExt, ext && !odd_row, int(id));
-  append(q1.ext, q1.counts + kCntExt, ext && odd_row, int(id));
+  for (int k = 0; k < parts.parts; ++k) append(parts.q[k].ext, parts.q[k].counts + kCntExt, ext && part == k, int(id));
   warp_add(ctr + 0, samples);
 }
 
@@ -547,10 +546,10 @@ __global__ void __launch_bounds__(128, 3) k_wf_tail(Scene s, Params p, GBufSoA g
 }  // namespace
 
 cudaError_t launch_wavefront_init(const Scene& s, const Params& p, uint64_t seed, const GBufSoA& gb, const ResSoA& rm,
-                                  const WfState& w, const WfQueues& q, const WfQueues& q1, float* hdr, uint32_t* dbg,
+                                  const WfState& w, const WfParts& parts, float* hdr, uint32_t* dbg,
                                   unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
   const uint32_t npix = uint32_t(p.width) * uint32_t(p.height);
-  k_wf_init<<<(npix + 255) / 256, 256, 0, st>>>(s, p, seed, gb, rm, w, q, q1, hdr, dbg, ctr, err);
+  k_wf_init<<<(npix + 255) / 256, 256, 0, st>>>(s, p, seed, gb, rm, w, parts, hdr, dbg, ctr, err);
   return cudaGetLastError();
 }
 

@@ -349,11 +349,11 @@ cudaError_t ensure_wavefront(rmcuda_ctx* c, size_t npix) {
   cudaError_t e;
   for (int i = 0; i < 14; ++i)
     if ((e = c->wf[i].reserve(npix * (i < 12 ? sizeof(float4) : sizeof(uint32_t)))) != cudaSuccess) return e;
-  for (int i = 0; i < 20; ++i)
+  for (int i = 0; i < 10 * kWfParts; ++i)
     if ((e = c->wq[i].reserve(npix * sizeof(int))) != cudaSuccess) return e;
-  if ((e = c->wq[20].reserve(4 * kCntSlots * sizeof(int))) != cudaSuccess) return e;
-  if (!c->h_counts &&
-      (e = cudaMallocHost(reinterpret_cast<void**>(&c->h_counts), 2 * kCntSlots * sizeof(int))) != cudaSuccess)
+  if ((e = c->wq[10 * kWfParts].reserve(2 * kWfParts * kCntSlots * sizeof(int))) != cudaSuccess) return e;
+  if (!c->h_counts && (e = cudaMallocHost(reinterpret_cast<void**>(&c->h_counts), kWfParts * kCntSlots * sizeof(int))) !=
+                          cudaSuccess)
     return e;
   c->wf_cap = npix;
   return cudaSuccess;
@@ -388,81 +388,99 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
   // RAYMOTION_CUDA_SPLIT_WAVES=1 launches each traversal and queue alone.
   const char* split_env = std::getenv("RAYMOTION_CUDA_SPLIT_WAVES");
   const bool merged = !(split_env && split_env[0] == '1');
-  // The frame's pixels in two halves (even and odd rows) with their own queues,
-  // waves and tail, on two streams: every launch ends with its slowest warps
-  // while the GPU idles, and the other half's launches fill that time.  A
-  // pixel's steps are the same either way.  RAYMOTION_CUDA_STREAMS=1: one.
-  const char* streams_env = std::getenv("RAYMOTION_CUDA_STREAMS");
-  bool two = merged && !(streams_env && streams_env[0] == '1') && p.height > 1;
-  if (two && !c->side_stream) {
-    if (cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
-      cudaGetLastError();
-      two = false;
-    }
+  // The frame's pixels in parts (row y in part y mod parts) with their own
+  // queues, waves and tail, on their own streams: every launch ends with its
+  // slowest warps while the GPU idles, and the other parts' launches fill that
+  // time.  A pixel's steps are the same either way.  RAYMOTION_CUDA_STREAMS
+  // sets the number of parts (1-4, default 3; on the 720p bench frame 2, 3
+  // and 4 parts measured 310, 314 and 311 M path samples/s, one part 292 M).
+  int parts = 3;
+  if (const char* v = std::getenv("RAYMOTION_CUDA_STREAMS")) parts = std::max(1, std::min(kWfParts, std::atoi(v)));
+  if (!merged || p.height < parts) parts = 1;
+  if (parts > 1 && !c->ev_fork && cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    parts = 1;
   }
-  const int halves = two ? 2 : 1;
-  cudaStream_t sts[2] = {c->stream, two ? c->side_stream : c->stream};
-  // on an early return (an error), the second half's queued work finishes
+  for (int h = 1; h < parts; ++h)
+    if (!c->side_stream[h - 1] &&
+        (cudaStreamCreateWithFlags(&c->side_stream[h - 1], cudaStreamNonBlocking) != cudaSuccess ||
+         cudaEventCreateWithFlags(&c->ev_join[h - 1], cudaEventDisableTiming) != cudaSuccess)) {
+      cudaGetLastError();
+      parts = h;
+      break;
+    }
+  cudaStream_t sts[kWfParts];
+  for (int h = 0; h < kWfParts; ++h) sts[h] = h == 0 || h >= parts ? c->stream : c->side_stream[h - 1];
+  // on an early return (an error), the other parts' queued work finishes
   // before the next frame can reuse the path state
   struct SideSync {
-    cudaStream_t st;
-    ~SideSync() { if (st) cudaStreamSynchronize(st); }
-  } side_sync{two ? c->side_stream : nullptr};
-  int* counts = c->wq[20].as<int>();
-  WfQueues q[2][2];
-  for (int h = 0; h < 2; ++h)
+    cudaStream_t* st;
+    int n;
+    ~SideSync() { for (int h = 1; h < n; ++h) cudaStreamSynchronize(st[h]); }
+  } side_sync{sts, parts};
+  int* counts = c->wq[10 * kWfParts].as<int>();
+  WfQueues q[kWfParts][2];
+  WfParts first{};
+  first.parts = parts;
+  for (int h = 0; h < kWfParts; ++h) {
     for (int k = 0; k < 2; ++k) {
       DevBuf* b = c->wq + 10 * h + 5 * k;
       q[h][k] = WfQueues{b[0].as<int>(), b[1].as<int>(), b[2].as<int>(), b[3].as<int>(), b[4].as<int>(),
                          counts + kCntSlots * (2 * h + k)};
     }
+    first.q[h] = q[h][0];
+  }
   unsigned long long* ctr = c->ctr.as<unsigned long long>();
   uint32_t* err = c->err.as<uint32_t>();
-  if ((e = cudaMemsetAsync(counts, 0, 4 * kCntSlots * sizeof(int), c->stream)) != cudaSuccess) {
+  if ((e = cudaMemsetAsync(counts, 0, 2 * kWfParts * kCntSlots * sizeof(int), c->stream)) != cudaSuccess) {
     msg = cuda_msg("memset", e);
     return e;
   }
   e = staged2(c, RM_STAGE_WF_SHADE, [&] {
-    return launch_wavefront_init(s, p, seed, c->gb.view(), c->rmerged.view(), w, q[0][0], q[halves - 1][0],
-                                 c->hdr.as<float>(), c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err,
-                                 c->stream);
+    return launch_wavefront_init(s, p, seed, c->gb.view(), c->rmerged.view(), w, first, c->hdr.as<float>(),
+                                 c->dbg.as<uint32_t>(), ctr + 4 * RM_STAGE_WF_SHADE, err, c->stream);
   });
   if (e != cudaSuccess) { msg = cuda_msg("wavefront init failed", e); return e; }
-  if (two && ((e = cudaEventRecord(c->ev_fork, c->stream)) != cudaSuccess ||
-              (e = cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0)) != cudaSuccess)) {
+  if (parts > 1 && (e = cudaEventRecord(c->ev_fork, c->stream)) != cudaSuccess) {
     msg = cuda_msg("stream fork failed", e);
     return e;
   }
+  for (int h = 1; h < parts; ++h)
+    if ((e = cudaStreamWaitEvent(sts[h], c->ev_fork, 0)) != cudaSuccess) {
+      msg = cuda_msg("stream fork failed", e);
+      return e;
+    }
   c->wave_log.clear();
-  // Every unfinished pixel of a half has its path either in the half's
+  // Every unfinished pixel of a part has its path either in the part's
   // extension queue or (if it only waits for a shadow ray) in its queue c,
   // and the number of unfinished pixels only shrinks: ext + c read every
-  // kBatch waves bounds all queues of the half's next waves, which size their
-  // grids; kernels read exact lengths on the device.
-  const int kBatch = 4;
+  // kBatch waves bounds all queues of the part's next waves, which size their
+  // grids; kernels read exact lengths on the device.  RAYMOTION_CUDA_WAVE_BATCH
+  // sets kBatch (default 4).
+  int kBatch = 4;
+  if (const char* v = std::getenv("RAYMOTION_CUDA_WAVE_BATCH")) kBatch = std::max(1, std::min(64, std::atoi(v)));
   const uint64_t max_waves = uint64_t(p.spp) * uint64_t(p.bounces + 2) * 4 + 64;
-  int cur[2] = {0, 0};
-  bool done[2] = {false, halves < 2};
-  int bound[2] = {0, 0};
+  int cur[kWfParts] = {};
+  bool done[kWfParts];
+  for (int h = 0; h < kWfParts; ++h) done[h] = h >= parts;
+  int bound[kWfParts] = {};
   std::chrono::steady_clock::time_point t0;
   int tail = 0;
   for (uint64_t wave = 0;; wave += kBatch) {
     if (wave > max_waves) { msg = "wavefront did not drain"; return cudaErrorLaunchFailure; }
-    for (int h = 0; h < 2; ++h)
+    for (int h = 0; h < parts; ++h)
       if (!done[h] && (e = cudaMemcpyAsync(c->h_counts + kCntSlots * h, q[h][cur[h]].counts, kCntSlots * sizeof(int),
                                            cudaMemcpyDeviceToHost, sts[h])) != cudaSuccess) {
         msg = cuda_msg("wavefront count read failed", e);
         return e;
       }
-    for (int h = 0; h < 2; ++h)
+    for (int h = 0; h < parts; ++h)
       if (!done[h] && (e = cudaStreamSynchronize(sts[h])) != cudaSuccess) {
         msg = cuda_msg("wavefront count read failed", e);
         return e;
       }
     int b_all = 0, ext_all = 0, shd_all = 0;
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < parts; ++h) {
       if (done[h]) continue;
       const int* hc = c->h_counts + kCntSlots * h;
       bound[h] = hc[kCntExt] + hc[kCntC];
@@ -471,11 +489,12 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
     const auto now = std::chrono::steady_clock::now();
     if (wave == 0) {
       t0 = now;
-      tail = tail_paths(b_all, p.opaque != 0) / halves;
+      tail = tail_paths(b_all, p.opaque != 0) / parts;
     }
     c->wave_log.insert(c->wave_log.end(), {b_all, ext_all, shd_all,
                                            int(std::chrono::duration_cast<std::chrono::microseconds>(now - t0).count())});
-    for (int h = 0; h < 2; ++h) {
+    bool all_done = true;
+    for (int h = 0; h < parts; ++h) {
       if (done[h]) continue;
       if (bound[h] == 0) { done[h] = true; continue; }
       if (bound[h] <= tail) {
@@ -489,11 +508,12 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
         if (e != cudaSuccess) { msg = cuda_msg("wavefront tail failed", e); return e; }
         done[h] = true;
       }
+      all_done = all_done && done[h];
     }
-    if (done[0] && done[1]) break;
+    if (all_done) break;
     for (int k = 0; k < kBatch; ++k) {
       c->waves++;
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < parts; ++h) {
         if (done[h]) continue;
         const WfQueues& Q = q[h][cur[h]];
         const WfQueues& N = q[h][cur[h] ^ 1];
@@ -533,12 +553,13 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
       }
     }
   }
-  // join: the frame's later stages on the context stream wait for both halves
-  if (two && ((e = cudaEventRecord(c->ev_join, c->side_stream)) != cudaSuccess ||
-              (e = cudaStreamWaitEvent(c->stream, c->ev_join, 0)) != cudaSuccess)) {
-    msg = cuda_msg("stream join failed", e);
-    return e;
-  }
+  // join: the frame's later stages on the context stream wait for every part
+  for (int h = 1; h < parts; ++h)
+    if ((e = cudaEventRecord(c->ev_join[h - 1], sts[h])) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(c->stream, c->ev_join[h - 1], 0)) != cudaSuccess) {
+      msg = cuda_msg("stream join failed", e);
+      return e;
+    }
   if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) { msg = cuda_msg("wavefront tail failed", e); return e; }
   // the end of the loop (the tails included), as a last record with empty queues
   c->wave_log.insert(c->wave_log.end(), {0, 0, 0, int(std::chrono::duration_cast<std::chrono::microseconds>(
@@ -737,9 +758,11 @@ void rmcuda_destroy(rmcuda_ctx* c) {
                     &c->adj_scratch, &c->differ, &c->ctr_save})
     b->release();
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
-  if (c->side_stream) cudaStreamDestroy(c->side_stream);
+  for (int h = 0; h < kWfParts - 1; ++h) {
+    if (c->side_stream[h]) cudaStreamDestroy(c->side_stream[h]);
+    if (c->ev_join[h]) cudaEventDestroy(c->ev_join[h]);
+  }
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
-  if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->h_differ) cudaFreeHost(c->h_differ);
   for (DevBuf& b : c->wf) b.release();
   for (DevBuf& b : c->wq) b.release();

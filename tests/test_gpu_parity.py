@@ -110,14 +110,17 @@ def _restir_cfg(flags=0):
 
 
 @pytest.mark.parametrize("shading", ["wavefront", "wavefront-no-tail", "wavefront-all-tail", "wavefront-wide",
-                                     "wavefront-split", "wavefront-one-stream", "megakernel"])
+                                     "wavefront-split", "wavefront-one-stream", "wavefront-four-streams",
+                                     "megakernel"])
 def test_restir_chain_matches_oracle(backend, oracle, small_field, shading, monkeypatch):
     if shading == "megakernel":
         monkeypatch.setenv("RAYMOTION_CUDA_MEGAKERNEL", "1")
     if shading == "wavefront-split":  # each traversal and shading queue in a launch of its own
         monkeypatch.setenv("RAYMOTION_CUDA_SPLIT_WAVES", "1")
-    if shading == "wavefront-one-stream":  # both halves of the frame's pixels on one stream
+    if shading == "wavefront-one-stream":  # the frame's pixels in one part, on one stream
         monkeypatch.setenv("RAYMOTION_CUDA_STREAMS", "1")
+    if shading == "wavefront-four-streams":  # rows in four parts on four streams
+        monkeypatch.setenv("RAYMOTION_CUDA_STREAMS", "4")
     if shading == "wavefront-wide":
         monkeypatch.setenv("RAYMOTION_CUDA_WIDE", "1")  # every traversal on the 8-wide BVH
     # the wavefront loop hands its last paths to one tail launch; "no-tail"
@@ -318,3 +321,22 @@ def test_speculative_reupload_frames_equal_plain_frames(backend, small_field, mo
         assert np.array_equal(h1.view(np.uint32), h0.view(np.uint32)), k
         assert s1 == s0 and b1 == b0, (k, s1, s0, b1, b0)
     assert on[-1][2] == 3  # built for the first frame, the moved triangles and their return
+
+
+@pytest.mark.parametrize("parts,height", [(4, 3), (3, 7), (2, 1)])
+def test_wavefront_parts_with_few_rows(backend, oracle, small_field, parts, height, monkeypatch):
+    """Frames whose height is below or not a multiple of the number of row
+    parts (fewer rows than parts run as one part): bit-exact radiance, RNG
+    state and sample counts."""
+    monkeypatch.setenv("RAYMOTION_CUDA_STREAMS", str(parts))
+    sc, cam, _ = small_field
+    cfg = RenderConfig(width=96, height=height, spp=4, max_bounces=6, adapt_min=0, restir_candidates=8,
+                       restir_spatial=4, restir_radius=12.0, flags=_abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_DENOISE_OFF)
+    o = oracle.Oracle()
+    backend.reset_history()
+    _, o_hdr, o_st = o.render(sc, cam, cfg, 31)
+    _, g_hdr = backend.render(sc, cam, cfg, 31, hdr=True)
+    assert o_st["chain"] == 2 and backend.stats()["kernel_chain"] == 2
+    npix = cfg.width * cfg.height
+    assert np.array_equal(backend.debug_read(4, npix), o.debug_read(4, npix))
+    assert exact_fraction(g_hdr, o_hdr) == 1.0
