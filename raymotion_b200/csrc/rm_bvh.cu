@@ -661,6 +661,26 @@ __global__ void k_ploc_layout(int n, int root, const float4* __restrict__ blo, c
   atomicMax(depth, d);
 }
 
+// Depth-first (pre-order) record index of each internal node among the
+// internal nodes: one slot per ancestor, plus the internal nodes of every left
+// sibling's subtree on the way up (a subtree of s leaves has s - 1).  The
+// nearer child of a descent then usually sits in the next record.
+__global__ void k_ploc_preorder(int n, int root, const float4* __restrict__ blo, const float4* __restrict__ bhi,
+                                const int2* __restrict__ child, int* __restrict__ pre) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;  // internal node n + k
+  if (k >= n - 1) return;
+  int off = 0, d = 0, cur = n + k;
+  while (cur != root) {
+    const int p = __float_as_int(bhi[cur].w);
+    const int2 c = child[p - n];
+    off += 1;
+    if (c.y == cur) off += __float_as_int(blo[c.x].w) - 1;
+    cur = p;
+    if (++d > 4 * kStack) break;  // a corrupt tree cannot loop forever
+  }
+  pre[k] = off;
+}
+
 __device__ __forceinline__ int ploc_first(int node, int n, const int2* __restrict__ child,
                                           const int* __restrict__ pos) {
   while (node >= n) node = child[node - n].x;
@@ -668,11 +688,12 @@ __device__ __forceinline__ int ploc_first(int node, int n, const int2* __restric
 }
 
 __global__ void k_ploc_emit(int n, int leaf_max, const float4* __restrict__ blo, const float4* __restrict__ bhi,
-                            const int2* __restrict__ child, const int* __restrict__ pos, float4* recs, int* parents) {
+                            const int2* __restrict__ child, const int* __restrict__ pos, const int* __restrict__ pre,
+                            float4* recs, int* parents) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;  // internal node n + k
   if (k >= n - 1) return;
   const int node = n + k;
-  const int rec_id = 2 * n - 2 - node;
+  const int rec_id = pre[k];
   float4* rec = recs + size_t(rec_id) * 4;
   if (__float_as_int(blo[node].w) <= leaf_max) {
     // collapsed into an ancestor's leaf: an unreachable record
@@ -696,7 +717,7 @@ __global__ void k_ploc_emit(int n, int leaf_max, const float4* __restrict__ blo,
       links[s] = ploc_first(c, n, child, pos);
       counts[s] = size;
     } else {
-      links[s] = 2 * n - 2 - c;
+      links[s] = pre[c - n];
       counts[s] = 0;
       parents[links[s]] = (rec_id << 1) | s;
     }
@@ -789,10 +810,12 @@ cudaError_t build_ploc(const rm_triangle* d_tris, int n, int leaf_max, DevBvh& b
   RM_TRY(cudaMemsetAsync(b.depth.ptr, 0, sizeof(int), st));
   k_ploc_layout<<<(n + 255) / 256, 256, 0, st>>>(n, root, blo, bhi, child, sorted, pos, b.order.as<int>(),
                                                  b.depth.as<int>());
+  int* pre = nn;  // the cluster arrays are free once the tree is built
+  k_ploc_preorder<<<(n - 1 + 255) / 256, 256, 0, st>>>(n, root, blo, bhi, child, pre);
   RM_TRY(b.records.reserve(size_t(n - 1) * 4 * sizeof(float4)));
   RM_TRY(b.parents.reserve(size_t(n - 1) * sizeof(int)));
   RM_TRY(b.counters.reserve(size_t(n - 1) * sizeof(int)));
-  k_ploc_emit<<<(n - 1 + 255) / 256, 256, 0, st>>>(n, leaf_max, blo, bhi, child, pos, b.records.as<float4>(),
+  k_ploc_emit<<<(n - 1 + 255) / 256, 256, 0, st>>>(n, leaf_max, blo, bhi, child, pos, pre, b.records.as<float4>(),
                                                    b.parents.as<int>());
   RM_TRY(cudaGetLastError());
   RM_TRY(cudaMemcpyAsync(&b.max_depth, b.depth.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
