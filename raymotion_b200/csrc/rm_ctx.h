@@ -167,7 +167,8 @@ struct rmcuda_ctx {
   // queues of the parts of a frame (rows y mod parts), two wave sets each (5
   // arrays per set), then their counts; the streams of the parts after the first
   rmd::DevBuf wq[10 * rmd::kWfParts + 1];
-  int* h_counts = nullptr;  // pinned: the current wave's queue lengths, per part
+  int* h_counts = nullptr;  // pinned: two reads of the parts' queue lengths (2 x kWfParts x kCntSlots)
+  cudaEvent_t ev_counts[2][rmd::kWfParts] = {};  // the end of each of those reads
   cudaStream_t side_stream[rmd::kWfParts - 1] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[rmd::kWfParts - 1] = {};
   size_t wf_cap = 0;

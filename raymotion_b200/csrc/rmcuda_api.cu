@@ -352,9 +352,13 @@ cudaError_t ensure_wavefront(rmcuda_ctx* c, size_t npix) {
   for (int i = 0; i < 10 * kWfParts; ++i)
     if ((e = c->wq[i].reserve(npix * sizeof(int))) != cudaSuccess) return e;
   if ((e = c->wq[10 * kWfParts].reserve(2 * kWfParts * kCntSlots * sizeof(int))) != cudaSuccess) return e;
-  if (!c->h_counts && (e = cudaMallocHost(reinterpret_cast<void**>(&c->h_counts), kWfParts * kCntSlots * sizeof(int))) !=
-                          cudaSuccess)
+  if (!c->h_counts &&
+      (e = cudaMallocHost(reinterpret_cast<void**>(&c->h_counts), 2 * kWfParts * kCntSlots * sizeof(int))) !=
+          cudaSuccess)
     return e;
+  for (auto& row : c->ev_counts)
+    for (cudaEvent_t& ev : row)
+      if (!ev && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
   c->wf_cap = npix;
   return cudaSuccess;
 }
@@ -454,11 +458,19 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
   // Every unfinished pixel of a part has its path either in the part's
   // extension queue or (if it only waits for a shadow ray) in its queue c,
   // and the number of unfinished pixels only shrinks: ext + c read every
-  // kBatch waves bounds all queues of the part's next waves, which size their
+  // kBatch waves bounds all queues of the part's later waves, which size their
   // grids; kernels read exact lengths on the device.  RAYMOTION_CUDA_WAVE_BATCH
-  // sets kBatch (default 4).
+  // sets kBatch (default 4).  Each batch's waves are sized by the read taken
+  // one batch earlier (its copy has finished while the previous batch's
+  // waves run), so the host never waits for the GPU to drain; the bound is at
+  // most kBatch waves older, the tail starts up to kBatch waves later, and
+  // the pixels come out the same.  RAYMOTION_CUDA_COUNT_LAG=0 sizes each
+  // batch by a read of its own queues, waiting for them.
   int kBatch = 4;
   if (const char* v = std::getenv("RAYMOTION_CUDA_WAVE_BATCH")) kBatch = std::max(1, std::min(64, std::atoi(v)));
+  const char* lag_env = std::getenv("RAYMOTION_CUDA_COUNT_LAG");
+  const bool lag = !(lag_env && lag_env[0] == '0');
+  int slot = 0;
   const uint64_t max_waves = uint64_t(p.spp) * uint64_t(p.bounces + 2) * 4 + 64;
   int cur[kWfParts] = {};
   bool done[kWfParts];
@@ -469,20 +481,25 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
   for (uint64_t wave = 0;; wave += kBatch) {
     if (wave > max_waves) { msg = "wavefront did not drain"; return cudaErrorLaunchFailure; }
     for (int h = 0; h < parts; ++h)
-      if (!done[h] && (e = cudaMemcpyAsync(c->h_counts + kCntSlots * h, q[h][cur[h]].counts, kCntSlots * sizeof(int),
-                                           cudaMemcpyDeviceToHost, sts[h])) != cudaSuccess) {
+      if (!done[h] &&
+          ((e = cudaMemcpyAsync(c->h_counts + kCntSlots * (kWfParts * slot + h), q[h][cur[h]].counts,
+                                kCntSlots * sizeof(int), cudaMemcpyDeviceToHost, sts[h])) != cudaSuccess ||
+           (e = cudaEventRecord(c->ev_counts[slot][h], sts[h])) != cudaSuccess)) {
         msg = cuda_msg("wavefront count read failed", e);
         return e;
       }
+    // the first batch has nothing queued behind its read: it waits for it
+    const int use = lag && wave > 0 ? slot ^ 1 : slot;
+    slot ^= 1;
     for (int h = 0; h < parts; ++h)
-      if (!done[h] && (e = cudaStreamSynchronize(sts[h])) != cudaSuccess) {
+      if (!done[h] && (e = cudaEventSynchronize(c->ev_counts[use][h])) != cudaSuccess) {
         msg = cuda_msg("wavefront count read failed", e);
         return e;
       }
     int b_all = 0, ext_all = 0, shd_all = 0;
     for (int h = 0; h < parts; ++h) {
       if (done[h]) continue;
-      const int* hc = c->h_counts + kCntSlots * h;
+      const int* hc = c->h_counts + kCntSlots * (kWfParts * use + h);
       bound[h] = hc[kCntExt] + hc[kCntC];
       b_all += bound[h]; ext_all += hc[kCntExt]; shd_all += hc[kCntShd];
     }
@@ -767,6 +784,9 @@ void rmcuda_destroy(rmcuda_ctx* c) {
   for (DevBuf& b : c->wf) b.release();
   for (DevBuf& b : c->wq) b.release();
   if (c->h_counts) cudaFreeHost(c->h_counts);
+  for (auto& row : c->ev_counts)
+    for (cudaEvent_t ev : row)
+      if (ev) cudaEventDestroy(ev);
   for (auto& m : c->models) m.tris.release();
   for (DevBuf* b : {&c->prep_inst, &c->prep_mptr, &c->prep_start, &c->prep_keep, &c->prep_kscan, &c->prep_light,
                     &c->prep_lscan, &c->prep_temp, &c->prep_weight, &c->prep_small})

@@ -111,7 +111,7 @@ def _restir_cfg(flags=0):
 
 @pytest.mark.parametrize("shading", ["wavefront", "wavefront-no-tail", "wavefront-all-tail", "wavefront-wide",
                                      "wavefront-split", "wavefront-one-stream", "wavefront-four-streams",
-                                     "megakernel"])
+                                     "wavefront-count-wait", "megakernel"])
 def test_restir_chain_matches_oracle(backend, oracle, small_field, shading, monkeypatch):
     if shading == "megakernel":
         monkeypatch.setenv("RAYMOTION_CUDA_MEGAKERNEL", "1")
@@ -121,6 +121,8 @@ def test_restir_chain_matches_oracle(backend, oracle, small_field, shading, monk
         monkeypatch.setenv("RAYMOTION_CUDA_STREAMS", "1")
     if shading == "wavefront-four-streams":  # rows in four parts on four streams
         monkeypatch.setenv("RAYMOTION_CUDA_STREAMS", "4")
+    if shading == "wavefront-count-wait":  # each batch of waves sized by a read of its own queues
+        monkeypatch.setenv("RAYMOTION_CUDA_COUNT_LAG", "0")
     if shading == "wavefront-wide":
         monkeypatch.setenv("RAYMOTION_CUDA_WIDE", "1")  # every traversal on the 8-wide BVH
     # the wavefront loop hands its last paths to one tail launch; "no-tail"
