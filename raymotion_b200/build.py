@@ -35,7 +35,7 @@ NVFLAGS = ARCH + [
 ]
 CU_SOURCES = ["rm_kernels.cu", "rm_denoise.cu", "rm_bvh.cu", "rmcuda_api.cu", "rm_noalloc.cu", "rm_wavefront.cu",
               "rm_atrous.cu", "rm_batch.cu", "rmcuda_batch.cu", "rm_adjoint.cu", "rm_denoise_adjoint.cu",
-              "rmcuda_adjoint.cu", "rm_wide.cu", "rm_prep.cu"]
+              "rmcuda_adjoint.cu", "rm_wide.cu", "rm_prep.cu", "rm_sort.cu"]
 # Tolerance-checked kernels (approximate exp2 / rsqrt anyway) are compiled with FMA contraction.
 FMA_SOURCES = {"rm_atrous.cu"}
 CXX_SOURCES = ["shim_metal.cpp"]

@@ -8,7 +8,7 @@
 //    child-pair layout of rm_device.cuh on the host in O(nodes), and uploaded;
 //  * without a caller BVH the device builds a linear BVH (Karras, "Maximizing
 //    Parallelism in the Construction of BVHs, Octrees, and k-d Trees", HPG
-//    2012): 30-bit Morton codes of the centroids, a radix sort (CUB), one
+//    2012): 30-bit Morton codes of the centroids, a radix sort (rm_sort.cu), one
 //    thread per internal node to find its range and split, bottom-up boxes
 //    with arrival counters; subtrees of at most `leaf_max` triangles collapse
 //    into leaves;
@@ -16,8 +16,6 @@
 //    same arrival-counter scheme (one pass, no per-level launches).
 // Triangle boxes come from the caller's fp32 vertices, so every box bounds its
 // float triangle exactly.
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,6 +23,7 @@
 #include <vector>
 
 #include "rm_launch.h"
+#include "rm_sort.h"
 
 namespace rmd {
 
@@ -459,14 +458,13 @@ cudaError_t build_lbvh(const rm_triangle* d_tris, int n, int leaf_max, DevBvh& b
   int* vals = reinterpret_cast<int*>(keys + n);
   k_morton<<<(n + 255) / 256, 256, 0, st>>>(d_tris, n, b.bounds.as<unsigned int>(), keys, vals);
   RM_TRY(cudaGetLastError());
-  cub::DoubleBuffer<unsigned int> dk(keys, b.keys_alt.as<unsigned int>());
-  cub::DoubleBuffer<int> dv(vals, b.vals_alt.as<int>());
-  size_t temp_bytes = 0;
-  RM_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, dk, dv, n, 0, 30, st));
+  const size_t temp_bytes = radix_sort_temp_bytes(n);
   RM_TRY(b.temp.reserve(temp_bytes));
-  RM_TRY(cub::DeviceRadixSort::SortPairs(b.temp.ptr, temp_bytes, dk, dv, n, 0, 30, st));
-  const unsigned int* skeys = dk.Current();
-  const int* sorder = dv.Current();
+  bool in_alt = false;
+  RM_TRY(radix_sort_pairs(keys, b.keys_alt.as<unsigned int>(), vals, b.vals_alt.as<int>(), n, 30, b.temp.ptr,
+                          temp_bytes, in_alt, st));
+  const unsigned int* skeys = in_alt ? b.keys_alt.as<unsigned int>() : keys;
+  const int* sorder = in_alt ? b.vals_alt.as<int>() : vals;
   RM_TRY(cudaMemcpyAsync(b.order.ptr, sorder, size_t(n) * sizeof(int), cudaMemcpyDeviceToDevice, st));
   int2* children = b.knodes.as<int2>();
   int2* ranges = children + ni;
@@ -512,15 +510,15 @@ cudaError_t build_lbvh_into(const rm_triangle* d_tris, int n, int leaf_max, cons
     k_centroid_bounds<<<148 * 4, 256, 0, st>>>(d_tris, n, w.bounds);
     k_morton<<<(n + 255) / 256, 256, 0, st>>>(d_tris, n, w.bounds, w.keys, w.vals);
     RM_TRY(cudaGetLastError());
-    cub::DoubleBuffer<unsigned int> dk(w.keys, w.keys_alt);
-    cub::DoubleBuffer<int> dv(w.vals, w.vals_alt);
-    size_t temp_bytes = 0;
-    RM_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, dk, dv, n, 0, 30, st));
-    if (temp_bytes > w.sort_temp_bytes) { err = "sort scratch too small"; return cudaErrorInvalidValue; }
-    RM_TRY(cub::DeviceRadixSort::SortPairs(w.sort_temp, temp_bytes, dk, dv, n, 0, 30, st));
-    RM_TRY(cudaMemcpyAsync(w.order, dv.Current(), size_t(n) * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    if (radix_sort_temp_bytes(n) > w.sort_temp_bytes) { err = "sort scratch too small"; return cudaErrorInvalidValue; }
+    bool in_alt = false;
+    RM_TRY(radix_sort_pairs(w.keys, w.keys_alt, w.vals, w.vals_alt, n, 30, w.sort_temp, w.sort_temp_bytes, in_alt,
+                            st));
+    RM_TRY(cudaMemcpyAsync(w.order, in_alt ? w.vals_alt : w.vals, size_t(n) * sizeof(int), cudaMemcpyDeviceToDevice,
+                           st));
     RM_TRY(cudaMemsetAsync(w.parent_int, 0xff, size_t(ni) * sizeof(int), st));
-    k_karras<<<(ni + 255) / 256, 256, 0, st>>>(dk.Current(), n, w.children, w.ranges, w.parent_int, w.parent_leaf);
+    k_karras<<<(ni + 255) / 256, 256, 0, st>>>(in_alt ? w.keys_alt : w.keys, n, w.children, w.ranges, w.parent_int,
+                                               w.parent_leaf);
     RM_TRY(cudaMemsetAsync(w.kcount, 0, size_t(ni) * sizeof(int), st));
     k_karras_boxes<<<(n + 255) / 256, 256, 0, st>>>(d_tris, w.order, n, w.children, w.parent_int, w.parent_leaf,
                                                     reinterpret_cast<Box*>(w.kbox), w.kcount);
@@ -750,15 +748,12 @@ cudaError_t build_ploc(const rm_triangle* d_tris, int n, int leaf_max, DevBvh& b
   int* vals = reinterpret_cast<int*>(keys + n);
   k_morton<<<(n + 255) / 256, 256, 0, st>>>(d_tris, n, b.bounds.as<unsigned int>(), keys, vals);
   RM_TRY(cudaGetLastError());
-  cub::DoubleBuffer<unsigned int> dk(keys, b.keys_alt.as<unsigned int>());
-  cub::DoubleBuffer<int> dv(vals, b.vals_alt.as<int>());
-  size_t sort_bytes = 0, scan_bytes = 0;
-  RM_TRY(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, dk, dv, n, 0, 30, st));
-  RM_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, static_cast<int*>(nullptr), static_cast<int*>(nullptr), n,
-                                       st));
+  const size_t sort_bytes = radix_sort_temp_bytes(n), scan_bytes = exclusive_scan_temp_bytes(n);
   RM_TRY(b.temp.reserve(std::max(sort_bytes, scan_bytes)));
-  RM_TRY(cub::DeviceRadixSort::SortPairs(b.temp.ptr, sort_bytes, dk, dv, n, 0, 30, st));
-  const int* sorted = dv.Current();
+  bool in_alt = false;
+  RM_TRY(radix_sort_pairs(keys, b.keys_alt.as<unsigned int>(), vals, b.vals_alt.as<int>(), n, 30, b.temp.ptr,
+                          sort_bytes, in_alt, st));
+  const int* sorted = in_alt ? b.vals_alt.as<int>() : vals;
   // node and cluster arrays (kbox: box lo/hi; knodes: children; ranges: 2 cluster lists + nn + 4 flag arrays)
   RM_TRY(b.kbox.reserve(size_t(total) * 2 * sizeof(float4)));
   RM_TRY(b.knodes.reserve(size_t(n) * sizeof(int2)));
@@ -788,8 +783,8 @@ cudaError_t build_ploc(const rm_triangle* d_tris, int n, int leaf_max, DevBvh& b
     for (int attempt = 0; attempt < 2; ++attempt) {
       if (!force) k_ploc_nn<<<g, 256, 0, st>>>(cl, C, blo, bhi, nn);
       k_ploc_flags<<<g, 256, 0, st>>>(nn, C, force, mflag, kflag);
-      RM_TRY(cub::DeviceScan::ExclusiveSum(b.temp.ptr, scan_bytes, mflag, mscan, C, st));
-      RM_TRY(cub::DeviceScan::ExclusiveSum(b.temp.ptr, scan_bytes, kflag, kscan, C, st));
+      RM_TRY(exclusive_scan(mflag, mscan, C, b.temp.ptr, scan_bytes, st));
+      RM_TRY(exclusive_scan(kflag, kscan, C, b.temp.ptr, scan_bytes, st));
       k_ploc_totals<<<1, 1, 0, st>>>(mflag, mscan, kflag, kscan, C, totals);
       RM_TRY(cudaMemcpyAsync(h_tot, totals, sizeof(h_tot), cudaMemcpyDeviceToHost, st));
       RM_TRY(cudaStreamSynchronize(st));

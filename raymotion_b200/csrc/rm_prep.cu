@@ -18,9 +18,9 @@
 // Textures are not carried (models have none: texture_offset -1).
 #include <cuda_runtime.h>
 
-#include <cub/device/device_scan.cuh>
 
 #include "rm_launch.h"
+#include "rm_sort.h"
 
 static_assert(sizeof(rm_model_tri) == 280, "rm_model_tri layout");
 static_assert(sizeof(rm_instance) == 184, "rm_instance layout");
@@ -202,9 +202,8 @@ __global__ void k_prep_cdf(const int* __restrict__ keep, const int* __restrict__
 }  // namespace
 
 cudaError_t prep_scan_bytes(int total, size_t& bytes) {
-  bytes = 0;
-  return cub::DeviceScan::ExclusiveSum(nullptr, bytes, static_cast<int*>(nullptr), static_cast<int*>(nullptr),
-                                       total > 0 ? total : 1);
+  bytes = exclusive_scan_temp_bytes(total > 0 ? total : 1);
+  return cudaSuccess;
 }
 
 cudaError_t prep_world(const PrepArgs& a, cudaStream_t st) {
@@ -214,10 +213,8 @@ cudaError_t prep_world(const PrepArgs& a, cudaStream_t st) {
     const unsigned g = unsigned((a.total + 255) / 256);
     k_prep_flags<<<g, 256, 0, st>>>(a.inst, a.mptr, a.start, a.n_inst, a.total, a.keep, a.light);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    size_t bytes = a.scan_bytes;
-    if ((e = cub::DeviceScan::ExclusiveSum(a.scan_temp, bytes, a.keep, a.kscan, a.total, st)) != cudaSuccess) return e;
-    bytes = a.scan_bytes;
-    if ((e = cub::DeviceScan::ExclusiveSum(a.scan_temp, bytes, a.light, a.lscan, a.total, st)) != cudaSuccess) return e;
+    if ((e = exclusive_scan(a.keep, a.kscan, a.total, a.scan_temp, a.scan_bytes, st)) != cudaSuccess) return e;
+    if ((e = exclusive_scan(a.light, a.lscan, a.total, a.scan_temp, a.scan_bytes, st)) != cudaSuccess) return e;
     k_prep_write<<<g, 256, 0, st>>>(a.inst, a.mptr, a.start, a.n_inst, a.total, a.keep, a.kscan, a.light, a.lscan,
                                     a.out, a.light_tri, a.weight, a.flags);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -37,6 +37,27 @@ def test_device_builders_give_identical_hits(backend, oracle, field, builder, le
     assert _check_hits(backend, oracle, sc, rays) > 0.2
 
 
+def test_device_bvh_quality_near_the_reference_sah_bvh(backend, oracle, field, monkeypatch):
+    """Hits do not depend on the BVH, so a correct tree over a badly ordered
+    build (a broken Morton sort, say) would pass every hit test; its node
+    visits per ray would not.  The device builds stay near the reference's SAH
+    BVH (converted) on the same frame."""
+    from raymotion_b200 import _abi
+    _, cam, cfg = icosphere_field(seed=11, n_spheres=20, subdiv=3, n_emitters=32, width=64, height=36)
+    cfg.flags = _abi.RM_FLAG_NO_ENV | _abi.RM_FLAG_DENOISE_OFF
+    sc = oracle.with_reference_bvh(field)
+    per_ray = {}
+    for name, use_nodes, builder in (("sah", True, "ploc"), ("ploc", False, "ploc"), ("lbvh", False, "lbvh")):
+        monkeypatch.setenv("RAYMOTION_CUDA_BVH", builder)
+        backend.stats_reset()
+        backend.render(sc, cam, cfg, 7, use_nodes=use_nodes)
+        st = backend.stats()
+        assert st["rays"] > 10000
+        per_ray[name] = st["nodes_visited"] / st["rays"]
+    assert per_ray["ploc"] < 2.0 * per_ray["sah"], per_ray
+    assert per_ray["lbvh"] < 3.0 * per_ray["sah"], per_ray
+
+
 def test_degenerate_clusters(backend, oracle):
     """300 copies of one triangle: no mutual nearest neighbours by area ties; the
     build must still terminate, and ties resolve to the smallest index."""
