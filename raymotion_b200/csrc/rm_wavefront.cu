@@ -319,8 +319,12 @@ __global__ void __launch_bounds__(128) k_wf_trace(Scene s, WfState w, WfQueues q
 // (any hit), with the any-hit rule as a per-thread flag so that the two kinds
 // run one instruction stream.  Each launch's time is set by its slowest rays
 // while most of the GPU idles; in one launch the shadow rays fill that time.
-// ctr_ext / ctr_shd: the counters of each kind.
-__global__ void __launch_bounds__(128) k_wf_trace2(Scene s, WfState w, WfQueues q, unsigned long long* ctr_ext,
+// ctr_ext / ctr_shd: the counters of each kind.  Ten blocks per SM (48
+// registers, no spills; nine at 55 by default): 51.5 against 53.1 ms of
+// traversal a frame and 320.9 / 325.2 against 318.7 / 317.4 M path
+// samples/s on the 720p frame; eleven or twelve (40 registers) spill and
+// lose 6 %.
+__global__ void __launch_bounds__(128, 10) k_wf_trace2(Scene s, WfState w, WfQueues q, unsigned long long* ctr_ext,
                                                    unsigned long long* ctr_shd, uint32_t* err) {
   const int n_ext = q.counts[kCntExt], n_shd = q.counts[kCntShd];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -438,9 +442,15 @@ __global__ void __launch_bounds__(256) k_wf_shade(Scene s, Params p, GBufSoA gb,
 // The three shading queues of a wave in one launch: block b serves queue
 // b % 3 (0 opaque hits, 1 dielectric hits, 2 no vertex), so a block's
 // warps take one branch as in k_wf_shade while the three queues' work
-// overlaps instead of running in three launches one after another.
+// overlaps instead of running in three launches one after another.  The
+// opaque variant runs three blocks per SM (80 registers, ~250 bytes of
+// spills, against two at 128): a launch alone runs 8 % slower, but beside the
+// other parts' traversal launches its blocks fit where two did not, and the
+// frame is faster (on the 720p frame 318.1 / 319.7 against 314.3 / 312.6 M
+// path samples/s).  The variant with in-place shadow traversal would spill
+// 600 bytes at 80 registers and keeps two.
 template <int NEE>
-__global__ void __launch_bounds__(256) k_wf_shade3(Scene s, Params p, GBufSoA gb, WfState w, WfQueues cq,
+__global__ void __launch_bounds__(256, NEE == 2 ? 3 : 2) k_wf_shade3(Scene s, Params p, GBufSoA gb, WfState w, WfQueues cq,
                                                    WfQueues nq, float* __restrict__ hdr, uint32_t* __restrict__ dbg,
                                                    unsigned long long* ctr, uint32_t* err) {
   const int vk = int(blockIdx.x % 3u);
