@@ -319,12 +319,13 @@ __global__ void __launch_bounds__(128) k_wf_trace(Scene s, WfState w, WfQueues q
 // (any hit), with the any-hit rule as a per-thread flag so that the two kinds
 // run one instruction stream.  Each launch's time is set by its slowest rays
 // while most of the GPU idles; in one launch the shadow rays fill that time.
-// ctr_ext / ctr_shd: the counters of each kind.  Ten blocks per SM (48
-// registers, no spills; nine at 55 by default): 51.5 against 53.1 ms of
+// ctr_ext / ctr_shd: the counters of each kind.  40 warps per SM (48
+// registers, no spills; 36 at 55 by default): 51.5 against 53.1 ms of
 // traversal a frame and 320.9 / 325.2 against 318.7 / 317.4 M path
-// samples/s on the 720p frame; eleven or twelve (40 registers) spill and
-// lose 6 %.
-__global__ void __launch_bounds__(128, 10) k_wf_trace2(Scene s, WfState w, WfQueues q, unsigned long long* ctr_ext,
+// samples/s on the 720p frame; 44 or 48 warps (40 registers) spill and lose
+// 6 %.  64-thread blocks (20 per SM) fit beside the other parts' launches
+// more easily than 128-thread ones (~1 %).
+__global__ void __launch_bounds__(64, 20) k_wf_trace2(Scene s, WfState w, WfQueues q, unsigned long long* ctr_ext,
                                                    unsigned long long* ctr_shd, uint32_t* err) {
   const int n_ext = q.counts[kCntExt], n_shd = q.counts[kCntShd];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -443,18 +444,19 @@ __global__ void __launch_bounds__(256) k_wf_shade(Scene s, Params p, GBufSoA gb,
 // b % 3 (0 opaque hits, 1 dielectric hits, 2 no vertex), so a block's
 // warps take one branch as in k_wf_shade while the three queues' work
 // overlaps instead of running in three launches one after another.  The
-// opaque variant runs three blocks per SM (80 registers, ~250 bytes of
-// spills, against two at 128): a launch alone runs 8 % slower, but beside the
-// other parts' traversal launches its blocks fit where two did not, and the
-// frame is faster (on the 720p frame 318.1 / 319.7 against 314.3 / 312.6 M
-// path samples/s).  The variant with in-place shadow traversal would spill
-// 600 bytes at 80 registers and keeps two.
+// opaque variant runs 24 warps per SM (80 registers, ~250 bytes of spills,
+// against 16 at 128): a launch alone runs 8 % slower, but beside the other
+// parts' traversal launches its blocks fit where fewer did, and the frame is
+// faster (on the 720p frame 318.1 / 319.7 against 314.3 / 312.6 M path
+// samples/s with 256-thread blocks; 128-thread blocks, which fit into smaller
+// gaps, another ~1 %).  The variant with in-place shadow traversal would
+// spill 600 bytes at 80 registers and keeps 16 warps.
 template <int NEE>
-__global__ void __launch_bounds__(256, NEE == 2 ? 3 : 2) k_wf_shade3(Scene s, Params p, GBufSoA gb, WfState w, WfQueues cq,
+__global__ void __launch_bounds__(128, NEE == 2 ? 6 : 4) k_wf_shade3(Scene s, Params p, GBufSoA gb, WfState w, WfQueues cq,
                                                    WfQueues nq, float* __restrict__ hdr, uint32_t* __restrict__ dbg,
                                                    unsigned long long* ctr, uint32_t* err) {
   const int vk = int(blockIdx.x % 3u);
-  const int i = int(blockIdx.x / 3u) * 256 + int(threadIdx.x);
+  const int i = int(blockIdx.x / 3u) * 128 + int(threadIdx.x);
   const int count = cq.counts[vk == 0 ? kCntA : (vk == 1 ? kCntB : kCntC)];
   const int* queue = vk == 0 ? cq.qa : (vk == 1 ? cq.qb : cq.qc);
   bool ext = false, shd = false, fin = false;
@@ -585,7 +587,7 @@ cudaError_t launch_wavefront_trace2(const Scene& s, const WfState& w, const WfQu
                                     unsigned long long* ctr_ext, unsigned long long* ctr_shd, uint32_t* err,
                                     cudaStream_t st) {
   if (bound <= 0) return cudaSuccess;
-  k_wf_trace2<<<unsigned((2 * bound + 127) / 128), 128, 0, st>>>(s, w, q, ctr_ext, ctr_shd, err);
+  k_wf_trace2<<<unsigned((2 * bound + 63) / 64), 64, 0, st>>>(s, w, q, ctr_ext, ctr_shd, err);
   return cudaGetLastError();
 }
 
@@ -593,9 +595,9 @@ cudaError_t launch_wavefront_shade3(const Scene& s, const Params& p, const GBufS
                                     const WfQueues& cq, int bound, const WfQueues& nq, float* hdr, uint32_t* dbg,
                                     unsigned long long* ctr, uint32_t* err, cudaStream_t st) {
   if (bound <= 0) return cudaSuccess;
-  const unsigned g = unsigned(3 * ((bound + 255) / 256));
-  if (p.opaque) k_wf_shade3<2><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
-  else k_wf_shade3<1><<<g, 256, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+  const unsigned g = unsigned(3 * ((bound + 127) / 128));
+  if (p.opaque) k_wf_shade3<2><<<g, 128, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
+  else k_wf_shade3<1><<<g, 128, 0, st>>>(s, p, gb, w, cq, nq, hdr, dbg, ctr, err);
   return cudaGetLastError();
 }
 
