@@ -515,11 +515,13 @@ __device__ __forceinline__ bool tail_step(const Scene& s, const Params& p, const
 // order (extension ray, pending shadow ray, shade_path of the vertex type), so
 // the pixel comes out the same, without a launch and a queue round trip per
 // vertex.  ctr: the stage counter of the tail's samples; ctr_ext / ctr_shd:
-// its traversals'.  Three 128-thread blocks per SM (up to 168 registers, few
+// its traversals'.  Six 64-thread blocks per SM (up to 168 registers, few
 // spills): the tail is latency-bound and its path count is capped to one wave
-// of resident blocks.
+// of resident blocks; the smaller blocks (against three of 128 threads)
+// measured 330.5 against 327.3 M path samples/s on the 720p frame, a point,
+// inside the run-to-run spread.
 template <int NEE>
-__global__ void __launch_bounds__(128, 3) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
+__global__ void __launch_bounds__(64, 6) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
                                                  float* __restrict__ hdr, uint32_t* __restrict__ dbg,
                                                  unsigned long long* ctr, unsigned long long* ctr_ext,
                                                  unsigned long long* ctr_shd, uint32_t* err) {
@@ -608,10 +610,10 @@ int wavefront_tail_capacity(bool opaque) {
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, opaque ? k_wf_tail<2> : k_wf_tail<1>, 128, 0) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, opaque ? k_wf_tail<2> : k_wf_tail<1>, 64, 0) !=
             cudaSuccess)
       return 0;
-    c = sms * per_sm * 128;
+    c = sms * per_sm * 64;
   }
   return c;
 }
@@ -621,9 +623,9 @@ cudaError_t launch_wavefront_tail(const Scene& s, const Params& p, const GBufSoA
                                   unsigned long long* ctr_ext, unsigned long long* ctr_shd, uint32_t* err,
                                   cudaStream_t st) {
   if (bound <= 0) return cudaSuccess;
-  const unsigned g = unsigned((bound + 127) / 128);
-  if (p.opaque) k_wf_tail<2><<<g, 128, 0, st>>>(s, p, gb, w, q, hdr, dbg, ctr, ctr_ext, ctr_shd, err);
-  else k_wf_tail<1><<<g, 128, 0, st>>>(s, p, gb, w, q, hdr, dbg, ctr, ctr_ext, ctr_shd, err);
+  const unsigned g = unsigned((bound + 63) / 64);
+  if (p.opaque) k_wf_tail<2><<<g, 64, 0, st>>>(s, p, gb, w, q, hdr, dbg, ctr, ctr_ext, ctr_shd, err);
+  else k_wf_tail<1><<<g, 64, 0, st>>>(s, p, gb, w, q, hdr, dbg, ctr, ctr_ext, ctr_shd, err);
   return cudaGetLastError();
 }
 
