@@ -192,6 +192,9 @@ def dist_setup(args):
     if world > 1:
         import torch.distributed as dist
         backend = "nccl" if args.impl == "b200" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)  # each rank's communicator on its own GPU
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
