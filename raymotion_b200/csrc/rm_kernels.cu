@@ -131,8 +131,12 @@ __global__ void __launch_bounds__(256) k_render_paths(Scene s, Params p, uint64_
 
 __device__ __forceinline__ int gkind(const GBufSoA& g, uint32_t i) { return __float_as_int(g.pos_kind[i].w); }
 
-// K3 restir_generate (pathtrace.metal:817-917)
-__global__ void __launch_bounds__(128, 8) k_restir_generate(Scene s, Params p, uint64_t seed, GBufSoA gb, ResSoA ri,
+// K3 restir_generate (pathtrace.metal:817-917).  Ten 128-thread blocks per SM
+// (48 registers, ~360 bytes of spills): the 32 candidates' shadow rays are
+// latency-bound, and the extra warps outweigh the spills (13.1 / 13.3 against
+// 13.4 / 13.6 ms at eight blocks and 64 registers on the 720p frame; six
+// blocks at 80 registers, 15.0 ms).
+__global__ void __launch_bounds__(128, 10) k_restir_generate(Scene s, Params p, uint64_t seed, GBufSoA gb, ResSoA ri,
                                                          unsigned long long* ctr, uint32_t* err) {
   const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t npix = uint32_t(p.width) * uint32_t(p.height);
@@ -257,8 +261,11 @@ __device__ __forceinline__ bool reproject(const Params& p, float cx, float cy, f
   return true;
 }
 
-// K4 restir_spatial (pathtrace.metal:919-1054)
-__global__ void __launch_bounds__(256) k_restir_spatial(Scene s, Params p, uint64_t seed, GBufSoA gb, ResSoA ri,
+// K4 restir_spatial (pathtrace.metal:919-1054).  Three 256-thread blocks per
+// SM (80 registers, ~1 KB of spills, against two at 128): the neighbours'
+// visibility rays are latency-bound, and the pass took 1.76 against 2.13 ms
+// on the 720p frame (four blocks at 64 registers: 2.28 ms).
+__global__ void __launch_bounds__(256, 3) k_restir_spatial(Scene s, Params p, uint64_t seed, GBufSoA gb, ResSoA ri,
                                                         ResSoA ro, GBufSoA hg, ResSoA hr, unsigned long long* ctr,
                                                         uint32_t* err) {
   const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
