@@ -515,13 +515,15 @@ __device__ __forceinline__ bool tail_step(const Scene& s, const Params& p, const
 // order (extension ray, pending shadow ray, shade_path of the vertex type), so
 // the pixel comes out the same, without a launch and a queue round trip per
 // vertex.  ctr: the stage counter of the tail's samples; ctr_ext / ctr_shd:
-// its traversals'.  Six 64-thread blocks per SM (up to 168 registers, few
-// spills): the tail is latency-bound and its path count is capped to one wave
-// of resident blocks; the smaller blocks (against three of 128 threads)
-// measured 330.5 against 327.3 M path samples/s on the 720p frame, a point,
-// inside the run-to-run spread.
+// its traversals'.  Eight 64-thread blocks per SM (128 registers, ~200
+// bytes of spills): the tail is latency-bound and its path count is capped
+// to one wave of resident blocks, so more resident blocks take the paths
+// over earlier (75.8 k instead of 56.8 k on 148 SMs).  On the 720p frame:
+// six 64-thread blocks (168 registers) 330.5 against 327.3 M path samples/s
+// for three of 128 threads, and eight 334.1 against 331.2 M for six: a
+// point each, inside the run-to-run spread.
 template <int NEE>
-__global__ void __launch_bounds__(64, 6) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
+__global__ void __launch_bounds__(64, 8) k_wf_tail(Scene s, Params p, GBufSoA gb, WfState w, WfQueues q,
                                                  float* __restrict__ hdr, uint32_t* __restrict__ dbg,
                                                  unsigned long long* ctr, unsigned long long* ctr_ext,
                                                  unsigned long long* ctr_shd, uint32_t* err) {
