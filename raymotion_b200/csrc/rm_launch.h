@@ -69,9 +69,10 @@ cudaError_t launch_wavefront_shade(int vk, const Scene& s, const Params& p, cons
                                    unsigned long long* ctr, uint32_t* err, cudaStream_t st);
 // One launch per wave for both traversals (binary BVH) and for the three
 // shading queues; the counters of extension and shadow rays stay apart.
+// next_counts: the next wave's queue lengths, zeroed by this launch.
 cudaError_t launch_wavefront_trace2(const Scene& s, const WfState& w, const WfQueues& q, int bound,
                                     unsigned long long* ctr_ext, unsigned long long* ctr_shd, uint32_t* err,
-                                    cudaStream_t st);
+                                    int* next_counts, cudaStream_t st);
 cudaError_t launch_wavefront_shade3(const Scene& s, const Params& p, const GBufSoA& gb, const WfState& w,
                                     const WfQueues& cq, int bound, const WfQueues& nq, float* hdr, uint32_t* dbg,
                                     unsigned long long* ctr, uint32_t* err, cudaStream_t st);

@@ -326,7 +326,11 @@ __global__ void __launch_bounds__(128) k_wf_trace(Scene s, WfState w, WfQueues q
 // 6 %.  64-thread blocks (20 per SM) fit beside the other parts' launches
 // more easily than 128-thread ones (~1 %).
 __global__ void __launch_bounds__(64, 20) k_wf_trace2(Scene s, WfState w, WfQueues q, unsigned long long* ctr_ext,
-                                                   unsigned long long* ctr_shd, uint32_t* err) {
+                                                   unsigned long long* ctr_shd, uint32_t* err,
+                                                   int* __restrict__ next_counts) {
+  // the next wave's queue lengths start at zero: no launch reads or appends
+  // to them until the shading launch after this one
+  if (blockIdx.x == 0 && threadIdx.x < kCntSlots) next_counts[threadIdx.x] = 0;
   const int n_ext = q.counts[kCntExt], n_shd = q.counts[kCntShd];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t nodes = 0, tests = 0;
@@ -589,9 +593,9 @@ cudaError_t launch_wavefront_trace(const Scene& s, const WfState& w, const WfQue
 
 cudaError_t launch_wavefront_trace2(const Scene& s, const WfState& w, const WfQueues& q, int bound,
                                     unsigned long long* ctr_ext, unsigned long long* ctr_shd, uint32_t* err,
-                                    cudaStream_t st) {
-  if (bound <= 0) return cudaSuccess;
-  k_wf_trace2<<<unsigned((2 * bound + 63) / 64), 64, 0, st>>>(s, w, q, ctr_ext, ctr_shd, err);
+                                    int* next_counts, cudaStream_t st) {
+  if (bound <= 0) return cudaMemsetAsync(next_counts, 0, kCntSlots * sizeof(int), st);
+  k_wf_trace2<<<unsigned((2 * bound + 63) / 64), 64, 0, st>>>(s, w, q, ctr_ext, ctr_shd, err, next_counts);
   return cudaGetLastError();
 }
 

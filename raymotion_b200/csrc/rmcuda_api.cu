@@ -540,7 +540,7 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
           // both traversals in one launch (timed as the extension stage)
           e = staged2_on(c, RM_STAGE_WF_EXTEND, st, [&] {
             return launch_wavefront_trace2(s, w, Q, bd, ctr + 4 * RM_STAGE_WF_EXTEND, ctr + 4 * RM_STAGE_WF_SHADOW,
-                                           err, st);
+                                           err, N.counts, st);
           });
         } else {
           e = staged2_on(c, RM_STAGE_WF_EXTEND, st, [&] {
@@ -551,7 +551,8 @@ cudaError_t run_wavefront_shade(rmcuda_ctx* c, const Scene& s, const Params& p, 
               return launch_wavefront_trace(s, w, Q, bd, true, ctr + 4 * RM_STAGE_WF_SHADOW, err, st);
             });
         }
-        if (e == cudaSuccess) e = cudaMemsetAsync(N.counts, 0, kCntSlots * sizeof(int), st);
+        // (k_wf_trace2 zeroes the next wave's queue lengths itself)
+        if (e == cudaSuccess && !(merged && !s.wnodes)) e = cudaMemsetAsync(N.counts, 0, kCntSlots * sizeof(int), st);
         if (merged) {
           if (e == cudaSuccess)
             e = staged2_on(c, RM_STAGE_WF_SHADE, st, [&] {
