@@ -521,8 +521,10 @@ __device__ __forceinline__ bool tail_step(const Scene& s, const Params& p, const
 // vertex.  ctr: the stage counter of the tail's samples; ctr_ext / ctr_shd:
 // its traversals'.  Eight 64-thread blocks per SM (128 registers, ~200
 // bytes of spills): the tail is latency-bound and its path count is capped
-// to one wave of resident blocks, so more resident blocks take the paths
-// over earlier (75.8 k instead of 56.8 k on 148 SMs).  On the 720p frame:
+// to one wave of resident blocks, so more resident blocks can take the paths
+// over earlier (a capacity of 75.8 k instead of 56.8 k paths on 148 SMs; on
+// the 720p frame a tenth of the first wave, ~60.6 k, now sets the hand-off,
+// against 56.8 k before).  On the 720p frame:
 // six 64-thread blocks (168 registers) 330.5 against 327.3 M path samples/s
 // for three of 128 threads, and eight 334.1 against 331.2 M for six: a
 // point each, inside the run-to-run spread.
